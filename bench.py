@@ -1,0 +1,383 @@
+#!/usr/bin/env python
+"""Benchmark of the SPARC linear wave time step on B200.
+
+A step is one driver iteration (driver.f90:123-202): forcing, the five RK
+stages, the diagnostics reduction and FILTER_VARS at its cadence.  The
+workload is the plain MHD flux tube (256x256x300, FP64, 200 seeded PSR
+pulses, dt = 0.5 s, CPML on six faces), the configuration the headline
+grid-point-update rate is quoted on.  Prints one JSON line.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun (N > 1) every rank advances its own replica (the path does
+not shard across GPUs here) and the time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from sparc2_b200 import abi, workloads as W  # noqa: E402
+
+METRIC = "grid-pt updates/s"
+UNIT = "grid-pt updates/s"
+WORKLOAD = ("plain MHD flux tube 256x256x300 FP64 (100x100 Mm, z -25..+1 Mm, "
+            "B0 3 kG, maxVA 40 km/s, CPML 10 pts on 6 faces, 200 seeded PSR "
+            "pulses, dt 0.5 s, z filter every 10 / xy every 30 iterations)")
+CPU_SAMPLE = (64, 64, 300)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=120)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
+    ap.add_argument("--workload", default="cfg1", choices=["cfg1", "cfg0"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=30)
+    ap.add_argument("--kernel-steps", type=int, default=10)
+    ap.add_argument("--timed-only", action="store_true",
+                    help="only the warm-up and the timed region (profiling)")
+    return ap.parse_args()
+
+
+def algorithmic_bytes_per_point(p, with_filters=True):
+    """Bytes per grid-point update of one RK step:
+    w*[14V + 5C + 14*sum_faces(P*phi) + 2V/n_z + 2V/n_xy]; w word size,
+    V state fields, C 3-D background inputs (quiet: 0, MHD: 6), P CPML
+    fields per face, phi the fraction of points in that face's slab."""
+    w = 8 if p.precision == abi.SPARC_FP64 else 4
+    mhd = p.magnetic == 2
+    V = 8 if mhd else 5
+    C = 6 if mhd else (0 if p.magnetic == 0 and p.periodic else 5)
+    P = 6 if mhd else 2
+    phi = 0.0
+    if p.use_pml or p.use_hpml:
+        phi += (p.npml_zb + p.npml_zt) / p.nz
+    if p.use_hpml:
+        phi += (p.npml_xb + p.npml_xt) / p.nx + (p.npml_yb + p.npml_yt) / p.ny
+    b = 14 * V + 5 * C + 14 * P * phi
+    if with_filters:
+        nz = int(np.floor(max(p.t_z, p.timestep) / p.timestep + 1e-5))
+        nxy = int(np.floor(max(p.t_xy, p.timestep) / p.timestep + 1e-5))
+        b += 2 * V / nz + 2 * V / nxy
+    return w * b
+
+
+def workload(name, precision=abi.SPARC_FP64, grid=None):
+    if name == "cfg0":
+        p, bg, src = W.cfg0(precision=precision)
+        desc = ("plain quiet-Sun hydro 64x64x128 FP64 (50 Mm periodic, z -20..+1 "
+                "Mm, z-CPML 10, v_z pulse 3 mHz, dt 1 s)")
+        return p, bg, src, desc
+    if grid is None:
+        p, bg, src = W.cfg1(precision=precision)
+        return p, bg, src, WORKLOAD
+    nx, ny, nz = grid
+    p, bg, src = W.cfg1(nx=nx, ny=ny, nz=nz, precision=precision,
+                        length_mm=100.0 * nx / 256)
+    return p, bg, src, WORKLOAD
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--id={index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        time.sleep(0.3)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline(steps=None, threads=None):
+    """The oracle (C++/OpenMP FP64 restatement of the reference) on a
+    64x64x300 sub-grid of the same physics, all host threads."""
+    import oracle
+    oracle.build()
+    threads = threads or os.cpu_count()
+    oracle.set_threads(threads)
+    p, bg, src, _ = workload("cfg1", grid=CPU_SAMPLE)
+    o = oracle.Oracle(p, bg, src)
+    o.run(0, 1)                      # warm (first iteration doubles PSR)
+    n = steps or 12
+    t = time.perf_counter()
+    o.run(1, n)
+    dt = time.perf_counter() - t
+    pts = p.nx * p.ny * p.nz
+    return {"value": pts * n / dt, "unit": UNIT, "cores": threads,
+            "kind": "port",
+            "sample": (f"oracle (C++17/OpenMP FP64 restatement of the "
+                       f"reference) on a {CPU_SAMPLE[0]}x{CPU_SAMPLE[1]}x"
+                       f"{CPU_SAMPLE[2]} sub-grid of the same flux-tube "
+                       f"physics, {n} driver iterations, {threads} threads")}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    import oracle
+    oracle.build()
+    threads = os.cpu_count()
+    oracle.set_threads(threads)
+    p, bg, src, desc = workload("cfg1", grid=CPU_SAMPLE)
+    o = oracle.Oracle(p, bg, src)
+    o.run(0, args.warmup)
+    t = time.perf_counter()
+    o.run(args.warmup, args.steps)
+    dt = time.perf_counter() - t
+    pts = p.nx * p.ny * p.nz
+    v = pts * args.steps / dt
+    sample = (f"each step one driver iteration of the oracle (FP64 C++/OpenMP "
+              f"restatement of the reference; the Fortran/MPI reference cannot "
+              f"be built here) on a {CPU_SAMPLE[0]}x{CPU_SAMPLE[1]}x"
+              f"{CPU_SAMPLE[2]} sub-grid of the same flux-tube physics")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded analytic background and pulse table)",
+        "config": {"workload": desc, "sample_grid": list(CPU_SAMPLE)},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads,
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_gpu(args, world, rank, local):
+    import torch
+    from sparc2_b200 import Simulation
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = local
+    torch.cuda.set_device(dev)
+    p, bg, src, desc = workload(args.workload)
+    sim = Simulation(p, bg, src, device=dev)
+    del bg
+    pts = p.nx * p.ny * p.nz
+    stream = torch.cuda.ExternalStream(sim.stream, device=dev)
+
+    def barrier():
+        if dist is not None:
+            t = torch.zeros(1, device=f"cuda:{dev}")
+            dist.all_reduce(t)
+            torch.cuda.synchronize(dev)
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up iterations (graph capture happens here)
+    W_ = args.warmup
+    K = args.steps
+    sim.run(0, W_)
+    sim.synchronize()
+    torch.cuda.synchronize(dev)
+    clocks = Clocks(dev) if rank == 0 or True else None
+    n0 = sim.launch_count
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.run(W_, K)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize(dev)
+    barrier()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop() if clocks else None
+    launches = sim.launch_count - n0
+    d, status = sim.diagnostics()
+    ms_max = max_over_ranks(ms)
+    value = world * pts * K / (ms_max / 1e3)
+    if args.timed_only:
+        if rank == 0:
+            print(json.dumps({"timed_only": True, "value": value,
+                              "ms_per_step": ms_max / K}), flush=True)
+        return
+
+    # stage kernels alone (five fused RK-stage launches + the PSR forcing
+    # of an iteration, no filter) for the roofline figure
+    M = args.kernel_steps
+    k0 = torch.cuda.Event(enable_timing=True)
+    k1 = torch.cuda.Event(enable_timing=True)
+    k0.record(stream)
+    for nn in range(W_ + K, W_ + K + M):
+        sim.step(nn)
+    k1.record(stream)
+    k1.synchronize()
+    kms = k0.elapsed_time(k1) / M
+    hbm, peak_kind = peaks()
+    stage_bytes = algorithmic_bytes_per_point(p, with_filters=False) * pts
+    achieved = stage_bytes / (kms / 1e3) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "stage_traffic.json")
+    if os.path.exists(tfile):
+        try:
+            with open(tfile) as f:
+                t = json.load(f)
+            if t.get("workload") == args.workload:
+                traffic = t.get("bytes_per_step")
+        except Exception:
+            traffic = None
+
+    # end to end through the per-iteration C-ABI calls of the reference's
+    # driver loop (STEP, norm readback, FILTER_VARS): state uploaded from
+    # pinned host memory at the start, read back at the end, diagnostics
+    # read back every iteration
+    E = args.e2e_steps
+    a_host, psi_host = sim.get_state()
+    pin_a = torch.empty(a_host.size, dtype=torch.float64, pin_memory=True).numpy()
+    pin_p = torch.empty(max(psi_host.size, 1), dtype=torch.float64,
+                        pin_memory=True).numpy()
+    pin_a[:] = a_host.ravel()
+    pin_p[:psi_host.size] = psi_host
+    first = W_ + K + M
+    barrier()
+    torch.cuda.synchronize(dev)
+    x0 = torch.cuda.Event(enable_timing=True)
+    x1 = torch.cuda.Event(enable_timing=True)
+    x0.record(stream)
+    sim.set_state(pin_a, pin_p[:psi_host.size] if psi_host.size else None)
+    for nn in range(first, first + E):
+        sim.step(nn)
+        sim.diagnostics()
+        sim.filter_vars(nn)
+    sim.lib.sparc_get_state(sim.h, abi.dptr(pin_a), abi.dptr(pin_p))
+    x1.record(stream)
+    x1.synchronize()
+    ems = max_over_ranks(x0.elapsed_time(x1))
+    e2e = world * pts * E / (ems / 1e3)
+    state_bytes = 8 * (a_host.size + psi_host.size)
+    h2d = (state_bytes + 8 * E) / E
+    d2h = (state_bytes + 40 * E) / E
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline()
+
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": K, "warmup": W_, "ms_per_step": ms_max / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded analytic background and "
+        "pulse table; no public dataset)",
+        "config": {"workload": desc, "grid": [p.nx, p.ny, p.nz],
+                   "precision": "fp64 plain", "parallelism":
+                   "replicas" if world > 1 else "single GPU",
+                   "l2": "working set %.1f GB > 126 MB L2 (no flush needed)"
+                   % (3 * 8 * 8 * pts / 1e9)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_kind": peak_kind, "traffic": traffic,
+                     "kernel": "5 fused RK-stage launches + PSR forcing of "
+                     "one iteration",
+                     "algorithmic_bytes_per_launch": stage_bytes,
+                     "ms_per_launch": kms},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "steps": E},
+        "gpu_launches": launches,
+        "diag": {"ke_norm": d.ke_norm, "iteration": d.iteration,
+                 "status": int(status)},
+    }
+    if clk:
+        line["clocks"] = clk
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    sim.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    run_gpu(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,207 @@
+/*
+ * sparc_gpu.h -- C ABI of the B200 implementation of SPARC's linear wave
+ * time step (libsparc_gpu.so).
+ *
+ * The reference (damoprz/SPARC2, Fortran 90 + MPI) keeps every quantity in
+ * module globals and calls argument-less subroutines from driver.f90.  This
+ * header replaces those calls with handle-based entry points that take plain
+ * pointers and sizes, so a Fortran ISO_C_BINDING shim (or ctypes, or C++) can
+ * bind them.  Every entry point returns an int status: SPARC_OK (0) or a
+ * negative SPARC_ERR_* code.  No exception crosses the ABI.
+ *
+ * Layout conventions: every 3-D array is Fortran order (x fastest, then y,
+ * then z), exactly as the reference's a(dim1,dim2,dim3,l).  Host buffers are
+ * owned by the caller and copied; device memory is owned by the library.
+ * A handle is not thread safe: use one host thread per handle.
+ */
+#ifndef SPARC_GPU_H
+#define SPARC_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define SPARC_OK               0
+#define SPARC_ERR_INVALID     -1  /* bad argument or unsupported option      */
+#define SPARC_ERR_CUDA        -2  /* a CUDA runtime call failed              */
+#define SPARC_ERR_NOMEM       -3  /* device allocation failed                */
+#define SPARC_ERR_UNSTABLE    -4  /* driver.f90:175-183 fail criterion hit   */
+#define SPARC_ERR_ORDER       -5  /* call made before its prerequisites      */
+#define SPARC_ERR_TIMEOUT     -6  /* a bounded device wait gave up           */
+#define SPARC_ERR_NODEVICE    -7  /* no usable sm_100 device                 */
+
+/* precision of the device state */
+#define SPARC_FP64 0   /* plain form: FP64 state, coefficients and arithmetic */
+#define SPARC_FP32 1   /* precision form: FP32 state/coefficients, FP64 setup */
+
+/* source kinds (driver.f90:130-155) */
+#define SPARC_SRC_NONE  0
+#define SPARC_SRC_PULSE 1  /* PULSE = 1: one analytic pulse                   */
+#define SPARC_SRC_PSR   2  /* PULSE = 2: table of "random-ish" pulses         */
+
+/*
+ * Run parameters: the subset of the .trol keys (initialize.f90:1385-1924)
+ * that the time step reads.  Units are the .trol units (cgs, seconds).
+ */
+typedef struct sparc_params {
+    int32_t nx, ny, nz;            /* global grid                            */
+    int32_t magnetic;              /* MAGNETIC: 0 quiet, 1 thermal, 2 MHD    */
+    int32_t periodic;              /* PERIODIC (x,y)                          */
+    int32_t use_pml;               /* USE_PML  (z CPML)                       */
+    int32_t use_hpml;              /* USE_HPML (x,y CPML)                     */
+    int32_t stabilise;             /* STABILISE                               */
+    int32_t filter_mode_xy;        /* 1: 11-pt filter, 2: 7-pt filter         */
+    int32_t filter_mode_z;
+    int32_t block_x, block_y, block_z; /* reference MPI block counts; fix the
+                                          rank-local quirks that the oracle
+                                          and the kernels reproduce          */
+    int32_t npml_xb, npml_xt, npml_yb, npml_yt, npml_zb, npml_zt;
+    double  pml_xb[4], pml_xt[4];  /* RC, n, kappa, sponge (xpmlb, xpmlt)    */
+    double  pml_yb[4], pml_yt[4];
+    double  pml_zb[4], pml_zt[4];
+    double  xlength, ylength;      /* cm                                      */
+    double  timestep;              /* s                                       */
+    double  s_xy, s_z;             /* 7-pt filter strengths                   */
+    double  t_xy, t_z;             /* filter cadences, s                      */
+    double  maxva;                 /* Alfven limiter, cm/s                    */
+    double  sp_str, sp_length, sp_decay; /* horizontal sponge (no HPML)      */
+    int32_t precision;             /* SPARC_FP64 or SPARC_FP32                */
+    int32_t reserved[7];
+} sparc_params;
+
+/* One entry of a PULSE = 2 table: the reference's psr_* arrays
+ * (all_modules.f90:159-160, drawn at all_modules.f90:566-586), code units:
+ * px, py in [0,1) of the box, pz, sr, sz in solar radii, t0, t1 in s. */
+typedef struct sparc_pulse {
+    double px, py, pz, sr, sz, amp, t0, t1;
+} sparc_pulse;
+
+typedef struct sparc_source {
+    int32_t kind;        /* SPARC_SRC_*                                      */
+    int32_t dir;         /* pulse_dir: 1 v_x, 2 v_y, 3 v_z                   */
+    int64_t init;        /* first driver iteration of the run (driver init);
+                            PULSE = 2 adds every pulse twice at this step    */
+    /* SPARC_SRC_PULSE, .trol units (driver.f90:140-145) */
+    double  amp, t0, t1, st, px, py, pz, sr, sz;
+    /* SPARC_SRC_PSR */
+    double  psr_st;      /* time width, 120 s in the reference               */
+    int32_t npulses;
+    int32_t pad;
+    const sparc_pulse *pulses;
+} sparc_source;
+
+typedef struct sparc_handle sparc_handle;
+
+/* Diagnostics of the last completed driver iteration (driver.f90:161-183). */
+typedef struct sparc_diag {
+    double  ke_norm;     /* norm((rho0+rho)|v|^2/2)*dimc^2*dimrho            */
+    double  min_rho;     /* min(rho + rho0) over the stage-5 fields          */
+    double  min_p;       /* min(p + p0) over the stage-5 fields              */
+    int64_t iteration;   /* driver iteration these belong to (-1: none)      */
+    int64_t fail_iteration; /* first iteration that failed, -1 if none      */
+} sparc_diag;
+
+/* ------------------------------------------------------------- lifecycle */
+
+/* Replaces INIT_MPI + INITANDALLOCATE (initialize.f90:12, 463): validates
+ * the parameters, allocates the device state on CUDA device `device`. */
+int sparc_create(const sparc_params *p, int device, sparc_handle **out);
+
+/* Frees all device memory of the handle. */
+int sparc_destroy(sparc_handle *h);
+
+/* Replaces READ_IN_HDF5 (all_modules.f90:179-416) + INITIALISE_RHS
+ * (initialize.f90:883-1273) + INITIALIZE_STEP (initialize.f90:1366):
+ * the background arrays in dimensional cgs units, nx*ny*nz each (bx0, by0,
+ * bz0 may be NULL unless magnetic == 2), zaxis in Mm and grav in cm/s^2
+ * (nz each).  The FP64 coefficient setup runs on the device.  Resets the
+ * state and the CPML auxiliary fields to zero. */
+int sparc_set_background(sparc_handle *h,
+                         const double *rho0, const double *pre0,
+                         const double *cs0, const double *bx0,
+                         const double *by0, const double *bz0,
+                         const double *zaxis_mm, const double *grav);
+
+/* Replaces the forcing fill of driver.f90:130-155 / RUN_PSR_PULSE
+ * (all_modules.f90:521-663); the forcing is evaluated inside the kernels. */
+int sparc_set_source(sparc_handle *h, const sparc_source *src);
+
+/* Number of doubles of the state (V*nx*ny*nz, V = 5 or 8) and of the
+ * concatenated CPML auxiliary state [z-bot, z-top, x-bot, x-top, y-bot,
+ * y-top], each face in the reference's (dim1,dim2,npml,P) /
+ * (npml,dim2,dim3,P) / (dim1,npml,dim3,P) layout, P = 2 or 6. */
+int sparc_sizes(const sparc_handle *h, int64_t *n_state, int64_t *n_psi);
+
+/* Checkpoint / restart of a(:,:,:,l) and zpmlvars/xpmlvars/ypmlvars
+ * (all_modules.f90:741-1562 without the HDF5 container). psi may be NULL. */
+int sparc_set_state(sparc_handle *h, const double *a, const double *psi);
+int sparc_get_state(sparc_handle *h, double *a, double *psi);
+
+/* ------------------------------------------------------------ time step */
+
+/* One call of STEP (step.f90:20-63) for driver iteration nn: the forcing
+ * of iteration nn, five RK stages with fused derivatives, CPML and RHS,
+ * the final update, and the diagnostics of driver.f90:161-183.  Asynchronous
+ * on the handle's stream. */
+int sparc_step(sparc_handle *h, int64_t nn);
+
+/* FILTER_VARS (derivatives.f90:659-703) as called at driver.f90:200 after
+ * iteration nn (nothing happens at nn == 0 or off cadence).  Asynchronous. */
+int sparc_filter_vars(sparc_handle *h, int64_t nn);
+
+/* Iterations first .. first+count-1 of the driver loop (driver.f90:123-202:
+ * step, diagnostics, filter at cadence), launched as CUDA graphs.
+ * Asynchronous; errors of the fail criterion surface in sparc_diagnostics. */
+int sparc_run(sparc_handle *h, int64_t first, int64_t count);
+
+/* Waits for the handle's stream and returns the diagnostics of the last
+ * iteration.  Returns SPARC_ERR_UNSTABLE when an iteration met the fail
+ * criterion of driver.f90:175-183 (the diagnostics are still filled). */
+int sparc_diagnostics(sparc_handle *h, sparc_diag *out);
+
+/* Waits for all work queued on the handle. */
+int sparc_synchronize(sparc_handle *h);
+
+/* The cudaStream_t the handle launches on (for event timing by callers). */
+int sparc_stream(sparc_handle *h, void **stream);
+
+/* Number of kernels the library has launched on this handle so far
+ * (graph launches count every kernel node). */
+int sparc_launch_count(const sparc_handle *h, int64_t *count);
+
+/* ----------------------------------------------------- unit primitives */
+
+/* ddx/ddy/ddz (derivatives.f90:10-116, 226-341, 451-562) of one host field
+ * with boundary flag bc (1 or 5), on the device; dir 0 = x, 1 = y, 2 = z.
+ * Needs sparc_set_background (for the z metric). */
+int sparc_derivative(sparc_handle *h, int dir, int bc,
+                     const double *in, double *out);
+
+/* filtx/filty/filtz (derivatives.f90:119-223, 345-447, 565-642) of one host
+ * field (no edge pre-averaging; that belongs to FILTER_VARS). */
+int sparc_filter_field(sparc_handle *h, int dir, const double *in,
+                       double *out);
+
+/* Copies one FP64 coefficient array of the setup to the host, by the
+ * reference's variable name ("rho0", "gradp0_z", "spongexyz", "reduction",
+ * "curlbox", "stretch", "g", "az_bot", ...).  *count is the element count
+ * on return; out may be NULL to query it. */
+int sparc_get_coeff(sparc_handle *h, const char *name, double *out,
+                    int64_t *count);
+
+/* Scalars of the setup: dimc, dimrho, diml, dimb, deltat, stretchx,
+ * stretchy, betas[5] (12 doubles in that order). */
+int sparc_get_scalars(sparc_handle *h, double *out12);
+
+/* Human-readable text of the last error on this handle (or of the last
+ * failed sparc_create when h is NULL). */
+const char *sparc_last_error(const sparc_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPARC_GPU_H */

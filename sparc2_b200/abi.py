@@ -1,0 +1,171 @@
+"""ctypes mirror of include/sparc_gpu.h (structs, status codes, loader).
+
+The structures here must match the C header field for field; the CPU test
+suite checks their sizes against the compiled library's view of them.
+"""
+import ctypes as C
+import os
+
+SPARC_OK = 0
+SPARC_ERR_INVALID = -1
+SPARC_ERR_CUDA = -2
+SPARC_ERR_NOMEM = -3
+SPARC_ERR_UNSTABLE = -4
+SPARC_ERR_ORDER = -5
+SPARC_ERR_TIMEOUT = -6
+SPARC_ERR_NODEVICE = -7
+
+ERR_NAMES = {
+    SPARC_ERR_INVALID: "SPARC_ERR_INVALID",
+    SPARC_ERR_CUDA: "SPARC_ERR_CUDA",
+    SPARC_ERR_NOMEM: "SPARC_ERR_NOMEM",
+    SPARC_ERR_UNSTABLE: "SPARC_ERR_UNSTABLE",
+    SPARC_ERR_ORDER: "SPARC_ERR_ORDER",
+    SPARC_ERR_TIMEOUT: "SPARC_ERR_TIMEOUT",
+    SPARC_ERR_NODEVICE: "SPARC_ERR_NODEVICE",
+}
+
+SPARC_FP64 = 0
+SPARC_FP32 = 1
+
+SPARC_SRC_NONE = 0
+SPARC_SRC_PULSE = 1
+SPARC_SRC_PSR = 2
+
+
+class SparcParams(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("magnetic", C.c_int32), ("periodic", C.c_int32),
+        ("use_pml", C.c_int32), ("use_hpml", C.c_int32),
+        ("stabilise", C.c_int32),
+        ("filter_mode_xy", C.c_int32), ("filter_mode_z", C.c_int32),
+        ("block_x", C.c_int32), ("block_y", C.c_int32), ("block_z", C.c_int32),
+        ("npml_xb", C.c_int32), ("npml_xt", C.c_int32),
+        ("npml_yb", C.c_int32), ("npml_yt", C.c_int32),
+        ("npml_zb", C.c_int32), ("npml_zt", C.c_int32),
+        ("pml_xb", C.c_double * 4), ("pml_xt", C.c_double * 4),
+        ("pml_yb", C.c_double * 4), ("pml_yt", C.c_double * 4),
+        ("pml_zb", C.c_double * 4), ("pml_zt", C.c_double * 4),
+        ("xlength", C.c_double), ("ylength", C.c_double),
+        ("timestep", C.c_double),
+        ("s_xy", C.c_double), ("s_z", C.c_double),
+        ("t_xy", C.c_double), ("t_z", C.c_double),
+        ("maxva", C.c_double),
+        ("sp_str", C.c_double), ("sp_length", C.c_double),
+        ("sp_decay", C.c_double),
+        ("precision", C.c_int32),
+        ("reserved", C.c_int32 * 7),
+    ]
+
+
+class SparcPulse(C.Structure):
+    _fields_ = [(n, C.c_double) for n in
+                ("px", "py", "pz", "sr", "sz", "amp", "t0", "t1")]
+
+
+class SparcSource(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32), ("dir", C.c_int32), ("init", C.c_int64),
+        ("amp", C.c_double), ("t0", C.c_double), ("t1", C.c_double),
+        ("st", C.c_double), ("px", C.c_double), ("py", C.c_double),
+        ("pz", C.c_double), ("sr", C.c_double), ("sz", C.c_double),
+        ("psr_st", C.c_double),
+        ("npulses", C.c_int32), ("pad", C.c_int32),
+        ("pulses", C.POINTER(SparcPulse)),
+    ]
+
+
+class SparcDiag(C.Structure):
+    _fields_ = [
+        ("ke_norm", C.c_double), ("min_rho", C.c_double),
+        ("min_p", C.c_double), ("iteration", C.c_int64),
+        ("fail_iteration", C.c_int64),
+    ]
+
+
+class SparcError(RuntimeError):
+    """A negative status returned across the C ABI."""
+
+    def __init__(self, code, where, detail=""):
+        self.code = code
+        name = ERR_NAMES.get(code, str(code))
+        msg = f"{where} failed with {name}"
+        if detail:
+            msg += f": {detail}"
+        super().__init__(msg)
+
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "_lib", "libsparc_gpu.so")
+
+# Every entry point declared in include/sparc_gpu.h.
+EXPORTS = [
+    "sparc_create", "sparc_destroy", "sparc_set_background",
+    "sparc_set_source", "sparc_sizes", "sparc_set_state", "sparc_get_state",
+    "sparc_step", "sparc_filter_vars", "sparc_run", "sparc_diagnostics",
+    "sparc_synchronize", "sparc_stream", "sparc_launch_count",
+    "sparc_derivative", "sparc_filter_field", "sparc_get_coeff",
+    "sparc_get_scalars", "sparc_last_error",
+]
+
+_lib = None
+
+
+def _declare(lib):
+    P = C.POINTER
+    d = C.POINTER(C.c_double)
+    h = C.c_void_p
+    sig = {
+        "sparc_create": (C.c_int, [P(SparcParams), C.c_int, P(C.c_void_p)]),
+        "sparc_destroy": (C.c_int, [h]),
+        "sparc_set_background": (C.c_int, [h, d, d, d, d, d, d, d, d]),
+        "sparc_set_source": (C.c_int, [h, P(SparcSource)]),
+        "sparc_sizes": (C.c_int, [h, P(C.c_int64), P(C.c_int64)]),
+        "sparc_set_state": (C.c_int, [h, d, d]),
+        "sparc_get_state": (C.c_int, [h, d, d]),
+        "sparc_step": (C.c_int, [h, C.c_int64]),
+        "sparc_filter_vars": (C.c_int, [h, C.c_int64]),
+        "sparc_run": (C.c_int, [h, C.c_int64, C.c_int64]),
+        "sparc_diagnostics": (C.c_int, [h, P(SparcDiag)]),
+        "sparc_synchronize": (C.c_int, [h]),
+        "sparc_stream": (C.c_int, [h, P(C.c_void_p)]),
+        "sparc_launch_count": (C.c_int, [h, P(C.c_int64)]),
+        "sparc_derivative": (C.c_int, [h, C.c_int, C.c_int, d, d]),
+        "sparc_filter_field": (C.c_int, [h, C.c_int, d, d]),
+        "sparc_get_coeff": (C.c_int, [h, C.c_char_p, d, P(C.c_int64)]),
+        "sparc_get_scalars": (C.c_int, [h, d]),
+        "sparc_last_error": (C.c_char_p, [h]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+def load(path=None):
+    """Load libsparc_gpu.so (built in-tree by sparc2_b200.build).
+
+    Raises FileNotFoundError when the library has not been built: there is
+    no fallback implementation."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise FileNotFoundError(
+            f"{p} is missing; build it with `python -c 'import "
+            f"sparc2_b200.build as b; b.build()'`")
+    lib = _declare(C.CDLL(p))
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def dptr(arr):
+    """double* of a C-contiguous float64 numpy array (or NULL for None)."""
+    if arr is None:
+        return C.cast(None, C.POINTER(C.c_double))
+    assert arr.dtype.name == "float64" and arr.flags["C_CONTIGUOUS"]
+    return arr.ctypes.data_as(C.POINTER(C.c_double))

@@ -1,0 +1,176 @@
+// internal.h -- device-side data layout shared by the translation units of
+// libsparc_gpu.so (setup.cu, step.cu, api.cu).  Host C++ only; kernels get
+// the POD structs below by value.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/sparc_gpu.h"
+
+namespace sparc {
+
+constexpr double RSUN = 69598946770.0;   // all_modules.f90:56
+constexpr double PI = 3.14159265358979;  // all_modules.f90:56 (truncated pi)
+
+// One CPML face on the device.  Auxiliary fields are stored in the
+// reference's layout (n0 fastest, P slots); profiles a, b, kappa are either
+// per point of the slab or, when `uniform`, one value per PML layer.
+struct FaceDev {
+  int on;
+  int n0, n1, n2, np, P;
+  int uniform;          // profiles depend on the layer index only
+  long long cnt;        // n0*n1*n2
+  double *vars;         // RK state (zpmlvars...), cnt*P
+  double *scr;          // stage right-hand side (scrzpml...), cnt*P
+  const double *pa, *pb, *pk;
+};
+
+// Forcing description consumed by the stage kernels.
+struct ForcingDev {
+  int kind;             // SPARC_SRC_*
+  int dir;              // 1..3
+  long long init;
+  // PULSE = 1: f = T(t) * fz[k] * fy[j] * fx[i], T on the device
+  const double *fx, *fy, *fz;
+  double amp_c, t0, t1, st, timestep;  // amp_c = pulse_amp/0.56458272/dimc
+  // PULSE = 2: precomputed per iteration for layers [klo, khi)
+  const double *psr;     // (khi-klo)*nx*ny
+  int klo, khi;
+};
+
+// Everything the fused stage kernels read.  Background arrays are either
+// 3-D (N) or, for the horizontally uniform quiet background, 1-D (nz).
+struct SimDev {
+  int nx, ny, nz;
+  long long N;
+  int periodic, magnetic, bg1d;
+  int V;
+  double stretchx, stretchy;
+  const double *stretch;       // nz
+  double deltat;
+  double dimc2rho;             // dimc^2*dimrho for the KE norm
+  // background (code units)
+  const double *rho0, *p0, *rhoinv, *c2rho0, *grz, *gpz, *sponge;
+  const double *box, *boy, *boz, *cbx, *cby, *cbz;
+  const double *grx, *gry, *gpx, *gpy, *red;
+  const double *gblk;          // (block_x*block_y) * nz gravity
+  const int *colx, *coly;      // block index of each x / y
+  int bxdim;
+  FaceDev zb, zt, xb, xt, yb, yt;
+  ForcingDev frc;
+  // iteration bookkeeping and diagnostics (device)
+  long long *iter;             // current driver iteration
+  double *partials;            // 3 per block of the last stage
+  unsigned int *counter;
+  double *diag;                // ke, min_rho, min_p, iteration(double)
+  long long *fail_iter;
+};
+
+struct Handle {
+  sparc_params P{};
+  int device = 0;
+  int nx = 0, ny = 0, nz = 0, V = 0, Pp = 0;
+  long long N = 0;
+  bool magnetic = false, quiet = false, periodic = false;
+  bool use_pml = false, use_hpml = false;
+  int gxy = 5, gz = 5, xyfreq = 1, zfreq = 1;
+  bool bg_ready = false;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  long long launches = 0;
+
+  // host-side 1-D setup
+  std::vector<double> xaxis, yaxis, zaxis, g, stretch, cq, invrho0q;
+  std::vector<int> colx, coly, bxs, bys, bzs, bxl, byl, bzl;
+  double stretchx = 0, stretchy = 0, dimc = 0, dimrho = 0, diml = 0,
+         dimb = 0, deltat = 0, betas[5] = {0, 0, 0, 0, 0};
+
+  // device memory (all owned)
+  std::vector<void *> allocs;
+  double *buf[3] = {nullptr, nullptr, nullptr};  // rotating state buffers
+  int ra = 0, rf1 = 1, rf2 = 2;                  // roles: a, free1, free2
+  // 3-D FP64 setup arrays (code units)
+  double *rho0 = nullptr, *p0 = nullptr, *c2 = nullptr, *rhoinv = nullptr,
+         *c2rho0 = nullptr, *grz = nullptr, *gpz = nullptr, *sponge = nullptr,
+         *box = nullptr, *boy = nullptr, *boz = nullptr, *cbx = nullptr,
+         *cby = nullptr, *cbz = nullptr, *grx = nullptr, *gry = nullptr,
+         *gpx = nullptr, *gpy = nullptr, *red = nullptr,
+         *source_damp = nullptr, *ssb = nullptr;
+  // 1-D profiles for the uniform quiet background
+  double *rho0_1 = nullptr, *p0_1 = nullptr, *rhoinv_1 = nullptr,
+         *c2rho0_1 = nullptr, *grz_1 = nullptr, *gpz_1 = nullptr,
+         *sponge_1 = nullptr;
+  double *d_stretch = nullptr, *d_gblk = nullptr;
+  int *d_colx = nullptr, *d_coly = nullptr;
+  FaceDev faces[6]{};  // z_bot, z_top, x_bot, x_top, y_bot, y_top
+  std::vector<double> g_blk;  // host copy of the gravity table
+  bool bg1d = false;
+
+  // forcing
+  sparc_source src{};
+  std::vector<sparc_pulse> pulses;
+  double *d_fx = nullptr, *d_fy = nullptr, *d_fz = nullptr;
+  double *d_psr = nullptr;          // forcing buffer for PULSE = 2
+  int psr_klo = 0, psr_khi = 0;
+  // PULSE = 2 tables
+  double *d_px = nullptr, *d_py = nullptr;  // npulses*nx, npulses*ny
+  int *d_plane_off = nullptr, *d_plane_idx = nullptr;
+  double *d_plane_z = nullptr;              // Z_n(k) per CSR entry
+  unsigned char *d_pmask = nullptr;         // npulses * nblocks
+  double *d_ptime = nullptr;                // amp, t0, t1 per pulse
+  double *d_damp2 = nullptr;                // source_damp(i,j) (N/nz)
+  int nblocks = 1;
+
+  // device bookkeeping
+  long long *d_iter = nullptr, *d_fail = nullptr;
+  double *d_partials = nullptr, *d_diag = nullptr;
+  unsigned int *d_counter = nullptr;
+  long long *h_pinned_iter = nullptr;
+  int max_stage_blocks = 0;
+
+  // stage launch geometry
+  int tx = 32, ty = 8, zchunk = 32;
+
+  // captured graphs keyed by (ra, rf1, rf2, filter kind)
+  struct GraphEntry {
+    int ra, rf1, rf2, fk;
+    cudaGraphExec_t exec;
+    int nkernels;
+  };
+  std::vector<GraphEntry> graphs;
+};
+
+// setup.cu: published coefficient tables (initialize.f90:1929-2031)
+extern const double kDerivRows[6][11];
+extern const double kFilter11[11];
+extern const double kFilter7[7];
+int setup_background(Handle *h, const double *rho0, const double *pre0,
+                     const double *cs0, const double *bx0, const double *by0,
+                     const double *bz0, const double *zaxis_mm,
+                     const double *grav);
+int setup_constants();
+int launch_derivative(Handle *h, int dir, int bc, const double *in,
+                      double *out, cudaStream_t s);
+int launch_filter_raw(Handle *h, int dir, const double *in, double *out,
+                      cudaStream_t s);
+
+// step.cu
+int step_constants();
+int filter_constants(int gxy, int gz);
+SimDev make_simdev(Handle *h);
+int launch_stage(Handle *h, const SimDev &S, int stage, const double *a,
+                 const double *sprev, double *sout, cudaStream_t s);
+int launch_psr_forcing(Handle *h, const SimDev &S, cudaStream_t s);
+int launch_filter_pass(Handle *h, int dir, const double *in, double *out,
+                       cudaStream_t s);
+int stage_geometry(Handle *h);
+
+// api.cu
+void *dev_alloc(Handle *h, size_t bytes);
+bool cuda_ok(Handle *h, cudaError_t e, const char *what);
+
+}  // namespace sparc

@@ -1,0 +1,918 @@
+// step.cu -- the time step on the device: one fused kernel per RK stage
+// (stage values, 11-point derivatives, CPML, RHS, boundary zeroing, stage or
+// final update, diagnostics), the PULSE = 2 forcing of an iteration, and
+// the FILTER_VARS passes.
+//
+// Stage kernel layout: a CTA owns a TX x TY tile of (x, y) columns and
+// marches up a chunk of z layers.  z derivatives come from an 11-deep
+// register window per z-differentiated field (the thread's own column);
+// x and y derivatives from a shared-memory layer tile with a 5-point halo.
+// Stage values a + beta*scr are formed on load, so no temp_step array
+// exists (step.f90:27-37 never touches HBM).
+
+#include <cmath>
+
+#include "internal.h"
+
+namespace sparc {
+
+__constant__ double c_dp[6][11];   // derivative rows, initialize.f90:1959-2031
+__constant__ double c_df[2][11];   // filter stencils: [0] xy, [1] z
+
+enum { FIRST = 0, MID = 1, LAST = 2 };
+
+int step_constants() {
+  if (cudaMemcpyToSymbol(c_dp, kDerivRows, sizeof(double) * 66) != cudaSuccess)
+    return SPARC_ERR_CUDA;
+  return SPARC_OK;
+}
+
+// Stage value a + beta*scr_prev (step.f90:33).
+template <int MODE>
+__device__ __forceinline__ double sval(const double *__restrict__ a,
+                                       const double *__restrict__ s,
+                                       long long idx, double beta) {
+  double v = __ldg(a + idx);
+  if (MODE != FIRST) v = v + beta * __ldg(s + idx);
+  return v;
+}
+
+// CPML correction of one derivative (RHS.f90:50-93, 424-546):
+// RHSpsi = a*d + b*psi ; d = d/kappa + psi.  LAST applies the final RK
+// update of the auxiliary field in place (step.f90:59-61).
+template <int MODE>
+__device__ __forceinline__ void cpml(const FaceDev &F, long long f, int layer,
+                                     int slot, double beta, double dt,
+                                     double &d) {
+  const long long pf = F.uniform ? (long long)layer : f;
+  const double pa = __ldg(F.pa + pf), pb = __ldg(F.pb + pf),
+               pk = __ldg(F.pk + pf);
+  const long long o = (long long)slot * F.cnt + f;
+  const double v = F.vars[o];
+  double psi = v;
+  if (MODE != FIRST) psi = v + beta * F.scr[o];
+  const double rhs = pa * d + pb * psi;
+  d = d / pk + psi;
+  if (MODE == LAST) F.vars[o] = v + dt * rhs;
+  else F.scr[o] = rhs;
+}
+
+// Forcing of driver.f90:137-153 at point (i, j, k) of iteration `it`.
+__device__ __forceinline__ double forcing_at(const SimDev &S, long long it,
+                                             double T, int i, int j, int k) {
+  const ForcingDev &F = S.frc;
+  if (F.kind == SPARC_SRC_PULSE)
+    return T * __ldg(F.fz + k) * (__ldg(F.fy + j) * __ldg(F.fx + i));
+  if (F.kind == SPARC_SRC_PSR && k >= F.klo && k < F.khi)
+    return F.psr[((long long)(k - F.klo) * S.ny + j) * S.nx + i];
+  return 0.0;
+}
+
+__device__ __forceinline__ double pulse_time(const SimDev &S, long long it) {
+  const ForcingDev &F = S.frc;
+  if (F.kind != SPARC_SRC_PULSE) return 0.0;
+  const double t = (double)it * F.timestep;
+  double T = F.amp_c * sin(2.0 * PI * (t - F.t1 + 2.0 * F.t0) / F.t0);
+  return T * exp(-1.0 * ((t - F.t1) * (t - F.t1)) / (2.0 * (F.st * F.st)));
+}
+
+// ------------------------------------------------------------ diagnostics
+// Block partial of the KE norm and the two minima, then the last CTA to
+// finish reduces all partials (no waiting: it is simply the last to arrive)
+// and applies the fail criterion of driver.f90:175-183.
+__device__ void diag_reduce(const SimDev &S, double ke, double mr, double mp) {
+  __shared__ double r[3][32];
+  __shared__ int am_last;
+  const int nt = blockDim.x * blockDim.y;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5, nw = (nt + 31) >> 5;
+  const long long nb = (long long)gridDim.x * gridDim.y * gridDim.z;
+  const long long bid = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+  for (int o = 16; o > 0; o >>= 1) {
+    ke += __shfl_down_sync(0xffffffffu, ke, o);
+    mr = fmin(mr, __shfl_down_sync(0xffffffffu, mr, o));
+    mp = fmin(mp, __shfl_down_sync(0xffffffffu, mp, o));
+  }
+  if (lane == 0) { r[0][warp] = ke; r[1][warp] = mr; r[2][warp] = mp; }
+  __syncthreads();
+  if (warp == 0) {
+    ke = lane < nw ? r[0][lane] : 0.0;
+    mr = lane < nw ? r[1][lane] : 1e300;
+    mp = lane < nw ? r[2][lane] : 1e300;
+    for (int o = 16; o > 0; o >>= 1) {
+      ke += __shfl_down_sync(0xffffffffu, ke, o);
+      mr = fmin(mr, __shfl_down_sync(0xffffffffu, mr, o));
+      mp = fmin(mp, __shfl_down_sync(0xffffffffu, mp, o));
+    }
+    if (lane == 0) {
+      S.partials[3 * bid] = ke;
+      S.partials[3 * bid + 1] = mr;
+      S.partials[3 * bid + 2] = mp;
+      __threadfence();
+      unsigned t = atomicAdd(S.counter, 1u);
+      am_last = (t == (unsigned)(nb - 1));
+    }
+  }
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+  ke = 0.0; mr = 1e300; mp = 1e300;
+  for (long long b = tid; b < nb; b += nt) {
+    ke += __ldcg(S.partials + 3 * b);
+    mr = fmin(mr, __ldcg(S.partials + 3 * b + 1));
+    mp = fmin(mp, __ldcg(S.partials + 3 * b + 2));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    ke += __shfl_down_sync(0xffffffffu, ke, o);
+    mr = fmin(mr, __shfl_down_sync(0xffffffffu, mr, o));
+    mp = fmin(mp, __shfl_down_sync(0xffffffffu, mp, o));
+  }
+  __syncthreads();
+  if (lane == 0) { r[0][warp] = ke; r[1][warp] = mr; r[2][warp] = mp; }
+  __syncthreads();
+  if (tid == 0) {
+    ke = 0.0; mr = 1e300; mp = 1e300;
+    for (int w = 0; w < nw; ++w) {
+      ke += r[0][w]; mr = fmin(mr, r[1][w]); mp = fmin(mp, r[2][w]);
+    }
+    const long long it = *S.iter;
+    // norm(): sqrt(sum/(nx*ny*nz)) (all_modules.f90:703), times dimc^2*dimrho
+    double nrm = sqrt(ke / ((double)S.nx * (double)S.ny * (double)S.nz));
+    double kev = nrm * S.dimc2rho;
+    S.diag[0] = kev;
+    S.diag[1] = mr;
+    S.diag[2] = mp;
+    S.diag[3] = (double)it;
+    // driver.f90:175-183; a NaN norm also counts as a failure
+    bool fail = !(kev <= 1000.0) || !(mr > 0.0) || !(mp > 0.0);
+    if (fail && *S.fail_iter < 0) *S.fail_iter = it;
+    *S.iter = it + 1;
+    *S.counter = 0u;
+  }
+}
+
+// ------------------------------------------------------------ helpers
+__device__ __forceinline__ int wrapi(int q, int n) {
+  q = q < 0 ? q + n : q;
+  return q >= n ? q - n : q;
+}
+
+// Global index of local tile position 0 along one axis.  Normally t0 - 5;
+// on a non-periodic axis the last tile may start closer than 6 points to
+// the edge, and its origin then moves down to n - 11 so that the one-sided
+// window f(n-11 .. n-1) is in the tile (interior points still see +-5).
+__device__ __forceinline__ int tile_origin(int t0, int T, int n, bool per) {
+  int o = t0 - 5;
+  if (!per && t0 + T >= n) o = min(o, n - 11);
+  return o;
+}
+
+// x or y derivative at local tile position from a row/column of shared
+// memory: `t(m)` returns the tile value at global index g0 + m.  Periodic
+// axes and interior points use the centred row (RHS bh = 5 / interior),
+// non-periodic edges the one-sided rows (derivatives.f90:72, 98).
+template <class Get>
+__device__ __forceinline__ double dxy(int q, int n, bool per, double sc,
+                                      Get t) {
+  double s = 0.0;
+  if (per || (q >= 5 && q < n - 5)) {
+#pragma unroll
+    for (int m = 0; m < 11; ++m) s += t(q - 5 + m) * c_dp[5][m];
+    return sc * s;
+  }
+  if (q < 5) {
+#pragma unroll
+    for (int m = 0; m < 11; ++m) s += t(m) * c_dp[q][m];
+    return sc * s;
+  }
+  const int row = n - 1 - q;
+#pragma unroll
+  for (int m = 0; m < 11; ++m) s += t(n - 1 - m) * c_dp[row][m];
+  return -sc * s;
+}
+
+// z derivative from the 11-deep window w (w[m] = f(base + m)), with the
+// bottom zero ghosts already in the window and the top one-sided rows
+// (derivatives.f90:509-545).
+__device__ __forceinline__ double dz(const double (&w)[11], int k, int nz,
+                                     double sc) {
+  double s = 0.0;
+  if (k < nz - 5) {
+#pragma unroll
+    for (int m = 0; m < 11; ++m) s += w[m] * c_dp[5][m];
+    return sc * s;
+  }
+  const int row = nz - 1 - k;
+#pragma unroll
+  for (int m = 0; m < 11; ++m) s += w[10 - m] * c_dp[row][m];
+  return -sc * s;
+}
+
+__device__ __forceinline__ void shift(double (&w)[11], double v) {
+#pragma unroll
+  for (int m = 0; m < 10; ++m) w[m] = w[m + 1];
+  w[10] = v;
+}
+
+// value of layer k held in a window whose base is b
+__device__ __forceinline__ double wsel(const double (&w)[11], int off) {
+  double v = w[5];
+#pragma unroll
+  for (int m = 0; m < 11; ++m)
+    if (m == off) v = w[m];
+  return v;
+}
+
+// ------------------------------------------------ MP_QUIET_3D stage kernel
+// RHS.f90:18-175 fused with one RK stage of step.f90:26-61.
+template <int TX, int TY, int MODE, bool BG1D>
+__global__ void __launch_bounds__(TX *TY)
+    k_stage_quiet(const SimDev S, const double *__restrict__ a,
+                  const double *__restrict__ sp, double *__restrict__ so,
+                  double beta, int zchunk) {
+  constexpr int HX = TX + 10, HY = TY + 10;
+  __shared__ double t_vx[HY][HX], t_vy[HY][HX], t_p[HY][HX];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int nx = S.nx, ny = S.ny, nz = S.nz;
+  const long long N = S.N, NXY = (long long)nx * ny;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int i = x0 + tx, j = y0 + ty;
+  const bool act = i < nx && j < ny;
+  const bool per = S.periodic;
+  const int k0 = blockIdx.z * zchunk, k1 = min(nz, k0 + zchunk);
+  const long long col = (long long)j * nx + i;
+  const long long it = *S.iter;
+  const double Tp = pulse_time(S, it);
+  const double dt = S.deltat;
+  const int gc = act ? S.colx[i] + S.bxdim * S.coly[j] : 0;
+  const int xo = tile_origin(x0, TX, nx, per), yo = tile_origin(y0, TY, ny, per);
+  const int cx0 = x0 - xo, cy0 = y0 - yo;  // interior offset in the tile
+
+  double wvz[11], wp[11];
+  const int b0 = min(k0 - 5, nz - 11);
+#pragma unroll
+  for (int m = 0; m < 11; ++m) {
+    const int kk = b0 + m;
+    const bool ok = act && kk >= 0;
+    const long long id = (long long)kk * NXY + col;
+    wvz[m] = ok ? sval<MODE>(a + 3 * N, sp + 3 * N, id, beta) : 0.0;
+    wp[m] = ok ? sval<MODE>(a + 4 * N, sp + 4 * N, id, beta) : 0.0;
+  }
+  double ke = 0.0, mr = 1e300, mp = 1e300;
+
+  for (int k = k0; k < k1; ++k) {
+    if (k > k0 && k <= nz - 6) {
+      const long long id = (long long)(k + 5) * NXY + col;
+      shift(wvz, act ? sval<MODE>(a + 3 * N, sp + 3 * N, id, beta) : 0.0);
+      shift(wp, act ? sval<MODE>(a + 4 * N, sp + 4 * N, id, beta) : 0.0);
+    }
+    const long long kb = (long long)k * NXY;
+    __syncthreads();
+    for (int t = tid; t < HY * HX; t += TX * TY) {
+      const int ly = t / HX, lx = t - ly * HX;
+      const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
+      if (!inx && !iny) continue;
+      int gx = xo + lx, gy = yo + ly;
+      bool ok;
+      if (per) {
+        gx = wrapi(gx, nx);
+        gy = wrapi(gy, ny);
+        ok = true;
+      } else {
+        ok = gx >= 0 && gx < nx && gy >= 0 && gy < ny;
+      }
+      const long long id = kb + (long long)gy * nx + gx;
+      if (iny) t_vx[ly][lx] = ok ? sval<MODE>(a + N, sp + N, id, beta) : 0.0;
+      if (inx) t_vy[ly][lx] = ok ? sval<MODE>(a + 2 * N, sp + 2 * N, id, beta) : 0.0;
+      t_p[ly][lx] = ok ? sval<MODE>(a + 4 * N, sp + 4 * N, id, beta) : 0.0;
+    }
+    __syncthreads();
+    if (!act) continue;
+    const long long id = kb + col;
+    double av[5], tv[5];
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+      av[l] = __ldg(a + l * N + id);
+      tv[l] = av[l];
+      if (MODE != FIRST) tv[l] = av[l] + beta * __ldg(sp + l * N + id);
+    }
+    const double rho = tv[0], vx = tv[1], vy = tv[2], vz = tv[3], p = tv[4];
+    // derivatives (RHS.f90:42-48)
+    const int ry = cy0 + ty, rx = cx0 + tx;  // own tile row / column
+    double dvxdx = dxy(i, nx, per, S.stretchx, [&](int g) { return t_vx[ry][g - xo]; });
+    double gpx = dxy(i, nx, per, S.stretchx, [&](int g) { return t_p[ry][g - xo]; });
+    double dvydy = dxy(j, ny, per, S.stretchy, [&](int g) { return t_vy[g - yo][rx]; });
+    double gpy = dxy(j, ny, per, S.stretchy, [&](int g) { return t_p[g - yo][rx]; });
+    const double szk = __ldg(S.stretch + k);
+    double dvzdz = dz(wvz, k, nz, szk);
+    double gpz = dz(wp, k, nz, szk);
+    // CPML (RHS.f90:50-93); psi slots: 0 vz/vx/vy, 1 p
+    if (k < S.zb.np) {
+      const long long f = kb + col;
+      cpml<MODE>(S.zb, f, k, 1, beta, dt, gpz);
+      cpml<MODE>(S.zb, f, k, 0, beta, dt, dvzdz);
+    } else if (S.zt.on && k >= nz - S.zt.np) {
+      const int kl = k - (nz - S.zt.np);
+      const long long f = (long long)kl * NXY + col;
+      cpml<MODE>(S.zt, f, kl, 1, beta, dt, gpz);
+      cpml<MODE>(S.zt, f, kl, 0, beta, dt, dvzdz);
+    }
+    if (S.xb.on) {
+      if (i < S.xb.np) {
+        const long long f = i + (long long)S.xb.np * (j + (long long)ny * k);
+        cpml<MODE>(S.xb, f, i, 1, beta, dt, gpx);
+        cpml<MODE>(S.xb, f, i, 0, beta, dt, dvxdx);
+      } else if (i >= nx - S.xt.np) {
+        const int il = i - (nx - S.xt.np);
+        const long long f = il + (long long)S.xt.np * (j + (long long)ny * k);
+        cpml<MODE>(S.xt, f, il, 1, beta, dt, gpx);
+        cpml<MODE>(S.xt, f, il, 0, beta, dt, dvxdx);
+      }
+      if (j < S.yb.np) {
+        const long long f = i + (long long)nx * (j + (long long)S.yb.np * k);
+        cpml<MODE>(S.yb, f, j, 1, beta, dt, gpy);
+        cpml<MODE>(S.yb, f, j, 0, beta, dt, dvydy);
+      } else if (j >= ny - S.yt.np) {
+        const int jl = j - (ny - S.yt.np);
+        const long long f = i + (long long)nx * (jl + (long long)S.yt.np * k);
+        cpml<MODE>(S.yt, f, jl, 1, beta, dt, gpy);
+        cpml<MODE>(S.yt, f, jl, 0, beta, dt, dvydy);
+      }
+    }
+    // RHS algebra (RHS.f90:95-152)
+    const long long bi = BG1D ? (long long)k : id;
+    const double r0 = __ldg(S.rho0 + bi), ri = __ldg(S.rhoinv + bi),
+                 c2r = __ldg(S.c2rho0 + bi), grz = __ldg(S.grz + bi),
+                 gp0 = __ldg(S.gpz + bi), sg = __ldg(S.sponge + bi);
+    const double gk = __ldg(S.gblk + (long long)gc * nz + k);
+    const double div = dvxdx + dvydy + dvzdz;
+    double R[5];
+    R[0] = -grz * vz - r0 * div - sg * rho;
+    R[1] = -ri * gpx - sg * vx;
+    R[2] = -ri * gpy - sg * vy;
+    R[3] = -ri * (gpz + rho * gk) - vz * sg;
+    if (S.frc.kind != SPARC_SRC_NONE) {
+      const double frc = forcing_at(S, it, Tp, i, j, k);
+      if (S.frc.dir == 1) R[1] = R[1] + frc;
+      else if (S.frc.dir == 2) R[2] = R[2] + frc;
+      else R[3] = R[3] + frc;
+    }
+    R[4] = -c2r * div - vz * gp0 - sg * p;
+    // boundary planes (RHS.f90:154-164)
+    const bool zero = k == 0 || k == nz - 1 ||
+                      (!per && (i == 0 || i == nx - 1 || j == 0 || j == ny - 1));
+    if (MODE == LAST) {
+      double an[5];
+#pragma unroll
+      for (int l = 0; l < 5; ++l) {
+        an[l] = zero ? av[l] : av[l] + dt * R[l];
+        so[l * N + id] = an[l];
+      }
+      const double p0v = __ldg(S.p0 + bi);
+      double m = (r0 + an[0]) * (an[1] * an[1] + an[2] * an[2] + an[3] * an[3]) / 2.0;
+      ke += m * m;
+      mr = fmin(mr, rho + r0);
+      mp = fmin(mp, p + p0v);
+    } else {
+#pragma unroll
+      for (int l = 0; l < 5; ++l) so[l * N + id] = zero ? 0.0 : R[l];
+    }
+  }
+  if (MODE == LAST) diag_reduce(S, ke, mr, mp);
+}
+
+// -------------------------------------------------- MP_MHD_3D stage kernel
+// RHS.f90:363-668 fused with one RK stage.  Tile slots of the dynamic
+// shared memory: 0 vx, 1 vy, 2 p, 3 bx, 4 by, 5 bz, 6 flux1, 7 flux2,
+// 8 flux3 (flux = v x B0 of RHS.f90:394-396).
+template <int TX, int TY, int MODE>
+__global__ void __launch_bounds__(TX *TY, 1)
+    k_stage_mhd(const SimDev S, const double *__restrict__ a,
+                const double *__restrict__ sp, double *__restrict__ so,
+                double beta, int zchunk) {
+  constexpr int HX = TX + 10, HY = TY + 10, HS = HX * HY;
+  extern __shared__ double tile[];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int nx = S.nx, ny = S.ny, nz = S.nz;
+  const long long N = S.N, NXY = (long long)nx * ny;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int i = x0 + tx, j = y0 + ty;
+  const bool act = i < nx && j < ny;
+  const bool per = S.periodic;
+  const int k0 = blockIdx.z * zchunk, k1 = min(nz, k0 + zchunk);
+  const long long col = (long long)j * nx + i;
+  const long long it = *S.iter;
+  const double Tp = pulse_time(S, it);
+  const double dt = S.deltat;
+  const int gc = act ? S.colx[i] + S.bxdim * S.coly[j] : 0;
+  auto T = [&](int slot, int ly, int lx) -> double & {
+    return tile[slot * HS + ly * HX + lx];
+  };
+  const int xo = tile_origin(x0, TX, nx, per), yo = tile_origin(y0, TY, ny, per);
+  const int cx0 = x0 - xo, cy0 = y0 - yo;
+
+  // windows: vz, p, flux1, flux2, bx, by
+  double w_vz[11], w_p[11], w_f1[11], w_f2[11], w_bx[11], w_by[11];
+  auto head = [&](int kk, double &vz_, double &p_, double &f1_, double &f2_,
+                  double &bx_, double &by_) {
+    const long long id = (long long)kk * NXY + col;
+    const double vx_ = sval<MODE>(a + N, sp + N, id, beta);
+    const double vy_ = sval<MODE>(a + 2 * N, sp + 2 * N, id, beta);
+    vz_ = sval<MODE>(a + 3 * N, sp + 3 * N, id, beta);
+    p_ = sval<MODE>(a + 4 * N, sp + 4 * N, id, beta);
+    bx_ = sval<MODE>(a + 5 * N, sp + 5 * N, id, beta);
+    by_ = sval<MODE>(a + 6 * N, sp + 6 * N, id, beta);
+    const double ox = __ldg(S.box + id), oy = __ldg(S.boy + id),
+                 oz = __ldg(S.boz + id);
+    f1_ = -vz_ * oy + vy_ * oz;
+    f2_ = -vx_ * oz + vz_ * ox;
+  };
+  const int b0 = min(k0 - 5, nz - 11);
+#pragma unroll
+  for (int m = 0; m < 11; ++m) {
+    const int kk = b0 + m;
+    if (act && kk >= 0) {
+      head(kk, w_vz[m], w_p[m], w_f1[m], w_f2[m], w_bx[m], w_by[m]);
+    } else {
+      w_vz[m] = w_p[m] = w_f1[m] = w_f2[m] = w_bx[m] = w_by[m] = 0.0;
+    }
+  }
+  double ke = 0.0, mr = 1e300, mp = 1e300;
+
+  for (int k = k0; k < k1; ++k) {
+    if (k > k0 && k <= nz - 6) {
+      double v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;
+      if (act) head(k + 5, v0, v1, v2, v3, v4, v5);
+      shift(w_vz, v0); shift(w_p, v1); shift(w_f1, v2);
+      shift(w_f2, v3); shift(w_bx, v4); shift(w_by, v5);
+    }
+    const long long kb = (long long)k * NXY;
+    __syncthreads();
+    for (int t = tid; t < HS; t += TX * TY) {
+      const int ly = t / HX, lx = t - ly * HX;
+      const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
+      if (!inx && !iny) continue;
+      int gx = xo + lx, gy = yo + ly;
+      bool ok;
+      if (per) {
+        gx = wrapi(gx, nx);
+        gy = wrapi(gy, ny);
+        ok = true;
+      } else {
+        ok = gx >= 0 && gx < nx && gy >= 0 && gy < ny;
+      }
+      double vx_ = 0, vy_ = 0, vz_ = 0, p_ = 0, bx_ = 0, by_ = 0, bz_ = 0,
+             ox = 0, oy = 0, oz = 0;
+      if (ok) {
+        const long long id = kb + (long long)gy * nx + gx;
+        vx_ = sval<MODE>(a + N, sp + N, id, beta);
+        vy_ = sval<MODE>(a + 2 * N, sp + 2 * N, id, beta);
+        vz_ = sval<MODE>(a + 3 * N, sp + 3 * N, id, beta);
+        p_ = sval<MODE>(a + 4 * N, sp + 4 * N, id, beta);
+        bx_ = sval<MODE>(a + 5 * N, sp + 5 * N, id, beta);
+        by_ = sval<MODE>(a + 6 * N, sp + 6 * N, id, beta);
+        bz_ = sval<MODE>(a + 7 * N, sp + 7 * N, id, beta);
+        ox = __ldg(S.box + id); oy = __ldg(S.boy + id); oz = __ldg(S.boz + id);
+      }
+      T(0, ly, lx) = vx_;
+      T(1, ly, lx) = vy_;
+      T(2, ly, lx) = p_;
+      T(3, ly, lx) = bx_;
+      T(4, ly, lx) = by_;
+      T(5, ly, lx) = bz_;
+      T(6, ly, lx) = -vz_ * oy + vy_ * oz;
+      T(7, ly, lx) = -vx_ * oz + vz_ * ox;
+      T(8, ly, lx) = -vy_ * ox + vx_ * oy;
+    }
+    __syncthreads();
+    if (!act) continue;
+    const long long id = kb + col;
+    double av[8], tv[8];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+      av[l] = __ldg(a + l * N + id);
+      tv[l] = av[l];
+      if (MODE != FIRST) tv[l] = av[l] + beta * __ldg(sp + l * N + id);
+    }
+    const int ry = cy0 + ty, rx = cx0 + tx;
+    auto DX = [&](int slot) {
+      return dxy(i, nx, per, S.stretchx, [&](int g) { return T(slot, ry, g - xo); });
+    };
+    auto DY = [&](int slot) {
+      return dxy(j, ny, per, S.stretchy, [&](int g) { return T(slot, g - yo, rx); });
+    };
+    // the 15 derivatives of RHS.f90:400-422
+    double dvxdx = DX(0), dxflux3 = DX(8), gpx = DX(2), dxflux2 = DX(7),
+           dxby = DX(4), dxbz = DX(5);
+    double dvydy = DY(1), gpy = DY(2), dyflux3 = DY(8), dybz = DY(5),
+           dybx = DY(3), dyflux1 = DY(6);
+    const double szk = __ldg(S.stretch + k);
+    double dvzdz = dz(w_vz, k, nz, szk), dzflux1 = dz(w_f1, k, nz, szk),
+           dzflux2 = dz(w_f2, k, nz, szk), dzbx = dz(w_bx, k, nz, szk),
+           gpz = dz(w_p, k, nz, szk), dzby = dz(w_by, k, nz, szk);
+    // CPML, RHS.f90:424-546.  Slots: z 0 vz, 1 p, 2 dzbx, 3 dzby,
+    // 4 dzflux2, 5 dzflux1; x 0 vx, 1 p, 2 dxby, 3 dxbz, 4 dxflux3,
+    // 5 dxflux2; y 0 vy, 1 p, 2 dybx, 3 dybz, 4 dyflux3, 5 dyflux1.
+    if (S.zb.on && (k < S.zb.np || k >= nz - S.zt.np)) {
+      const bool bot = k < S.zb.np;
+      const FaceDev &F = bot ? S.zb : S.zt;
+      const int kl = bot ? k : k - (nz - S.zt.np);
+      const long long f = (long long)kl * NXY + col;
+      cpml<MODE>(F, f, kl, 1, beta, dt, gpz);
+      cpml<MODE>(F, f, kl, 0, beta, dt, dvzdz);
+      cpml<MODE>(F, f, kl, 4, beta, dt, dzflux2);
+      cpml<MODE>(F, f, kl, 5, beta, dt, dzflux1);
+      cpml<MODE>(F, f, kl, 2, beta, dt, dzbx);
+      cpml<MODE>(F, f, kl, 3, beta, dt, dzby);
+    }
+    if (S.xb.on) {
+      if (i < S.xb.np || i >= nx - S.xt.np) {
+        const bool bot = i < S.xb.np;
+        const FaceDev &F = bot ? S.xb : S.xt;
+        const int il = bot ? i : i - (nx - S.xt.np);
+        const long long f = il + (long long)F.np * (j + (long long)ny * k);
+        cpml<MODE>(F, f, il, 1, beta, dt, gpx);
+        cpml<MODE>(F, f, il, 0, beta, dt, dvxdx);
+        cpml<MODE>(F, f, il, 4, beta, dt, dxflux3);
+        cpml<MODE>(F, f, il, 5, beta, dt, dxflux2);
+        cpml<MODE>(F, f, il, 2, beta, dt, dxby);
+        cpml<MODE>(F, f, il, 3, beta, dt, dxbz);
+      }
+      if (j < S.yb.np || j >= ny - S.yt.np) {
+        const bool bot = j < S.yb.np;
+        const FaceDev &F = bot ? S.yb : S.yt;
+        const int jl = bot ? j : j - (ny - S.yt.np);
+        const long long f = i + (long long)nx * (jl + (long long)F.np * k);
+        cpml<MODE>(F, f, jl, 1, beta, dt, gpy);
+        cpml<MODE>(F, f, jl, 0, beta, dt, dvydy);
+        cpml<MODE>(F, f, jl, 4, beta, dt, dyflux3);
+        cpml<MODE>(F, f, jl, 5, beta, dt, dyflux1);
+        cpml<MODE>(F, f, jl, 2, beta, dt, dybx);
+        cpml<MODE>(F, f, jl, 3, beta, dt, dybz);
+      }
+    }
+    // RHS algebra, RHS.f90:548-645
+    const double rho = tv[0], vx = tv[1], vy = tv[2], vz = tv[3], p = tv[4],
+                 bx = tv[5], by = tv[6], bz = tv[7];
+    const double red = __ldg(S.red + id);
+    const double ox = __ldg(S.box + id), oy = __ldg(S.boy + id),
+                 oz = __ldg(S.boz + id);
+    double R[8];
+    R[5] = red * (dyflux3 - dzflux2);
+    R[6] = red * (dzflux1 - dxflux3);
+    R[7] = red * (dxflux2 - dyflux1);
+    const double div = dvxdx + dvydy + dvzdz;
+    const double cbx = dybz - dzby, cby = -dxbz + dzbx, cbz = dxby - dybx;
+    const double sg = __ldg(S.sponge + id), r0 = __ldg(S.rho0 + id);
+    R[0] = -__ldg(S.grx + id) * vx - __ldg(S.gry + id) * vy -
+           __ldg(S.grz + id) * vz - r0 * div - sg * rho;
+    R[4] = -__ldg(S.c2rho0 + id) * div - vx * __ldg(S.gpx + id) -
+           vy * __ldg(S.gpy + id) - vz * __ldg(S.gpz + id) - sg * p;
+    const double c1 = cby * oz - cbz * oy, c2 = ox * cbz - cbx * oz,
+                 c3 = cbx * oy - cby * ox;
+    const double ri = __ldg(S.rhoinv + id);
+    double vxr = -ri * (gpx - (c1 * red)) - sg * vx;
+    double vyr = -ri * (gpy - (c2 * red)) - sg * vy;
+    double vzr = -ri * (gpz - (c3 * red)) - sg * vz;
+    const double qx = __ldg(S.cbx + id), qy = __ldg(S.cby + id),
+                 qz = __ldg(S.cbz + id);
+    const double d1 = qy * bz - qz * by, d2 = bx * qz - qx * bz,
+                 d3 = qx * by - qy * bx;
+    vxr = vxr + ri * d1 * red;
+    vyr = vyr + ri * d2 * red;
+    vzr = vzr + ri * d3 * red;
+    vzr = vzr - ri * rho * __ldg(S.gblk + (long long)gc * nz + k);
+    R[1] = vxr;
+    R[2] = vyr;
+    R[3] = vzr;
+    if (S.frc.kind != SPARC_SRC_NONE) {
+      const double frc = forcing_at(S, it, Tp, i, j, k);
+      if (S.frc.dir == 1) R[1] = R[1] + frc;
+      else if (S.frc.dir == 2) R[2] = R[2] + frc;
+      else R[3] = R[3] + frc;
+    }
+    const bool zero = k == 0 || k == nz - 1 ||
+                      (!per && (i == 0 || i == nx - 1 || j == 0 || j == ny - 1));
+    if (MODE == LAST) {
+      double an[8];
+#pragma unroll
+      for (int l = 0; l < 8; ++l) {
+        an[l] = zero ? av[l] : av[l] + dt * R[l];
+        so[l * N + id] = an[l];
+      }
+      const double p0v = __ldg(S.p0 + id);
+      double m = (r0 + an[0]) * (an[1] * an[1] + an[2] * an[2] + an[3] * an[3]) / 2.0;
+      ke += m * m;
+      mr = fmin(mr, rho + r0);
+      mp = fmin(mp, p + p0v);
+    } else {
+#pragma unroll
+      for (int l = 0; l < 8; ++l) so[l * N + id] = zero ? 0.0 : R[l];
+    }
+  }
+  if (MODE == LAST) diag_reduce(S, ke, mr, mp);
+}
+
+// ------------------------------------------------------- stage dispatch
+int stage_geometry(Handle *h) {
+  // tile shape: (32, 8) unless the grid is too small to fill the GPU
+  h->tx = 32;
+  h->ty = 8;
+  long long tiles = (long long)((h->nx + h->tx - 1) / h->tx) *
+                    ((h->ny + h->ty - 1) / h->ty);
+  if (tiles < 64) {
+    h->tx = 16;
+    tiles = (long long)((h->nx + 15) / 16) * ((h->ny + 7) / 8);
+  }
+  // z chunk: aim for >= 4 CTAs per SM on 148 SMs
+  int zc = h->nz;
+  while (zc > 16 && tiles * ((h->nz + zc - 1) / zc) < 148 * 4) zc = (zc + 1) / 2;
+  h->zchunk = zc;
+  h->max_stage_blocks = (int)(tiles * ((h->nz + zc - 1) / zc));
+  return SPARC_OK;
+}
+
+template <int TX, int TY>
+static int launch_quiet(Handle *h, const SimDev &S, int stage,
+                        const double *a, const double *sp, double *so,
+                        cudaStream_t s) {
+  dim3 blk(TX, TY);
+  dim3 grd((h->nx + TX - 1) / TX, (h->ny + TY - 1) / TY,
+           (h->nz + h->zchunk - 1) / h->zchunk);
+  const double beta = h->betas[stage - 1];
+  const int mode = stage == 1 ? FIRST : (stage == 5 ? LAST : MID);
+#define QL(M, B) k_stage_quiet<TX, TY, M, B><<<grd, blk, 0, s>>>(S, a, sp, so, beta, h->zchunk)
+  if (S.bg1d) {
+    if (mode == FIRST) QL(FIRST, true);
+    else if (mode == MID) QL(MID, true);
+    else QL(LAST, true);
+  } else {
+    if (mode == FIRST) QL(FIRST, false);
+    else if (mode == MID) QL(MID, false);
+    else QL(LAST, false);
+  }
+#undef QL
+  return SPARC_OK;
+}
+
+template <int TX, int TY>
+static int launch_mhd(Handle *h, const SimDev &S, int stage, const double *a,
+                      const double *sp, double *so, cudaStream_t s) {
+  dim3 blk(TX, TY);
+  dim3 grd((h->nx + TX - 1) / TX, (h->ny + TY - 1) / TY,
+           (h->nz + h->zchunk - 1) / h->zchunk);
+  const double beta = h->betas[stage - 1];
+  const size_t smem = sizeof(double) * 9 * (TX + 10) * (TY + 10);
+  const int mode = stage == 1 ? FIRST : (stage == 5 ? LAST : MID);
+  if (mode == FIRST)
+    cudaFuncSetAttribute(k_stage_mhd<TX, TY, FIRST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  else if (mode == MID)
+    cudaFuncSetAttribute(k_stage_mhd<TX, TY, MID>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  else
+    cudaFuncSetAttribute(k_stage_mhd<TX, TY, LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (mode == FIRST) k_stage_mhd<TX, TY, FIRST><<<grd, blk, smem, s>>>(S, a, sp, so, beta, h->zchunk);
+  else if (mode == MID) k_stage_mhd<TX, TY, MID><<<grd, blk, smem, s>>>(S, a, sp, so, beta, h->zchunk);
+  else k_stage_mhd<TX, TY, LAST><<<grd, blk, smem, s>>>(S, a, sp, so, beta, h->zchunk);
+  return SPARC_OK;
+}
+
+int launch_stage(Handle *h, const SimDev &S, int stage, const double *a,
+                 const double *sp, double *so, cudaStream_t s) {
+  int r = SPARC_ERR_INVALID;
+  const int key = h->tx * 100 + h->ty;
+#define DISPATCH(FN)                                            \
+  switch (key) {                                                \
+    case 3208: r = FN<32, 8>(h, S, stage, a, sp, so, s); break; \
+    case 1608: r = FN<16, 8>(h, S, stage, a, sp, so, s); break; \
+    default: r = SPARC_ERR_INVALID;                             \
+  }
+  if (h->magnetic) { DISPATCH(launch_mhd) } else { DISPATCH(launch_quiet) }
+#undef DISPATCH
+  ++h->launches;
+  if (r == SPARC_OK && cudaGetLastError() != cudaSuccess) r = SPARC_ERR_CUDA;
+  return r;
+}
+
+// ------------------------------------------------------- PULSE = 2 forcing
+// all_modules.f90:592-611 / 644-660 and driver.f90:153 for the layers that
+// carry any pulse: sum over the layer's pulses of
+// T_n(t) * Z_n(k) * X_n(i) * Y_n(j), culled per reference rank block, twice
+// at the run's first iteration, times source_damp * src_scale_beta.
+struct PsrDev {
+  int nx, ny, nz, klo, npulses, nblocks;
+  long long init;
+  double timestep, st;
+  const int *off, *idx;
+  const double *zv, *px, *py, *ptime, *sd, *ssb;
+  const unsigned char *mask;
+  const int *colx, *coly, *colz;
+  int bx, bxy;
+  double *out;
+  const long long *iter;
+};
+
+__global__ void k_psr(PsrDev D) {
+  extern __shared__ double sh[];
+  const int k = D.klo + blockIdx.z;
+  const int e0 = D.off[k], e1 = D.off[k + 1], ne = e1 - e0;
+  double *sT = sh;
+  int *sN = (int *)(sh + ne);
+  const long long it = *D.iter;
+  const double t = (double)it * D.timestep;
+  const double passes = (it == D.init) ? 2.0 : 1.0;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  for (int e = tid; e < ne; e += blockDim.x * blockDim.y) {
+    const int n = D.idx[e0 + e];
+    const double amp = D.ptime[3 * n], t0 = D.ptime[3 * n + 1],
+                 t1 = D.ptime[3 * n + 2];
+    double v = amp * sin(2.0 * PI * (t - t1) / t0);
+    v = v * exp(-((t - t1) * (t - t1)) / (2.0 * (D.st * D.st)));
+    sT[e] = v * D.zv[e0 + e] * passes;
+    sN[e] = n;
+  }
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= D.nx || j >= D.ny) return;
+  const int blk = D.colx[i] + D.bx * D.coly[j] + D.bxy * D.colz[k];
+  double f = 0.0;
+  for (int e = 0; e < ne; ++e) {
+    const int n = sN[e];
+    if (!D.mask[(long long)n * D.nblocks + blk]) continue;
+    f = f + sT[e] * (D.px[(long long)n * D.nx + i] * D.py[(long long)n * D.ny + j]);
+  }
+  const long long g = ((long long)k * D.ny + j) * D.nx + i;
+  D.out[((long long)blockIdx.z * D.ny + j) * D.nx + i] = f * D.sd[g] * D.ssb[g];
+}
+
+int launch_psr_forcing(Handle *h, const SimDev &S, cudaStream_t s);
+
+// ------------------------------------------------------ FILTER_VARS pass
+// One direction of FILTER_VARS (derivatives.f90:659-703) over all fields:
+// out = filt(pre(in)) (mode 1) or pre(in) - s*filt(pre(in)) (mode 2), where
+// pre() is the edge pre-averaging of :672-693 applied on the fly from the
+// unmodified input.
+struct FiltDev {
+  int nx, ny, nz, periodic, g, mode2, V;
+  long long N;
+  double s;
+};
+
+template <int DIR>
+__global__ void k_filter_pass(FiltDev F, const double *__restrict__ in,
+                              double *__restrict__ out) {
+  const long long total = F.N * F.V;
+  const int n = DIR == 0 ? F.nx : (DIR == 1 ? F.ny : F.nz);
+  const long long st = DIR == 0 ? 1 : (DIR == 1 ? F.nx : (long long)F.nx * F.ny);
+  const bool per = DIR != 2 && F.periodic;
+  const bool avg = DIR == 2 || !F.periodic;
+  const int g = F.g;
+  const double *c = c_df[DIR == 2 ? 1 : 0];
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long pnt = t % F.N;
+    int q;
+    if (DIR == 0) q = (int)(pnt % F.nx);
+    else if (DIR == 1) q = (int)((pnt / F.nx) % F.ny);
+    else q = (int)(pnt / ((long long)F.nx * F.ny));
+    const long long base = t - (long long)q * st;
+    auto pre = [&](int qq) -> double {
+      const long long id = base + (long long)qq * st;
+      if (avg && ((qq >= 1 && qq <= g - 1) || (qq >= n - g && qq <= n - 2)))
+        return (__ldg(in + id + st) + __ldg(in + id - st)) / 2.0;
+      return __ldg(in + id);
+    };
+    const double pq = pre(q);
+    double filt;
+    if (!per && (q < g || q >= n - g)) {
+      filt = (DIR != 2 && g == 3) ? 0.0 : pq;
+    } else {
+      double s = 0.0;
+      for (int m = 0; m < 2 * g + 1; ++m) {
+        int qq = q - g + m;
+        if (per) qq = wrapi(qq, n);
+        s += pre(qq) * c[m];
+      }
+      filt = s;
+    }
+    out[t] = F.mode2 ? pq - F.s * filt : filt;
+  }
+}
+
+int launch_filter_pass(Handle *h, int dir, const double *in, double *out,
+                       cudaStream_t s) {
+  FiltDev F;
+  F.nx = h->nx; F.ny = h->ny; F.nz = h->nz;
+  F.periodic = h->periodic ? 1 : 0;
+  F.g = dir == 2 ? h->gz : h->gxy;
+  F.mode2 = F.g == 3;
+  F.V = h->V;
+  F.N = h->N;
+  F.s = dir == 2 ? h->P.s_z : h->P.s_xy;
+  long long total = F.N * F.V;
+  unsigned nb = (unsigned)std::min<long long>((total + 255) / 256, 148 * 32);
+  if (dir == 0) k_filter_pass<0><<<nb, 256, 0, s>>>(F, in, out);
+  else if (dir == 1) k_filter_pass<1><<<nb, 256, 0, s>>>(F, in, out);
+  else k_filter_pass<2><<<nb, 256, 0, s>>>(F, in, out);
+  ++h->launches;
+  return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
+}
+
+int filter_constants(int gxy, int gz) {
+  double t[2][11] = {};
+  for (int d = 0; d < 2; ++d) {
+    int g = d == 0 ? gxy : gz;
+    for (int m = 0; m < 11; ++m)
+      t[d][m] = g == 5 ? kFilter11[m] : (m < 7 ? kFilter7[m] : 0.0);
+  }
+  return cudaMemcpyToSymbol(c_df, t, sizeof(t)) == cudaSuccess ? SPARC_OK
+                                                               : SPARC_ERR_CUDA;
+}
+
+int launch_psr_forcing(Handle *h, const SimDev &S, cudaStream_t s) {
+  (void)S;
+  if (h->src.kind != SPARC_SRC_PSR || h->psr_khi <= h->psr_klo) return SPARC_OK;
+  PsrDev D;
+  D.nx = h->nx; D.ny = h->ny; D.nz = h->nz;
+  D.klo = h->psr_klo;
+  D.npulses = (int)h->pulses.size();
+  D.nblocks = h->nblocks;
+  D.init = h->src.init;
+  D.timestep = h->P.timestep;
+  D.st = h->src.psr_st;
+  D.off = h->d_plane_off;
+  D.idx = h->d_plane_idx;
+  D.zv = h->d_plane_z;
+  D.px = h->d_px;
+  D.py = h->d_py;
+  D.ptime = h->d_ptime;
+  D.sd = h->source_damp;
+  D.ssb = h->ssb;
+  D.mask = h->d_pmask;
+  D.colx = h->d_colx;
+  D.coly = h->d_coly;
+  D.colz = h->d_colx + h->nx + h->ny;  // packed after colx, coly
+  D.bx = h->P.block_x;
+  D.bxy = h->P.block_x * h->P.block_y;
+  D.out = h->d_psr;
+  D.iter = h->d_iter;
+  dim3 blk(32, 8);
+  dim3 grd((h->nx + 31) / 32, (h->ny + 7) / 8, h->psr_khi - h->psr_klo);
+  size_t smem = (size_t)D.npulses * (sizeof(double) + sizeof(int));
+  k_psr<<<grd, blk, smem, s>>>(D);
+  ++h->launches;
+  return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
+}
+
+SimDev make_simdev(Handle *h) {
+  SimDev S{};
+  S.nx = h->nx; S.ny = h->ny; S.nz = h->nz; S.N = h->N;
+  S.periodic = h->periodic ? 1 : 0;
+  S.magnetic = h->magnetic ? 1 : 0;
+  S.bg1d = h->bg1d ? 1 : 0;
+  S.V = h->V;
+  S.stretchx = h->stretchx;
+  S.stretchy = h->stretchy;
+  S.stretch = h->d_stretch;
+  S.deltat = h->deltat;
+  S.dimc2rho = (h->dimc * h->dimc) * h->dimrho;
+  if (h->bg1d) {
+    S.rho0 = h->rho0_1; S.p0 = h->p0_1; S.rhoinv = h->rhoinv_1;
+    S.c2rho0 = h->c2rho0_1; S.grz = h->grz_1; S.gpz = h->gpz_1;
+    S.sponge = h->sponge_1;
+  } else {
+    S.rho0 = h->rho0; S.p0 = h->p0; S.rhoinv = h->rhoinv;
+    S.c2rho0 = h->c2rho0; S.grz = h->grz; S.gpz = h->gpz;
+    S.sponge = h->sponge;
+  }
+  S.box = h->box; S.boy = h->boy; S.boz = h->boz;
+  S.cbx = h->cbx; S.cby = h->cby; S.cbz = h->cbz;
+  S.grx = h->grx; S.gry = h->gry; S.gpx = h->gpx; S.gpy = h->gpy;
+  S.red = h->red;
+  S.gblk = h->d_gblk;
+  S.colx = h->d_colx;
+  S.coly = h->d_coly;
+  S.bxdim = h->P.block_x;
+  S.zb = h->faces[0]; S.zt = h->faces[1];
+  S.xb = h->faces[2]; S.xt = h->faces[3];
+  S.yb = h->faces[4]; S.yt = h->faces[5];
+  ForcingDev &F = S.frc;
+  F.kind = h->src.kind;
+  F.dir = h->src.dir;
+  F.init = h->src.init;
+  F.fx = h->d_fx; F.fy = h->d_fy; F.fz = h->d_fz;
+  F.amp_c = h->src.amp / 0.56458272 / h->dimc;
+  F.t0 = h->src.t0; F.t1 = h->src.t1; F.st = h->src.st;
+  F.timestep = h->P.timestep;
+  F.psr = h->d_psr;
+  F.klo = h->psr_klo;
+  F.khi = h->psr_khi;
+  S.iter = h->d_iter;
+  S.partials = h->d_partials;
+  S.counter = h->d_counter;
+  S.diag = h->d_diag;
+  S.fail_iter = h->d_fail;
+  return S;
+}
+
+}  // namespace sparc

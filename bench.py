@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--kernel-steps", type=int, default=10)
     ap.add_argument("--timed-only", action="store_true",
                     help="only the warm-up and the timed region (profiling)")
+    ap.add_argument("--grid", type=int, nargs=3, default=None,
+                    metavar=("NX", "NY", "NZ"),
+                    help="same physics on a smaller grid (profiling only)")
     return ap.parse_args()
 
 
@@ -154,6 +157,9 @@ def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus and args.impl == "gpu":
+        print(f"warning: WORLD_SIZE={world} but --gpus {args.gpus}",
+              file=sys.stderr)
     return world, rank, local
 
 
@@ -217,32 +223,17 @@ def run_reference(args, world, rank):
 def run_gpu(args, world, rank, local):
     import torch
     from sparc2_b200 import Simulation
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from sparc2_b200.replicas import Replicas
     dev = local
     torch.cuda.set_device(dev)
-    p, bg, src, desc = workload(args.workload)
+    rep = Replicas("nccl")
+    p, bg, src, desc = workload(args.workload, grid=args.grid)
     sim = Simulation(p, bg, src, device=dev)
     del bg
     pts = p.nx * p.ny * p.nz
     stream = torch.cuda.ExternalStream(sim.stream, device=dev)
-
-    def barrier():
-        if dist is not None:
-            t = torch.zeros(1, device=f"cuda:{dev}")
-            dist.all_reduce(t)
-            torch.cuda.synchronize(dev)
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = rep.barrier
+    max_over_ranks = rep.max
 
     # warm-up iterations (graph capture happens here)
     W_ = args.warmup
@@ -250,7 +241,7 @@ def run_gpu(args, world, rank, local):
     sim.run(0, W_)
     sim.synchronize()
     torch.cuda.synchronize(dev)
-    clocks = Clocks(dev) if rank == 0 or True else None
+    clocks = Clocks(dev)
     n0 = sim.launch_count
     barrier()
     torch.cuda.synchronize(dev)
@@ -272,6 +263,8 @@ def run_gpu(args, world, rank, local):
         if rank == 0:
             print(json.dumps({"timed_only": True, "value": value,
                               "ms_per_step": ms_max / K}), flush=True)
+        sim.close()
+        rep.close()
         return
 
     # stage kernels alone (five fused RK-stage launches + the PSR forcing
@@ -335,6 +328,8 @@ def run_gpu(args, world, rank, local):
         cpu = cpu_baseline()
 
     if rank != 0:
+        sim.close()
+        rep.close()
         return
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -366,8 +361,7 @@ def run_gpu(args, world, rank, local):
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
     sim.close()
-    if dist is not None:
-        dist.destroy_process_group()
+    rep.close()
 
 
 def main():

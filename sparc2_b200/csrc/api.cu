@@ -138,7 +138,8 @@ static int enqueue_step(Handle *h, cudaStream_t s, int *nk) {
     r |= launch_psr_forcing(h, S, s);
     ++*nk;
   }
-  r |= launch_stage(h, S, 1, a, nullptr, f1, s);
+  // stage k reads temp_k and writes temp_{k+1}; stage 5 writes a_new
+  r |= launch_stage(h, S, 1, a, a, f1, s);
   r |= launch_stage(h, S, 2, a, f1, f2, s);
   r |= launch_stage(h, S, 3, a, f2, f1, s);
   r |= launch_stage(h, S, 4, a, f1, f2, s);
@@ -175,10 +176,16 @@ static int enqueue_filter(Handle *h, int fk, cudaStream_t s, int *nk) {
   return r ? SPARC_ERR_CUDA : SPARC_OK;
 }
 
+// The driver iteration lives in device memory so that captured graphs
+// replay without parameter updates; it is set by a one-thread kernel whose
+// argument is captured at launch (a pinned staging word could be rewritten
+// by the host before an earlier asynchronous copy from it has run).
+__global__ void k_set_iter(long long *d, long long nn) { *d = nn; }
+
 static int set_iter(Handle *h, long long nn) {
-  *h->h_pinned_iter = nn;
-  CK(h, cudaMemcpyAsync(h->d_iter, h->h_pinned_iter, 8, cudaMemcpyHostToDevice,
-                        h->stream));
+  k_set_iter<<<1, 1, 0, h->stream>>>(h->d_iter, nn);
+  ++h->launches;
+  CK(h, cudaGetLastError());
   return SPARC_OK;
 }
 
@@ -329,7 +336,6 @@ int sparc_create(const sparc_params *p, int device, sparc_handle **out) {
     if (!h->d_iter || !h->d_fail || !h->d_partials || !h->d_diag || !h->d_counter)
       r = SPARC_ERR_NOMEM;
   }
-  if (!r && cudaMallocHost(&h->h_pinned_iter, 8) != cudaSuccess) r = SPARC_ERR_NOMEM;
   if (!r) {
     long long m1 = -1;
     double d4[4] = {0, 0, 0, -1};
@@ -356,7 +362,6 @@ int sparc_destroy(sparc_handle *h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   drop_graphs(h);
   for (void *p : h->allocs) cudaFree(p);
-  if (h->h_pinned_iter) cudaFreeHost(h->h_pinned_iter);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return SPARC_OK;

@@ -129,7 +129,6 @@ struct Handle {
   long long *d_iter = nullptr, *d_fail = nullptr;
   double *d_partials = nullptr, *d_diag = nullptr;
   unsigned int *d_counter = nullptr;
-  long long *h_pinned_iter = nullptr;
   int max_stage_blocks = 0;
 
   // stage launch geometry
@@ -163,7 +162,7 @@ int step_constants();
 int filter_constants(int gxy, int gz);
 SimDev make_simdev(Handle *h);
 int launch_stage(Handle *h, const SimDev &S, int stage, const double *a,
-                 const double *sprev, double *sout, cudaStream_t s);
+                 const double *tin, double *tout, cudaStream_t s);
 int launch_psr_forcing(Handle *h, const SimDev &S, cudaStream_t s);
 int launch_filter_pass(Handle *h, int dir, const double *in, double *out,
                        cudaStream_t s);

@@ -537,8 +537,18 @@ int setup_background(Handle *h, const double *rho0_in, const double *pre0_in,
     for (int f = 0; f < 6; ++f) {
       FaceDev &F = h->faces[f];
       if (!F.on) continue;
-      const int axis = f / 2;
+      // face order z_bot, z_top, x_bot, x_top, y_bot, y_top; axis 0 x, 1 y, 2 z
+      const int axis = f < 2 ? 2 : (f < 4 ? 0 : 1);
       const bool top = f & 1;
+      {  // the slab's normal extent must be the PML width (guards the kernel)
+        const int ext = axis == 0 ? F.n0 : (axis == 1 ? F.n1 : F.n2);
+        const int o1 = axis == 0 ? F.n1 : F.n0, o2 = axis == 2 ? F.n1 : F.n2;
+        const int w1 = axis == 0 ? ny : nx, w2 = axis == 2 ? ny : nz;
+        if (ext != F.np || o1 != w1 || o2 != w2) {
+          h->err = "CPML face layout mismatch";
+          return SPARC_ERR_INVALID;
+        }
+      }
       const double *q = axis == 0 ? (top ? P.pml_xt : P.pml_xb)
                                   : axis == 1 ? (top ? P.pml_yt : P.pml_yb)
                                               : (top ? P.pml_zt : P.pml_zb);

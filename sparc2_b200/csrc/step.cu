@@ -7,8 +7,11 @@
 // marches up a chunk of z layers.  z derivatives come from an 11-deep
 // register window per z-differentiated field (the thread's own column);
 // x and y derivatives from a shared-memory layer tile with a 5-point halo.
-// Stage values a + beta*scr are formed on load, so no temp_step array
-// exists (step.f90:27-37 never touches HBM).
+// Stage values are forwarded: stage k writes temp_{k+1} = a + beta_{k+1}*F_k
+// (step.f90:33) instead of F_k, so every halo and window load of the next
+// stage reads one array; stage 5 writes a + deltat*F_5 (step.f90:58).  The
+// HBM traffic is that of the reference's scheme (14 V words per point and
+// step) and the values are bitwise those of forming a + beta*F on load.
 
 #include <cmath>
 
@@ -27,15 +30,6 @@ int step_constants() {
   return SPARC_OK;
 }
 
-// Stage value a + beta*scr_prev (step.f90:33).
-template <int MODE>
-__device__ __forceinline__ double sval(const double *__restrict__ a,
-                                       const double *__restrict__ s,
-                                       long long idx, double beta) {
-  double v = __ldg(a + idx);
-  if (MODE != FIRST) v = v + beta * __ldg(s + idx);
-  return v;
-}
 
 // CPML correction of one derivative (RHS.f90:50-93, 424-546):
 // RHSpsi = a*d + b*psi ; d = d/kappa + psi.  LAST applies the final RK
@@ -228,8 +222,8 @@ __device__ __forceinline__ double wsel(const double (&w)[11], int off) {
 template <int TX, int TY, int MODE, bool BG1D>
 __global__ void __launch_bounds__(TX *TY)
     k_stage_quiet(const SimDev S, const double *__restrict__ a,
-                  const double *__restrict__ sp, double *__restrict__ so,
-                  double beta, int zchunk) {
+                  const double *__restrict__ tin, double *__restrict__ so,
+                  double beta, double bnext, int zchunk) {
   constexpr int HX = TX + 10, HY = TY + 10;
   __shared__ double t_vx[HY][HX], t_vy[HY][HX], t_p[HY][HX];
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -255,16 +249,16 @@ __global__ void __launch_bounds__(TX *TY)
     const int kk = b0 + m;
     const bool ok = act && kk >= 0;
     const long long id = (long long)kk * NXY + col;
-    wvz[m] = ok ? sval<MODE>(a + 3 * N, sp + 3 * N, id, beta) : 0.0;
-    wp[m] = ok ? sval<MODE>(a + 4 * N, sp + 4 * N, id, beta) : 0.0;
+    wvz[m] = ok ? __ldg(tin + 3 * N + id) : 0.0;
+    wp[m] = ok ? __ldg(tin + 4 * N + id) : 0.0;
   }
   double ke = 0.0, mr = 1e300, mp = 1e300;
 
   for (int k = k0; k < k1; ++k) {
     if (k > k0 && k <= nz - 6) {
       const long long id = (long long)(k + 5) * NXY + col;
-      shift(wvz, act ? sval<MODE>(a + 3 * N, sp + 3 * N, id, beta) : 0.0);
-      shift(wp, act ? sval<MODE>(a + 4 * N, sp + 4 * N, id, beta) : 0.0);
+      shift(wvz, act ? __ldg(tin + 3 * N + id) : 0.0);
+      shift(wp, act ? __ldg(tin + 4 * N + id) : 0.0);
     }
     const long long kb = (long long)k * NXY;
     __syncthreads();
@@ -282,9 +276,9 @@ __global__ void __launch_bounds__(TX *TY)
         ok = gx >= 0 && gx < nx && gy >= 0 && gy < ny;
       }
       const long long id = kb + (long long)gy * nx + gx;
-      if (iny) t_vx[ly][lx] = ok ? sval<MODE>(a + N, sp + N, id, beta) : 0.0;
-      if (inx) t_vy[ly][lx] = ok ? sval<MODE>(a + 2 * N, sp + 2 * N, id, beta) : 0.0;
-      t_p[ly][lx] = ok ? sval<MODE>(a + 4 * N, sp + 4 * N, id, beta) : 0.0;
+      if (iny) t_vx[ly][lx] = ok ? __ldg(tin + N + id) : 0.0;
+      if (inx) t_vy[ly][lx] = ok ? __ldg(tin + 2 * N + id) : 0.0;
+      t_p[ly][lx] = ok ? __ldg(tin + 4 * N + id) : 0.0;
     }
     __syncthreads();
     if (!act) continue;
@@ -292,9 +286,8 @@ __global__ void __launch_bounds__(TX *TY)
     double av[5], tv[5];
 #pragma unroll
     for (int l = 0; l < 5; ++l) {
-      av[l] = __ldg(a + l * N + id);
-      tv[l] = av[l];
-      if (MODE != FIRST) tv[l] = av[l] + beta * __ldg(sp + l * N + id);
+      tv[l] = __ldg(tin + l * N + id);
+      av[l] = MODE == FIRST ? tv[l] : __ldg(a + l * N + id);
     }
     const double rho = tv[0], vx = tv[1], vy = tv[2], vz = tv[3], p = tv[4];
     // derivatives (RHS.f90:42-48)
@@ -375,7 +368,7 @@ __global__ void __launch_bounds__(TX *TY)
       mp = fmin(mp, p + p0v);
     } else {
 #pragma unroll
-      for (int l = 0; l < 5; ++l) so[l * N + id] = zero ? 0.0 : R[l];
+      for (int l = 0; l < 5; ++l) so[l * N + id] = zero ? av[l] : av[l] + bnext * R[l];
     }
   }
   if (MODE == LAST) diag_reduce(S, ke, mr, mp);
@@ -388,8 +381,8 @@ __global__ void __launch_bounds__(TX *TY)
 template <int TX, int TY, int MODE>
 __global__ void __launch_bounds__(TX *TY, 1)
     k_stage_mhd(const SimDev S, const double *__restrict__ a,
-                const double *__restrict__ sp, double *__restrict__ so,
-                double beta, int zchunk) {
+                const double *__restrict__ tin, double *__restrict__ so,
+                double beta, double bnext, int zchunk) {
   constexpr int HX = TX + 10, HY = TY + 10, HS = HX * HY;
   extern __shared__ double tile[];
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -416,12 +409,12 @@ __global__ void __launch_bounds__(TX *TY, 1)
   auto head = [&](int kk, double &vz_, double &p_, double &f1_, double &f2_,
                   double &bx_, double &by_) {
     const long long id = (long long)kk * NXY + col;
-    const double vx_ = sval<MODE>(a + N, sp + N, id, beta);
-    const double vy_ = sval<MODE>(a + 2 * N, sp + 2 * N, id, beta);
-    vz_ = sval<MODE>(a + 3 * N, sp + 3 * N, id, beta);
-    p_ = sval<MODE>(a + 4 * N, sp + 4 * N, id, beta);
-    bx_ = sval<MODE>(a + 5 * N, sp + 5 * N, id, beta);
-    by_ = sval<MODE>(a + 6 * N, sp + 6 * N, id, beta);
+    const double vx_ = __ldg(tin + N + id);
+    const double vy_ = __ldg(tin + 2 * N + id);
+    vz_ = __ldg(tin + 3 * N + id);
+    p_ = __ldg(tin + 4 * N + id);
+    bx_ = __ldg(tin + 5 * N + id);
+    by_ = __ldg(tin + 6 * N + id);
     const double ox = __ldg(S.box + id), oy = __ldg(S.boy + id),
                  oz = __ldg(S.boz + id);
     f1_ = -vz_ * oy + vy_ * oz;
@@ -465,13 +458,13 @@ __global__ void __launch_bounds__(TX *TY, 1)
              ox = 0, oy = 0, oz = 0;
       if (ok) {
         const long long id = kb + (long long)gy * nx + gx;
-        vx_ = sval<MODE>(a + N, sp + N, id, beta);
-        vy_ = sval<MODE>(a + 2 * N, sp + 2 * N, id, beta);
-        vz_ = sval<MODE>(a + 3 * N, sp + 3 * N, id, beta);
-        p_ = sval<MODE>(a + 4 * N, sp + 4 * N, id, beta);
-        bx_ = sval<MODE>(a + 5 * N, sp + 5 * N, id, beta);
-        by_ = sval<MODE>(a + 6 * N, sp + 6 * N, id, beta);
-        bz_ = sval<MODE>(a + 7 * N, sp + 7 * N, id, beta);
+        vx_ = __ldg(tin + N + id);
+        vy_ = __ldg(tin + 2 * N + id);
+        vz_ = __ldg(tin + 3 * N + id);
+        p_ = __ldg(tin + 4 * N + id);
+        bx_ = __ldg(tin + 5 * N + id);
+        by_ = __ldg(tin + 6 * N + id);
+        bz_ = __ldg(tin + 7 * N + id);
         ox = __ldg(S.box + id); oy = __ldg(S.boy + id); oz = __ldg(S.boz + id);
       }
       T(0, ly, lx) = vx_;
@@ -490,9 +483,8 @@ __global__ void __launch_bounds__(TX *TY, 1)
     double av[8], tv[8];
 #pragma unroll
     for (int l = 0; l < 8; ++l) {
-      av[l] = __ldg(a + l * N + id);
-      tv[l] = av[l];
-      if (MODE != FIRST) tv[l] = av[l] + beta * __ldg(sp + l * N + id);
+      tv[l] = __ldg(tin + l * N + id);
+      av[l] = MODE == FIRST ? tv[l] : __ldg(a + l * N + id);
     }
     const int ry = cy0 + ty, rx = cx0 + tx;
     auto DX = [&](int slot) {
@@ -607,7 +599,7 @@ __global__ void __launch_bounds__(TX *TY, 1)
       mp = fmin(mp, p + p0v);
     } else {
 #pragma unroll
-      for (int l = 0; l < 8; ++l) so[l * N + id] = zero ? 0.0 : R[l];
+      for (int l = 0; l < 8; ++l) so[l * N + id] = zero ? av[l] : av[l] + bnext * R[l];
     }
   }
   if (MODE == LAST) diag_reduce(S, ke, mr, mp);
@@ -634,14 +626,15 @@ int stage_geometry(Handle *h) {
 
 template <int TX, int TY>
 static int launch_quiet(Handle *h, const SimDev &S, int stage,
-                        const double *a, const double *sp, double *so,
+                        const double *a, const double *tin, double *so,
                         cudaStream_t s) {
   dim3 blk(TX, TY);
   dim3 grd((h->nx + TX - 1) / TX, (h->ny + TY - 1) / TY,
            (h->nz + h->zchunk - 1) / h->zchunk);
   const double beta = h->betas[stage - 1];
+  const double bnext = stage < 5 ? h->betas[stage] : h->deltat;
   const int mode = stage == 1 ? FIRST : (stage == 5 ? LAST : MID);
-#define QL(M, B) k_stage_quiet<TX, TY, M, B><<<grd, blk, 0, s>>>(S, a, sp, so, beta, h->zchunk)
+#define QL(M, B) k_stage_quiet<TX, TY, M, B><<<grd, blk, 0, s>>>(S, a, tin, so, beta, bnext, h->zchunk)
   if (S.bg1d) {
     if (mode == FIRST) QL(FIRST, true);
     else if (mode == MID) QL(MID, true);
@@ -657,11 +650,12 @@ static int launch_quiet(Handle *h, const SimDev &S, int stage,
 
 template <int TX, int TY>
 static int launch_mhd(Handle *h, const SimDev &S, int stage, const double *a,
-                      const double *sp, double *so, cudaStream_t s) {
+                      const double *tin, double *so, cudaStream_t s) {
   dim3 blk(TX, TY);
   dim3 grd((h->nx + TX - 1) / TX, (h->ny + TY - 1) / TY,
            (h->nz + h->zchunk - 1) / h->zchunk);
   const double beta = h->betas[stage - 1];
+  const double bnext = stage < 5 ? h->betas[stage] : h->deltat;
   const size_t smem = sizeof(double) * 9 * (TX + 10) * (TY + 10);
   const int mode = stage == 1 ? FIRST : (stage == 5 ? LAST : MID);
   if (mode == FIRST)
@@ -670,20 +664,20 @@ static int launch_mhd(Handle *h, const SimDev &S, int stage, const double *a,
     cudaFuncSetAttribute(k_stage_mhd<TX, TY, MID>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   else
     cudaFuncSetAttribute(k_stage_mhd<TX, TY, LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (mode == FIRST) k_stage_mhd<TX, TY, FIRST><<<grd, blk, smem, s>>>(S, a, sp, so, beta, h->zchunk);
-  else if (mode == MID) k_stage_mhd<TX, TY, MID><<<grd, blk, smem, s>>>(S, a, sp, so, beta, h->zchunk);
-  else k_stage_mhd<TX, TY, LAST><<<grd, blk, smem, s>>>(S, a, sp, so, beta, h->zchunk);
+  if (mode == FIRST) k_stage_mhd<TX, TY, FIRST><<<grd, blk, smem, s>>>(S, a, tin, so, beta, bnext, h->zchunk);
+  else if (mode == MID) k_stage_mhd<TX, TY, MID><<<grd, blk, smem, s>>>(S, a, tin, so, beta, bnext, h->zchunk);
+  else k_stage_mhd<TX, TY, LAST><<<grd, blk, smem, s>>>(S, a, tin, so, beta, bnext, h->zchunk);
   return SPARC_OK;
 }
 
 int launch_stage(Handle *h, const SimDev &S, int stage, const double *a,
-                 const double *sp, double *so, cudaStream_t s) {
+                 const double *tin, double *so, cudaStream_t s) {
   int r = SPARC_ERR_INVALID;
   const int key = h->tx * 100 + h->ty;
 #define DISPATCH(FN)                                            \
   switch (key) {                                                \
-    case 3208: r = FN<32, 8>(h, S, stage, a, sp, so, s); break; \
-    case 1608: r = FN<16, 8>(h, S, stage, a, sp, so, s); break; \
+    case 3208: r = FN<32, 8>(h, S, stage, a, tin, so, s); break; \
+    case 1608: r = FN<16, 8>(h, S, stage, a, tin, so, s); break; \
     default: r = SPARC_ERR_INVALID;                             \
   }
   if (h->magnetic) { DISPATCH(launch_mhd) } else { DISPATCH(launch_quiet) }

@@ -1,0 +1,99 @@
+"""The C ABI on a machine without a GPU: the library builds and loads,
+exports every entry point include/sparc_gpu.h declares, its structs match
+the ctypes mirror, and it refuses to run without an sm_100 device."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+from sparc2_b200 import abi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "sparc_gpu.h")
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from sparc2_b200 import build
+    build.build()
+    return abi.load()
+
+
+def declared():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(sparc_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_every_declared_entry_point_is_exported(lib):
+    names = declared()
+    assert len(names) >= 19
+    for n in names:
+        assert hasattr(lib, n), n
+    assert sorted(abi.EXPORTS) == names
+
+
+def _c_layout(tmp_path):
+    fields = {
+        "sparc_params": [f for f, _ in abi.SparcParams._fields_],
+        "sparc_pulse": [f for f, _ in abi.SparcPulse._fields_],
+        "sparc_source": [f for f, _ in abi.SparcSource._fields_],
+        "sparc_diag": [f for f, _ in abi.SparcDiag._fields_],
+    }
+    lines = ['#include <stdio.h>', '#include <stddef.h>',
+             f'#include "{HEADER}"', 'int main(void) {']
+    for s, fs in fields.items():
+        lines.append(f'printf("{s} size %zu\\n", sizeof({s}));')
+        for f in fs:
+            lines.append(f'printf("{s} {f} %zu\\n", offsetof({s}, {f}));')
+    lines += ['return 0;', '}']
+    src = tmp_path / "layout.c"
+    exe = tmp_path / "layout"
+    src.write_text("\n".join(lines))
+    subprocess.check_call(["gcc", "-std=c99", "-o", str(exe), str(src)])
+    out = subprocess.check_output([str(exe)]).decode().split("\n")
+    res = {}
+    for line in out:
+        if line:
+            parts = line.split()
+            res[tuple(parts[:-1])] = int(parts[-1])
+    return res
+
+
+def test_struct_layout_matches_header(tmp_path):
+    lay = _c_layout(tmp_path)
+    for cname, cls in (("sparc_params", abi.SparcParams),
+                       ("sparc_pulse", abi.SparcPulse),
+                       ("sparc_source", abi.SparcSource),
+                       ("sparc_diag", abi.SparcDiag)):
+        assert lay[(cname, "size")] == C.sizeof(cls), cname
+        for f, _ in cls._fields_:
+            assert lay[(cname, f)] == getattr(cls, f).offset, (cname, f)
+
+
+def test_create_without_device_fails_loudly(lib):
+    from sparc2_b200 import workloads as W
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    p, _, _ = W.cfg0(nx=32, ny=32, nz=48, blocks=(2, 2, 2))
+    h = C.c_void_p()
+    r = lib.sparc_create(C.byref(p), 0, C.byref(h))
+    assert r == abi.SPARC_ERR_NODEVICE
+    assert lib.sparc_last_error(None)
+    from sparc2_b200 import Simulation
+    with pytest.raises(abi.SparcError):
+        Simulation(p, W.quiet_background(32, 32, 48))
+
+
+def test_invalid_parameters_are_rejected_before_any_device_call(lib):
+    from sparc2_b200 import workloads as W
+    p, _, _ = W.cfg0(nx=32, ny=32, nz=48, blocks=(2, 2, 2))
+    p.filter_mode_z = 3
+    h = C.c_void_p()
+    assert lib.sparc_create(C.byref(p), 0, C.byref(h)) == abi.SPARC_ERR_INVALID
+    p.filter_mode_z = 1
+    p.block_z = 1
+    assert lib.sparc_create(C.byref(p), 0, C.byref(h)) == abi.SPARC_ERR_INVALID
+    assert b"block" in lib.sparc_last_error(None)

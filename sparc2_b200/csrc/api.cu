@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -295,6 +296,8 @@ int sparc_create(const sparc_params *p, int device, sparc_handle **out) {
     while (b + 1 < p->block_z && k >= h->bzs[b + 1]) ++b;
     cols[h->nx + h->ny + k] = b;
   }
+  if (const char *kv = std::getenv("SPARC_MHD_KERNEL"))  // A/B timing only
+    h->mhd_kernel = std::atoi(kv) == 1 ? 1 : 2;
   int r = SPARC_OK;
   if (!cuda_ok(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream")) {
     r = SPARC_ERR_CUDA;

@@ -131,8 +131,10 @@ struct Handle {
   unsigned int *d_counter = nullptr;
   int max_stage_blocks = 0;
 
-  // stage launch geometry
+  // stage launch geometry; mhd_kernel 1: register/shared-tile kernel,
+  // 2: cp.async-pipelined kernel (32x8 tiles only)
   int tx = 32, ty = 8, zchunk = 32;
+  int mhd_kernel = 2;
 
   // captured graphs keyed by (ra, rf1, rf2, filter kind)
   struct GraphEntry {

@@ -605,14 +605,323 @@ __global__ void __launch_bounds__(TX *TY, 1)
   if (MODE == LAST) diag_reduce(S, ke, mr, mp);
 }
 
+// ------------------------------------ MP_MHD_3D, pipelined stage kernel
+// Same arithmetic as k_stage_mhd, restructured for HBM bandwidth: every
+// array a layer needs is copied into shared memory with cp.async one layer
+// ahead (double buffer), so the loads of layer k+1 stream while layer k is
+// computed.  Per buffer: 10 halo slots over the cross-shaped tile (stage
+// fields vx vy vz p bx by bz and B0; the B0 slots become flux1..3 in place
+// once the layer has landed) and 24 own-point slots (stage rho, a[0..7],
+// 14 background arrays, p0).  1 CTA of 32x8 threads per SM, 219 KB smem.
+namespace pipe {
+constexpr int TX = 32, TY = 8, NT = TX * TY;
+constexpr int HX = TX + 10, HY = TY + 10, HS = HX * HY;
+constexpr int NH = 10, NO = 24;
+constexpr int BUF = NH * HS + NO * TY * TX;  // doubles per buffer
+constexpr size_t SMEM = 2 * BUF * sizeof(double);
+// own slots
+constexpr int O_RHO = 0, O_A = 1, O_BG = 9, O_P0 = 23;
+// background order in the own slots (O_BG + n)
+enum { B_RED, B_SPONGE, B_RHO0, B_GRX, B_GRY, B_GRZ, B_C2R, B_GPX, B_GPY,
+       B_GPZ, B_RHOINV, B_CBX, B_CBY, B_CBZ, NBG };
+}  // namespace pipe
+
+__device__ __forceinline__ void cp_async8(double *dst, const double *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async16(double *dst, const double *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_wait1() {
+  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(pipe::NT, 1)
+    k_stage_mhd_pipe(const SimDev S, const double *__restrict__ a,
+                     const double *__restrict__ tin, double *__restrict__ so,
+                     double beta, double bnext, int zchunk) {
+  using namespace pipe;
+  extern __shared__ double smem[];
+  __shared__ const double *optr[NO];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int nx = S.nx, ny = S.ny, nz = S.nz;
+  const long long N = S.N, NXY = (long long)nx * ny;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int i = x0 + tx, j = y0 + ty;
+  const bool act = i < nx && j < ny;
+  const bool per = S.periodic;
+  const int k0 = blockIdx.z * zchunk, k1 = min(nz, k0 + zchunk);
+  const long long col = (long long)j * nx + i;
+  const long long it = *S.iter;
+  const double Tp = pulse_time(S, it);
+  const double dt = S.deltat;
+  const int gc = act ? S.colx[i] + S.bxdim * S.coly[j] : 0;
+  const int xo = tile_origin(x0, TX, nx, per), yo = tile_origin(y0, TY, ny, per);
+  const int cx0 = x0 - xo, cy0 = y0 - yo;
+  const int ry = cy0 + ty, rx = cx0 + tx;
+  const bool vec2 = (nx & 1) == 0;
+  if (tid == 0) {
+    optr[O_RHO] = tin;
+    for (int l = 0; l < 8; ++l) optr[O_A + l] = a + l * N;
+    optr[O_BG + B_RED] = S.red;    optr[O_BG + B_SPONGE] = S.sponge;
+    optr[O_BG + B_RHO0] = S.rho0;  optr[O_BG + B_GRX] = S.grx;
+    optr[O_BG + B_GRY] = S.gry;    optr[O_BG + B_GRZ] = S.grz;
+    optr[O_BG + B_C2R] = S.c2rho0; optr[O_BG + B_GPX] = S.gpx;
+    optr[O_BG + B_GPY] = S.gpy;    optr[O_BG + B_GPZ] = S.gpz;
+    optr[O_BG + B_RHOINV] = S.rhoinv;
+    optr[O_BG + B_CBX] = S.cbx;    optr[O_BG + B_CBY] = S.cby;
+    optr[O_BG + B_CBZ] = S.cbz;
+    optr[O_P0] = S.p0;
+  }
+  __syncthreads();
+  auto H = [&](int b, int slot, int ly, int lx) -> double & {
+    return smem[(size_t)b * BUF + ((size_t)slot * HY + ly) * HX + lx];
+  };
+  auto O = [&](int b, int slot, int r, int c) -> double & {
+    return smem[(size_t)b * BUF + NH * HS + ((size_t)slot * TY + r) * TX + c];
+  };
+  auto own_active = [&](int slot) -> bool {
+    if (slot >= O_A && slot < O_BG) return MODE != FIRST;
+    if (slot == O_P0) return MODE == LAST;
+    return true;
+  };
+  // issue the copies of layer k into buffer b (one commit group)
+  auto issue = [&](int k, int b) {
+    const long long kb = (long long)k * NXY;
+    for (int t = tid; t < HS; t += NT) {
+      const int ly = t / HX, lx = t - ly * HX;
+      const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
+      if (!inx && !iny) continue;
+      int gx = xo + lx, gy = yo + ly;
+      if (per) {
+        gx = wrapi(gx, nx);
+        gy = wrapi(gy, ny);
+      } else if (gx < 0 || gx >= nx || gy < 0 || gy >= ny) {
+        continue;  // never read: one-sided stencils stay inside the domain
+      }
+      const long long id = kb + (long long)gy * nx + gx;
+#pragma unroll
+      for (int sl = 0; sl < 7; ++sl) cp_async8(&H(b, sl, ly, lx), tin + (sl + 1) * N + id);
+      cp_async8(&H(b, 7, ly, lx), S.box + id);
+      cp_async8(&H(b, 8, ly, lx), S.boy + id);
+      cp_async8(&H(b, 9, ly, lx), S.boz + id);
+    }
+    if (vec2) {
+      constexpr int PAIRS = TY * TX / 2;
+      for (int t = tid; t < NO * PAIRS; t += NT) {
+        const int slot = t / PAIRS, rem = t - slot * PAIRS;
+        if (!own_active(slot)) continue;
+        const int r = rem / (TX / 2), c = 2 * (rem - r * (TX / 2));
+        const int gx = x0 + c, gy = y0 + r;
+        if (gx >= nx || gy >= ny) continue;
+        cp_async16(&O(b, slot, r, c), optr[slot] + kb + (long long)gy * nx + gx);
+      }
+    } else {
+      for (int t = tid; t < NO * TY * TX; t += NT) {
+        const int slot = t / (TY * TX), rem = t - slot * (TY * TX);
+        if (!own_active(slot)) continue;
+        const int r = rem / TX, c = rem - r * TX;
+        const int gx = x0 + c, gy = y0 + r;
+        if (gx >= nx || gy >= ny) continue;
+        cp_async8(&O(b, slot, r, c), optr[slot] + kb + (long long)gy * nx + gx);
+      }
+    }
+    cp_commit();
+  };
+
+  // z windows: vz, p, flux1, flux2, bx, by (own column)
+  double w_vz[11], w_p[11], w_f1[11], w_f2[11], w_bx[11], w_by[11];
+  auto head = [&](int kk, double &vz_, double &p_, double &f1_, double &f2_,
+                  double &bx_, double &by_) {
+    const long long id = (long long)kk * NXY + col;
+    const double vx_ = __ldg(tin + N + id), vy_ = __ldg(tin + 2 * N + id);
+    vz_ = __ldg(tin + 3 * N + id);
+    p_ = __ldg(tin + 4 * N + id);
+    bx_ = __ldg(tin + 5 * N + id);
+    by_ = __ldg(tin + 6 * N + id);
+    const double ox = __ldg(S.box + id), oy = __ldg(S.boy + id),
+                 oz = __ldg(S.boz + id);
+    f1_ = -vz_ * oy + vy_ * oz;
+    f2_ = -vx_ * oz + vz_ * ox;
+  };
+  issue(k0, 0);
+  const int b0 = min(k0 - 5, nz - 11);
+#pragma unroll
+  for (int m = 0; m < 11; ++m) {
+    const int kk = b0 + m;
+    if (act && kk >= 0) {
+      head(kk, w_vz[m], w_p[m], w_f1[m], w_f2[m], w_bx[m], w_by[m]);
+    } else {
+      w_vz[m] = w_p[m] = w_f1[m] = w_f2[m] = w_bx[m] = w_by[m] = 0.0;
+    }
+  }
+  double h0 = 0, h1 = 0, h2 = 0, h3 = 0, h4 = 0, h5 = 0;  // next window head
+  double ke = 0.0, mr = 1e300, mp = 1e300;
+
+  for (int k = k0; k < k1; ++k) {
+    const int b = (k - k0) & 1;
+    if (k > k0 && k <= nz - 6) {
+      shift(w_vz, h0); shift(w_p, h1); shift(w_f1, h2);
+      shift(w_f2, h3); shift(w_bx, h4); shift(w_by, h5);
+    }
+    if (k + 1 < k1) issue(k + 1, b ^ 1);
+    else cp_commit();  // keep one group per iteration
+    cp_wait1();
+    __syncthreads();
+    // own B0, then flux1..3 over the cross tile in place of B0
+    const double ox = H(b, 7, ry, rx), oy = H(b, 8, ry, rx), oz = H(b, 9, ry, rx);
+    __syncthreads();
+    for (int t = tid; t < HS; t += NT) {
+      const int ly = t / HX, lx = t - ly * HX;
+      const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
+      if (!inx && !iny) continue;
+      const double vx_ = H(b, 0, ly, lx), vy_ = H(b, 1, ly, lx), vz_ = H(b, 2, ly, lx);
+      const double bx0 = H(b, 7, ly, lx), by0 = H(b, 8, ly, lx), bz0 = H(b, 9, ly, lx);
+      H(b, 7, ly, lx) = -vz_ * by0 + vy_ * bz0;   // flux1
+      H(b, 8, ly, lx) = -vx_ * bz0 + vz_ * bx0;   // flux2
+      H(b, 9, ly, lx) = -vy_ * bx0 + vx_ * by0;   // flux3
+    }
+    __syncthreads();
+    if (act) {
+      const long long kb = (long long)k * NXY;
+      const long long id = kb + col;
+      double tv[8], av[8];
+      tv[0] = O(b, O_RHO, ty, tx);
+#pragma unroll
+      for (int l = 1; l < 8; ++l) tv[l] = H(b, l - 1, ry, rx);
+#pragma unroll
+      for (int l = 0; l < 8; ++l) av[l] = MODE == FIRST ? tv[l] : O(b, O_A + l, ty, tx);
+      auto DX = [&](int slot) {
+        return dxy(i, nx, per, S.stretchx, [&](int g) { return H(b, slot, ry, g - xo); });
+      };
+      auto DY = [&](int slot) {
+        return dxy(j, ny, per, S.stretchy, [&](int g) { return H(b, slot, g - yo, rx); });
+      };
+      // halo slots: 0 vx, 1 vy, 2 vz, 3 p, 4 bx, 5 by, 6 bz, 7-9 flux1..3
+      double dvxdx = DX(0), dxflux3 = DX(9), gpx = DX(3), dxflux2 = DX(8),
+             dxby = DX(5), dxbz = DX(6);
+      double dvydy = DY(1), gpy = DY(3), dyflux3 = DY(9), dybz = DY(6),
+             dybx = DY(4), dyflux1 = DY(7);
+      const double szk = __ldg(S.stretch + k);
+      double dvzdz = dz(w_vz, k, nz, szk), dzflux1 = dz(w_f1, k, nz, szk),
+             dzflux2 = dz(w_f2, k, nz, szk), dzbx = dz(w_bx, k, nz, szk),
+             gpz = dz(w_p, k, nz, szk), dzby = dz(w_by, k, nz, szk);
+      if (S.zb.on && (k < S.zb.np || k >= nz - S.zt.np)) {
+        const bool bot = k < S.zb.np;
+        const FaceDev &F = bot ? S.zb : S.zt;
+        const int kl = bot ? k : k - (nz - S.zt.np);
+        const long long f = (long long)kl * NXY + col;
+        cpml<MODE>(F, f, kl, 1, beta, dt, gpz);
+        cpml<MODE>(F, f, kl, 0, beta, dt, dvzdz);
+        cpml<MODE>(F, f, kl, 4, beta, dt, dzflux2);
+        cpml<MODE>(F, f, kl, 5, beta, dt, dzflux1);
+        cpml<MODE>(F, f, kl, 2, beta, dt, dzbx);
+        cpml<MODE>(F, f, kl, 3, beta, dt, dzby);
+      }
+      if (S.xb.on) {
+        if (i < S.xb.np || i >= nx - S.xt.np) {
+          const bool bot = i < S.xb.np;
+          const FaceDev &F = bot ? S.xb : S.xt;
+          const int il = bot ? i : i - (nx - S.xt.np);
+          const long long f = il + (long long)F.np * (j + (long long)ny * k);
+          cpml<MODE>(F, f, il, 1, beta, dt, gpx);
+          cpml<MODE>(F, f, il, 0, beta, dt, dvxdx);
+          cpml<MODE>(F, f, il, 4, beta, dt, dxflux3);
+          cpml<MODE>(F, f, il, 5, beta, dt, dxflux2);
+          cpml<MODE>(F, f, il, 2, beta, dt, dxby);
+          cpml<MODE>(F, f, il, 3, beta, dt, dxbz);
+        }
+        if (j < S.yb.np || j >= ny - S.yt.np) {
+          const bool bot = j < S.yb.np;
+          const FaceDev &F = bot ? S.yb : S.yt;
+          const int jl = bot ? j : j - (ny - S.yt.np);
+          const long long f = i + (long long)nx * (jl + (long long)F.np * k);
+          cpml<MODE>(F, f, jl, 1, beta, dt, gpy);
+          cpml<MODE>(F, f, jl, 0, beta, dt, dvydy);
+          cpml<MODE>(F, f, jl, 4, beta, dt, dyflux3);
+          cpml<MODE>(F, f, jl, 5, beta, dt, dyflux1);
+          cpml<MODE>(F, f, jl, 2, beta, dt, dybx);
+          cpml<MODE>(F, f, jl, 3, beta, dt, dybz);
+        }
+      }
+      const double rho = tv[0], vx = tv[1], vy = tv[2], vz = tv[3], p = tv[4],
+                   bx = tv[5], by = tv[6], bz = tv[7];
+      auto BG = [&](int n) { return O(b, O_BG + n, ty, tx); };
+      const double red = BG(B_RED);
+      double R[8];
+      R[5] = red * (dyflux3 - dzflux2);
+      R[6] = red * (dzflux1 - dxflux3);
+      R[7] = red * (dxflux2 - dyflux1);
+      const double div = dvxdx + dvydy + dvzdz;
+      const double cbx = dybz - dzby, cby = -dxbz + dzbx, cbz = dxby - dybx;
+      const double sg = BG(B_SPONGE), r0 = BG(B_RHO0);
+      R[0] = -BG(B_GRX) * vx - BG(B_GRY) * vy - BG(B_GRZ) * vz - r0 * div - sg * rho;
+      R[4] = -BG(B_C2R) * div - vx * BG(B_GPX) - vy * BG(B_GPY) - vz * BG(B_GPZ) - sg * p;
+      const double c1 = cby * oz - cbz * oy, c2 = ox * cbz - cbx * oz,
+                   c3 = cbx * oy - cby * ox;
+      const double ri = BG(B_RHOINV);
+      double vxr = -ri * (gpx - (c1 * red)) - sg * vx;
+      double vyr = -ri * (gpy - (c2 * red)) - sg * vy;
+      double vzr = -ri * (gpz - (c3 * red)) - sg * vz;
+      const double qx = BG(B_CBX), qy = BG(B_CBY), qz = BG(B_CBZ);
+      const double d1 = qy * bz - qz * by, d2 = bx * qz - qx * bz,
+                   d3 = qx * by - qy * bx;
+      vxr = vxr + ri * d1 * red;
+      vyr = vyr + ri * d2 * red;
+      vzr = vzr + ri * d3 * red;
+      vzr = vzr - ri * rho * __ldg(S.gblk + (long long)gc * nz + k);
+      R[1] = vxr;
+      R[2] = vyr;
+      R[3] = vzr;
+      if (S.frc.kind != SPARC_SRC_NONE) {
+        const double frc = forcing_at(S, it, Tp, i, j, k);
+        if (S.frc.dir == 1) R[1] = R[1] + frc;
+        else if (S.frc.dir == 2) R[2] = R[2] + frc;
+        else R[3] = R[3] + frc;
+      }
+      const bool zero = k == 0 || k == nz - 1 ||
+                        (!per && (i == 0 || i == nx - 1 || j == 0 || j == ny - 1));
+      if (MODE == LAST) {
+        double an[8];
+#pragma unroll
+        for (int l = 0; l < 8; ++l) {
+          an[l] = zero ? av[l] : av[l] + dt * R[l];
+          so[l * N + id] = an[l];
+        }
+        const double p0v = O(b, O_P0, ty, tx);
+        double m = (r0 + an[0]) * (an[1] * an[1] + an[2] * an[2] + an[3] * an[3]) / 2.0;
+        ke += m * m;
+        mr = fmin(mr, rho + r0);
+        mp = fmin(mp, p + p0v);
+      } else {
+#pragma unroll
+        for (int l = 0; l < 8; ++l) so[l * N + id] = zero ? av[l] : av[l] + bnext * R[l];
+      }
+    }
+    // next window head (layer k+6), consumed at the start of iteration k+1
+    if (act && k + 1 < k1 && k + 1 <= nz - 6) head(k + 6, h0, h1, h2, h3, h4, h5);
+    __syncthreads();  // buffer b is refilled by the issue of iteration k+1
+  }
+  if (MODE == LAST) diag_reduce(S, ke, mr, mp);
+}
+
 // ------------------------------------------------------- stage dispatch
 int stage_geometry(Handle *h) {
-  // tile shape: (32, 8) unless the grid is too small to fill the GPU
+  // tile shape: (32, 8); the quiet kernel drops to (16, 8) on grids too
+  // small to fill the GPU.  The MHD kernels always use (32, 8).
   h->tx = 32;
   h->ty = 8;
   long long tiles = (long long)((h->nx + h->tx - 1) / h->tx) *
                     ((h->ny + h->ty - 1) / h->ty);
-  if (tiles < 64) {
+  if (tiles < 64 && !h->magnetic) {
     h->tx = 16;
     tiles = (long long)((h->nx + 15) / 16) * ((h->ny + 7) / 8);
   }
@@ -670,9 +979,38 @@ static int launch_mhd(Handle *h, const SimDev &S, int stage, const double *a,
   return SPARC_OK;
 }
 
+static int launch_mhd_pipe(Handle *h, const SimDev &S, int stage,
+                           const double *a, const double *tin, double *so,
+                           cudaStream_t s) {
+  using namespace pipe;
+  dim3 blk(TX, TY);
+  dim3 grd((h->nx + TX - 1) / TX, (h->ny + TY - 1) / TY,
+           (h->nz + h->zchunk - 1) / h->zchunk);
+  const double beta = h->betas[stage - 1];
+  const double bnext = stage < 5 ? h->betas[stage] : h->deltat;
+  const int mode = stage == 1 ? FIRST : (stage == 5 ? LAST : MID);
+  if (mode == FIRST) {
+    cudaFuncSetAttribute(k_stage_mhd_pipe<FIRST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    k_stage_mhd_pipe<FIRST><<<grd, blk, SMEM, s>>>(S, a, tin, so, beta, bnext, h->zchunk);
+  } else if (mode == MID) {
+    cudaFuncSetAttribute(k_stage_mhd_pipe<MID>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    k_stage_mhd_pipe<MID><<<grd, blk, SMEM, s>>>(S, a, tin, so, beta, bnext, h->zchunk);
+  } else {
+    cudaFuncSetAttribute(k_stage_mhd_pipe<LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    k_stage_mhd_pipe<LAST><<<grd, blk, SMEM, s>>>(S, a, tin, so, beta, bnext, h->zchunk);
+  }
+  return SPARC_OK;
+}
+
 int launch_stage(Handle *h, const SimDev &S, int stage, const double *a,
                  const double *tin, double *so, cudaStream_t s) {
   int r = SPARC_ERR_INVALID;
+  if (h->magnetic && h->mhd_kernel == 2 && h->tx == 32 && h->ty == 8) {
+    r = launch_mhd_pipe(h, S, stage, a, tin, so, s);
+    ++h->launches;
+    if (r == SPARC_OK && cudaGetLastError() != cudaSuccess) r = SPARC_ERR_CUDA;
+    return r;
+  }
   const int key = h->tx * 100 + h->ty;
 #define DISPATCH(FN)                                            \
   switch (key) {                                                \

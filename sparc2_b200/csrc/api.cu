@@ -297,7 +297,7 @@ int sparc_create(const sparc_params *p, int device, sparc_handle **out) {
     cols[h->nx + h->ny + k] = b;
   }
   if (const char *kv = std::getenv("SPARC_MHD_KERNEL"))  // A/B timing only
-    h->mhd_kernel = std::atoi(kv) == 1 ? 1 : 2;
+    h->mhd_kernel = std::max(1, std::min(3, std::atoi(kv)));
   int r = SPARC_OK;
   if (!cuda_ok(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream")) {
     r = SPARC_ERR_CUDA;

@@ -132,9 +132,9 @@ struct Handle {
   int max_stage_blocks = 0;
 
   // stage launch geometry; mhd_kernel 1: register/shared-tile kernel,
-  // 2: cp.async-pipelined kernel (32x8 tiles only)
+  // 2: cp.async-pipelined kernel, 3: two-role pipelined kernel (32x8 tiles)
   int tx = 32, ty = 8, zchunk = 32;
-  int mhd_kernel = 2;
+  int mhd_kernel = 3;
 
   // captured graphs keyed by (ra, rf1, rf2, filter kind)
   struct GraphEntry {

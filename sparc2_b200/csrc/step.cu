@@ -77,8 +77,8 @@ __device__ __forceinline__ double pulse_time(const SimDev &S, long long it) {
 __device__ void diag_reduce(const SimDev &S, double ke, double mr, double mp) {
   __shared__ double r[3][32];
   __shared__ int am_last;
-  const int nt = blockDim.x * blockDim.y;
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int nt = blockDim.x * blockDim.y * blockDim.z;
+  const int tid = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5, nw = (nt + 31) >> 5;
   const long long nb = (long long)gridDim.x * gridDim.y * gridDim.z;
   const long long bid = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
@@ -913,6 +913,334 @@ __global__ void __launch_bounds__(pipe::NT, 1)
   if (MODE == LAST) diag_reduce(S, ke, mr, mp);
 }
 
+// ------------------------- MP_MHD_3D, two-role pipelined stage kernel
+// The pipelined layer tiles of k_stage_mhd_pipe, with each column served by
+// two warps-groups (threadIdx.z = role) so that a thread holds only three
+// z windows (66 FP64 registers) and the CTA keeps 16 warps resident:
+//   role 0: momentum (RHS.f90:570-580, 630-645); windows vz, p, bx;
+//           derivatives gpx gpy gpz dvzdz dybz dxbz dzbx dxby dybx
+//   role 1: continuity, pressure, induction (RHS.f90:548-568); windows
+//           flux1, flux2, by; derivatives dvxdx dvydy dxflux3 dxflux2
+//           dyflux3 dyflux1 dzflux1 dzflux2 dzby
+// dvzdz and dzby cross over through shared memory after their CPML
+// corrections.  Arithmetic and summation order equal k_stage_mhd's.
+namespace duo {
+constexpr int TX = 32, TY = 8, NC = TX * TY, NT = 2 * NC;
+constexpr int HX = TX + 10, HY = TY + 10, HS = HX * HY;
+constexpr int NH = 10, NO = 24;
+constexpr int BUF = NH * HS + NO * NC;
+constexpr int XCH = 3 * NC;                       // exchange slots
+constexpr size_t SMEM = (2 * BUF + XCH) * sizeof(double);
+}  // namespace duo
+
+template <int MODE>
+__global__ void __launch_bounds__(duo::NT, 1)
+    k_stage_mhd_duo(const SimDev S, const double *__restrict__ a,
+                    const double *__restrict__ tin, double *__restrict__ so,
+                    double beta, double bnext, int zchunk) {
+  using namespace duo;
+  using pipe::O_RHO;
+  using pipe::O_A;
+  using pipe::O_BG;
+  using pipe::O_P0;
+  extern __shared__ double smem[];
+  __shared__ const double *optr[NO];
+  const int tx = threadIdx.x, ty = threadIdx.y, role = threadIdx.z;
+  const int tid = (role * TY + ty) * TX + tx, cid = ty * TX + tx;
+  const int nx = S.nx, ny = S.ny, nz = S.nz;
+  const long long N = S.N, NXY = (long long)nx * ny;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int i = x0 + tx, j = y0 + ty;
+  const bool act = i < nx && j < ny;
+  const bool per = S.periodic;
+  const int k0 = blockIdx.z * zchunk, k1 = min(nz, k0 + zchunk);
+  const long long col = (long long)j * nx + i;
+  const long long it = *S.iter;
+  const double dt = S.deltat;
+  const int xo = tile_origin(x0, TX, nx, per), yo = tile_origin(y0, TY, ny, per);
+  const int cx0 = x0 - xo, cy0 = y0 - yo;
+  const int ry = cy0 + ty, rx = cx0 + tx;
+  const bool vec2 = (nx & 1) == 0;
+  if (tid == 0) {
+    optr[O_RHO] = tin;
+    for (int l = 0; l < 8; ++l) optr[O_A + l] = a + l * N;
+    optr[O_BG + pipe::B_RED] = S.red;    optr[O_BG + pipe::B_SPONGE] = S.sponge;
+    optr[O_BG + pipe::B_RHO0] = S.rho0;  optr[O_BG + pipe::B_GRX] = S.grx;
+    optr[O_BG + pipe::B_GRY] = S.gry;    optr[O_BG + pipe::B_GRZ] = S.grz;
+    optr[O_BG + pipe::B_C2R] = S.c2rho0; optr[O_BG + pipe::B_GPX] = S.gpx;
+    optr[O_BG + pipe::B_GPY] = S.gpy;    optr[O_BG + pipe::B_GPZ] = S.gpz;
+    optr[O_BG + pipe::B_RHOINV] = S.rhoinv;
+    optr[O_BG + pipe::B_CBX] = S.cbx;    optr[O_BG + pipe::B_CBY] = S.cby;
+    optr[O_BG + pipe::B_CBZ] = S.cbz;
+    optr[O_P0] = S.p0;
+  }
+  __syncthreads();
+  auto H = [&](int b, int slot, int ly, int lx) -> double & {
+    return smem[b * BUF + (slot * HY + ly) * HX + lx];
+  };
+  auto O = [&](int b, int slot) -> double & {
+    return smem[b * BUF + NH * HS + slot * NC + cid];
+  };
+  double *X = smem + 2 * BUF;  // [0] dvzdz, [1] dzby, [2] |v_new|^2
+  auto own_active = [&](int slot) -> bool {
+    if (slot >= O_A && slot < O_BG) return MODE != FIRST;
+    if (slot == O_P0) return MODE == LAST;
+    return true;
+  };
+  auto issue = [&](int k, int b) {
+    const long long kb = (long long)k * NXY;
+    for (int t = tid; t < HS; t += NT) {
+      const int ly = t / HX, lx = t - ly * HX;
+      const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
+      if (!inx && !iny) continue;
+      int gx = xo + lx, gy = yo + ly;
+      if (per) {
+        gx = wrapi(gx, nx);
+        gy = wrapi(gy, ny);
+      } else if (gx < 0 || gx >= nx || gy < 0 || gy >= ny) {
+        continue;
+      }
+      const long long id = kb + (long long)gy * nx + gx;
+#pragma unroll
+      for (int sl = 0; sl < 7; ++sl) cp_async8(&H(b, sl, ly, lx), tin + (sl + 1) * N + id);
+      cp_async8(&H(b, 7, ly, lx), S.box + id);
+      cp_async8(&H(b, 8, ly, lx), S.boy + id);
+      cp_async8(&H(b, 9, ly, lx), S.boz + id);
+    }
+    double *ob = smem + b * BUF + NH * HS;
+    if (vec2) {
+      constexpr int PAIRS = NC / 2;
+      for (int t = tid; t < NO * PAIRS; t += NT) {
+        const int slot = t / PAIRS, rem = t - slot * PAIRS;
+        if (!own_active(slot)) continue;
+        const int r = rem / (TX / 2), c = 2 * (rem - r * (TX / 2));
+        const int gx = x0 + c, gy = y0 + r;
+        if (gx >= nx || gy >= ny) continue;
+        cp_async16(ob + slot * NC + r * TX + c, optr[slot] + kb + (long long)gy * nx + gx);
+      }
+    } else {
+      for (int t = tid; t < NO * NC; t += NT) {
+        const int slot = t / NC, rem = t - slot * NC;
+        if (!own_active(slot)) continue;
+        const int r = rem / TX, c = rem - r * TX;
+        const int gx = x0 + c, gy = y0 + r;
+        if (gx >= nx || gy >= ny) continue;
+        cp_async8(ob + slot * NC + r * TX + c, optr[slot] + kb + (long long)gy * nx + gx);
+      }
+    }
+    cp_commit();
+  };
+
+  // role 0 windows: vz, p, bx ; role 1 windows: flux1, flux2, by
+  double w0[11], w1[11], w2[11];
+  auto head = [&](int kk, double &v0, double &v1, double &v2) {
+    const long long id = (long long)kk * NXY + col;
+    if (role == 0) {
+      v0 = __ldg(tin + 3 * N + id);
+      v1 = __ldg(tin + 4 * N + id);
+      v2 = __ldg(tin + 5 * N + id);
+    } else {
+      const double vx_ = __ldg(tin + N + id), vy_ = __ldg(tin + 2 * N + id),
+                   vz_ = __ldg(tin + 3 * N + id);
+      const double ox = __ldg(S.box + id), oy = __ldg(S.boy + id),
+                   oz = __ldg(S.boz + id);
+      v0 = -vz_ * oy + vy_ * oz;       // flux1
+      v1 = -vx_ * oz + vz_ * ox;       // flux2
+      v2 = __ldg(tin + 6 * N + id);    // by
+    }
+  };
+  issue(k0, 0);
+  const int b0 = min(k0 - 5, nz - 11);
+#pragma unroll
+  for (int m = 0; m < 11; ++m) {
+    const int kk = b0 + m;
+    if (act && kk >= 0) head(kk, w0[m], w1[m], w2[m]);
+    else w0[m] = w1[m] = w2[m] = 0.0;
+  }
+  double h0 = 0, h1 = 0, h2 = 0;
+  double ke = 0.0, mr = 1e300, mp = 1e300;
+
+  for (int k = k0; k < k1; ++k) {
+    const int b = (k - k0) & 1;
+    if (k > k0 && k <= nz - 6) {
+      shift(w0, h0); shift(w1, h1); shift(w2, h2);
+    }
+    if (k + 1 < k1) issue(k + 1, b ^ 1);
+    else cp_commit();
+    cp_wait1();
+    __syncthreads();
+    const double ox = H(b, 7, ry, rx), oy = H(b, 8, ry, rx), oz = H(b, 9, ry, rx);
+    __syncthreads();
+    for (int t = tid; t < HS; t += NT) {
+      const int ly = t / HX, lx = t - ly * HX;
+      const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
+      if (!inx && !iny) continue;
+      const double vx_ = H(b, 0, ly, lx), vy_ = H(b, 1, ly, lx), vz_ = H(b, 2, ly, lx);
+      const double bx0 = H(b, 7, ly, lx), by0 = H(b, 8, ly, lx), bz0 = H(b, 9, ly, lx);
+      H(b, 7, ly, lx) = -vz_ * by0 + vy_ * bz0;
+      H(b, 8, ly, lx) = -vx_ * bz0 + vz_ * bx0;
+      H(b, 9, ly, lx) = -vy_ * bx0 + vx_ * by0;
+    }
+    __syncthreads();
+    const long long id = (long long)k * NXY + col;
+    const double szk = __ldg(S.stretch + k);
+    auto DX = [&](int slot) {
+      return dxy(i, nx, per, S.stretchx, [&](int g) { return H(b, slot, ry, g - xo); });
+    };
+    auto DY = [&](int slot) {
+      return dxy(j, ny, per, S.stretchy, [&](int g) { return H(b, slot, g - yo, rx); });
+    };
+    const bool zpml = S.zb.on && (k < S.zb.np || k >= nz - S.zt.np);
+    const bool zbot = k < S.zb.np;
+    const FaceDev &FZ = zbot ? S.zb : S.zt;
+    const int kl = zbot ? k : k - (nz - S.zt.np);
+    const long long fz = (long long)kl * NXY + col;
+    const bool xpml = S.xb.on && act && (i < S.xb.np || i >= nx - S.xt.np);
+    const bool xbot = i < S.xb.np;
+    const FaceDev &FX = xbot ? S.xb : S.xt;
+    const int il = xbot ? i : i - (nx - S.xt.np);
+    const long long fx = il + (long long)FX.np * (j + (long long)ny * k);
+    const bool ypml = S.xb.on && act && (j < S.yb.np || j >= ny - S.yt.np);
+    const bool ybot = j < S.yb.np;
+    const FaceDev &FY = ybot ? S.yb : S.yt;
+    const int jl = ybot ? j : j - (ny - S.yt.np);
+    const long long fy = i + (long long)nx * (jl + (long long)FY.np * k);
+    const bool zero = k == 0 || k == nz - 1 ||
+                      (!per && (i == 0 || i == nx - 1 || j == 0 || j == ny - 1));
+    // halo slots: 0 vx, 1 vy, 2 vz, 3 p, 4 bx, 5 by, 6 bz, 7-9 flux1..3
+    // phase A: the role's nine derivatives with their CPML corrections.
+    // role 0: d0 gpx d1 gpy d2 gpz d3 dvzdz d4 dybz d5 dxbz d6 dzbx d7 dxby d8 dybx
+    // role 1: d0 dvxdx d1 dvydy d2 dxflux3 d3 dxflux2 d4 dyflux3 d5 dyflux1
+    //         d6 dzflux1 d7 dzflux2 d8 dzby
+    double d0 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0, d6 = 0, d7 = 0, d8 = 0;
+    if (act) {
+      if (role == 0) {
+        d0 = DX(3); d5 = DX(6); d7 = DX(5);
+        d1 = DY(3); d4 = DY(6); d8 = DY(4);
+        d3 = dz(w0, k, nz, szk); d2 = dz(w1, k, nz, szk); d6 = dz(w2, k, nz, szk);
+        if (zpml) {
+          cpml<MODE>(FZ, fz, kl, 1, beta, dt, d2);
+          cpml<MODE>(FZ, fz, kl, 0, beta, dt, d3);
+          cpml<MODE>(FZ, fz, kl, 2, beta, dt, d6);
+        }
+        if (xpml) {
+          cpml<MODE>(FX, fx, il, 1, beta, dt, d0);
+          cpml<MODE>(FX, fx, il, 3, beta, dt, d5);
+          cpml<MODE>(FX, fx, il, 2, beta, dt, d7);
+        }
+        if (ypml) {
+          cpml<MODE>(FY, fy, jl, 1, beta, dt, d1);
+          cpml<MODE>(FY, fy, jl, 3, beta, dt, d4);
+          cpml<MODE>(FY, fy, jl, 2, beta, dt, d8);
+        }
+        X[cid] = d3;          // dvzdz for role 1
+      } else {
+        d0 = DX(0); d2 = DX(9); d3 = DX(8);
+        d1 = DY(1); d4 = DY(9); d5 = DY(7);
+        d6 = dz(w0, k, nz, szk); d7 = dz(w1, k, nz, szk); d8 = dz(w2, k, nz, szk);
+        if (zpml) {
+          cpml<MODE>(FZ, fz, kl, 4, beta, dt, d7);
+          cpml<MODE>(FZ, fz, kl, 5, beta, dt, d6);
+          cpml<MODE>(FZ, fz, kl, 3, beta, dt, d8);
+        }
+        if (xpml) {
+          cpml<MODE>(FX, fx, il, 0, beta, dt, d0);
+          cpml<MODE>(FX, fx, il, 4, beta, dt, d2);
+          cpml<MODE>(FX, fx, il, 5, beta, dt, d3);
+        }
+        if (ypml) {
+          cpml<MODE>(FY, fy, jl, 0, beta, dt, d1);
+          cpml<MODE>(FY, fy, jl, 4, beta, dt, d4);
+          cpml<MODE>(FY, fy, jl, 5, beta, dt, d5);
+        }
+        X[NC + cid] = d8;     // dzby for role 0
+      }
+    }
+    __syncthreads();
+    // phase B: right-hand sides and the stage (or final) update
+    double an_rho = 0.0;
+    if (act) {
+      const double rho = O(b, O_RHO), vx = H(b, 0, ry, rx), vy = H(b, 1, ry, rx),
+                   vz = H(b, 2, ry, rx);
+      const double red = O(b, O_BG + pipe::B_RED), sg = O(b, O_BG + pipe::B_SPONGE);
+      if (role == 0) {
+        const double bx = H(b, 4, ry, rx), by = H(b, 5, ry, rx), bz = H(b, 6, ry, rx);
+        const double dzby = X[NC + cid];
+        const double cbx = d4 - dzby, cby = -d5 + d6, cbz = d7 - d8;
+        const double c1 = cby * oz - cbz * oy, c2 = ox * cbz - cbx * oz,
+                     c3 = cbx * oy - cby * ox;
+        const double ri = O(b, O_BG + pipe::B_RHOINV);
+        double vxr = -ri * (d0 - (c1 * red)) - sg * vx;
+        double vyr = -ri * (d1 - (c2 * red)) - sg * vy;
+        double vzr = -ri * (d2 - (c3 * red)) - sg * vz;
+        const double qx = O(b, O_BG + pipe::B_CBX), qy = O(b, O_BG + pipe::B_CBY),
+                     qz = O(b, O_BG + pipe::B_CBZ);
+        const double e1 = qy * bz - qz * by, e2 = bx * qz - qx * bz,
+                     e3 = qx * by - qy * bx;
+        vxr = vxr + ri * e1 * red;
+        vyr = vyr + ri * e2 * red;
+        vzr = vzr + ri * e3 * red;
+        const int gc = S.colx[i] + S.bxdim * S.coly[j];
+        vzr = vzr - ri * rho * __ldg(S.gblk + (long long)gc * nz + k);
+        if (S.frc.kind != SPARC_SRC_NONE) {
+          const double frc = forcing_at(S, it, pulse_time(S, it), i, j, k);
+          if (S.frc.dir == 1) vxr = vxr + frc;
+          else if (S.frc.dir == 2) vyr = vyr + frc;
+          else vzr = vzr + frc;
+        }
+        const double R[3] = {vxr, vyr, vzr};
+        double vsq = 0.0;
+#pragma unroll
+        for (int l = 1; l < 4; ++l) {
+          const double av = MODE == FIRST ? H(b, l - 1, ry, rx) : O(b, O_A + l);
+          const double an = zero ? av : av + (MODE == LAST ? dt : bnext) * R[l - 1];
+          so[l * N + id] = an;
+          vsq = l == 1 ? an * an : vsq + an * an;
+        }
+        if (MODE == LAST) X[2 * NC + cid] = vsq;
+      } else {
+        const double p = H(b, 3, ry, rx);
+        const double dvzdz = X[cid];
+        double R[5];  // rho, p, bx, by, bz
+        R[2] = red * (d4 - d7);
+        R[3] = red * (d6 - d2);
+        R[4] = red * (d3 - d5);
+        const double div = d0 + d1 + dvzdz;
+        const double r0 = O(b, O_BG + pipe::B_RHO0);
+        R[0] = -O(b, O_BG + pipe::B_GRX) * vx - O(b, O_BG + pipe::B_GRY) * vy -
+               O(b, O_BG + pipe::B_GRZ) * vz - r0 * div - sg * rho;
+        R[1] = -O(b, O_BG + pipe::B_C2R) * div - vx * O(b, O_BG + pipe::B_GPX) -
+               vy * O(b, O_BG + pipe::B_GPY) - vz * O(b, O_BG + pipe::B_GPZ) - sg * p;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+          const int l = q == 0 ? 0 : q + 3;   // fields rho, p(4), bx(5), by(6), bz(7)
+          const int ls = q == 1 ? 4 : l;
+          const double av = MODE == FIRST ? (ls == 0 ? rho : H(b, ls - 1, ry, rx))
+                                          : O(b, O_A + ls);
+          const double an = zero ? av : av + (MODE == LAST ? dt : bnext) * R[q];
+          so[ls * N + id] = an;
+          if (q == 0) an_rho = an;
+        }
+        if (MODE == LAST) {
+          mr = fmin(mr, rho + r0);
+          mp = fmin(mp, p + O(b, O_P0));
+        }
+      }
+    }
+    if (MODE == LAST) {
+      __syncthreads();
+      if (act && role == 1) {  // KE density of driver.f90:161 on a_new
+        const double r0 = O(b, O_BG + pipe::B_RHO0);
+        const double m = (r0 + an_rho) * X[2 * NC + cid] / 2.0;
+        ke += m * m;
+      }
+    }
+    if (act && k + 1 < k1 && k + 1 <= nz - 6) head(k + 6, h0, h1, h2);
+    __syncthreads();
+  }
+  if (MODE == LAST) diag_reduce(S, ke, mr, mp);
+}
+
 // ------------------------------------------------------- stage dispatch
 int stage_geometry(Handle *h) {
   // tile shape: (32, 8); the quiet kernel drops to (16, 8) on grids too
@@ -1002,9 +1330,38 @@ static int launch_mhd_pipe(Handle *h, const SimDev &S, int stage,
   return SPARC_OK;
 }
 
+static int launch_mhd_duo(Handle *h, const SimDev &S, int stage,
+                          const double *a, const double *tin, double *so,
+                          cudaStream_t s) {
+  using namespace duo;
+  dim3 blk(TX, TY, 2);
+  dim3 grd((h->nx + TX - 1) / TX, (h->ny + TY - 1) / TY,
+           (h->nz + h->zchunk - 1) / h->zchunk);
+  const double beta = h->betas[stage - 1];
+  const double bnext = stage < 5 ? h->betas[stage] : h->deltat;
+  const int mode = stage == 1 ? FIRST : (stage == 5 ? LAST : MID);
+  if (mode == FIRST) {
+    cudaFuncSetAttribute(k_stage_mhd_duo<FIRST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    k_stage_mhd_duo<FIRST><<<grd, blk, SMEM, s>>>(S, a, tin, so, beta, bnext, h->zchunk);
+  } else if (mode == MID) {
+    cudaFuncSetAttribute(k_stage_mhd_duo<MID>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    k_stage_mhd_duo<MID><<<grd, blk, SMEM, s>>>(S, a, tin, so, beta, bnext, h->zchunk);
+  } else {
+    cudaFuncSetAttribute(k_stage_mhd_duo<LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    k_stage_mhd_duo<LAST><<<grd, blk, SMEM, s>>>(S, a, tin, so, beta, bnext, h->zchunk);
+  }
+  return SPARC_OK;
+}
+
 int launch_stage(Handle *h, const SimDev &S, int stage, const double *a,
                  const double *tin, double *so, cudaStream_t s) {
   int r = SPARC_ERR_INVALID;
+  if (h->magnetic && h->mhd_kernel == 3 && h->tx == 32 && h->ty == 8) {
+    r = launch_mhd_duo(h, S, stage, a, tin, so, s);
+    ++h->launches;
+    if (r == SPARC_OK && cudaGetLastError() != cudaSuccess) r = SPARC_ERR_CUDA;
+    return r;
+  }
   if (h->magnetic && h->mhd_kernel == 2 && h->tx == 32 && h->ty == 8) {
     r = launch_mhd_pipe(h, S, stage, a, tin, so, s);
     ++h->launches;

@@ -297,7 +297,7 @@ int sparc_create(const sparc_params *p, int device, sparc_handle **out) {
     cols[h->nx + h->ny + k] = b;
   }
   if (const char *kv = std::getenv("SPARC_MHD_KERNEL"))  // A/B timing only
-    h->mhd_kernel = std::max(1, std::min(3, std::atoi(kv)));
+    h->mhd_kernel = std::max(1, std::min(4, std::atoi(kv)));
   int r = SPARC_OK;
   if (!cuda_ok(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream")) {
     r = SPARC_ERR_CUDA;
@@ -329,6 +329,10 @@ int sparc_create(const sparc_params *p, int device, sparc_handle **out) {
     r |= alloc_face(h, 3, p->npml_xt, h->ny, h->nz, p->npml_xt);
     r |= alloc_face(h, 4, h->nx, p->npml_yb, h->nz, p->npml_yb);
     r |= alloc_face(h, 5, h->nx, p->npml_yt, h->nz, p->npml_yt);
+  }
+  if (!r) {
+    h->d_err = (int *)dev_alloc(h, 4);
+    if (!h->d_err || cudaMemset(h->d_err, 0, 4) != cudaSuccess) r = SPARC_ERR_NOMEM;
   }
   if (!r) {
     h->d_iter = (long long *)dev_alloc(h, 8);
@@ -382,6 +386,8 @@ int sparc_set_background(sparc_handle *h, const double *rho0,
   if (h->bg_ready) return fail(h, SPARC_ERR_ORDER, "background already set");
   cudaSetDevice(h->device);
   int r = setup_background(h, rho0, pre0, cs0, bx0, by0, bz0, zaxis_mm, grav);
+  if (r) return r;
+  r = encode_tensor_maps(h);
   if (r) return r;
   r = zero_state(h);
   if (r) return r;
@@ -605,9 +611,12 @@ int sparc_diagnostics(sparc_handle *h, sparc_diag *out) {
   cudaSetDevice(h->device);
   double d[4];
   long long f;
+  int e = 0;
   CK(h, cudaMemcpyAsync(d, h->d_diag, 32, cudaMemcpyDeviceToHost, h->stream));
   CK(h, cudaMemcpyAsync(&f, h->d_fail, 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaMemcpyAsync(&e, h->d_err, 4, cudaMemcpyDeviceToHost, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
+  if (e) return fail(h, SPARC_ERR_TIMEOUT, "a bounded device wait gave up");
   out->ke_norm = d[0];
   out->min_rho = d[1];
   out->min_p = d[2];

@@ -3,6 +3,7 @@
 // the POD structs below by value.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -64,6 +65,7 @@ struct SimDev {
   ForcingDev frc;
   // iteration bookkeeping and diagnostics (device)
   long long *iter;             // current driver iteration
+  int *err;                    // device error flag (bounded waits)
   double *partials;            // 3 per block of the last stage
   unsigned int *counter;
   double *diag;                // ke, min_rho, min_p, iteration(double)
@@ -125,16 +127,22 @@ struct Handle {
   double *d_damp2 = nullptr;                // source_damp(i,j) (N/nz)
   int nblocks = 1;
 
+  // TMA tensor maps of the own-point arrays: [0..2] the state buffers
+  // (nx, ny, nz*V), [3..17] the background arrays read per layer
+  bool tma = false;
+  CUtensorMap tmaps[18];
   // device bookkeeping
+  int *d_err = nullptr;
   long long *d_iter = nullptr, *d_fail = nullptr;
   double *d_partials = nullptr, *d_diag = nullptr;
   unsigned int *d_counter = nullptr;
   int max_stage_blocks = 0;
 
   // stage launch geometry; mhd_kernel 1: register/shared-tile kernel,
-  // 2: cp.async-pipelined kernel, 3: two-role pipelined kernel (32x8 tiles)
+  // 2: cp.async-pipelined kernel, 3: two-role pipelined kernel, 4: two-role
+  // kernel with TMA own-point loads (32x8 tiles, even nx; else 3)
   int tx = 32, ty = 8, zchunk = 32;
-  int mhd_kernel = 3;
+  int mhd_kernel = 4;
 
   // captured graphs keyed by (ra, rf1, rf2, filter kind)
   struct GraphEntry {
@@ -169,6 +177,7 @@ int launch_psr_forcing(Handle *h, const SimDev &S, cudaStream_t s);
 int launch_filter_pass(Handle *h, int dir, const double *in, double *out,
                        cudaStream_t s);
 int stage_geometry(Handle *h);
+int encode_tensor_maps(Handle *h);
 
 // api.cu
 void *dev_alloc(Handle *h, size_t bytes);

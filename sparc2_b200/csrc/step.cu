@@ -1241,6 +1241,405 @@ __global__ void __launch_bounds__(duo::NT, 1)
   if (MODE == LAST) diag_reduce(S, ke, mr, mp);
 }
 
+// --------------------- MP_MHD_3D, two-role stage kernel with TMA loads
+// k_stage_mhd_duo with the 24 own-point arrays of a layer fetched by TMA
+// (one elected thread, 3-D tensor maps, 32x8 boxes, one mbarrier per
+// buffer) instead of per-thread copies, halo copy addresses computed once
+// per CTA, and branch-free centred x/y stencils for interior columns.
+// Shared memory per buffer: 24 own slots (2 KB each, 128-B aligned) then
+// the 10 halo slots.  Needs an even nx (16-B row strides).
+struct TmaSet {
+  CUtensorMap m[18];
+};
+
+namespace tmak {
+constexpr int TX = 32, TY = 8, NC = TX * TY, NT = 2 * NC;
+constexpr int HX = TX + 10, HY = TY + 10, HS = HX * HY;
+constexpr int NH = 10, NO = 24;
+constexpr int BUF = ((NO * NC + NH * HS) + 15) / 16 * 16;  // 128-B multiple
+constexpr int XCH = 3 * NC;
+constexpr size_t SMEM = (2 * (size_t)BUF + XCH) * sizeof(double) + 128;  // + align slack
+constexpr long long WAIT_LIMIT = 1LL << 26;
+}  // namespace tmak
+
+__device__ __forceinline__ unsigned sm_addr(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sm_addr(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sm_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(double *dst, const CUtensorMap *map, int x,
+                                            int y, int z, unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(sm_addr(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(sm_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(sm_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait: false (and the error flag set) if the copies never land
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity,
+                                          int *err) {
+  for (long long n = 0; n < tmak::WAIT_LIMIT; ++n)
+    if (mbar_try_wait(bar, parity)) return true;
+  atomicExch(err, 1);
+  return false;
+}
+
+// centred 11-point sum along a shared-memory line with element stride st
+__device__ __forceinline__ double csum(const double *p, int st) {
+  double s = 0.0;
+#pragma unroll
+  for (int m = 0; m < 11; ++m) s += p[m * st] * c_dp[5][m];
+  return s;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(tmak::NT, 1)
+    k_stage_mhd_tma(const SimDev S, const __grid_constant__ TmaSet T,
+                    const double *__restrict__ a, const double *__restrict__ tin,
+                    double *__restrict__ so, double beta, double bnext,
+                    int zchunk, int mt, int ma) {
+  using namespace tmak;
+  using pipe::O_RHO;
+  using pipe::O_A;
+  using pipe::O_BG;
+  using pipe::O_P0;
+  extern __shared__ __align__(1024) double smem_raw[];
+  __shared__ unsigned long long bar[2];
+  const int tx = threadIdx.x, ty = threadIdx.y, role = threadIdx.z;
+  const int tid = (role * TY + ty) * TX + tx, cid = ty * TX + tx;
+  // TMA destinations must be 128-byte aligned: align the base explicitly
+  double *smem = (double *)(((size_t)smem_raw + 127) & ~(size_t)127);
+  if (sm_addr(smem) & 127u) {  // cannot happen after the rounding; never issue TMA then
+    if (tid == 0) atomicExch(S.err, 2);
+    return;
+  }
+  const int nx = S.nx, ny = S.ny, nz = S.nz;
+  const long long N = S.N, NXY = (long long)nx * ny;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int i = x0 + tx, j = y0 + ty;
+  const bool act = i < nx && j < ny;
+  const bool per = S.periodic;
+  const int k0 = blockIdx.z * zchunk, k1 = min(nz, k0 + zchunk);
+  const long long col = (long long)j * nx + i;
+  const long long it = *S.iter;
+  const double dt = S.deltat;
+  const int xo = tile_origin(x0, TX, nx, per), yo = tile_origin(y0, TY, ny, per);
+  const int cx0 = x0 - xo, cy0 = y0 - yo;
+  const int ry = cy0 + ty, rx = cx0 + tx;
+  const bool xint = per || (i >= 5 && i < nx - 5);
+  const bool yint = per || (j >= 5 && j < ny - 5);
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  // buffer b: own slots at b*BUF, halo slots after them
+  auto O = [&](int b, int slot) -> double & { return smem[b * BUF + slot * NC + cid]; };
+  auto Hp = [&](int b, int slot) -> double * { return smem + b * BUF + NO * NC + slot * HS; };
+  double *X = smem + 2 * BUF;
+  // halo positions of this thread (layer independent)
+  int hs0 = -1, hs1 = -1;
+  long long ho0 = 0, ho1 = 0;
+  {
+    auto pos = [&](int t, int &hs, long long &ho) {
+      if (t >= HS) return;
+      const int ly = t / HX, lx = t - ly * HX;
+      const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
+      if (!inx && !iny) return;
+      int gx = xo + lx, gy = yo + ly;
+      if (per) {
+        gx = wrapi(gx, nx);
+        gy = wrapi(gy, ny);
+      } else if (gx < 0 || gx >= nx || gy < 0 || gy >= ny) {
+        return;
+      }
+      hs = t;
+      ho = (long long)gy * nx + gx;
+    };
+    pos(tid, hs0, ho0);
+    pos(tid + NT, hs1, ho1);
+  }
+  const unsigned own_bytes =
+      (MODE == FIRST ? 15u : (MODE == MID ? 23u : 24u)) * NC * (unsigned)sizeof(double);
+  auto issue = [&](int k, int b) {
+    const long long kb = (long long)k * NXY;
+    if (hs0 >= 0) {
+      double *h = Hp(b, 0) + hs0;
+      const long long id = kb + ho0;
+#pragma unroll
+      for (int sl = 0; sl < 7; ++sl) cp_async8(h + sl * HS, tin + (sl + 1) * N + id);
+      cp_async8(h + 7 * HS, S.box + id);
+      cp_async8(h + 8 * HS, S.boy + id);
+      cp_async8(h + 9 * HS, S.boz + id);
+    }
+    if (hs1 >= 0) {
+      double *h = Hp(b, 0) + hs1;
+      const long long id = kb + ho1;
+#pragma unroll
+      for (int sl = 0; sl < 7; ++sl) cp_async8(h + sl * HS, tin + (sl + 1) * N + id);
+      cp_async8(h + 7 * HS, S.box + id);
+      cp_async8(h + 8 * HS, S.boy + id);
+      cp_async8(h + 9 * HS, S.boz + id);
+    }
+    cp_commit();
+    if (tid == 0) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_expect_tx(&bar[b], own_bytes);
+      double *ob = smem + b * BUF;
+      tma_load_3d(ob + O_RHO * NC, &T.m[mt], x0, y0, k, &bar[b]);
+      if (MODE != FIRST)
+        for (int l = 0; l < 8; ++l)
+          tma_load_3d(ob + (O_A + l) * NC, &T.m[ma], x0, y0, l * nz + k, &bar[b]);
+      for (int n = 0; n < 14; ++n)
+        tma_load_3d(ob + (O_BG + n) * NC, &T.m[3 + n], x0, y0, k, &bar[b]);
+      if (MODE == LAST) tma_load_3d(ob + O_P0 * NC, &T.m[17], x0, y0, k, &bar[b]);
+    }
+  };
+
+  double w0[11], w1[11], w2[11];
+  auto head = [&](int kk, double &v0, double &v1, double &v2) {
+    const long long id = (long long)kk * NXY + col;
+    if (role == 0) {
+      v0 = __ldg(tin + 3 * N + id);
+      v1 = __ldg(tin + 4 * N + id);
+      v2 = __ldg(tin + 5 * N + id);
+    } else {
+      const double vx_ = __ldg(tin + N + id), vy_ = __ldg(tin + 2 * N + id),
+                   vz_ = __ldg(tin + 3 * N + id);
+      const double ox = __ldg(S.box + id), oy = __ldg(S.boy + id),
+                   oz = __ldg(S.boz + id);
+      v0 = -vz_ * oy + vy_ * oz;
+      v1 = -vx_ * oz + vz_ * ox;
+      v2 = __ldg(tin + 6 * N + id);
+    }
+  };
+  issue(k0, 0);
+  const int b0 = min(k0 - 5, nz - 11);
+#pragma unroll
+  for (int m = 0; m < 11; ++m) {
+    const int kk = b0 + m;
+    if (act && kk >= 0) head(kk, w0[m], w1[m], w2[m]);
+    else w0[m] = w1[m] = w2[m] = 0.0;
+  }
+  double h0 = 0, h1 = 0, h2 = 0;
+  double ke = 0.0, mr = 1e300, mp = 1e300;
+  unsigned phase = 0;  // bit b: parity of buffer b's next completion
+  bool ok = true;
+
+  for (int k = k0; k < k1 && ok; ++k) {
+    const int b = (k - k0) & 1;
+    if (k > k0 && k <= nz - 6) {
+      shift(w0, h0); shift(w1, h1); shift(w2, h2);
+    }
+    if (k + 1 < k1) issue(k + 1, b ^ 1);
+    else cp_commit();
+    cp_wait1();
+    ok = mbar_wait(&bar[b], (phase >> b) & 1u, S.err);
+    phase ^= 1u << b;
+    __syncthreads();
+    if (!__syncthreads_and(ok)) { ok = false; break; }
+    double *H7 = Hp(b, 7), *H8 = Hp(b, 8), *H9 = Hp(b, 9);
+    const int own = ry * HX + rx;
+    const double ox = H7[own], oy = H8[own], oz = H9[own];
+    __syncthreads();
+    {
+      const double *H0 = Hp(b, 0), *H1 = Hp(b, 1), *H2 = Hp(b, 2);
+      for (int t = tid; t < HS; t += NT) {
+        const int ly = t / HX, lx = t - ly * HX;
+        const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
+        if (!inx && !iny) continue;
+        const double vx_ = H0[t], vy_ = H1[t], vz_ = H2[t];
+        const double bx0 = H7[t], by0 = H8[t], bz0 = H9[t];
+        H7[t] = -vz_ * by0 + vy_ * bz0;
+        H8[t] = -vx_ * bz0 + vz_ * bx0;
+        H9[t] = -vy_ * bx0 + vx_ * by0;
+      }
+    }
+    __syncthreads();
+    const long long id = (long long)k * NXY + col;
+    const double szk = __ldg(S.stretch + k);
+    // x and y derivatives of halo slot `slot` at this thread's column
+    auto DX = [&](int slot) {
+      const double *row = Hp(b, slot) + ry * HX;
+      if (xint) return S.stretchx * csum(row + (i - 5 - xo), 1);
+      return dxy(i, nx, per, S.stretchx, [&](int g) { return row[g - xo]; });
+    };
+    auto DY = [&](int slot) {
+      const double *colp = Hp(b, slot) + rx;
+      if (yint) return S.stretchy * csum(colp + (j - 5 - yo) * HX, HX);
+      return dxy(j, ny, per, S.stretchy, [&](int g) { return colp[(g - yo) * HX]; });
+    };
+    const bool zpml = S.zb.on && (k < S.zb.np || k >= nz - S.zt.np);
+    const bool zbot = k < S.zb.np;
+    const FaceDev &FZ = zbot ? S.zb : S.zt;
+    const int kl = zbot ? k : k - (nz - S.zt.np);
+    const long long fz = (long long)kl * NXY + col;
+    const bool xpml = S.xb.on && act && (i < S.xb.np || i >= nx - S.xt.np);
+    const bool xbot = i < S.xb.np;
+    const FaceDev &FX = xbot ? S.xb : S.xt;
+    const int il = xbot ? i : i - (nx - S.xt.np);
+    const long long fx = il + (long long)FX.np * (j + (long long)ny * k);
+    const bool ypml = S.xb.on && act && (j < S.yb.np || j >= ny - S.yt.np);
+    const bool ybot = j < S.yb.np;
+    const FaceDev &FY = ybot ? S.yb : S.yt;
+    const int jl = ybot ? j : j - (ny - S.yt.np);
+    const long long fy = i + (long long)nx * (jl + (long long)FY.np * k);
+    const bool zero = k == 0 || k == nz - 1 ||
+                      (!per && (i == 0 || i == nx - 1 || j == 0 || j == ny - 1));
+    auto Hv = [&](int slot) { return Hp(b, slot)[own]; };
+    double d0 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0, d6 = 0, d7 = 0, d8 = 0;
+    if (act) {
+      if (role == 0) {
+        d0 = DX(3); d5 = DX(6); d7 = DX(5);
+        d1 = DY(3); d4 = DY(6); d8 = DY(4);
+        d3 = dz(w0, k, nz, szk); d2 = dz(w1, k, nz, szk); d6 = dz(w2, k, nz, szk);
+        if (zpml) {
+          cpml<MODE>(FZ, fz, kl, 1, beta, dt, d2);
+          cpml<MODE>(FZ, fz, kl, 0, beta, dt, d3);
+          cpml<MODE>(FZ, fz, kl, 2, beta, dt, d6);
+        }
+        if (xpml) {
+          cpml<MODE>(FX, fx, il, 1, beta, dt, d0);
+          cpml<MODE>(FX, fx, il, 3, beta, dt, d5);
+          cpml<MODE>(FX, fx, il, 2, beta, dt, d7);
+        }
+        if (ypml) {
+          cpml<MODE>(FY, fy, jl, 1, beta, dt, d1);
+          cpml<MODE>(FY, fy, jl, 3, beta, dt, d4);
+          cpml<MODE>(FY, fy, jl, 2, beta, dt, d8);
+        }
+        X[cid] = d3;
+      } else {
+        d0 = DX(0); d2 = DX(9); d3 = DX(8);
+        d1 = DY(1); d4 = DY(9); d5 = DY(7);
+        d6 = dz(w0, k, nz, szk); d7 = dz(w1, k, nz, szk); d8 = dz(w2, k, nz, szk);
+        if (zpml) {
+          cpml<MODE>(FZ, fz, kl, 4, beta, dt, d7);
+          cpml<MODE>(FZ, fz, kl, 5, beta, dt, d6);
+          cpml<MODE>(FZ, fz, kl, 3, beta, dt, d8);
+        }
+        if (xpml) {
+          cpml<MODE>(FX, fx, il, 0, beta, dt, d0);
+          cpml<MODE>(FX, fx, il, 4, beta, dt, d2);
+          cpml<MODE>(FX, fx, il, 5, beta, dt, d3);
+        }
+        if (ypml) {
+          cpml<MODE>(FY, fy, jl, 0, beta, dt, d1);
+          cpml<MODE>(FY, fy, jl, 4, beta, dt, d4);
+          cpml<MODE>(FY, fy, jl, 5, beta, dt, d5);
+        }
+        X[NC + cid] = d8;
+      }
+    }
+    __syncthreads();
+    double an_rho = 0.0;
+    if (act) {
+      const double rho = O(b, O_RHO), vx = Hv(0), vy = Hv(1), vz = Hv(2);
+      const double red = O(b, O_BG + pipe::B_RED), sg = O(b, O_BG + pipe::B_SPONGE);
+      if (role == 0) {
+        const double bx = Hv(4), by = Hv(5), bz = Hv(6);
+        const double dzby = X[NC + cid];
+        const double cbx = d4 - dzby, cby = -d5 + d6, cbz = d7 - d8;
+        const double c1 = cby * oz - cbz * oy, c2 = ox * cbz - cbx * oz,
+                     c3 = cbx * oy - cby * ox;
+        const double ri = O(b, O_BG + pipe::B_RHOINV);
+        double vxr = -ri * (d0 - (c1 * red)) - sg * vx;
+        double vyr = -ri * (d1 - (c2 * red)) - sg * vy;
+        double vzr = -ri * (d2 - (c3 * red)) - sg * vz;
+        const double qx = O(b, O_BG + pipe::B_CBX), qy = O(b, O_BG + pipe::B_CBY),
+                     qz = O(b, O_BG + pipe::B_CBZ);
+        const double e1 = qy * bz - qz * by, e2 = bx * qz - qx * bz,
+                     e3 = qx * by - qy * bx;
+        vxr = vxr + ri * e1 * red;
+        vyr = vyr + ri * e2 * red;
+        vzr = vzr + ri * e3 * red;
+        const int gc = S.colx[i] + S.bxdim * S.coly[j];
+        vzr = vzr - ri * rho * __ldg(S.gblk + (long long)gc * nz + k);
+        if (S.frc.kind != SPARC_SRC_NONE) {
+          const double frc = forcing_at(S, it, pulse_time(S, it), i, j, k);
+          if (S.frc.dir == 1) vxr = vxr + frc;
+          else if (S.frc.dir == 2) vyr = vyr + frc;
+          else vzr = vzr + frc;
+        }
+        const double R[3] = {vxr, vyr, vzr};
+        double vsq = 0.0;
+#pragma unroll
+        for (int l = 1; l < 4; ++l) {
+          const double av = MODE == FIRST ? Hv(l - 1) : O(b, O_A + l);
+          const double an = zero ? av : av + (MODE == LAST ? dt : bnext) * R[l - 1];
+          so[l * N + id] = an;
+          vsq = l == 1 ? an * an : vsq + an * an;
+        }
+        if (MODE == LAST) X[2 * NC + cid] = vsq;
+      } else {
+        const double p = Hv(3);
+        const double dvzdz = X[cid];
+        double R[5];
+        R[2] = red * (d4 - d7);
+        R[3] = red * (d6 - d2);
+        R[4] = red * (d3 - d5);
+        const double div = d0 + d1 + dvzdz;
+        const double r0 = O(b, O_BG + pipe::B_RHO0);
+        R[0] = -O(b, O_BG + pipe::B_GRX) * vx - O(b, O_BG + pipe::B_GRY) * vy -
+               O(b, O_BG + pipe::B_GRZ) * vz - r0 * div - sg * rho;
+        R[1] = -O(b, O_BG + pipe::B_C2R) * div - vx * O(b, O_BG + pipe::B_GPX) -
+               vy * O(b, O_BG + pipe::B_GPY) - vz * O(b, O_BG + pipe::B_GPZ) - sg * p;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+          const int ls = q == 0 ? 0 : (q == 1 ? 4 : q + 3);
+          const double av = MODE == FIRST ? (ls == 0 ? rho : Hv(ls - 1)) : O(b, O_A + ls);
+          const double an = zero ? av : av + (MODE == LAST ? dt : bnext) * R[q];
+          so[ls * N + id] = an;
+          if (q == 0) an_rho = an;
+        }
+        if (MODE == LAST) {
+          mr = fmin(mr, rho + r0);
+          mp = fmin(mp, p + O(b, O_P0));
+        }
+      }
+    }
+    if (MODE == LAST) {
+      __syncthreads();
+      if (act && role == 1) {
+        const double r0 = O(b, O_BG + pipe::B_RHO0);
+        const double m = (r0 + an_rho) * X[2 * NC + cid] / 2.0;
+        ke += m * m;
+      }
+    }
+    if (act && k + 1 < k1 && k + 1 <= nz - 6) head(k + 6, h0, h1, h2);
+    __syncthreads();
+  }
+  if (!ok) {
+    // a bounded wait gave up: drain (again bounded) what this CTA issued
+    cp_wait1();
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    if (tid == 0) {
+      mbar_wait(&bar[0], phase & 1u, S.err);
+      mbar_wait(&bar[1], (phase >> 1) & 1u, S.err);
+    }
+    return;
+  }
+  if (MODE == LAST) diag_reduce(S, ke, mr, mp);
+}
+
 // ------------------------------------------------------- stage dispatch
 int stage_geometry(Handle *h) {
   // tile shape: (32, 8); the quiet kernel drops to (16, 8) on grids too
@@ -1353,10 +1752,82 @@ static int launch_mhd_duo(Handle *h, const SimDev &S, int stage,
   return SPARC_OK;
 }
 
+static int launch_mhd_tma(Handle *h, const SimDev &S, int stage,
+                          const double *a, const double *tin, double *so,
+                          cudaStream_t s) {
+  using namespace tmak;
+  int mt = -1, ma = -1;
+  for (int b = 0; b < 3; ++b) {
+    if (h->buf[b] == tin) mt = b;
+    if (h->buf[b] == a) ma = b;
+  }
+  if (mt < 0 || ma < 0) return SPARC_ERR_INVALID;
+  TmaSet T;
+  for (int n = 0; n < 18; ++n) T.m[n] = h->tmaps[n];
+  dim3 blk(TX, TY, 2);
+  dim3 grd((h->nx + TX - 1) / TX, (h->ny + TY - 1) / TY,
+           (h->nz + h->zchunk - 1) / h->zchunk);
+  const double beta = h->betas[stage - 1];
+  const double bnext = stage < 5 ? h->betas[stage] : h->deltat;
+  const int mode = stage == 1 ? FIRST : (stage == 5 ? LAST : MID);
+  if (mode == FIRST) {
+    cudaFuncSetAttribute(k_stage_mhd_tma<FIRST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    k_stage_mhd_tma<FIRST><<<grd, blk, SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt, ma);
+  } else if (mode == MID) {
+    cudaFuncSetAttribute(k_stage_mhd_tma<MID>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    k_stage_mhd_tma<MID><<<grd, blk, SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt, ma);
+  } else {
+    cudaFuncSetAttribute(k_stage_mhd_tma<LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    k_stage_mhd_tma<LAST><<<grd, blk, SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt, ma);
+  }
+  return SPARC_OK;
+}
+
+// Tensor maps (3-D, FP64, 32x8x1 boxes) of the arrays the TMA kernel loads
+// per layer; needs 16-byte row strides, i.e. an even nx.
+int encode_tensor_maps(Handle *h) {
+  h->tma = false;
+  if (!h->magnetic || (h->nx & 1)) return SPARC_OK;
+  void *fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+          cudaSuccess || !fn || q != cudaDriverEntryPointSuccess) {
+    cudaGetLastError();
+    return SPARC_OK;  // the cp.async kernel serves instead
+  }
+  auto enc = (CUresult(*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                          const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                          const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                          CUtensorMapL2promotion, CUtensorMapFloatOOBfill))fn;
+  auto one = [&](CUtensorMap *m, const double *base, unsigned long long depth) {
+    cuuint64_t dims[3] = {(cuuint64_t)h->nx, (cuuint64_t)h->ny, (cuuint64_t)depth};
+    cuuint64_t strides[2] = {(cuuint64_t)h->nx * 8, (cuuint64_t)h->nx * h->ny * 8};
+    cuuint32_t box[3] = {32, 8, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void *)base, dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  };
+  bool ok = true;
+  for (int b = 0; b < 3; ++b) ok = ok && one(&h->tmaps[b], h->buf[b], (unsigned long long)h->nz * h->V);
+  const double *bg[15] = {h->red, h->sponge, h->rho0, h->grx, h->gry, h->grz, h->c2rho0,
+                          h->gpx, h->gpy, h->gpz, h->rhoinv, h->cbx, h->cby, h->cbz, h->p0};
+  for (int n = 0; n < 15; ++n) ok = ok && bg[n] && one(&h->tmaps[3 + n], bg[n], h->nz);
+  h->tma = ok;
+  return SPARC_OK;
+}
+
 int launch_stage(Handle *h, const SimDev &S, int stage, const double *a,
                  const double *tin, double *so, cudaStream_t s) {
   int r = SPARC_ERR_INVALID;
-  if (h->magnetic && h->mhd_kernel == 3 && h->tx == 32 && h->ty == 8) {
+  if (h->magnetic && h->mhd_kernel == 4 && h->tma && h->tx == 32 && h->ty == 8) {
+    r = launch_mhd_tma(h, S, stage, a, tin, so, s);
+    ++h->launches;
+    if (r == SPARC_OK && cudaGetLastError() != cudaSuccess) r = SPARC_ERR_CUDA;
+    return r;
+  }
+  if (h->magnetic && h->mhd_kernel >= 3 && h->tx == 32 && h->ty == 8) {
     r = launch_mhd_duo(h, S, stage, a, tin, so, s);
     ++h->launches;
     if (r == SPARC_OK && cudaGetLastError() != cudaSuccess) r = SPARC_ERR_CUDA;
@@ -1597,6 +2068,7 @@ SimDev make_simdev(Handle *h) {
   F.klo = h->psr_klo;
   F.khi = h->psr_khi;
   S.iter = h->d_iter;
+  S.err = h->d_err;
   S.partials = h->d_partials;
   S.counter = h->d_counter;
   S.diag = h->d_diag;

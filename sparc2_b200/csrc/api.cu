@@ -297,7 +297,11 @@ int sparc_create(const sparc_params *p, int device, sparc_handle **out) {
     cols[h->nx + h->ny + k] = b;
   }
   if (const char *kv = std::getenv("SPARC_MHD_KERNEL"))  // A/B timing only
-    h->mhd_kernel = std::max(1, std::min(4, std::atoi(kv)));
+    h->mhd_kernel = std::atoi(kv) == 4 ? 4 : 3;
+  if (const char *kv = std::getenv("SPARC_TMA_TY")) {  // A/B timing only
+    int t = std::atoi(kv);
+    if (t == 6 || t == 8) h->tma_ty = t;
+  }
   int r = SPARC_OK;
   if (!cuda_ok(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream")) {
     r = SPARC_ERR_CUDA;

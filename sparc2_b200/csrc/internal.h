@@ -20,49 +20,60 @@ constexpr double PI = 3.14159265358979;  // all_modules.f90:56 (truncated pi)
 // One CPML face on the device.  Auxiliary fields are stored in the
 // reference's layout (n0 fastest, P slots); profiles a, b, kappa are either
 // per point of the slab or, when `uniform`, one value per PML layer.
-struct FaceDev {
+// R is the storage type: double (plain form) or float (precision form).
+template <class R>
+struct FaceT {
   int on;
   int n0, n1, n2, np, P;
   int uniform;          // profiles depend on the layer index only
   long long cnt;        // n0*n1*n2
-  double *vars;         // RK state (zpmlvars...), cnt*P
-  double *scr;          // stage right-hand side (scrzpml...), cnt*P
-  const double *pa, *pb, *pk;
+  R *vars;              // RK state (zpmlvars...), cnt*P
+  R *scr;               // stage right-hand side (scrzpml...), cnt*P
+  const R *pa, *pb, *pk;
 };
+using FaceDev = FaceT<double>;
 
 // Forcing description consumed by the stage kernels.
-struct ForcingDev {
+template <class R>
+struct ForcingT {
   int kind;             // SPARC_SRC_*
   int dir;              // 1..3
   long long init;
   // PULSE = 1: f = T(t) * fz[k] * fy[j] * fx[i], T on the device
-  const double *fx, *fy, *fz;
+  const R *fx, *fy, *fz;
   double amp_c, t0, t1, st, timestep;  // amp_c = pulse_amp/0.56458272/dimc
   // PULSE = 2: precomputed per iteration for layers [klo, khi)
-  const double *psr;     // (khi-klo)*nx*ny
+  const R *psr;          // (khi-klo)*nx*ny
   int klo, khi;
 };
+using ForcingDev = ForcingT<double>;
 
 // Everything the fused stage kernels read.  Background arrays are either
 // 3-D (N) or, for the horizontally uniform quiet background, 1-D (nz).
-struct SimDev {
+// In the precision form (R = float) the state is stored scaled by depth
+// profiles: stored = sc[l*nz + k] * physical (isc = 1/sc), and the final
+// RK update carries a compensated-sum term per state value.
+template <class R>
+struct SimT {
   int nx, ny, nz;
   long long N;
   int periodic, magnetic, bg1d;
   int V;
   double stretchx, stretchy;
-  const double *stretch;       // nz
+  const R *stretch;            // nz
   double deltat;
   double dimc2rho;             // dimc^2*dimrho for the KE norm
   // background (code units)
-  const double *rho0, *p0, *rhoinv, *c2rho0, *grz, *gpz, *sponge;
-  const double *box, *boy, *boz, *cbx, *cby, *cbz;
-  const double *grx, *gry, *gpx, *gpy, *red;
-  const double *gblk;          // (block_x*block_y) * nz gravity
+  const R *rho0, *p0, *rhoinv, *c2rho0, *grz, *gpz, *sponge;
+  const R *box, *boy, *boz, *cbx, *cby, *cbz;
+  const R *grx, *gry, *gpx, *gpy, *red;
+  const R *gblk;               // (block_x*block_y) * nz gravity
   const int *colx, *coly;      // block index of each x / y
   int bxdim;
-  FaceDev zb, zt, xb, xt, yb, yt;
-  ForcingDev frc;
+  FaceT<R> zb, zt, xb, xt, yb, yt;
+  ForcingT<R> frc;
+  const R *sc, *isc;           // V x nz depth scales (precision form)
+  R *carry;                    // V x N compensated-sum carry (precision form)
   // iteration bookkeeping and diagnostics (device)
   long long *iter;             // current driver iteration
   int *err;                    // device error flag (bounded waits)
@@ -71,6 +82,7 @@ struct SimDev {
   double *diag;                // ke, min_rho, min_p, iteration(double)
   long long *fail_iter;
 };
+using SimDev = SimT<double>;
 
 struct Handle {
   sparc_params P{};
@@ -130,7 +142,8 @@ struct Handle {
   // TMA tensor maps of the own-point arrays: [0..2] the state buffers
   // (nx, ny, nz*V), [3..17] the background arrays read per layer
   bool tma = false;
-  CUtensorMap tmaps[18];
+  int tma_ty = 8;           // tile height of the TMA kernel (8 or 6)
+  CUtensorMap tmaps_ty[18];
   // device bookkeeping
   int *d_err = nullptr;
   long long *d_iter = nullptr, *d_fail = nullptr;
@@ -138,11 +151,10 @@ struct Handle {
   unsigned int *d_counter = nullptr;
   int max_stage_blocks = 0;
 
-  // stage launch geometry; mhd_kernel 1: register/shared-tile kernel,
-  // 2: cp.async-pipelined kernel, 3: two-role pipelined kernel, 4: two-role
-  // kernel with TMA own-point loads (32x8 tiles, even nx; else 3)
+  // stage launch geometry; mhd_kernel 3: two-role cp.async-pipelined MHD
+  // kernel (default), 4: its variant with TMA own-point loads (even nx)
   int tx = 32, ty = 8, zchunk = 32;
-  int mhd_kernel = 4;
+  int mhd_kernel = 3;
 
   // captured graphs keyed by (ra, rf1, rf2, filter kind)
   struct GraphEntry {

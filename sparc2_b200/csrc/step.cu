@@ -374,239 +374,8 @@ __global__ void __launch_bounds__(TX *TY)
   if (MODE == LAST) diag_reduce(S, ke, mr, mp);
 }
 
-// -------------------------------------------------- MP_MHD_3D stage kernel
-// RHS.f90:363-668 fused with one RK stage.  Tile slots of the dynamic
-// shared memory: 0 vx, 1 vy, 2 p, 3 bx, 4 by, 5 bz, 6 flux1, 7 flux2,
-// 8 flux3 (flux = v x B0 of RHS.f90:394-396).
-template <int TX, int TY, int MODE>
-__global__ void __launch_bounds__(TX *TY, 1)
-    k_stage_mhd(const SimDev S, const double *__restrict__ a,
-                const double *__restrict__ tin, double *__restrict__ so,
-                double beta, double bnext, int zchunk) {
-  constexpr int HX = TX + 10, HY = TY + 10, HS = HX * HY;
-  extern __shared__ double tile[];
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  const int nx = S.nx, ny = S.ny, nz = S.nz;
-  const long long N = S.N, NXY = (long long)nx * ny;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-  const int i = x0 + tx, j = y0 + ty;
-  const bool act = i < nx && j < ny;
-  const bool per = S.periodic;
-  const int k0 = blockIdx.z * zchunk, k1 = min(nz, k0 + zchunk);
-  const long long col = (long long)j * nx + i;
-  const long long it = *S.iter;
-  const double Tp = pulse_time(S, it);
-  const double dt = S.deltat;
-  const int gc = act ? S.colx[i] + S.bxdim * S.coly[j] : 0;
-  auto T = [&](int slot, int ly, int lx) -> double & {
-    return tile[slot * HS + ly * HX + lx];
-  };
-  const int xo = tile_origin(x0, TX, nx, per), yo = tile_origin(y0, TY, ny, per);
-  const int cx0 = x0 - xo, cy0 = y0 - yo;
-
-  // windows: vz, p, flux1, flux2, bx, by
-  double w_vz[11], w_p[11], w_f1[11], w_f2[11], w_bx[11], w_by[11];
-  auto head = [&](int kk, double &vz_, double &p_, double &f1_, double &f2_,
-                  double &bx_, double &by_) {
-    const long long id = (long long)kk * NXY + col;
-    const double vx_ = __ldg(tin + N + id);
-    const double vy_ = __ldg(tin + 2 * N + id);
-    vz_ = __ldg(tin + 3 * N + id);
-    p_ = __ldg(tin + 4 * N + id);
-    bx_ = __ldg(tin + 5 * N + id);
-    by_ = __ldg(tin + 6 * N + id);
-    const double ox = __ldg(S.box + id), oy = __ldg(S.boy + id),
-                 oz = __ldg(S.boz + id);
-    f1_ = -vz_ * oy + vy_ * oz;
-    f2_ = -vx_ * oz + vz_ * ox;
-  };
-  const int b0 = min(k0 - 5, nz - 11);
-#pragma unroll
-  for (int m = 0; m < 11; ++m) {
-    const int kk = b0 + m;
-    if (act && kk >= 0) {
-      head(kk, w_vz[m], w_p[m], w_f1[m], w_f2[m], w_bx[m], w_by[m]);
-    } else {
-      w_vz[m] = w_p[m] = w_f1[m] = w_f2[m] = w_bx[m] = w_by[m] = 0.0;
-    }
-  }
-  double ke = 0.0, mr = 1e300, mp = 1e300;
-
-  for (int k = k0; k < k1; ++k) {
-    if (k > k0 && k <= nz - 6) {
-      double v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;
-      if (act) head(k + 5, v0, v1, v2, v3, v4, v5);
-      shift(w_vz, v0); shift(w_p, v1); shift(w_f1, v2);
-      shift(w_f2, v3); shift(w_bx, v4); shift(w_by, v5);
-    }
-    const long long kb = (long long)k * NXY;
-    __syncthreads();
-    for (int t = tid; t < HS; t += TX * TY) {
-      const int ly = t / HX, lx = t - ly * HX;
-      const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
-      if (!inx && !iny) continue;
-      int gx = xo + lx, gy = yo + ly;
-      bool ok;
-      if (per) {
-        gx = wrapi(gx, nx);
-        gy = wrapi(gy, ny);
-        ok = true;
-      } else {
-        ok = gx >= 0 && gx < nx && gy >= 0 && gy < ny;
-      }
-      double vx_ = 0, vy_ = 0, vz_ = 0, p_ = 0, bx_ = 0, by_ = 0, bz_ = 0,
-             ox = 0, oy = 0, oz = 0;
-      if (ok) {
-        const long long id = kb + (long long)gy * nx + gx;
-        vx_ = __ldg(tin + N + id);
-        vy_ = __ldg(tin + 2 * N + id);
-        vz_ = __ldg(tin + 3 * N + id);
-        p_ = __ldg(tin + 4 * N + id);
-        bx_ = __ldg(tin + 5 * N + id);
-        by_ = __ldg(tin + 6 * N + id);
-        bz_ = __ldg(tin + 7 * N + id);
-        ox = __ldg(S.box + id); oy = __ldg(S.boy + id); oz = __ldg(S.boz + id);
-      }
-      T(0, ly, lx) = vx_;
-      T(1, ly, lx) = vy_;
-      T(2, ly, lx) = p_;
-      T(3, ly, lx) = bx_;
-      T(4, ly, lx) = by_;
-      T(5, ly, lx) = bz_;
-      T(6, ly, lx) = -vz_ * oy + vy_ * oz;
-      T(7, ly, lx) = -vx_ * oz + vz_ * ox;
-      T(8, ly, lx) = -vy_ * ox + vx_ * oy;
-    }
-    __syncthreads();
-    if (!act) continue;
-    const long long id = kb + col;
-    double av[8], tv[8];
-#pragma unroll
-    for (int l = 0; l < 8; ++l) {
-      tv[l] = __ldg(tin + l * N + id);
-      av[l] = MODE == FIRST ? tv[l] : __ldg(a + l * N + id);
-    }
-    const int ry = cy0 + ty, rx = cx0 + tx;
-    auto DX = [&](int slot) {
-      return dxy(i, nx, per, S.stretchx, [&](int g) { return T(slot, ry, g - xo); });
-    };
-    auto DY = [&](int slot) {
-      return dxy(j, ny, per, S.stretchy, [&](int g) { return T(slot, g - yo, rx); });
-    };
-    // the 15 derivatives of RHS.f90:400-422
-    double dvxdx = DX(0), dxflux3 = DX(8), gpx = DX(2), dxflux2 = DX(7),
-           dxby = DX(4), dxbz = DX(5);
-    double dvydy = DY(1), gpy = DY(2), dyflux3 = DY(8), dybz = DY(5),
-           dybx = DY(3), dyflux1 = DY(6);
-    const double szk = __ldg(S.stretch + k);
-    double dvzdz = dz(w_vz, k, nz, szk), dzflux1 = dz(w_f1, k, nz, szk),
-           dzflux2 = dz(w_f2, k, nz, szk), dzbx = dz(w_bx, k, nz, szk),
-           gpz = dz(w_p, k, nz, szk), dzby = dz(w_by, k, nz, szk);
-    // CPML, RHS.f90:424-546.  Slots: z 0 vz, 1 p, 2 dzbx, 3 dzby,
-    // 4 dzflux2, 5 dzflux1; x 0 vx, 1 p, 2 dxby, 3 dxbz, 4 dxflux3,
-    // 5 dxflux2; y 0 vy, 1 p, 2 dybx, 3 dybz, 4 dyflux3, 5 dyflux1.
-    if (S.zb.on && (k < S.zb.np || k >= nz - S.zt.np)) {
-      const bool bot = k < S.zb.np;
-      const FaceDev &F = bot ? S.zb : S.zt;
-      const int kl = bot ? k : k - (nz - S.zt.np);
-      const long long f = (long long)kl * NXY + col;
-      cpml<MODE>(F, f, kl, 1, beta, dt, gpz);
-      cpml<MODE>(F, f, kl, 0, beta, dt, dvzdz);
-      cpml<MODE>(F, f, kl, 4, beta, dt, dzflux2);
-      cpml<MODE>(F, f, kl, 5, beta, dt, dzflux1);
-      cpml<MODE>(F, f, kl, 2, beta, dt, dzbx);
-      cpml<MODE>(F, f, kl, 3, beta, dt, dzby);
-    }
-    if (S.xb.on) {
-      if (i < S.xb.np || i >= nx - S.xt.np) {
-        const bool bot = i < S.xb.np;
-        const FaceDev &F = bot ? S.xb : S.xt;
-        const int il = bot ? i : i - (nx - S.xt.np);
-        const long long f = il + (long long)F.np * (j + (long long)ny * k);
-        cpml<MODE>(F, f, il, 1, beta, dt, gpx);
-        cpml<MODE>(F, f, il, 0, beta, dt, dvxdx);
-        cpml<MODE>(F, f, il, 4, beta, dt, dxflux3);
-        cpml<MODE>(F, f, il, 5, beta, dt, dxflux2);
-        cpml<MODE>(F, f, il, 2, beta, dt, dxby);
-        cpml<MODE>(F, f, il, 3, beta, dt, dxbz);
-      }
-      if (j < S.yb.np || j >= ny - S.yt.np) {
-        const bool bot = j < S.yb.np;
-        const FaceDev &F = bot ? S.yb : S.yt;
-        const int jl = bot ? j : j - (ny - S.yt.np);
-        const long long f = i + (long long)nx * (jl + (long long)F.np * k);
-        cpml<MODE>(F, f, jl, 1, beta, dt, gpy);
-        cpml<MODE>(F, f, jl, 0, beta, dt, dvydy);
-        cpml<MODE>(F, f, jl, 4, beta, dt, dyflux3);
-        cpml<MODE>(F, f, jl, 5, beta, dt, dyflux1);
-        cpml<MODE>(F, f, jl, 2, beta, dt, dybx);
-        cpml<MODE>(F, f, jl, 3, beta, dt, dybz);
-      }
-    }
-    // RHS algebra, RHS.f90:548-645
-    const double rho = tv[0], vx = tv[1], vy = tv[2], vz = tv[3], p = tv[4],
-                 bx = tv[5], by = tv[6], bz = tv[7];
-    const double red = __ldg(S.red + id);
-    const double ox = __ldg(S.box + id), oy = __ldg(S.boy + id),
-                 oz = __ldg(S.boz + id);
-    double R[8];
-    R[5] = red * (dyflux3 - dzflux2);
-    R[6] = red * (dzflux1 - dxflux3);
-    R[7] = red * (dxflux2 - dyflux1);
-    const double div = dvxdx + dvydy + dvzdz;
-    const double cbx = dybz - dzby, cby = -dxbz + dzbx, cbz = dxby - dybx;
-    const double sg = __ldg(S.sponge + id), r0 = __ldg(S.rho0 + id);
-    R[0] = -__ldg(S.grx + id) * vx - __ldg(S.gry + id) * vy -
-           __ldg(S.grz + id) * vz - r0 * div - sg * rho;
-    R[4] = -__ldg(S.c2rho0 + id) * div - vx * __ldg(S.gpx + id) -
-           vy * __ldg(S.gpy + id) - vz * __ldg(S.gpz + id) - sg * p;
-    const double c1 = cby * oz - cbz * oy, c2 = ox * cbz - cbx * oz,
-                 c3 = cbx * oy - cby * ox;
-    const double ri = __ldg(S.rhoinv + id);
-    double vxr = -ri * (gpx - (c1 * red)) - sg * vx;
-    double vyr = -ri * (gpy - (c2 * red)) - sg * vy;
-    double vzr = -ri * (gpz - (c3 * red)) - sg * vz;
-    const double qx = __ldg(S.cbx + id), qy = __ldg(S.cby + id),
-                 qz = __ldg(S.cbz + id);
-    const double d1 = qy * bz - qz * by, d2 = bx * qz - qx * bz,
-                 d3 = qx * by - qy * bx;
-    vxr = vxr + ri * d1 * red;
-    vyr = vyr + ri * d2 * red;
-    vzr = vzr + ri * d3 * red;
-    vzr = vzr - ri * rho * __ldg(S.gblk + (long long)gc * nz + k);
-    R[1] = vxr;
-    R[2] = vyr;
-    R[3] = vzr;
-    if (S.frc.kind != SPARC_SRC_NONE) {
-      const double frc = forcing_at(S, it, Tp, i, j, k);
-      if (S.frc.dir == 1) R[1] = R[1] + frc;
-      else if (S.frc.dir == 2) R[2] = R[2] + frc;
-      else R[3] = R[3] + frc;
-    }
-    const bool zero = k == 0 || k == nz - 1 ||
-                      (!per && (i == 0 || i == nx - 1 || j == 0 || j == ny - 1));
-    if (MODE == LAST) {
-      double an[8];
-#pragma unroll
-      for (int l = 0; l < 8; ++l) {
-        an[l] = zero ? av[l] : av[l] + dt * R[l];
-        so[l * N + id] = an[l];
-      }
-      const double p0v = __ldg(S.p0 + id);
-      double m = (r0 + an[0]) * (an[1] * an[1] + an[2] * an[2] + an[3] * an[3]) / 2.0;
-      ke += m * m;
-      mr = fmin(mr, rho + r0);
-      mp = fmin(mp, p + p0v);
-    } else {
-#pragma unroll
-      for (int l = 0; l < 8; ++l) so[l * N + id] = zero ? av[l] : av[l] + bnext * R[l];
-    }
-  }
-  if (MODE == LAST) diag_reduce(S, ke, mr, mp);
-}
-
 // ------------------------------------ MP_MHD_3D, pipelined stage kernel
-// Same arithmetic as k_stage_mhd, restructured for HBM bandwidth: every
+// Shared-memory layout of the pipelined MHD kernels: every
 // array a layer needs is copied into shared memory with cp.async one layer
 // ahead (double buffer), so the loads of layer k+1 stream while layer k is
 // computed.  Per buffer: 10 halo slots over the cross-shaped tile (stage
@@ -643,276 +412,6 @@ __device__ __forceinline__ void cp_wait1() {
   asm volatile("cp.async.wait_group 1;\n" ::: "memory");
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(pipe::NT, 1)
-    k_stage_mhd_pipe(const SimDev S, const double *__restrict__ a,
-                     const double *__restrict__ tin, double *__restrict__ so,
-                     double beta, double bnext, int zchunk) {
-  using namespace pipe;
-  extern __shared__ double smem[];
-  __shared__ const double *optr[NO];
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  const int nx = S.nx, ny = S.ny, nz = S.nz;
-  const long long N = S.N, NXY = (long long)nx * ny;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-  const int i = x0 + tx, j = y0 + ty;
-  const bool act = i < nx && j < ny;
-  const bool per = S.periodic;
-  const int k0 = blockIdx.z * zchunk, k1 = min(nz, k0 + zchunk);
-  const long long col = (long long)j * nx + i;
-  const long long it = *S.iter;
-  const double Tp = pulse_time(S, it);
-  const double dt = S.deltat;
-  const int gc = act ? S.colx[i] + S.bxdim * S.coly[j] : 0;
-  const int xo = tile_origin(x0, TX, nx, per), yo = tile_origin(y0, TY, ny, per);
-  const int cx0 = x0 - xo, cy0 = y0 - yo;
-  const int ry = cy0 + ty, rx = cx0 + tx;
-  const bool vec2 = (nx & 1) == 0;
-  if (tid == 0) {
-    optr[O_RHO] = tin;
-    for (int l = 0; l < 8; ++l) optr[O_A + l] = a + l * N;
-    optr[O_BG + B_RED] = S.red;    optr[O_BG + B_SPONGE] = S.sponge;
-    optr[O_BG + B_RHO0] = S.rho0;  optr[O_BG + B_GRX] = S.grx;
-    optr[O_BG + B_GRY] = S.gry;    optr[O_BG + B_GRZ] = S.grz;
-    optr[O_BG + B_C2R] = S.c2rho0; optr[O_BG + B_GPX] = S.gpx;
-    optr[O_BG + B_GPY] = S.gpy;    optr[O_BG + B_GPZ] = S.gpz;
-    optr[O_BG + B_RHOINV] = S.rhoinv;
-    optr[O_BG + B_CBX] = S.cbx;    optr[O_BG + B_CBY] = S.cby;
-    optr[O_BG + B_CBZ] = S.cbz;
-    optr[O_P0] = S.p0;
-  }
-  __syncthreads();
-  auto H = [&](int b, int slot, int ly, int lx) -> double & {
-    return smem[(size_t)b * BUF + ((size_t)slot * HY + ly) * HX + lx];
-  };
-  auto O = [&](int b, int slot, int r, int c) -> double & {
-    return smem[(size_t)b * BUF + NH * HS + ((size_t)slot * TY + r) * TX + c];
-  };
-  auto own_active = [&](int slot) -> bool {
-    if (slot >= O_A && slot < O_BG) return MODE != FIRST;
-    if (slot == O_P0) return MODE == LAST;
-    return true;
-  };
-  // issue the copies of layer k into buffer b (one commit group)
-  auto issue = [&](int k, int b) {
-    const long long kb = (long long)k * NXY;
-    for (int t = tid; t < HS; t += NT) {
-      const int ly = t / HX, lx = t - ly * HX;
-      const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
-      if (!inx && !iny) continue;
-      int gx = xo + lx, gy = yo + ly;
-      if (per) {
-        gx = wrapi(gx, nx);
-        gy = wrapi(gy, ny);
-      } else if (gx < 0 || gx >= nx || gy < 0 || gy >= ny) {
-        continue;  // never read: one-sided stencils stay inside the domain
-      }
-      const long long id = kb + (long long)gy * nx + gx;
-#pragma unroll
-      for (int sl = 0; sl < 7; ++sl) cp_async8(&H(b, sl, ly, lx), tin + (sl + 1) * N + id);
-      cp_async8(&H(b, 7, ly, lx), S.box + id);
-      cp_async8(&H(b, 8, ly, lx), S.boy + id);
-      cp_async8(&H(b, 9, ly, lx), S.boz + id);
-    }
-    if (vec2) {
-      constexpr int PAIRS = TY * TX / 2;
-      for (int t = tid; t < NO * PAIRS; t += NT) {
-        const int slot = t / PAIRS, rem = t - slot * PAIRS;
-        if (!own_active(slot)) continue;
-        const int r = rem / (TX / 2), c = 2 * (rem - r * (TX / 2));
-        const int gx = x0 + c, gy = y0 + r;
-        if (gx >= nx || gy >= ny) continue;
-        cp_async16(&O(b, slot, r, c), optr[slot] + kb + (long long)gy * nx + gx);
-      }
-    } else {
-      for (int t = tid; t < NO * TY * TX; t += NT) {
-        const int slot = t / (TY * TX), rem = t - slot * (TY * TX);
-        if (!own_active(slot)) continue;
-        const int r = rem / TX, c = rem - r * TX;
-        const int gx = x0 + c, gy = y0 + r;
-        if (gx >= nx || gy >= ny) continue;
-        cp_async8(&O(b, slot, r, c), optr[slot] + kb + (long long)gy * nx + gx);
-      }
-    }
-    cp_commit();
-  };
-
-  // z windows: vz, p, flux1, flux2, bx, by (own column)
-  double w_vz[11], w_p[11], w_f1[11], w_f2[11], w_bx[11], w_by[11];
-  auto head = [&](int kk, double &vz_, double &p_, double &f1_, double &f2_,
-                  double &bx_, double &by_) {
-    const long long id = (long long)kk * NXY + col;
-    const double vx_ = __ldg(tin + N + id), vy_ = __ldg(tin + 2 * N + id);
-    vz_ = __ldg(tin + 3 * N + id);
-    p_ = __ldg(tin + 4 * N + id);
-    bx_ = __ldg(tin + 5 * N + id);
-    by_ = __ldg(tin + 6 * N + id);
-    const double ox = __ldg(S.box + id), oy = __ldg(S.boy + id),
-                 oz = __ldg(S.boz + id);
-    f1_ = -vz_ * oy + vy_ * oz;
-    f2_ = -vx_ * oz + vz_ * ox;
-  };
-  issue(k0, 0);
-  const int b0 = min(k0 - 5, nz - 11);
-#pragma unroll
-  for (int m = 0; m < 11; ++m) {
-    const int kk = b0 + m;
-    if (act && kk >= 0) {
-      head(kk, w_vz[m], w_p[m], w_f1[m], w_f2[m], w_bx[m], w_by[m]);
-    } else {
-      w_vz[m] = w_p[m] = w_f1[m] = w_f2[m] = w_bx[m] = w_by[m] = 0.0;
-    }
-  }
-  double h0 = 0, h1 = 0, h2 = 0, h3 = 0, h4 = 0, h5 = 0;  // next window head
-  double ke = 0.0, mr = 1e300, mp = 1e300;
-
-  for (int k = k0; k < k1; ++k) {
-    const int b = (k - k0) & 1;
-    if (k > k0 && k <= nz - 6) {
-      shift(w_vz, h0); shift(w_p, h1); shift(w_f1, h2);
-      shift(w_f2, h3); shift(w_bx, h4); shift(w_by, h5);
-    }
-    if (k + 1 < k1) issue(k + 1, b ^ 1);
-    else cp_commit();  // keep one group per iteration
-    cp_wait1();
-    __syncthreads();
-    // own B0, then flux1..3 over the cross tile in place of B0
-    const double ox = H(b, 7, ry, rx), oy = H(b, 8, ry, rx), oz = H(b, 9, ry, rx);
-    __syncthreads();
-    for (int t = tid; t < HS; t += NT) {
-      const int ly = t / HX, lx = t - ly * HX;
-      const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
-      if (!inx && !iny) continue;
-      const double vx_ = H(b, 0, ly, lx), vy_ = H(b, 1, ly, lx), vz_ = H(b, 2, ly, lx);
-      const double bx0 = H(b, 7, ly, lx), by0 = H(b, 8, ly, lx), bz0 = H(b, 9, ly, lx);
-      H(b, 7, ly, lx) = -vz_ * by0 + vy_ * bz0;   // flux1
-      H(b, 8, ly, lx) = -vx_ * bz0 + vz_ * bx0;   // flux2
-      H(b, 9, ly, lx) = -vy_ * bx0 + vx_ * by0;   // flux3
-    }
-    __syncthreads();
-    if (act) {
-      const long long kb = (long long)k * NXY;
-      const long long id = kb + col;
-      double tv[8], av[8];
-      tv[0] = O(b, O_RHO, ty, tx);
-#pragma unroll
-      for (int l = 1; l < 8; ++l) tv[l] = H(b, l - 1, ry, rx);
-#pragma unroll
-      for (int l = 0; l < 8; ++l) av[l] = MODE == FIRST ? tv[l] : O(b, O_A + l, ty, tx);
-      auto DX = [&](int slot) {
-        return dxy(i, nx, per, S.stretchx, [&](int g) { return H(b, slot, ry, g - xo); });
-      };
-      auto DY = [&](int slot) {
-        return dxy(j, ny, per, S.stretchy, [&](int g) { return H(b, slot, g - yo, rx); });
-      };
-      // halo slots: 0 vx, 1 vy, 2 vz, 3 p, 4 bx, 5 by, 6 bz, 7-9 flux1..3
-      double dvxdx = DX(0), dxflux3 = DX(9), gpx = DX(3), dxflux2 = DX(8),
-             dxby = DX(5), dxbz = DX(6);
-      double dvydy = DY(1), gpy = DY(3), dyflux3 = DY(9), dybz = DY(6),
-             dybx = DY(4), dyflux1 = DY(7);
-      const double szk = __ldg(S.stretch + k);
-      double dvzdz = dz(w_vz, k, nz, szk), dzflux1 = dz(w_f1, k, nz, szk),
-             dzflux2 = dz(w_f2, k, nz, szk), dzbx = dz(w_bx, k, nz, szk),
-             gpz = dz(w_p, k, nz, szk), dzby = dz(w_by, k, nz, szk);
-      if (S.zb.on && (k < S.zb.np || k >= nz - S.zt.np)) {
-        const bool bot = k < S.zb.np;
-        const FaceDev &F = bot ? S.zb : S.zt;
-        const int kl = bot ? k : k - (nz - S.zt.np);
-        const long long f = (long long)kl * NXY + col;
-        cpml<MODE>(F, f, kl, 1, beta, dt, gpz);
-        cpml<MODE>(F, f, kl, 0, beta, dt, dvzdz);
-        cpml<MODE>(F, f, kl, 4, beta, dt, dzflux2);
-        cpml<MODE>(F, f, kl, 5, beta, dt, dzflux1);
-        cpml<MODE>(F, f, kl, 2, beta, dt, dzbx);
-        cpml<MODE>(F, f, kl, 3, beta, dt, dzby);
-      }
-      if (S.xb.on) {
-        if (i < S.xb.np || i >= nx - S.xt.np) {
-          const bool bot = i < S.xb.np;
-          const FaceDev &F = bot ? S.xb : S.xt;
-          const int il = bot ? i : i - (nx - S.xt.np);
-          const long long f = il + (long long)F.np * (j + (long long)ny * k);
-          cpml<MODE>(F, f, il, 1, beta, dt, gpx);
-          cpml<MODE>(F, f, il, 0, beta, dt, dvxdx);
-          cpml<MODE>(F, f, il, 4, beta, dt, dxflux3);
-          cpml<MODE>(F, f, il, 5, beta, dt, dxflux2);
-          cpml<MODE>(F, f, il, 2, beta, dt, dxby);
-          cpml<MODE>(F, f, il, 3, beta, dt, dxbz);
-        }
-        if (j < S.yb.np || j >= ny - S.yt.np) {
-          const bool bot = j < S.yb.np;
-          const FaceDev &F = bot ? S.yb : S.yt;
-          const int jl = bot ? j : j - (ny - S.yt.np);
-          const long long f = i + (long long)nx * (jl + (long long)F.np * k);
-          cpml<MODE>(F, f, jl, 1, beta, dt, gpy);
-          cpml<MODE>(F, f, jl, 0, beta, dt, dvydy);
-          cpml<MODE>(F, f, jl, 4, beta, dt, dyflux3);
-          cpml<MODE>(F, f, jl, 5, beta, dt, dyflux1);
-          cpml<MODE>(F, f, jl, 2, beta, dt, dybx);
-          cpml<MODE>(F, f, jl, 3, beta, dt, dybz);
-        }
-      }
-      const double rho = tv[0], vx = tv[1], vy = tv[2], vz = tv[3], p = tv[4],
-                   bx = tv[5], by = tv[6], bz = tv[7];
-      auto BG = [&](int n) { return O(b, O_BG + n, ty, tx); };
-      const double red = BG(B_RED);
-      double R[8];
-      R[5] = red * (dyflux3 - dzflux2);
-      R[6] = red * (dzflux1 - dxflux3);
-      R[7] = red * (dxflux2 - dyflux1);
-      const double div = dvxdx + dvydy + dvzdz;
-      const double cbx = dybz - dzby, cby = -dxbz + dzbx, cbz = dxby - dybx;
-      const double sg = BG(B_SPONGE), r0 = BG(B_RHO0);
-      R[0] = -BG(B_GRX) * vx - BG(B_GRY) * vy - BG(B_GRZ) * vz - r0 * div - sg * rho;
-      R[4] = -BG(B_C2R) * div - vx * BG(B_GPX) - vy * BG(B_GPY) - vz * BG(B_GPZ) - sg * p;
-      const double c1 = cby * oz - cbz * oy, c2 = ox * cbz - cbx * oz,
-                   c3 = cbx * oy - cby * ox;
-      const double ri = BG(B_RHOINV);
-      double vxr = -ri * (gpx - (c1 * red)) - sg * vx;
-      double vyr = -ri * (gpy - (c2 * red)) - sg * vy;
-      double vzr = -ri * (gpz - (c3 * red)) - sg * vz;
-      const double qx = BG(B_CBX), qy = BG(B_CBY), qz = BG(B_CBZ);
-      const double d1 = qy * bz - qz * by, d2 = bx * qz - qx * bz,
-                   d3 = qx * by - qy * bx;
-      vxr = vxr + ri * d1 * red;
-      vyr = vyr + ri * d2 * red;
-      vzr = vzr + ri * d3 * red;
-      vzr = vzr - ri * rho * __ldg(S.gblk + (long long)gc * nz + k);
-      R[1] = vxr;
-      R[2] = vyr;
-      R[3] = vzr;
-      if (S.frc.kind != SPARC_SRC_NONE) {
-        const double frc = forcing_at(S, it, Tp, i, j, k);
-        if (S.frc.dir == 1) R[1] = R[1] + frc;
-        else if (S.frc.dir == 2) R[2] = R[2] + frc;
-        else R[3] = R[3] + frc;
-      }
-      const bool zero = k == 0 || k == nz - 1 ||
-                        (!per && (i == 0 || i == nx - 1 || j == 0 || j == ny - 1));
-      if (MODE == LAST) {
-        double an[8];
-#pragma unroll
-        for (int l = 0; l < 8; ++l) {
-          an[l] = zero ? av[l] : av[l] + dt * R[l];
-          so[l * N + id] = an[l];
-        }
-        const double p0v = O(b, O_P0, ty, tx);
-        double m = (r0 + an[0]) * (an[1] * an[1] + an[2] * an[2] + an[3] * an[3]) / 2.0;
-        ke += m * m;
-        mr = fmin(mr, rho + r0);
-        mp = fmin(mp, p + p0v);
-      } else {
-#pragma unroll
-        for (int l = 0; l < 8; ++l) so[l * N + id] = zero ? av[l] : av[l] + bnext * R[l];
-      }
-    }
-    // next window head (layer k+6), consumed at the start of iteration k+1
-    if (act && k + 1 < k1 && k + 1 <= nz - 6) head(k + 6, h0, h1, h2, h3, h4, h5);
-    __syncthreads();  // buffer b is refilled by the issue of iteration k+1
-  }
-  if (MODE == LAST) diag_reduce(S, ke, mr, mp);
-}
-
 // ------------------------- MP_MHD_3D, two-role pipelined stage kernel
 // The pipelined layer tiles of k_stage_mhd_pipe, with each column served by
 // two warps-groups (threadIdx.z = role) so that a thread holds only three
@@ -923,7 +422,8 @@ __global__ void __launch_bounds__(pipe::NT, 1)
 //           flux1, flux2, by; derivatives dvxdx dvydy dxflux3 dxflux2
 //           dyflux3 dyflux1 dzflux1 dzflux2 dzby
 // dvzdz and dzby cross over through shared memory after their CPML
-// corrections.  Arithmetic and summation order equal k_stage_mhd's.
+// corrections.  Arithmetic and summation order follow RHS.f90 as in the
+// oracle (11-tap sums from the first tap, operand order of each term).
 namespace duo {
 constexpr int TX = 32, TY = 8, NC = TX * TY, NT = 2 * NC;
 constexpr int HX = TX + 10, HY = TY + 10, HS = HX * HY;
@@ -1253,14 +753,19 @@ struct TmaSet {
 };
 
 namespace tmak {
-constexpr int TX = 32, TY = 8, NC = TX * TY, NT = 2 * NC;
-constexpr int HX = TX + 10, HY = TY + 10, HS = HX * HY;
-constexpr int NH = 10, NO = 24;
-constexpr int BUF = ((NO * NC + NH * HS) + 15) / 16 * 16;  // 128-B multiple
-constexpr int XCH = 3 * NC;
-constexpr size_t SMEM = (2 * (size_t)BUF + XCH) * sizeof(double) + 128;  // + align slack
 constexpr long long WAIT_LIMIT = 1LL << 26;
 }  // namespace tmak
+// geometry of the TMA kernel for a tile height TY (tile 32 x TY columns,
+// two roles -> 64*TY threads)
+template <int TY_>
+struct TmaGeo {
+  static constexpr int TX = 32, TY = TY_, NC = TX * TY, NT = 2 * NC;
+  static constexpr int HX = TX + 10, HY = TY + 10, HS = HX * HY;
+  static constexpr int NH = 10, NO = 24;
+  static constexpr int BUF = ((NO * NC + NH * HS) + 15) / 16 * 16;  // 128-B multiple
+  static constexpr int XCH = 3 * NC;
+  static constexpr size_t SMEM = (2 * (size_t)BUF + XCH) * sizeof(double) + 128;
+};
 
 __device__ __forceinline__ unsigned sm_addr(const void *p) {
   return (unsigned)__cvta_generic_to_shared(p);
@@ -1309,13 +814,16 @@ __device__ __forceinline__ double csum(const double *p, int st) {
   return s;
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(tmak::NT, 1)
+template <int MODE, int TYV>
+__global__ void __launch_bounds__(TmaGeo<TYV>::NT, 1)
     k_stage_mhd_tma(const SimDev S, const __grid_constant__ TmaSet T,
                     const double *__restrict__ a, const double *__restrict__ tin,
                     double *__restrict__ so, double beta, double bnext,
                     int zchunk, int mt, int ma) {
-  using namespace tmak;
+  // 32-bit indexing throughout (the launcher checks V*N < 2^31)
+  using G = TmaGeo<TYV>;
+  constexpr int TX = G::TX, TY = G::TY, NC = G::NC, NT = G::NT, HX = G::HX,
+                HS = G::HS, NO = G::NO, BUF = G::BUF;
   using pipe::O_RHO;
   using pipe::O_A;
   using pipe::O_BG;
@@ -1324,42 +832,36 @@ __global__ void __launch_bounds__(tmak::NT, 1)
   __shared__ unsigned long long bar[2];
   const int tx = threadIdx.x, ty = threadIdx.y, role = threadIdx.z;
   const int tid = (role * TY + ty) * TX + tx, cid = ty * TX + tx;
-  // TMA destinations must be 128-byte aligned: align the base explicitly
   double *smem = (double *)(((size_t)smem_raw + 127) & ~(size_t)127);
-  if (sm_addr(smem) & 127u) {  // cannot happen after the rounding; never issue TMA then
+  if (sm_addr(smem) & 127u) {
     if (tid == 0) atomicExch(S.err, 2);
     return;
   }
   const int nx = S.nx, ny = S.ny, nz = S.nz;
-  const long long N = S.N, NXY = (long long)nx * ny;
+  const int N = (int)S.N, NXY = nx * ny;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   const int i = x0 + tx, j = y0 + ty;
   const bool act = i < nx && j < ny;
   const bool per = S.periodic;
   const int k0 = blockIdx.z * zchunk, k1 = min(nz, k0 + zchunk);
-  const long long col = (long long)j * nx + i;
-  const long long it = *S.iter;
-  const double dt = S.deltat;
+  const int col = j * nx + i;
   const int xo = tile_origin(x0, TX, nx, per), yo = tile_origin(y0, TY, ny, per);
-  const int cx0 = x0 - xo, cy0 = y0 - yo;
-  const int ry = cy0 + ty, rx = cx0 + tx;
-  const bool xint = per || (i >= 5 && i < nx - 5);
-  const bool yint = per || (j >= 5 && j < ny - 5);
+  const int ry = y0 - yo + ty, rx = x0 - xo + tx;
+  const int own = ry * HX + rx;
   if (tid == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  // buffer b: own slots at b*BUF, halo slots after them
-  auto O = [&](int b, int slot) -> double & { return smem[b * BUF + slot * NC + cid]; };
+  auto O = [&](int b, int slot) -> double { return smem[b * BUF + slot * NC + cid]; };
   auto Hp = [&](int b, int slot) -> double * { return smem + b * BUF + NO * NC + slot * HS; };
   double *X = smem + 2 * BUF;
-  // halo positions of this thread (layer independent)
-  int hs0 = -1, hs1 = -1;
-  long long ho0 = 0, ho1 = 0;
+  // this thread's halo positions (smem index, global xy offset), or -1
+  int hs0 = -1, hs1 = -1, ho0 = 0, ho1 = 0;
   {
-    auto pos = [&](int t, int &hs, long long &ho) {
+    const int cx0 = x0 - xo, cy0 = y0 - yo;
+    auto pos = [&](int t, int &hs, int &ho) {
       if (t >= HS) return;
       const int ly = t / HX, lx = t - ly * HX;
       const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
@@ -1372,7 +874,7 @@ __global__ void __launch_bounds__(tmak::NT, 1)
         return;
       }
       hs = t;
-      ho = (long long)gy * nx + gx;
+      ho = gy * nx + gx;
     };
     pos(tid, hs0, ho0);
     pos(tid + NT, hs1, ho1);
@@ -1380,10 +882,10 @@ __global__ void __launch_bounds__(tmak::NT, 1)
   const unsigned own_bytes =
       (MODE == FIRST ? 15u : (MODE == MID ? 23u : 24u)) * NC * (unsigned)sizeof(double);
   auto issue = [&](int k, int b) {
-    const long long kb = (long long)k * NXY;
+    const int kb = k * NXY;
     if (hs0 >= 0) {
       double *h = Hp(b, 0) + hs0;
-      const long long id = kb + ho0;
+      const int id = kb + ho0;
 #pragma unroll
       for (int sl = 0; sl < 7; ++sl) cp_async8(h + sl * HS, tin + (sl + 1) * N + id);
       cp_async8(h + 7 * HS, S.box + id);
@@ -1392,7 +894,7 @@ __global__ void __launch_bounds__(tmak::NT, 1)
     }
     if (hs1 >= 0) {
       double *h = Hp(b, 0) + hs1;
-      const long long id = kb + ho1;
+      const int id = kb + ho1;
 #pragma unroll
       for (int sl = 0; sl < 7; ++sl) cp_async8(h + sl * HS, tin + (sl + 1) * N + id);
       cp_async8(h + 7 * HS, S.box + id);
@@ -1413,10 +915,10 @@ __global__ void __launch_bounds__(tmak::NT, 1)
       if (MODE == LAST) tma_load_3d(ob + O_P0 * NC, &T.m[17], x0, y0, k, &bar[b]);
     }
   };
-
+  // role 0 windows vz, p, bx; role 1 windows flux1, flux2, by
   double w0[11], w1[11], w2[11];
   auto head = [&](int kk, double &v0, double &v1, double &v2) {
-    const long long id = (long long)kk * NXY + col;
+    const int id = kk * NXY + col;
     if (role == 0) {
       v0 = __ldg(tin + 3 * N + id);
       v1 = __ldg(tin + 4 * N + id);
@@ -1432,36 +934,37 @@ __global__ void __launch_bounds__(tmak::NT, 1)
     }
   };
   issue(k0, 0);
-  const int b0 = min(k0 - 5, nz - 11);
+  {
+    const int b0 = min(k0 - 5, nz - 11);
 #pragma unroll
-  for (int m = 0; m < 11; ++m) {
-    const int kk = b0 + m;
-    if (act && kk >= 0) head(kk, w0[m], w1[m], w2[m]);
-    else w0[m] = w1[m] = w2[m] = 0.0;
+    for (int m = 0; m < 11; ++m) {
+      const int kk = b0 + m;
+      if (act && kk >= 0) head(kk, w0[m], w1[m], w2[m]);
+      else w0[m] = w1[m] = w2[m] = 0.0;
+    }
   }
-  double h0 = 0, h1 = 0, h2 = 0;
   double ke = 0.0, mr = 1e300, mp = 1e300;
-  unsigned phase = 0;  // bit b: parity of buffer b's next completion
+  unsigned phase = 0;
   bool ok = true;
 
-  for (int k = k0; k < k1 && ok; ++k) {
+  for (int k = k0; k < k1; ++k) {
     const int b = (k - k0) & 1;
-    if (k > k0 && k <= nz - 6) {
-      shift(w0, h0); shift(w1, h1); shift(w2, h2);
-    }
+    double h0 = 0, h1 = 0, h2 = 0;
+    const bool sh = k > k0 && k <= nz - 6;
+    if (sh && act) head(k + 5, h0, h1, h2);   // in flight during the waits
     if (k + 1 < k1) issue(k + 1, b ^ 1);
     else cp_commit();
     cp_wait1();
     ok = mbar_wait(&bar[b], (phase >> b) & 1u, S.err);
     phase ^= 1u << b;
-    __syncthreads();
     if (!__syncthreads_and(ok)) { ok = false; break; }
+    if (sh) { shift(w0, h0); shift(w1, h1); shift(w2, h2); }
     double *H7 = Hp(b, 7), *H8 = Hp(b, 8), *H9 = Hp(b, 9);
-    const int own = ry * HX + rx;
     const double ox = H7[own], oy = H8[own], oz = H9[own];
     __syncthreads();
     {
       const double *H0 = Hp(b, 0), *H1 = Hp(b, 1), *H2 = Hp(b, 2);
+      const int cx0 = x0 - xo, cy0 = y0 - yo;
       for (int t = tid; t < HS; t += NT) {
         const int ly = t / HX, lx = t - ly * HX;
         const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
@@ -1474,36 +977,42 @@ __global__ void __launch_bounds__(tmak::NT, 1)
       }
     }
     __syncthreads();
-    const long long id = (long long)k * NXY + col;
+    const int id = k * NXY + col;
     const double szk = __ldg(S.stretch + k);
-    // x and y derivatives of halo slot `slot` at this thread's column
+    const double dt = S.deltat;
     auto DX = [&](int slot) {
       const double *row = Hp(b, slot) + ry * HX;
-      if (xint) return S.stretchx * csum(row + (i - 5 - xo), 1);
+      if (per || (i >= 5 && i < nx - 5)) return S.stretchx * csum(row + (i - 5 - xo), 1);
       return dxy(i, nx, per, S.stretchx, [&](int g) { return row[g - xo]; });
     };
     auto DY = [&](int slot) {
       const double *colp = Hp(b, slot) + rx;
-      if (yint) return S.stretchy * csum(colp + (j - 5 - yo) * HX, HX);
+      if (per || (j >= 5 && j < ny - 5)) return S.stretchy * csum(colp + (j - 5 - yo) * HX, HX);
       return dxy(j, ny, per, S.stretchy, [&](int g) { return colp[(g - yo) * HX]; });
     };
     const bool zpml = S.zb.on && (k < S.zb.np || k >= nz - S.zt.np);
-    const bool zbot = k < S.zb.np;
-    const FaceDev &FZ = zbot ? S.zb : S.zt;
-    const int kl = zbot ? k : k - (nz - S.zt.np);
-    const long long fz = (long long)kl * NXY + col;
     const bool xpml = S.xb.on && act && (i < S.xb.np || i >= nx - S.xt.np);
-    const bool xbot = i < S.xb.np;
-    const FaceDev &FX = xbot ? S.xb : S.xt;
-    const int il = xbot ? i : i - (nx - S.xt.np);
-    const long long fx = il + (long long)FX.np * (j + (long long)ny * k);
     const bool ypml = S.xb.on && act && (j < S.yb.np || j >= ny - S.yt.np);
-    const bool ybot = j < S.yb.np;
-    const FaceDev &FY = ybot ? S.yb : S.yt;
-    const int jl = ybot ? j : j - (ny - S.yt.np);
-    const long long fy = i + (long long)nx * (jl + (long long)FY.np * k);
-    const bool zero = k == 0 || k == nz - 1 ||
-                      (!per && (i == 0 || i == nx - 1 || j == 0 || j == ny - 1));
+    // CPML correction of derivative d with auxiliary slot `slot` on the
+    // z, x or y face this point lies in (RHS.f90:424-546)
+    auto pz = [&](int slot, double &d) {
+      const bool bot = k < S.zb.np;
+      const FaceDev &F = bot ? S.zb : S.zt;
+      const int kl = bot ? k : k - (nz - S.zt.np);
+      cpml<MODE>(F, (long long)kl * NXY + col, kl, slot, beta, dt, d);
+    };
+    auto px = [&](int slot, double &d) {
+      const bool bot = i < S.xb.np;
+      const FaceDev &F = bot ? S.xb : S.xt;
+      const int il = bot ? i : i - (nx - S.xt.np);
+      cpml<MODE>(F, il + (long long)F.np * (j + (long long)ny * k), il, slot, beta, dt, d);
+    };
+    auto py = [&](int slot, double &d) {
+      const bool bot = j < S.yb.np;
+      const FaceDev &F = bot ? S.yb : S.yt;
+      const int jl = bot ? j : j - (ny - S.yt.np);
+      cpml<MODE>(F, i + (long long)nx * (jl + (long long)F.np * k), jl, slot, beta, dt, d);
+    };
     auto Hv = [&](int slot) { return Hp(b, slot)[own]; };
     double d0 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0, d6 = 0, d7 = 0, d8 = 0;
     if (act) {
@@ -1511,51 +1020,29 @@ __global__ void __launch_bounds__(tmak::NT, 1)
         d0 = DX(3); d5 = DX(6); d7 = DX(5);
         d1 = DY(3); d4 = DY(6); d8 = DY(4);
         d3 = dz(w0, k, nz, szk); d2 = dz(w1, k, nz, szk); d6 = dz(w2, k, nz, szk);
-        if (zpml) {
-          cpml<MODE>(FZ, fz, kl, 1, beta, dt, d2);
-          cpml<MODE>(FZ, fz, kl, 0, beta, dt, d3);
-          cpml<MODE>(FZ, fz, kl, 2, beta, dt, d6);
-        }
-        if (xpml) {
-          cpml<MODE>(FX, fx, il, 1, beta, dt, d0);
-          cpml<MODE>(FX, fx, il, 3, beta, dt, d5);
-          cpml<MODE>(FX, fx, il, 2, beta, dt, d7);
-        }
-        if (ypml) {
-          cpml<MODE>(FY, fy, jl, 1, beta, dt, d1);
-          cpml<MODE>(FY, fy, jl, 3, beta, dt, d4);
-          cpml<MODE>(FY, fy, jl, 2, beta, dt, d8);
-        }
+        if (zpml) { pz(1, d2); pz(0, d3); pz(2, d6); }
+        if (xpml) { px(1, d0); px(3, d5); px(2, d7); }
+        if (ypml) { py(1, d1); py(3, d4); py(2, d8); }
         X[cid] = d3;
       } else {
         d0 = DX(0); d2 = DX(9); d3 = DX(8);
         d1 = DY(1); d4 = DY(9); d5 = DY(7);
         d6 = dz(w0, k, nz, szk); d7 = dz(w1, k, nz, szk); d8 = dz(w2, k, nz, szk);
-        if (zpml) {
-          cpml<MODE>(FZ, fz, kl, 4, beta, dt, d7);
-          cpml<MODE>(FZ, fz, kl, 5, beta, dt, d6);
-          cpml<MODE>(FZ, fz, kl, 3, beta, dt, d8);
-        }
-        if (xpml) {
-          cpml<MODE>(FX, fx, il, 0, beta, dt, d0);
-          cpml<MODE>(FX, fx, il, 4, beta, dt, d2);
-          cpml<MODE>(FX, fx, il, 5, beta, dt, d3);
-        }
-        if (ypml) {
-          cpml<MODE>(FY, fy, jl, 0, beta, dt, d1);
-          cpml<MODE>(FY, fy, jl, 4, beta, dt, d4);
-          cpml<MODE>(FY, fy, jl, 5, beta, dt, d5);
-        }
+        if (zpml) { pz(4, d7); pz(5, d6); pz(3, d8); }
+        if (xpml) { px(0, d0); px(4, d2); px(5, d3); }
+        if (ypml) { py(0, d1); py(4, d4); py(5, d5); }
         X[NC + cid] = d8;
       }
     }
     __syncthreads();
     double an_rho = 0.0;
     if (act) {
+      const bool zero = k == 0 || k == nz - 1 ||
+                        (!per && (i == 0 || i == nx - 1 || j == 0 || j == ny - 1));
+      const double fac = MODE == LAST ? dt : bnext;
       const double rho = O(b, O_RHO), vx = Hv(0), vy = Hv(1), vz = Hv(2);
       const double red = O(b, O_BG + pipe::B_RED), sg = O(b, O_BG + pipe::B_SPONGE);
       if (role == 0) {
-        const double bx = Hv(4), by = Hv(5), bz = Hv(6);
         const double dzby = X[NC + cid];
         const double cbx = d4 - dzby, cby = -d5 + d6, cbz = d7 - d8;
         const double c1 = cby * oz - cbz * oy, c2 = ox * cbz - cbx * oz,
@@ -1564,6 +1051,7 @@ __global__ void __launch_bounds__(tmak::NT, 1)
         double vxr = -ri * (d0 - (c1 * red)) - sg * vx;
         double vyr = -ri * (d1 - (c2 * red)) - sg * vy;
         double vzr = -ri * (d2 - (c3 * red)) - sg * vz;
+        const double bx = Hv(4), by = Hv(5), bz = Hv(6);
         const double qx = O(b, O_BG + pipe::B_CBX), qy = O(b, O_BG + pipe::B_CBY),
                      qz = O(b, O_BG + pipe::B_CBZ);
         const double e1 = qy * bz - qz * by, e2 = bx * qz - qx * bz,
@@ -1572,44 +1060,46 @@ __global__ void __launch_bounds__(tmak::NT, 1)
         vyr = vyr + ri * e2 * red;
         vzr = vzr + ri * e3 * red;
         const int gc = S.colx[i] + S.bxdim * S.coly[j];
-        vzr = vzr - ri * rho * __ldg(S.gblk + (long long)gc * nz + k);
+        vzr = vzr - ri * rho * __ldg(S.gblk + gc * nz + k);
         if (S.frc.kind != SPARC_SRC_NONE) {
+          const long long it = *S.iter;
           const double frc = forcing_at(S, it, pulse_time(S, it), i, j, k);
           if (S.frc.dir == 1) vxr = vxr + frc;
           else if (S.frc.dir == 2) vyr = vyr + frc;
           else vzr = vzr + frc;
         }
-        const double R[3] = {vxr, vyr, vzr};
-        double vsq = 0.0;
-#pragma unroll
-        for (int l = 1; l < 4; ++l) {
-          const double av = MODE == FIRST ? Hv(l - 1) : O(b, O_A + l);
-          const double an = zero ? av : av + (MODE == LAST ? dt : bnext) * R[l - 1];
-          so[l * N + id] = an;
-          vsq = l == 1 ? an * an : vsq + an * an;
-        }
-        if (MODE == LAST) X[2 * NC + cid] = vsq;
+        const double a1 = MODE == FIRST ? vx : O(b, O_A + 1);
+        const double a2 = MODE == FIRST ? vy : O(b, O_A + 2);
+        const double a3 = MODE == FIRST ? vz : O(b, O_A + 3);
+        const double n1 = zero ? a1 : a1 + fac * vxr;
+        const double n2 = zero ? a2 : a2 + fac * vyr;
+        const double n3 = zero ? a3 : a3 + fac * vzr;
+        so[N + id] = n1;
+        so[2 * N + id] = n2;
+        so[3 * N + id] = n3;
+        if (MODE == LAST) X[2 * NC + cid] = n1 * n1 + n2 * n2 + n3 * n3;
       } else {
         const double p = Hv(3);
         const double dvzdz = X[cid];
-        double R[5];
-        R[2] = red * (d4 - d7);
-        R[3] = red * (d6 - d2);
-        R[4] = red * (d3 - d5);
         const double div = d0 + d1 + dvzdz;
         const double r0 = O(b, O_BG + pipe::B_RHO0);
-        R[0] = -O(b, O_BG + pipe::B_GRX) * vx - O(b, O_BG + pipe::B_GRY) * vy -
-               O(b, O_BG + pipe::B_GRZ) * vz - r0 * div - sg * rho;
-        R[1] = -O(b, O_BG + pipe::B_C2R) * div - vx * O(b, O_BG + pipe::B_GPX) -
-               vy * O(b, O_BG + pipe::B_GPY) - vz * O(b, O_BG + pipe::B_GPZ) - sg * p;
-#pragma unroll
-        for (int q = 0; q < 5; ++q) {
-          const int ls = q == 0 ? 0 : (q == 1 ? 4 : q + 3);
-          const double av = MODE == FIRST ? (ls == 0 ? rho : Hv(ls - 1)) : O(b, O_A + ls);
-          const double an = zero ? av : av + (MODE == LAST ? dt : bnext) * R[q];
-          so[ls * N + id] = an;
-          if (q == 0) an_rho = an;
-        }
+        const double Rr = -O(b, O_BG + pipe::B_GRX) * vx - O(b, O_BG + pipe::B_GRY) * vy -
+                          O(b, O_BG + pipe::B_GRZ) * vz - r0 * div - sg * rho;
+        const double Rp = -O(b, O_BG + pipe::B_C2R) * div - vx * O(b, O_BG + pipe::B_GPX) -
+                          vy * O(b, O_BG + pipe::B_GPY) - vz * O(b, O_BG + pipe::B_GPZ) -
+                          sg * p;
+        const double Rbx = red * (d4 - d7), Rby = red * (d6 - d2), Rbz = red * (d3 - d5);
+        const double ar = MODE == FIRST ? rho : O(b, O_A + 0);
+        const double ap = MODE == FIRST ? p : O(b, O_A + 4);
+        const double abx = MODE == FIRST ? Hv(4) : O(b, O_A + 5);
+        const double aby = MODE == FIRST ? Hv(5) : O(b, O_A + 6);
+        const double abz = MODE == FIRST ? Hv(6) : O(b, O_A + 7);
+        an_rho = zero ? ar : ar + fac * Rr;
+        so[id] = an_rho;
+        so[4 * N + id] = zero ? ap : ap + fac * Rp;
+        so[5 * N + id] = zero ? abx : abx + fac * Rbx;
+        so[6 * N + id] = zero ? aby : aby + fac * Rby;
+        so[7 * N + id] = zero ? abz : abz + fac * Rbz;
         if (MODE == LAST) {
           mr = fmin(mr, rho + r0);
           mp = fmin(mp, p + O(b, O_P0));
@@ -1618,18 +1108,15 @@ __global__ void __launch_bounds__(tmak::NT, 1)
     }
     if (MODE == LAST) {
       __syncthreads();
-      if (act && role == 1) {
-        const double r0 = O(b, O_BG + pipe::B_RHO0);
-        const double m = (r0 + an_rho) * X[2 * NC + cid] / 2.0;
+      if (act && role == 1) {  // KE density of driver.f90:161 on a_new
+        const double m = (O(b, O_BG + pipe::B_RHO0) + an_rho) * X[2 * NC + cid] / 2.0;
         ke += m * m;
       }
     }
-    if (act && k + 1 < k1 && k + 1 <= nz - 6) head(k + 6, h0, h1, h2);
     __syncthreads();
   }
   if (!ok) {
     // a bounded wait gave up: drain (again bounded) what this CTA issued
-    cp_wait1();
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     if (tid == 0) {
       mbar_wait(&bar[0], phase & 1u, S.err);
@@ -1646,6 +1133,7 @@ int stage_geometry(Handle *h) {
   // small to fill the GPU.  The MHD kernels always use (32, 8).
   h->tx = 32;
   h->ty = 8;
+  if (h->magnetic && h->mhd_kernel == 4 && (h->nx % 2) == 0) h->ty = h->tma_ty;  // TMA tiles: 32 x tma_ty
   long long tiles = (long long)((h->nx + h->tx - 1) / h->tx) *
                     ((h->ny + h->ty - 1) / h->ty);
   if (tiles < 64 && !h->magnetic) {
@@ -1684,51 +1172,6 @@ static int launch_quiet(Handle *h, const SimDev &S, int stage,
   return SPARC_OK;
 }
 
-template <int TX, int TY>
-static int launch_mhd(Handle *h, const SimDev &S, int stage, const double *a,
-                      const double *tin, double *so, cudaStream_t s) {
-  dim3 blk(TX, TY);
-  dim3 grd((h->nx + TX - 1) / TX, (h->ny + TY - 1) / TY,
-           (h->nz + h->zchunk - 1) / h->zchunk);
-  const double beta = h->betas[stage - 1];
-  const double bnext = stage < 5 ? h->betas[stage] : h->deltat;
-  const size_t smem = sizeof(double) * 9 * (TX + 10) * (TY + 10);
-  const int mode = stage == 1 ? FIRST : (stage == 5 ? LAST : MID);
-  if (mode == FIRST)
-    cudaFuncSetAttribute(k_stage_mhd<TX, TY, FIRST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  else if (mode == MID)
-    cudaFuncSetAttribute(k_stage_mhd<TX, TY, MID>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  else
-    cudaFuncSetAttribute(k_stage_mhd<TX, TY, LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (mode == FIRST) k_stage_mhd<TX, TY, FIRST><<<grd, blk, smem, s>>>(S, a, tin, so, beta, bnext, h->zchunk);
-  else if (mode == MID) k_stage_mhd<TX, TY, MID><<<grd, blk, smem, s>>>(S, a, tin, so, beta, bnext, h->zchunk);
-  else k_stage_mhd<TX, TY, LAST><<<grd, blk, smem, s>>>(S, a, tin, so, beta, bnext, h->zchunk);
-  return SPARC_OK;
-}
-
-static int launch_mhd_pipe(Handle *h, const SimDev &S, int stage,
-                           const double *a, const double *tin, double *so,
-                           cudaStream_t s) {
-  using namespace pipe;
-  dim3 blk(TX, TY);
-  dim3 grd((h->nx + TX - 1) / TX, (h->ny + TY - 1) / TY,
-           (h->nz + h->zchunk - 1) / h->zchunk);
-  const double beta = h->betas[stage - 1];
-  const double bnext = stage < 5 ? h->betas[stage] : h->deltat;
-  const int mode = stage == 1 ? FIRST : (stage == 5 ? LAST : MID);
-  if (mode == FIRST) {
-    cudaFuncSetAttribute(k_stage_mhd_pipe<FIRST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
-    k_stage_mhd_pipe<FIRST><<<grd, blk, SMEM, s>>>(S, a, tin, so, beta, bnext, h->zchunk);
-  } else if (mode == MID) {
-    cudaFuncSetAttribute(k_stage_mhd_pipe<MID>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
-    k_stage_mhd_pipe<MID><<<grd, blk, SMEM, s>>>(S, a, tin, so, beta, bnext, h->zchunk);
-  } else {
-    cudaFuncSetAttribute(k_stage_mhd_pipe<LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
-    k_stage_mhd_pipe<LAST><<<grd, blk, SMEM, s>>>(S, a, tin, so, beta, bnext, h->zchunk);
-  }
-  return SPARC_OK;
-}
-
 static int launch_mhd_duo(Handle *h, const SimDev &S, int stage,
                           const double *a, const double *tin, double *so,
                           cudaStream_t s) {
@@ -1752,35 +1195,45 @@ static int launch_mhd_duo(Handle *h, const SimDev &S, int stage,
   return SPARC_OK;
 }
 
+template <int TYV>
+static int launch_mhd_tma_ty(Handle *h, const SimDev &S, int stage, const double *a,
+                             const double *tin, double *so, cudaStream_t s, int mt,
+                             int ma) {
+  using G = TmaGeo<TYV>;
+  TmaSet T;
+  for (int n = 0; n < 18; ++n) T.m[n] = h->tmaps_ty[n];
+  dim3 blk(G::TX, G::TY, 2);
+  dim3 grd((h->nx + G::TX - 1) / G::TX, (h->ny + G::TY - 1) / G::TY,
+           (h->nz + h->zchunk - 1) / h->zchunk);
+  const double beta = h->betas[stage - 1];
+  const double bnext = stage < 5 ? h->betas[stage] : h->deltat;
+  const int mode = stage == 1 ? FIRST : (stage == 5 ? LAST : MID);
+  const int sm = (int)G::SMEM;
+  if (mode == FIRST) {
+    cudaFuncSetAttribute(k_stage_mhd_tma<FIRST, TYV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    k_stage_mhd_tma<FIRST, TYV><<<grd, blk, G::SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt, ma);
+  } else if (mode == MID) {
+    cudaFuncSetAttribute(k_stage_mhd_tma<MID, TYV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    k_stage_mhd_tma<MID, TYV><<<grd, blk, G::SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt, ma);
+  } else {
+    cudaFuncSetAttribute(k_stage_mhd_tma<LAST, TYV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    k_stage_mhd_tma<LAST, TYV><<<grd, blk, G::SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt, ma);
+  }
+  return SPARC_OK;
+}
+
 static int launch_mhd_tma(Handle *h, const SimDev &S, int stage,
                           const double *a, const double *tin, double *so,
                           cudaStream_t s) {
-  using namespace tmak;
   int mt = -1, ma = -1;
   for (int b = 0; b < 3; ++b) {
     if (h->buf[b] == tin) mt = b;
     if (h->buf[b] == a) ma = b;
   }
   if (mt < 0 || ma < 0) return SPARC_ERR_INVALID;
-  TmaSet T;
-  for (int n = 0; n < 18; ++n) T.m[n] = h->tmaps[n];
-  dim3 blk(TX, TY, 2);
-  dim3 grd((h->nx + TX - 1) / TX, (h->ny + TY - 1) / TY,
-           (h->nz + h->zchunk - 1) / h->zchunk);
-  const double beta = h->betas[stage - 1];
-  const double bnext = stage < 5 ? h->betas[stage] : h->deltat;
-  const int mode = stage == 1 ? FIRST : (stage == 5 ? LAST : MID);
-  if (mode == FIRST) {
-    cudaFuncSetAttribute(k_stage_mhd_tma<FIRST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
-    k_stage_mhd_tma<FIRST><<<grd, blk, SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt, ma);
-  } else if (mode == MID) {
-    cudaFuncSetAttribute(k_stage_mhd_tma<MID>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
-    k_stage_mhd_tma<MID><<<grd, blk, SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt, ma);
-  } else {
-    cudaFuncSetAttribute(k_stage_mhd_tma<LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
-    k_stage_mhd_tma<LAST><<<grd, blk, SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt, ma);
-  }
-  return SPARC_OK;
+  if ((long long)h->V * h->N >= (1LL << 31)) return SPARC_ERR_INVALID;
+  if (h->tma_ty == 6) return launch_mhd_tma_ty<6>(h, S, stage, a, tin, so, s, mt, ma);
+  return launch_mhd_tma_ty<8>(h, S, stage, a, tin, so, s, mt, ma);
 }
 
 // Tensor maps (3-D, FP64, 32x8x1 boxes) of the arrays the TMA kernel loads
@@ -1802,7 +1255,7 @@ int encode_tensor_maps(Handle *h) {
   auto one = [&](CUtensorMap *m, const double *base, unsigned long long depth) {
     cuuint64_t dims[3] = {(cuuint64_t)h->nx, (cuuint64_t)h->ny, (cuuint64_t)depth};
     cuuint64_t strides[2] = {(cuuint64_t)h->nx * 8, (cuuint64_t)h->nx * h->ny * 8};
-    cuuint32_t box[3] = {32, 8, 1};
+    cuuint32_t box[3] = {32, (cuuint32_t)h->tma_ty, 1};
     cuuint32_t es[3] = {1, 1, 1};
     return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void *)base, dims, strides, box, es,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -1810,10 +1263,10 @@ int encode_tensor_maps(Handle *h) {
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
   };
   bool ok = true;
-  for (int b = 0; b < 3; ++b) ok = ok && one(&h->tmaps[b], h->buf[b], (unsigned long long)h->nz * h->V);
+  for (int b = 0; b < 3; ++b) ok = ok && one(&h->tmaps_ty[b], h->buf[b], (unsigned long long)h->nz * h->V);
   const double *bg[15] = {h->red, h->sponge, h->rho0, h->grx, h->gry, h->grz, h->c2rho0,
                           h->gpx, h->gpy, h->gpz, h->rhoinv, h->cbx, h->cby, h->cbz, h->p0};
-  for (int n = 0; n < 15; ++n) ok = ok && bg[n] && one(&h->tmaps[3 + n], bg[n], h->nz);
+  for (int n = 0; n < 15; ++n) ok = ok && bg[n] && one(&h->tmaps_ty[3 + n], bg[n], h->nz);
   h->tma = ok;
   return SPARC_OK;
 }
@@ -1821,20 +1274,16 @@ int encode_tensor_maps(Handle *h) {
 int launch_stage(Handle *h, const SimDev &S, int stage, const double *a,
                  const double *tin, double *so, cudaStream_t s) {
   int r = SPARC_ERR_INVALID;
-  if (h->magnetic && h->mhd_kernel == 4 && h->tma && h->tx == 32 && h->ty == 8) {
+  if (h->magnetic && h->mhd_kernel == 4 && h->tma && h->tx == 32 &&
+      (long long)h->V * h->N < (1LL << 31)) {
     r = launch_mhd_tma(h, S, stage, a, tin, so, s);
     ++h->launches;
     if (r == SPARC_OK && cudaGetLastError() != cudaSuccess) r = SPARC_ERR_CUDA;
     return r;
   }
-  if (h->magnetic && h->mhd_kernel >= 3 && h->tx == 32 && h->ty == 8) {
+  if (h->magnetic) {
+    if (h->tx != 32 || h->ty != 8) return SPARC_ERR_INVALID;
     r = launch_mhd_duo(h, S, stage, a, tin, so, s);
-    ++h->launches;
-    if (r == SPARC_OK && cudaGetLastError() != cudaSuccess) r = SPARC_ERR_CUDA;
-    return r;
-  }
-  if (h->magnetic && h->mhd_kernel == 2 && h->tx == 32 && h->ty == 8) {
-    r = launch_mhd_pipe(h, S, stage, a, tin, so, s);
     ++h->launches;
     if (r == SPARC_OK && cudaGetLastError() != cudaSuccess) r = SPARC_ERR_CUDA;
     return r;
@@ -1846,7 +1295,7 @@ int launch_stage(Handle *h, const SimDev &S, int stage, const double *a,
     case 1608: r = FN<16, 8>(h, S, stage, a, tin, so, s); break; \
     default: r = SPARC_ERR_INVALID;                             \
   }
-  if (h->magnetic) { DISPATCH(launch_mhd) } else { DISPATCH(launch_quiet) }
+  DISPATCH(launch_quiet)
 #undef DISPATCH
   ++h->launches;
   if (r == SPARC_OK && cudaGetLastError() != cudaSuccess) r = SPARC_ERR_CUDA;

@@ -20,6 +20,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "--extended-lambda",
 UNITS = {
     "setup.cu": ["-fmad=false"],
     "step.cu": [],
+    "step32.cu": [],
     "api.cu": [],
 }
 HEADERS = ["internal.h"]

@@ -34,6 +34,15 @@ void *dev_alloc(Handle *h, size_t bytes) {
   return p;
 }
 
+void dev_free(Handle *h, const void *p) {
+  for (size_t n = 0; n < h->allocs.size(); ++n)
+    if (h->allocs[n] == p) {
+      cudaFree(h->allocs[n]);
+      h->allocs.erase(h->allocs.begin() + n);
+      return;
+    }
+}
+
 static int fail(Handle *h, int code, const std::string &msg) {
   if (h) h->err = msg;
   return code;
@@ -61,7 +70,10 @@ static std::string validate(const sparc_params &P) {
   if (P.filter_mode_xy != 1 && P.filter_mode_xy != 2) return "filter_mode_xy";
   if (P.filter_mode_z != 1 && P.filter_mode_z != 2) return "filter_mode_z";
   if (!(P.timestep > 0)) return "timestep must be positive";
-  if (P.precision != SPARC_FP64) return "only SPARC_FP64 is available in this build";
+  if (P.precision != SPARC_FP64 && P.precision != SPARC_FP32)
+    return "precision must be SPARC_FP64 or SPARC_FP32";
+  if (P.precision == SPARC_FP32 && (long long)P.nx * P.ny * P.nz * 8 >= (1LL << 31))
+    return "the precision form takes grids below 2^28 points";
   std::vector<int> s, l;
   const int dims[3] = {P.nx, P.ny, P.nz}, B[3] = {P.block_x, P.block_y, P.block_z};
   for (int a = 0; a < 3; ++a) {
@@ -98,6 +110,17 @@ static int alloc_face(Handle *h, int f, int n0, int n1, int n2, int np) {
   F.n0 = n0; F.n1 = n1; F.n2 = n2; F.np = np; F.P = h->Pp;
   F.uniform = 0;
   F.cnt = (long long)n0 * n1 * n2;
+  if (h->fp32) {  // FP32 auxiliary fields; FP64 face keeps the geometry
+    FaceT<float> &G = h->f_faces[f];
+    G.on = 1;
+    G.n0 = n0; G.n1 = n1; G.n2 = n2; G.np = np; G.P = F.P;
+    G.uniform = 0;
+    G.cnt = F.cnt;
+    G.vars = (float *)dev_alloc(h, G.cnt * G.P * 4);
+    G.scr = (float *)dev_alloc(h, G.cnt * G.P * 4);
+    if (!G.vars || !G.scr) return SPARC_ERR_NOMEM;
+    return SPARC_OK;
+  }
   F.vars = (double *)dev_alloc(h, F.cnt * F.P * 8);
   F.scr = (double *)dev_alloc(h, F.cnt * F.P * 8);
   if (!F.vars || !F.scr) return SPARC_ERR_NOMEM;
@@ -107,6 +130,17 @@ static int alloc_face(Handle *h, int f, int n0, int n1, int n2, int np) {
 }
 
 static int zero_state(Handle *h) {
+  if (h->fp32) {
+    for (int b = 0; b < 3; ++b)
+      CK(h, cudaMemsetAsync(h->fbuf[b], 0, (size_t)h->V * h->N * 4, h->stream));
+    CK(h, cudaMemsetAsync(h->f_carry, 0, (size_t)h->V * h->N * 4, h->stream));
+    for (auto &F : h->f_faces)
+      if (F.on) {
+        CK(h, cudaMemsetAsync(F.vars, 0, F.cnt * F.P * 4, h->stream));
+        CK(h, cudaMemsetAsync(F.scr, 0, F.cnt * F.P * 4, h->stream));
+      }
+    return SPARC_OK;
+  }
   for (int b = 0; b < 3; ++b)
     CK(h, cudaMemsetAsync(h->buf[b], 0, (size_t)h->V * h->N * 8, h->stream));
   for (auto &F : h->faces)
@@ -130,8 +164,28 @@ static void rotate(Handle *h) {
   h->rf2 = a;
 }
 
+// precision form of enqueue_step: FP32 buffers, same roles
+static int enqueue_step32(Handle *h, cudaStream_t s, int *nk) {
+  SimT<float> S = make_sim32(h);
+  float *a = h->fbuf[h->ra], *f1 = h->fbuf[h->rf1], *f2 = h->fbuf[h->rf2];
+  int r = SPARC_OK;
+  if (h->src.kind == SPARC_SRC_PSR && h->psr_khi > h->psr_klo) {
+    r |= launch_psr32(h, s);
+    ++*nk;
+  }
+  r |= launch_stage32(h, S, 1, a, a, f1, s);
+  r |= launch_stage32(h, S, 2, a, f1, f2, s);
+  r |= launch_stage32(h, S, 3, a, f2, f1, s);
+  r |= launch_stage32(h, S, 4, a, f1, f2, s);
+  r |= launch_stage32(h, S, 5, a, f2, f1, s);
+  *nk += 5;
+  rotate(h);
+  return r ? SPARC_ERR_CUDA : SPARC_OK;
+}
+
 // forcing + five stages (step.f90:26-61); a_new lands in buf[rf1]
 static int enqueue_step(Handle *h, cudaStream_t s, int *nk) {
+  if (h->fp32) return enqueue_step32(h, s, nk);
   SimDev S = make_simdev(h);
   double *a = h->buf[h->ra], *f1 = h->buf[h->rf1], *f2 = h->buf[h->rf2];
   int r = SPARC_OK;
@@ -160,7 +214,29 @@ static int filter_kind(Handle *h, long long nn) {
   return fk;
 }
 
+// precision form: the filtered state starts a new compensated sum (its
+// carry is cleared after the passes)
+static int enqueue_filter32(Handle *h, int fk, cudaStream_t s, int *nk) {
+  int r = SPARC_OK;
+  if (fk & 1) {
+    for (int dir = 1; dir >= 0; --dir) {  // y, then x
+      r |= launch_filter32(h, dir, h->fbuf[h->ra], h->fbuf[h->rf1], s);
+      rotate(h);
+      ++*nk;
+    }
+  }
+  if (fk & 2) {
+    r |= launch_filter32(h, 2, h->fbuf[h->ra], h->fbuf[h->rf1], s);
+    rotate(h);
+    ++*nk;
+  }
+  if (fk && cudaMemsetAsync(h->f_carry, 0, (size_t)h->V * h->N * 4, s) != cudaSuccess)
+    r = SPARC_ERR_CUDA;
+  return r ? SPARC_ERR_CUDA : SPARC_OK;
+}
+
 static int enqueue_filter(Handle *h, int fk, cudaStream_t s, int *nk) {
+  if (h->fp32) return enqueue_filter32(h, fk, s, nk);
   int r = SPARC_OK;
   if (fk & 1) {
     for (int dir = 1; dir >= 0; --dir) {  // y, then x
@@ -261,6 +337,7 @@ int sparc_create(const sparc_params *p, int device, sparc_handle **out) {
   h->use_hpml = p->use_hpml != 0;
   h->use_pml = p->use_pml != 0 || h->use_hpml;
   h->V = h->magnetic ? 8 : 5;
+  h->fp32 = p->precision == SPARC_FP32;
   h->Pp = h->magnetic ? 6 : 2;
   h->gxy = p->filter_mode_xy == 1 ? 5 : 3;
   h->gz = p->filter_mode_z == 1 ? 5 : 3;
@@ -306,7 +383,8 @@ int sparc_create(const sparc_params *p, int device, sparc_handle **out) {
   if (!cuda_ok(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream")) {
     r = SPARC_ERR_CUDA;
   }
-  if (!r && (setup_constants() || step_constants() || filter_constants(h->gxy, h->gz)))
+  if (!r && (setup_constants() || step_constants() || filter_constants(h->gxy, h->gz) ||
+             step32_constants(h->gxy, h->gz)))
     r = fail(h, SPARC_ERR_CUDA, "constant upload failed");
   if (!r && stage_geometry(h))
     r = fail(h, SPARC_ERR_INVALID, "no tile shape fits this grid");
@@ -321,8 +399,17 @@ int sparc_create(const sparc_params *p, int device, sparc_handle **out) {
     }
   }
   for (int b = 0; !r && b < 3; ++b) {
-    h->buf[b] = (double *)dev_alloc(h, (size_t)h->V * h->N * 8);
-    if (!h->buf[b]) r = SPARC_ERR_NOMEM;
+    if (h->fp32) {
+      h->fbuf[b] = (float *)dev_alloc(h, (size_t)h->V * h->N * 4);
+      if (!h->fbuf[b]) r = SPARC_ERR_NOMEM;
+    } else {
+      h->buf[b] = (double *)dev_alloc(h, (size_t)h->V * h->N * 8);
+      if (!h->buf[b]) r = SPARC_ERR_NOMEM;
+    }
+  }
+  if (!r && h->fp32) {
+    h->f_carry = (float *)dev_alloc(h, (size_t)h->V * h->N * 4);
+    if (!h->f_carry) r = SPARC_ERR_NOMEM;
   }
   if (!r && h->use_pml) {
     r |= alloc_face(h, 0, h->nx, h->ny, p->npml_zb, p->npml_zb);
@@ -391,8 +478,16 @@ int sparc_set_background(sparc_handle *h, const double *rho0,
   cudaSetDevice(h->device);
   int r = setup_background(h, rho0, pre0, cs0, bx0, by0, bz0, zaxis_mm, grav);
   if (r) return r;
-  r = encode_tensor_maps(h);
-  if (r) return r;
+  if (h->fp32) {
+    r = setup32(h);
+    if (r) return r;
+    h->h_scale.resize((size_t)2 * h->V * h->nz);
+    CK(h, cudaMemcpy(h->h_scale.data(), h->f_sc, h->h_scale.size() * 4,
+                     cudaMemcpyDeviceToHost));
+  } else {
+    r = encode_tensor_maps(h);
+    if (r) return r;
+  }
   r = zero_state(h);
   if (r) return r;
   h->bg_ready = true;
@@ -520,6 +615,7 @@ int sparc_set_source(sparc_handle *h, const sparc_source *s) {
     h->d_psr = (double *)dev_alloc(h, std::max<size_t>(8, (size_t)(khi - klo) * nx * ny * 8));
     if (r || !h->d_psr) return r ? r : SPARC_ERR_NOMEM;
   }
+  if (h->fp32) return source32(h);
   return SPARC_OK;
 }
 
@@ -533,9 +629,72 @@ int sparc_sizes(const sparc_handle *h, int64_t *ns, int64_t *np) {
   return SPARC_OK;
 }
 
+// precision form: stored = float(sc * a), carry 0; a = (stored - carry)/sc
+static int set_state32(Handle *h, const double *a, const double *psi) {
+  const long long N = h->N;
+  const int nz = h->nz;
+  const long long NXY = (long long)h->nx * h->ny;
+  if (a && h->h_scale.empty()) return fail(h, SPARC_ERR_ORDER, "set the background first");
+  if (a) {
+    std::vector<float> t((size_t)h->V * N);
+    for (int l = 0; l < h->V; ++l)
+      for (long long n = 0; n < N; ++n) {
+        const double sc = h->h_scale[(size_t)l * nz + n / NXY];
+        t[(size_t)l * N + n] = (float)(sc * a[(size_t)l * N + n]);
+      }
+    CK(h, cudaMemcpy(h->fbuf[h->ra], t.data(), t.size() * 4, cudaMemcpyHostToDevice));
+    CK(h, cudaMemset(h->f_carry, 0, t.size() * 4));
+  }
+  if (psi) {
+    size_t off = 0;
+    for (auto &F : h->f_faces)
+      if (F.on) {
+        std::vector<float> t(F.cnt * F.P);
+        for (size_t n = 0; n < t.size(); ++n) t[n] = (float)psi[off + n];
+        CK(h, cudaMemcpy(F.vars, t.data(), t.size() * 4, cudaMemcpyHostToDevice));
+        off += t.size();
+      }
+  }
+  return SPARC_OK;
+}
+
+static int get_state32(Handle *h, double *a, double *psi) {
+  const long long N = h->N;
+  const int nz = h->nz, V = h->V;
+  const long long NXY = (long long)h->nx * h->ny;
+  CK(h, cudaStreamSynchronize(h->stream));
+  if (a) {
+    if (h->h_scale.empty()) return fail(h, SPARC_ERR_ORDER, "set the background first");
+    std::vector<float> t((size_t)V * N), c((size_t)V * N);
+    CK(h, cudaMemcpy(t.data(), h->fbuf[h->ra], t.size() * 4, cudaMemcpyDeviceToHost));
+    CK(h, cudaMemcpy(c.data(), h->f_carry, c.size() * 4, cudaMemcpyDeviceToHost));
+    for (int l = 0; l < V; ++l)
+      for (long long n = 0; n < N; ++n) {
+        const size_t q = (size_t)l * N + n;
+        const double isc = h->h_scale[(size_t)(V + l) * nz + n / NXY];
+        a[q] = ((double)t[q] - (double)c[q]) * isc;
+      }
+  }
+  if (psi) {
+    size_t off = 0;
+    for (auto &F : h->f_faces)
+      if (F.on) {
+        std::vector<float> t(F.cnt * F.P);
+        CK(h, cudaMemcpy(t.data(), F.vars, t.size() * 4, cudaMemcpyDeviceToHost));
+        for (size_t n = 0; n < t.size(); ++n) psi[off + n] = t[n];
+        off += t.size();
+      }
+  }
+  return SPARC_OK;
+}
+
 int sparc_set_state(sparc_handle *h, const double *a, const double *psi) {
   if (!h) return SPARC_ERR_INVALID;
   cudaSetDevice(h->device);
+  if (h->fp32) {
+    CK(h, cudaStreamSynchronize(h->stream));
+    return set_state32(h, a, psi);
+  }
   if (a)
     CK(h, cudaMemcpyAsync(h->buf[h->ra], a, (size_t)h->V * h->N * 8,
                           cudaMemcpyHostToDevice, h->stream));
@@ -555,6 +714,7 @@ int sparc_set_state(sparc_handle *h, const double *a, const double *psi) {
 int sparc_get_state(sparc_handle *h, double *a, double *psi) {
   if (!h) return SPARC_ERR_INVALID;
   cudaSetDevice(h->device);
+  if (h->fp32) return get_state32(h, a, psi);
   if (a)
     CK(h, cudaMemcpyAsync(a, h->buf[h->ra], (size_t)h->V * h->N * 8,
                           cudaMemcpyDeviceToHost, h->stream));
@@ -652,6 +812,7 @@ int sparc_derivative(sparc_handle *h, int dir, int bc, const double *in,
                      double *out) {
   if (!h || !in || !out || dir < 0 || dir > 2 || (bc != 1 && bc != 5))
     return SPARC_ERR_INVALID;
+  if (h->fp32) return fail(h, SPARC_ERR_INVALID, "unit entry points need the FP64 form");
   if (!h->bg_ready) return fail(h, SPARC_ERR_ORDER, "set the background first");
   cudaSetDevice(h->device);
   double *dev_in = h->buf[h->rf1], *dev_out = h->buf[h->rf2];
@@ -665,6 +826,7 @@ int sparc_derivative(sparc_handle *h, int dir, int bc, const double *in,
 
 int sparc_filter_field(sparc_handle *h, int dir, const double *in, double *out) {
   if (!h || !in || !out || dir < 0 || dir > 2) return SPARC_ERR_INVALID;
+  if (h->fp32) return fail(h, SPARC_ERR_INVALID, "unit entry points need the FP64 form");
   cudaSetDevice(h->device);
   double *dev_in = h->buf[h->rf1], *dev_out = h->buf[h->rf2];
   CK(h, cudaMemcpyAsync(dev_in, in, h->N * 8, cudaMemcpyHostToDevice, h->stream));
@@ -681,6 +843,9 @@ int sparc_get_coeff(sparc_handle *h, const char *name, double *out,
   if (!h->bg_ready) return fail(h, SPARC_ERR_ORDER, "set the background first");
   cudaSetDevice(h->device);
   std::string s(name);
+  if (h->fp32 && s != "stretch" && s != "zaxis" && s != "xaxis" && s != "yaxis" && s != "g" &&
+      s != "gblk" && s != "invrho0q" && s != "cq")
+    return fail(h, SPARC_ERR_INVALID, "FP64 coefficients are released in the precision form");
   const double *dsrc = nullptr;
   const std::vector<double> *hsrc = nullptr;
   long long n = h->N;

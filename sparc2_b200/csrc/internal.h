@@ -84,6 +84,12 @@ struct SimT {
 };
 using SimDev = SimT<double>;
 
+// Background arrays of the precision form (FP32 copies of the FP64 setup).
+enum {
+  FB_RHO0, FB_P0, FB_RHOINV, FB_C2R, FB_GRZ, FB_GPZ, FB_SPONGE, FB_BOX, FB_BOY,
+  FB_BOZ, FB_CBX, FB_CBY, FB_CBZ, FB_GRX, FB_GRY, FB_GPX, FB_GPY, FB_RED, FB_COUNT
+};
+
 struct Handle {
   sparc_params P{};
   int device = 0;
@@ -156,6 +162,24 @@ struct Handle {
   int tx = 32, ty = 8, zchunk = 32;
   int mhd_kernel = 3;
 
+  // precision form (SPARC_FP32): FP32 state in fbuf (roles ra/rf1/rf2 as
+  // for buf), the compensated-sum carry of the state, depth scales
+  // (stored = f_sc[l*nz+k] * physical), FP32 background and CPML faces.
+  // The FP64 setup arrays are released once converted.
+  bool fp32 = false;
+  float *fbuf[3] = {nullptr, nullptr, nullptr};
+  float *f_carry = nullptr;
+  float *f_sc = nullptr, *f_isc = nullptr;  // V x nz
+  std::vector<float> h_scale;               // host copy: sc then isc
+  float *f_bg[FB_COUNT] = {};
+  float *f_stretch = nullptr, *f_gblk = nullptr;
+  FaceT<float> f_faces[6]{};
+  float *f_fx = nullptr, *f_fy = nullptr, *f_fz = nullptr;
+  float *f_psr = nullptr, *f_px = nullptr, *f_py = nullptr;
+  float *f_sd = nullptr, *f_ssb = nullptr;
+  bool tma32 = false;
+  CUtensorMap tmaps32[18];
+
   // captured graphs keyed by (ra, rf1, rf2, filter kind)
   struct GraphEntry {
     int ra, rf1, rf2, fk;
@@ -191,8 +215,20 @@ int launch_filter_pass(Handle *h, int dir, const double *in, double *out,
 int stage_geometry(Handle *h);
 int encode_tensor_maps(Handle *h);
 
+// step32.cu (precision form)
+int step32_constants(int gxy, int gz);
+SimT<float> make_sim32(Handle *h);
+int launch_stage32(Handle *h, const SimT<float> &S, int stage, const float *a,
+                   const float *tin, float *so, cudaStream_t s);
+int launch_psr32(Handle *h, cudaStream_t s);
+int launch_filter32(Handle *h, int dir, const float *in, float *out, cudaStream_t s);
+int encode_tensor_maps32(Handle *h);
+int setup32(Handle *h);
+int source32(Handle *h);
+
 // api.cu
 void *dev_alloc(Handle *h, size_t bytes);
+void dev_free(Handle *h, const void *p);
 bool cuda_ok(Handle *h, cudaError_t e, const char *what);
 
 }  // namespace sparc

@@ -1133,7 +1133,8 @@ int stage_geometry(Handle *h) {
   // small to fill the GPU.  The MHD kernels always use (32, 8).
   h->tx = 32;
   h->ty = 8;
-  if (h->magnetic && h->mhd_kernel == 4 && (h->nx % 2) == 0) h->ty = h->tma_ty;  // TMA tiles: 32 x tma_ty
+  if (h->magnetic && !h->fp32 && h->mhd_kernel == 4 && (h->nx % 2) == 0)
+    h->ty = h->tma_ty;  // TMA tiles: 32 x tma_ty
   long long tiles = (long long)((h->nx + h->tx - 1) / h->tx) *
                     ((h->ny + h->ty - 1) / h->ty);
   if (tiles < 64 && !h->magnetic) {

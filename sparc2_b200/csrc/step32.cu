@@ -1,0 +1,1234 @@
+// step32.cu -- the precision form of the time step: FP32 state, coefficients
+// and arithmetic (FP32 accumulation), FP64 only for the setup (setup.cu),
+// the CPML profiles (computed in FP64, stored in FP32) and the energy
+// diagnostics.
+//
+// Depth scaling.  The state is stored as sc_l(z) * physical value with
+//   rho: 1/rho0(z), v: sqrt(rho0(z)), p: 1/(rho0 c0^2)(z), b: 1,
+// profiles of the background column (1,1,:), so that wave amplitudes keep
+// the same magnitude across the ~1e6 density stratification.  Kernels turn
+// stored values into physical ones on load (x/y derivatives of a layer are
+// scaled once after the stencil; z windows hold physical values) and scale
+// the right-hand side back on store.
+//
+// Compensated update.  The final RK update a + deltat*F (step.f90:58) keeps
+// a per-value FP32 carry (Kahan summation), so the slow accumulation of
+// small increments onto the state does not lose the low-order digits.
+//
+// The stencils, CPML, RHS algebra, boundary zeroing and diagnostics follow
+// the same reference lines as the FP64 kernels of step.cu.
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "internal.h"
+
+namespace sparc {
+
+__constant__ float f_dp[6][11];
+__constant__ float f_df[2][11];
+
+enum { F_FIRST = 0, F_MID = 1, F_LAST = 2 };
+
+int step32_constants(int gxy, int gz) {
+  float t[6][11];
+  for (int r = 0; r < 6; ++r)
+    for (int m = 0; m < 11; ++m) t[r][m] = (float)kDerivRows[r][m];
+  if (cudaMemcpyToSymbol(f_dp, t, sizeof(t)) != cudaSuccess) return SPARC_ERR_CUDA;
+  float f[2][11] = {};
+  for (int d = 0; d < 2; ++d) {
+    int g = d == 0 ? gxy : gz;
+    for (int m = 0; m < 11; ++m)
+      f[d][m] = (float)(g == 5 ? kFilter11[m] : (m < 7 ? kFilter7[m] : 0.0));
+  }
+  return cudaMemcpyToSymbol(f_df, f, sizeof(f)) == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
+}
+
+using Sim32 = SimT<float>;
+using Face32 = FaceT<float>;
+
+// ------------------------------------------------------------- helpers
+__device__ __forceinline__ int wrap32(int q, int n) {
+  q = q < 0 ? q + n : q;
+  return q >= n ? q - n : q;
+}
+__device__ __forceinline__ int origin32(int t0, int T, int n, bool per) {
+  int o = t0 - 5;
+  if (!per && t0 + T >= n) o = min(o, n - 11);
+  return o;
+}
+
+template <int MODE>
+__device__ __forceinline__ void cpml32(const Face32 &F, long long f, int layer, int slot,
+                                       float beta, float dt, float &d) {
+  const long long pf = F.uniform ? (long long)layer : f;
+  const float pa = __ldg(F.pa + pf), pb = __ldg(F.pb + pf), pk = __ldg(F.pk + pf);
+  const long long o = (long long)slot * F.cnt + f;
+  const float v = F.vars[o];
+  float psi = v;
+  if (MODE != F_FIRST) psi = v + beta * F.scr[o];
+  const float rhs = pa * d + pb * psi;
+  d = d / pk + psi;
+  if (MODE == F_LAST) F.vars[o] = v + dt * rhs;
+  else F.scr[o] = rhs;
+}
+
+__device__ __forceinline__ float pulse_time32(const Sim32 &S, long long it) {
+  const ForcingT<float> &F = S.frc;
+  if (F.kind != SPARC_SRC_PULSE) return 0.f;
+  const double t = (double)it * F.timestep;
+  double T = F.amp_c * sin(2.0 * PI * (t - F.t1 + 2.0 * F.t0) / F.t0);
+  return (float)(T * exp(-1.0 * ((t - F.t1) * (t - F.t1)) / (2.0 * (F.st * F.st))));
+}
+
+__device__ __forceinline__ float forcing32(const Sim32 &S, float T, int i, int j, int k) {
+  const ForcingT<float> &F = S.frc;
+  if (F.kind == SPARC_SRC_PULSE)
+    return T * __ldg(F.fz + k) * (__ldg(F.fy + j) * __ldg(F.fx + i));
+  if (F.kind == SPARC_SRC_PSR && k >= F.klo && k < F.khi)
+    return F.psr[((long long)(k - F.klo) * S.ny + j) * S.nx + i];
+  return 0.f;
+}
+
+template <class Get>
+__device__ __forceinline__ float dxy32(int q, int n, bool per, float sc, Get t) {
+  float s = 0.f;
+  if (per || (q >= 5 && q < n - 5)) {
+#pragma unroll
+    for (int m = 0; m < 11; ++m) s += t(q - 5 + m) * f_dp[5][m];
+    return sc * s;
+  }
+  if (q < 5) {
+#pragma unroll
+    for (int m = 0; m < 11; ++m) s += t(m) * f_dp[q][m];
+    return sc * s;
+  }
+  const int row = n - 1 - q;
+#pragma unroll
+  for (int m = 0; m < 11; ++m) s += t(n - 1 - m) * f_dp[row][m];
+  return -sc * s;
+}
+
+__device__ __forceinline__ float dz32(const float (&w)[11], int k, int nz, float sc) {
+  float s = 0.f;
+  if (k < nz - 5) {
+#pragma unroll
+    for (int m = 0; m < 11; ++m) s += w[m] * f_dp[5][m];
+    return sc * s;
+  }
+  const int row = nz - 1 - k;
+#pragma unroll
+  for (int m = 0; m < 11; ++m) s += w[10 - m] * f_dp[row][m];
+  return -sc * s;
+}
+
+__device__ __forceinline__ void shift32(float (&w)[11], float v) {
+#pragma unroll
+  for (int m = 0; m < 10; ++m) w[m] = w[m + 1];
+  w[10] = v;
+}
+
+__device__ __forceinline__ float csum32(const float *p, int st) {
+  float s = 0.f;
+#pragma unroll
+  for (int m = 0; m < 11; ++m) s += p[m * st] * f_dp[5][m];
+  return s;
+}
+
+// Compensated final update (step.f90:58): a + dt*F with a Kahan carry c.
+__device__ __forceinline__ float kahan(float a, float inc, float &c) {
+  const float y = inc - c;
+  const float t = a + y;
+  c = (t - a) - y;
+  return t;
+}
+
+// Per-CTA partial of the KE norm and minima (FP64) and the last-CTA
+// reduction with the fail criterion of driver.f90:175-183.
+__device__ void diag_reduce32(const Sim32 &S, double ke, double mr, double mp) {
+  __shared__ double r[3][32];
+  __shared__ int am_last;
+  const int nt = blockDim.x * blockDim.y * blockDim.z;
+  const int tid = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5, nw = (nt + 31) >> 5;
+  const long long nb = (long long)gridDim.x * gridDim.y * gridDim.z;
+  const long long bid = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+  for (int o = 16; o > 0; o >>= 1) {
+    ke += __shfl_down_sync(0xffffffffu, ke, o);
+    mr = fmin(mr, __shfl_down_sync(0xffffffffu, mr, o));
+    mp = fmin(mp, __shfl_down_sync(0xffffffffu, mp, o));
+  }
+  if (lane == 0) { r[0][warp] = ke; r[1][warp] = mr; r[2][warp] = mp; }
+  __syncthreads();
+  if (warp == 0) {
+    ke = lane < nw ? r[0][lane] : 0.0;
+    mr = lane < nw ? r[1][lane] : 1e300;
+    mp = lane < nw ? r[2][lane] : 1e300;
+    for (int o = 16; o > 0; o >>= 1) {
+      ke += __shfl_down_sync(0xffffffffu, ke, o);
+      mr = fmin(mr, __shfl_down_sync(0xffffffffu, mr, o));
+      mp = fmin(mp, __shfl_down_sync(0xffffffffu, mp, o));
+    }
+    if (lane == 0) {
+      S.partials[3 * bid] = ke;
+      S.partials[3 * bid + 1] = mr;
+      S.partials[3 * bid + 2] = mp;
+      __threadfence();
+      unsigned t = atomicAdd(S.counter, 1u);
+      am_last = (t == (unsigned)(nb - 1));
+    }
+  }
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+  ke = 0.0; mr = 1e300; mp = 1e300;
+  for (long long b = tid; b < nb; b += nt) {
+    ke += __ldcg(S.partials + 3 * b);
+    mr = fmin(mr, __ldcg(S.partials + 3 * b + 1));
+    mp = fmin(mp, __ldcg(S.partials + 3 * b + 2));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    ke += __shfl_down_sync(0xffffffffu, ke, o);
+    mr = fmin(mr, __shfl_down_sync(0xffffffffu, mr, o));
+    mp = fmin(mp, __shfl_down_sync(0xffffffffu, mp, o));
+  }
+  __syncthreads();
+  if (lane == 0) { r[0][warp] = ke; r[1][warp] = mr; r[2][warp] = mp; }
+  __syncthreads();
+  if (tid == 0) {
+    ke = 0.0; mr = 1e300; mp = 1e300;
+    for (int w = 0; w < nw; ++w) {
+      ke += r[0][w]; mr = fmin(mr, r[1][w]); mp = fmin(mp, r[2][w]);
+    }
+    const long long it = *S.iter;
+    double nrm = sqrt(ke / ((double)S.nx * (double)S.ny * (double)S.nz));
+    double kev = nrm * S.dimc2rho;
+    S.diag[0] = kev;
+    S.diag[1] = mr;
+    S.diag[2] = mp;
+    S.diag[3] = (double)it;
+    bool fail = !(kev <= 1000.0) || !(mr > 0.0) || !(mp > 0.0);
+    if (fail && *S.fail_iter < 0) *S.fail_iter = it;
+    *S.iter = it + 1;
+    *S.counter = 0u;
+  }
+}
+
+// ------------------------------------------ MP_QUIET_3D, precision form
+// RHS.f90:18-175 fused with one RK stage (as k_stage_quiet of step.cu),
+// FP32 with depth-scaled state.  Field scales: l = 0 rho, 1-3 v, 4 p.
+template <int TX, int TY, int MODE, bool BG1D>
+__global__ void __launch_bounds__(TX *TY)
+    k_quiet32(const Sim32 S, const float *__restrict__ a, const float *__restrict__ tin,
+              float *__restrict__ so, float beta, float bnext, int zchunk) {
+  constexpr int HX = TX + 10, HY = TY + 10;
+  __shared__ float t_vx[HY][HX], t_vy[HY][HX], t_p[HY][HX];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int nx = S.nx, ny = S.ny, nz = S.nz;
+  const long long N = S.N, NXY = (long long)nx * ny;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int i = x0 + tx, j = y0 + ty;
+  const bool act = i < nx && j < ny;
+  const bool per = S.periodic;
+  const int k0 = blockIdx.z * zchunk, k1 = min(nz, k0 + zchunk);
+  const long long col = (long long)j * nx + i;
+  const long long it = *S.iter;
+  const float Tp = pulse_time32(S, it);
+  const float dt = (float)S.deltat;
+  const int gc = act ? S.colx[i] + S.bxdim * S.coly[j] : 0;
+  const int xo = origin32(x0, TX, nx, per), yo = origin32(y0, TY, ny, per);
+  const int cx0 = x0 - xo, cy0 = y0 - yo;
+  const float *isc = S.isc, *sc = S.sc;
+
+  float wvz[11], wp[11];  // physical values
+  const int b0 = min(k0 - 5, nz - 11);
+#pragma unroll
+  for (int m = 0; m < 11; ++m) {
+    const int kk = b0 + m;
+    const bool ok = act && kk >= 0;
+    const long long id = (long long)kk * NXY + col;
+    wvz[m] = ok ? __ldg(tin + 3 * N + id) * isc[3 * nz + kk] : 0.f;
+    wp[m] = ok ? __ldg(tin + 4 * N + id) * isc[4 * nz + kk] : 0.f;
+  }
+  double ke = 0.0, mr = 1e300, mp = 1e300;
+
+  for (int k = k0; k < k1; ++k) {
+    if (k > k0 && k <= nz - 6) {
+      const long long id = (long long)(k + 5) * NXY + col;
+      shift32(wvz, act ? __ldg(tin + 3 * N + id) * isc[3 * nz + k + 5] : 0.f);
+      shift32(wp, act ? __ldg(tin + 4 * N + id) * isc[4 * nz + k + 5] : 0.f);
+    }
+    const long long kb = (long long)k * NXY;
+    __syncthreads();
+    for (int t = tid; t < HY * HX; t += TX * TY) {
+      const int ly = t / HX, lx = t - ly * HX;
+      const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
+      if (!inx && !iny) continue;
+      int gx = xo + lx, gy = yo + ly;
+      bool ok;
+      if (per) {
+        gx = wrap32(gx, nx);
+        gy = wrap32(gy, ny);
+        ok = true;
+      } else {
+        ok = gx >= 0 && gx < nx && gy >= 0 && gy < ny;
+      }
+      const long long id = kb + (long long)gy * nx + gx;
+      if (iny) t_vx[ly][lx] = ok ? __ldg(tin + N + id) : 0.f;
+      if (inx) t_vy[ly][lx] = ok ? __ldg(tin + 2 * N + id) : 0.f;
+      t_p[ly][lx] = ok ? __ldg(tin + 4 * N + id) : 0.f;
+    }
+    __syncthreads();
+    if (!act) continue;
+    const long long id = kb + col;
+    float isv[5], scv[5];
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+      isv[l] = isc[l * nz + k];
+      scv[l] = sc[l * nz + k];
+    }
+    float av[5], tv[5];
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+      const float st = __ldg(tin + l * N + id);
+      av[l] = MODE == F_FIRST ? st : __ldg(a + l * N + id);
+      tv[l] = st * isv[l];
+    }
+    const float rho = tv[0], vx = tv[1], vy = tv[2], vz = tv[3], p = tv[4];
+    const int ry = cy0 + ty, rx = cx0 + tx;
+    const float sx = (float)S.stretchx, sy = (float)S.stretchy;
+    float dvxdx = isv[1] * dxy32(i, nx, per, sx, [&](int g) { return t_vx[ry][g - xo]; });
+    float gpx = isv[4] * dxy32(i, nx, per, sx, [&](int g) { return t_p[ry][g - xo]; });
+    float dvydy = isv[2] * dxy32(j, ny, per, sy, [&](int g) { return t_vy[g - yo][rx]; });
+    float gpy = isv[4] * dxy32(j, ny, per, sy, [&](int g) { return t_p[g - yo][rx]; });
+    const float szk = __ldg(S.stretch + k);
+    float dvzdz = dz32(wvz, k, nz, szk);
+    float gpz = dz32(wp, k, nz, szk);
+    if (k < S.zb.np) {
+      const long long f = kb + col;
+      cpml32<MODE>(S.zb, f, k, 1, beta, dt, gpz);
+      cpml32<MODE>(S.zb, f, k, 0, beta, dt, dvzdz);
+    } else if (S.zt.on && k >= nz - S.zt.np) {
+      const int kl = k - (nz - S.zt.np);
+      const long long f = (long long)kl * NXY + col;
+      cpml32<MODE>(S.zt, f, kl, 1, beta, dt, gpz);
+      cpml32<MODE>(S.zt, f, kl, 0, beta, dt, dvzdz);
+    }
+    if (S.xb.on) {
+      if (i < S.xb.np) {
+        const long long f = i + (long long)S.xb.np * (j + (long long)ny * k);
+        cpml32<MODE>(S.xb, f, i, 1, beta, dt, gpx);
+        cpml32<MODE>(S.xb, f, i, 0, beta, dt, dvxdx);
+      } else if (i >= nx - S.xt.np) {
+        const int il = i - (nx - S.xt.np);
+        const long long f = il + (long long)S.xt.np * (j + (long long)ny * k);
+        cpml32<MODE>(S.xt, f, il, 1, beta, dt, gpx);
+        cpml32<MODE>(S.xt, f, il, 0, beta, dt, dvxdx);
+      }
+      if (j < S.yb.np) {
+        const long long f = i + (long long)nx * (j + (long long)S.yb.np * k);
+        cpml32<MODE>(S.yb, f, j, 1, beta, dt, gpy);
+        cpml32<MODE>(S.yb, f, j, 0, beta, dt, dvydy);
+      } else if (j >= ny - S.yt.np) {
+        const int jl = j - (ny - S.yt.np);
+        const long long f = i + (long long)nx * (jl + (long long)S.yt.np * k);
+        cpml32<MODE>(S.yt, f, jl, 1, beta, dt, gpy);
+        cpml32<MODE>(S.yt, f, jl, 0, beta, dt, dvydy);
+      }
+    }
+    const long long bi = BG1D ? (long long)k : id;
+    const float r0 = __ldg(S.rho0 + bi), ri = __ldg(S.rhoinv + bi),
+                c2r = __ldg(S.c2rho0 + bi), grz = __ldg(S.grz + bi),
+                gp0 = __ldg(S.gpz + bi), sg = __ldg(S.sponge + bi);
+    const float gk = __ldg(S.gblk + (long long)gc * nz + k);
+    const float div = dvxdx + dvydy + dvzdz;
+    float R[5];
+    R[0] = -grz * vz - r0 * div - sg * rho;
+    R[1] = -ri * gpx - sg * vx;
+    R[2] = -ri * gpy - sg * vy;
+    R[3] = -ri * (gpz + rho * gk) - vz * sg;
+    if (S.frc.kind != SPARC_SRC_NONE) {
+      const float frc = forcing32(S, Tp, i, j, k);
+      if (S.frc.dir == 1) R[1] = R[1] + frc;
+      else if (S.frc.dir == 2) R[2] = R[2] + frc;
+      else R[3] = R[3] + frc;
+    }
+    R[4] = -c2r * div - vz * gp0 - sg * p;
+    const bool zero = k == 0 || k == nz - 1 ||
+                      (!per && (i == 0 || i == nx - 1 || j == 0 || j == ny - 1));
+    if (MODE == F_LAST) {
+      double an[5];
+#pragma unroll
+      for (int l = 0; l < 5; ++l) {
+        float c = S.carry[l * N + id];
+        const float t = zero ? av[l] : kahan(av[l], dt * (scv[l] * R[l]), c);
+        so[l * N + id] = t;
+        S.carry[l * N + id] = c;
+        an[l] = ((double)t - (double)c) * (double)isv[l];
+      }
+      const double p0v = __ldg(S.p0 + bi);
+      double m = ((double)r0 + an[0]) * (an[1] * an[1] + an[2] * an[2] + an[3] * an[3]) / 2.0;
+      ke += m * m;
+      mr = fmin(mr, (double)rho + (double)r0);
+      mp = fmin(mp, (double)p + p0v);
+    } else {
+#pragma unroll
+      for (int l = 0; l < 5; ++l)
+        so[l * N + id] = zero ? av[l] : av[l] + bnext * (scv[l] * R[l]);
+    }
+  }
+  if (MODE == F_LAST) diag_reduce32(S, ke, mr, mp);
+}
+
+// -------------------------------------------- MP_MHD_3D, precision form
+// The two-role TMA kernel of step.cu in FP32 with depth scaling (field
+// scales: 0 rho, 1-3 v, 4 p, 5-7 b).  Own-point arrays of a layer arrive by
+// TMA (32x8 FP32 boxes), halos by cp.async; one CTA of 512 threads per SM.
+struct TmaSet32 {
+  CUtensorMap m[18];
+};
+
+namespace t32 {
+constexpr int TX = 32, TY = 8, NC = TX * TY, NT = 2 * NC;
+constexpr int HX = TX + 10, HY = TY + 10, HS = HX * HY;
+constexpr int NH = 10, NO = 24;
+constexpr int BUF = ((NO * NC + NH * HS) + 31) / 32 * 32;  // 128-B multiple
+constexpr int XCH = 4 * NC;  // dvzdz, dzby (float) and |v_new|^2 (double)
+constexpr size_t SMEM = (2 * (size_t)BUF + XCH) * sizeof(float) + 128;
+constexpr long long WAIT_LIMIT = 1LL << 26;
+constexpr int O_RHO = 0, O_A = 1, O_BG = 9, O_P0 = 23;
+enum { B_RED, B_SPONGE, B_RHO0, B_GRX, B_GRY, B_GRZ, B_C2R, B_GPX, B_GPY,
+       B_GPZ, B_RHOINV, B_CBX, B_CBY, B_CBZ };
+}  // namespace t32
+
+__device__ __forceinline__ unsigned sm_addr32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void cp4(float *dst, const float *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sm_addr32(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit32() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_wait1_32() {
+  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_init32(unsigned long long *bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sm_addr32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_tx32(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sm_addr32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void tma3d32(float *dst, const CUtensorMap *map, int x, int y,
+                                        int z, unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(sm_addr32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(sm_addr32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_wait32(unsigned long long *bar, unsigned parity,
+                                            int *err) {
+  for (long long n = 0; n < t32::WAIT_LIMIT; ++n) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(sm_addr32(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  atomicExch(err, 1);
+  return false;
+}
+
+// TMA = false: the own-point arrays are fetched by cp.async too (any nx).
+template <int MODE, bool TMA>
+__global__ void __launch_bounds__(t32::NT, 1)
+    k_mhd32(const Sim32 S, const __grid_constant__ TmaSet32 T,
+            const float *__restrict__ a, const float *__restrict__ tin,
+            float *__restrict__ so, float beta, float bnext, int zchunk, int mt,
+            int ma) {
+  using namespace t32;
+  extern __shared__ __align__(1024) float smem_raw32[];
+  __shared__ unsigned long long bar[2];
+  const int tx = threadIdx.x, ty = threadIdx.y, role = threadIdx.z;
+  const int tid = (role * TY + ty) * TX + tx, cid = ty * TX + tx;
+  float *smem = (float *)(((size_t)smem_raw32 + 127) & ~(size_t)127);
+  if (sm_addr32(smem) & 127u) {
+    if (tid == 0) atomicExch(S.err, 2);
+    return;
+  }
+  const int nx = S.nx, ny = S.ny, nz = S.nz;
+  const int N = (int)S.N, NXY = nx * ny;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int i = x0 + tx, j = y0 + ty;
+  const bool act = i < nx && j < ny;
+  const bool per = S.periodic;
+  const int k0 = blockIdx.z * zchunk, k1 = min(nz, k0 + zchunk);
+  const int col = j * nx + i;
+  const int xo = origin32(x0, TX, nx, per), yo = origin32(y0, TY, ny, per);
+  const int ry = y0 - yo + ty, rx = x0 - xo + tx;
+  const int own = ry * HX + rx;
+  const float *isc = S.isc, *sc = S.sc;
+  if (tid == 0) {
+    mbar_init32(&bar[0]);
+    mbar_init32(&bar[1]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto O = [&](int b, int slot) -> float { return smem[b * BUF + slot * NC + cid]; };
+  auto Hp = [&](int b, int slot) -> float * { return smem + b * BUF + NO * NC + slot * HS; };
+  float *X = smem + 2 * BUF;
+  int hs0 = -1, hs1 = -1, ho0 = 0, ho1 = 0;
+  {
+    const int cx0 = x0 - xo, cy0 = y0 - yo;
+    auto pos = [&](int t, int &hs, int &ho) {
+      if (t >= HS) return;
+      const int ly = t / HX, lx = t - ly * HX;
+      const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
+      if (!inx && !iny) return;
+      int gx = xo + lx, gy = yo + ly;
+      if (per) {
+        gx = wrap32(gx, nx);
+        gy = wrap32(gy, ny);
+      } else if (gx < 0 || gx >= nx || gy < 0 || gy >= ny) {
+        return;
+      }
+      hs = t;
+      ho = gy * nx + gx;
+    };
+    pos(tid, hs0, ho0);
+    pos(tid + NT, hs1, ho1);
+  }
+  const unsigned own_bytes =
+      (MODE == F_FIRST ? 15u : (MODE == F_MID ? 23u : 24u)) * NC * (unsigned)sizeof(float);
+  auto issue = [&](int k, int b) {
+    const int kb = k * NXY;
+    if (hs0 >= 0) {
+      float *h = Hp(b, 0) + hs0;
+      const int id = kb + ho0;
+#pragma unroll
+      for (int sl = 0; sl < 7; ++sl) cp4(h + sl * HS, tin + (sl + 1) * N + id);
+      cp4(h + 7 * HS, S.box + id);
+      cp4(h + 8 * HS, S.boy + id);
+      cp4(h + 9 * HS, S.boz + id);
+    }
+    if (hs1 >= 0) {
+      float *h = Hp(b, 0) + hs1;
+      const int id = kb + ho1;
+#pragma unroll
+      for (int sl = 0; sl < 7; ++sl) cp4(h + sl * HS, tin + (sl + 1) * N + id);
+      cp4(h + 7 * HS, S.box + id);
+      cp4(h + 8 * HS, S.boy + id);
+      cp4(h + 9 * HS, S.boz + id);
+    }
+    if (!TMA && act) {
+      float *ob = smem + b * BUF + cid;
+      const int id = kb + col;
+      if (role == 0) {
+        cp4(ob + O_RHO * NC, tin + id);
+        if (MODE != F_FIRST)
+#pragma unroll
+          for (int l = 0; l < 8; ++l) cp4(ob + (O_A + l) * NC, a + l * N + id);
+      } else {
+        const float *bg[14] = {S.red, S.sponge, S.rho0, S.grx, S.gry, S.grz,
+                               S.c2rho0, S.gpx, S.gpy, S.gpz, S.rhoinv, S.cbx, S.cby, S.cbz};
+#pragma unroll
+        for (int n = 0; n < 14; ++n) cp4(ob + (O_BG + n) * NC, bg[n] + id);
+        if (MODE == F_LAST) cp4(ob + O_P0 * NC, S.p0 + id);
+      }
+    }
+    cp_commit32();
+    if (TMA && tid == 0) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_tx32(&bar[b], own_bytes);
+      float *ob = smem + b * BUF;
+      tma3d32(ob + O_RHO * NC, &T.m[mt], x0, y0, k, &bar[b]);
+      if (MODE != F_FIRST)
+        for (int l = 0; l < 8; ++l)
+          tma3d32(ob + (O_A + l) * NC, &T.m[ma], x0, y0, l * nz + k, &bar[b]);
+      for (int n = 0; n < 14; ++n)
+        tma3d32(ob + (O_BG + n) * NC, &T.m[3 + n], x0, y0, k, &bar[b]);
+      if (MODE == F_LAST) tma3d32(ob + O_P0 * NC, &T.m[17], x0, y0, k, &bar[b]);
+    }
+  };
+  float w0[11], w1[11], w2[11];  // physical values
+  auto head = [&](int kk, float &v0, float &v1, float &v2) {
+    const int id = kk * NXY + col;
+    if (role == 0) {
+      v0 = __ldg(tin + 3 * N + id) * isc[3 * nz + kk];
+      v1 = __ldg(tin + 4 * N + id) * isc[4 * nz + kk];
+      v2 = __ldg(tin + 5 * N + id) * isc[5 * nz + kk];
+    } else {
+      const float iv = isc[nz + kk];
+      const float vx_ = __ldg(tin + N + id) * iv, vy_ = __ldg(tin + 2 * N + id) * iv,
+                  vz_ = __ldg(tin + 3 * N + id) * iv;
+      const float ox = __ldg(S.box + id), oy = __ldg(S.boy + id), oz = __ldg(S.boz + id);
+      v0 = -vz_ * oy + vy_ * oz;
+      v1 = -vx_ * oz + vz_ * ox;
+      v2 = __ldg(tin + 6 * N + id) * isc[6 * nz + kk];
+    }
+  };
+  issue(k0, 0);
+  {
+    const int b0 = min(k0 - 5, nz - 11);
+#pragma unroll
+    for (int m = 0; m < 11; ++m) {
+      const int kk = b0 + m;
+      if (act && kk >= 0) head(kk, w0[m], w1[m], w2[m]);
+      else w0[m] = w1[m] = w2[m] = 0.f;
+    }
+  }
+  double ke = 0.0, mr = 1e300, mp = 1e300;
+  unsigned phase = 0;
+  bool ok = true;
+  const float dt = (float)S.deltat;
+
+  for (int k = k0; k < k1; ++k) {
+    const int b = (k - k0) & 1;
+    float h0 = 0, h1 = 0, h2 = 0;
+    const bool sh = k > k0 && k <= nz - 6;
+    if (sh && act) head(k + 5, h0, h1, h2);
+    if (k + 1 < k1) issue(k + 1, b ^ 1);
+    else cp_commit32();
+    cp_wait1_32();
+    if (TMA) {
+      ok = mbar_wait32(&bar[b], (phase >> b) & 1u, S.err);
+      phase ^= 1u << b;
+    }
+    if (!__syncthreads_and(ok)) { ok = false; break; }
+    if (sh) { shift32(w0, h0); shift32(w1, h1); shift32(w2, h2); }
+    float *H7 = Hp(b, 7), *H8 = Hp(b, 8), *H9 = Hp(b, 9);
+    const float ox = H7[own], oy = H8[own], oz = H9[own];
+    __syncthreads();
+    {
+      const float *H0 = Hp(b, 0), *H1 = Hp(b, 1), *H2 = Hp(b, 2);
+      const int cx0 = x0 - xo, cy0 = y0 - yo;
+      for (int t = tid; t < HS; t += NT) {
+        const int ly = t / HX, lx = t - ly * HX;
+        const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
+        if (!inx && !iny) continue;
+        const float vx_ = H0[t], vy_ = H1[t], vz_ = H2[t];
+        const float bx0 = H7[t], by0 = H8[t], bz0 = H9[t];
+        H7[t] = -vz_ * by0 + vy_ * bz0;  // fluxes in stored velocity units
+        H8[t] = -vx_ * bz0 + vz_ * bx0;
+        H9[t] = -vy_ * bx0 + vx_ * by0;
+      }
+    }
+    __syncthreads();
+    const int id = k * NXY + col;
+    const float szk = __ldg(S.stretch + k);
+    const float sx = (float)S.stretchx, sy = (float)S.stretchy;
+    auto DX = [&](int slot) {
+      const float *row = Hp(b, slot) + ry * HX;
+      if (per || (i >= 5 && i < nx - 5)) return sx * csum32(row + (i - 5 - xo), 1);
+      return dxy32(i, nx, per, sx, [&](int g) { return row[g - xo]; });
+    };
+    auto DY = [&](int slot) {
+      const float *colp = Hp(b, slot) + rx;
+      if (per || (j >= 5 && j < ny - 5)) return sy * csum32(colp + (j - 5 - yo) * HX, HX);
+      return dxy32(j, ny, per, sy, [&](int g) { return colp[(g - yo) * HX]; });
+    };
+    const bool zpml = S.zb.on && (k < S.zb.np || k >= nz - S.zt.np);
+    const bool xpml = S.xb.on && act && (i < S.xb.np || i >= nx - S.xt.np);
+    const bool ypml = S.xb.on && act && (j < S.yb.np || j >= ny - S.yt.np);
+    auto pz = [&](int slot, float &d) {
+      const bool bot = k < S.zb.np;
+      const Face32 &F = bot ? S.zb : S.zt;
+      const int kl = bot ? k : k - (nz - S.zt.np);
+      cpml32<MODE>(F, (long long)kl * NXY + col, kl, slot, beta, dt, d);
+    };
+    auto px = [&](int slot, float &d) {
+      const bool bot = i < S.xb.np;
+      const Face32 &F = bot ? S.xb : S.xt;
+      const int il = bot ? i : i - (nx - S.xt.np);
+      cpml32<MODE>(F, il + (long long)F.np * (j + (long long)ny * k), il, slot, beta, dt, d);
+    };
+    auto py = [&](int slot, float &d) {
+      const bool bot = j < S.yb.np;
+      const Face32 &F = bot ? S.yb : S.yt;
+      const int jl = bot ? j : j - (ny - S.yt.np);
+      cpml32<MODE>(F, i + (long long)nx * (jl + (long long)F.np * k), jl, slot, beta, dt, d);
+    };
+    auto Hv = [&](int slot) { return Hp(b, slot)[own]; };
+    const float iv = isc[nz + k];  // velocity (and flux) scale of this layer
+    float d0 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0, d6 = 0, d7 = 0, d8 = 0;
+    if (act) {
+      const float ip = isc[4 * nz + k], ib = isc[5 * nz + k];
+      if (role == 0) {
+        d0 = ip * DX(3); d5 = ib * DX(6); d7 = ib * DX(5);
+        d1 = ip * DY(3); d4 = ib * DY(6); d8 = ib * DY(4);
+        d3 = dz32(w0, k, nz, szk); d2 = dz32(w1, k, nz, szk); d6 = dz32(w2, k, nz, szk);
+        if (zpml) { pz(1, d2); pz(0, d3); pz(2, d6); }
+        if (xpml) { px(1, d0); px(3, d5); px(2, d7); }
+        if (ypml) { py(1, d1); py(3, d4); py(2, d8); }
+        X[cid] = d3;
+      } else {
+        d0 = iv * DX(0); d2 = iv * DX(9); d3 = iv * DX(8);
+        d1 = iv * DY(1); d4 = iv * DY(9); d5 = iv * DY(7);
+        d6 = dz32(w0, k, nz, szk); d7 = dz32(w1, k, nz, szk); d8 = dz32(w2, k, nz, szk);
+        if (zpml) { pz(4, d7); pz(5, d6); pz(3, d8); }
+        if (xpml) { px(0, d0); px(4, d2); px(5, d3); }
+        if (ypml) { py(0, d1); py(4, d4); py(5, d5); }
+        X[NC + cid] = d8;
+      }
+    }
+    __syncthreads();
+    double an_rho = 0.0;
+    if (act) {
+      const bool zero = k == 0 || k == nz - 1 ||
+                        (!per && (i == 0 || i == nx - 1 || j == 0 || j == ny - 1));
+      const float fac = MODE == F_LAST ? dt : bnext;
+      const float rho = O(b, O_RHO) * isc[k], vx = Hv(0) * iv, vy = Hv(1) * iv,
+                  vz = Hv(2) * iv;
+      const float red = O(b, O_BG + B_RED), sg = O(b, O_BG + B_SPONGE);
+      if (role == 0) {
+        const float ib = isc[5 * nz + k];
+        const float dzby = X[NC + cid];
+        const float cbx = d4 - dzby, cby = -d5 + d6, cbz = d7 - d8;
+        const float c1 = cby * oz - cbz * oy, c2 = ox * cbz - cbx * oz, c3 = cbx * oy - cby * ox;
+        const float ri = O(b, O_BG + B_RHOINV);
+        float vxr = -ri * (d0 - (c1 * red)) - sg * vx;
+        float vyr = -ri * (d1 - (c2 * red)) - sg * vy;
+        float vzr = -ri * (d2 - (c3 * red)) - sg * vz;
+        const float bx = Hv(4) * ib, by = Hv(5) * ib, bz = Hv(6) * ib;
+        const float qx = O(b, O_BG + B_CBX), qy = O(b, O_BG + B_CBY), qz = O(b, O_BG + B_CBZ);
+        const float e1 = qy * bz - qz * by, e2 = bx * qz - qx * bz, e3 = qx * by - qy * bx;
+        vxr = vxr + ri * e1 * red;
+        vyr = vyr + ri * e2 * red;
+        vzr = vzr + ri * e3 * red;
+        const int gc = S.colx[i] + S.bxdim * S.coly[j];
+        vzr = vzr - ri * rho * __ldg(S.gblk + gc * nz + k);
+        if (S.frc.kind != SPARC_SRC_NONE) {
+          const long long it = *S.iter;
+          const float frc = forcing32(S, pulse_time32(S, it), i, j, k);
+          if (S.frc.dir == 1) vxr = vxr + frc;
+          else if (S.frc.dir == 2) vyr = vyr + frc;
+          else vzr = vzr + frc;
+        }
+        const float sv = sc[nz + k];
+        const float R[3] = {vxr, vyr, vzr};
+        double vsq = 0.0;
+#pragma unroll
+        for (int l = 1; l < 4; ++l) {
+          const float av = MODE == F_FIRST ? Hv(l - 1) : O(b, O_A + l);
+          float an;
+          if (MODE == F_LAST) {
+            float c = S.carry[l * N + id];
+            an = zero ? av : kahan(av, fac * (sv * R[l - 1]), c);
+            S.carry[l * N + id] = c;
+            const double ph = ((double)an - (double)c) * (double)iv;
+            vsq += ph * ph;
+          } else {
+            an = zero ? av : av + fac * (sv * R[l - 1]);
+          }
+          so[l * N + id] = an;
+        }
+        if (MODE == F_LAST) ((double *)(X + 2 * NC))[cid] = vsq;
+      } else {
+        const float p = Hv(3) * isc[4 * nz + k];
+        const float dvzdz = X[cid];
+        const float div = d0 + d1 + dvzdz;
+        const float r0 = O(b, O_BG + B_RHO0);
+        const float Rr = -O(b, O_BG + B_GRX) * vx - O(b, O_BG + B_GRY) * vy -
+                         O(b, O_BG + B_GRZ) * vz - r0 * div - sg * rho;
+        const float Rp = -O(b, O_BG + B_C2R) * div - vx * O(b, O_BG + B_GPX) -
+                         vy * O(b, O_BG + B_GPY) - vz * O(b, O_BG + B_GPZ) - sg * p;
+        const float Rb[3] = {red * (d4 - d7), red * (d6 - d2), red * (d3 - d5)};
+        const float Rs[5] = {Rr, Rp, Rb[0], Rb[1], Rb[2]};
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+          const int l = q == 0 ? 0 : (q == 1 ? 4 : q + 3);
+          const float av = MODE == F_FIRST ? (l == 0 ? O(b, O_RHO) : Hv(l - 1)) : O(b, O_A + l);
+          const float s = sc[l * nz + k];
+          float an;
+          if (MODE == F_LAST) {
+            float c = S.carry[l * N + id];
+            an = zero ? av : kahan(av, fac * (s * Rs[q]), c);
+            S.carry[l * N + id] = c;
+            if (q == 0) an_rho = ((double)an - (double)c) * (double)isc[k];
+          } else {
+            an = zero ? av : av + fac * (s * Rs[q]);
+          }
+          so[l * N + id] = an;
+        }
+        if (MODE == F_LAST) {
+          mr = fmin(mr, (double)rho + (double)r0);
+          mp = fmin(mp, (double)p + (double)O(b, O_P0));
+        }
+      }
+    }
+    if (MODE == F_LAST) {
+      __syncthreads();
+      if (act && role == 1) {
+        const double m = ((double)O(b, O_BG + B_RHO0) + an_rho) *
+                         ((double *)(X + 2 * NC))[cid] / 2.0;
+        ke += m * m;
+      }
+    }
+    __syncthreads();
+  }
+  if (!ok) {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    if (TMA && tid == 0) {
+      mbar_wait32(&bar[0], phase & 1u, S.err);
+      mbar_wait32(&bar[1], (phase >> 1) & 1u, S.err);
+    }
+    return;
+  }
+  if (MODE == F_LAST) diag_reduce32(S, ke, mr, mp);
+}
+
+// ---------------------------------------------- FILTER_VARS, precision form
+// One direction of FILTER_VARS over all fields in FP32 (derivatives.f90:
+// 659-703).  x and y filters act on the stored values (their scale is
+// constant in a layer); the z filter and its edge pre-averaging act on
+// physical values and scale back.
+struct Filt32 {
+  int nx, ny, nz, periodic, g, mode2, V;
+  long long N;
+  float s;
+  const float *sc, *isc;
+};
+
+template <int DIR>
+__global__ void k_filter32(Filt32 F, const float *__restrict__ in, float *__restrict__ out) {
+  const long long total = F.N * F.V;
+  const int n = DIR == 0 ? F.nx : (DIR == 1 ? F.ny : F.nz);
+  const long long st = DIR == 0 ? 1 : (DIR == 1 ? F.nx : (long long)F.nx * F.ny);
+  const bool per = DIR != 2 && F.periodic;
+  const bool avg = DIR == 2 || !F.periodic;
+  const int g = F.g;
+  const float *c = f_df[DIR == 2 ? 1 : 0];
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int l = (int)(t / F.N);
+    const long long pnt = t - (long long)l * F.N;
+    int q;
+    if (DIR == 0) q = (int)(pnt % F.nx);
+    else if (DIR == 1) q = (int)((pnt / F.nx) % F.ny);
+    else q = (int)(pnt / ((long long)F.nx * F.ny));
+    const long long base = t - (long long)q * st;
+    // physical (z) or stored (x, y) value at index qq
+    auto val = [&](int qq) -> float {
+      const float v = __ldg(in + base + (long long)qq * st);
+      return DIR == 2 ? v * F.isc[l * F.nz + qq] : v;
+    };
+    auto pre = [&](int qq) -> float {
+      if (avg && ((qq >= 1 && qq <= g - 1) || (qq >= n - g && qq <= n - 2)))
+        return (val(qq + 1) + val(qq - 1)) / 2.0f;
+      return val(qq);
+    };
+    const float pq = pre(q);
+    float filt;
+    if (!per && (q < g || q >= n - g)) {
+      filt = (DIR != 2 && g == 3) ? 0.f : pq;
+    } else {
+      float s = 0.f;
+      for (int m = 0; m < 2 * g + 1; ++m) {
+        int qq = q - g + m;
+        if (per) qq = wrap32(qq, n);
+        s += pre(qq) * c[m];
+      }
+      filt = s;
+    }
+    float r = F.mode2 ? pq - F.s * filt : filt;
+    if (DIR == 2) r = r * F.sc[l * F.nz + q];
+    out[t] = r;
+  }
+}
+
+int launch_filter32(Handle *h, int dir, const float *in, float *out, cudaStream_t s) {
+  Filt32 F;
+  F.nx = h->nx; F.ny = h->ny; F.nz = h->nz;
+  F.periodic = h->periodic ? 1 : 0;
+  F.g = dir == 2 ? h->gz : h->gxy;
+  F.mode2 = F.g == 3;
+  F.V = h->V;
+  F.N = h->N;
+  F.s = (float)(dir == 2 ? h->P.s_z : h->P.s_xy);
+  F.sc = h->f_sc;
+  F.isc = h->f_isc;
+  long long total = F.N * F.V;
+  unsigned nb = (unsigned)std::min<long long>((total + 255) / 256, 148 * 32);
+  if (dir == 0) k_filter32<0><<<nb, 256, 0, s>>>(F, in, out);
+  else if (dir == 1) k_filter32<1><<<nb, 256, 0, s>>>(F, in, out);
+  else k_filter32<2><<<nb, 256, 0, s>>>(F, in, out);
+  ++h->launches;
+  return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
+}
+
+// ------------------------------------------------ PULSE = 2, precision form
+// As k_psr of step.cu with an FP32 forcing buffer (the sum over pulses is
+// accumulated in FP32).
+struct Psr32 {
+  int nx, ny, klo, nblocks, bx, bxy;
+  long long init;
+  double timestep, st;
+  const int *off, *idx, *colx, *coly, *colz;
+  const double *zv, *ptime;
+  const float *px, *py, *sd, *ssb;
+  const unsigned char *mask;
+  float *out;
+  const long long *iter;
+};
+
+__global__ void k_psr32(Psr32 D) {
+  extern __shared__ float shf[];
+  const int k = D.klo + blockIdx.z;
+  const int e0 = D.off[k], e1 = D.off[k + 1], ne = e1 - e0;
+  float *sT = shf;
+  int *sN = (int *)(shf + ne);
+  const long long it = *D.iter;
+  const double t = (double)it * D.timestep;
+  const double passes = (it == D.init) ? 2.0 : 1.0;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  for (int e = tid; e < ne; e += blockDim.x * blockDim.y) {
+    const int n = D.idx[e0 + e];
+    const double amp = D.ptime[3 * n], t0 = D.ptime[3 * n + 1], t1 = D.ptime[3 * n + 2];
+    double v = amp * sin(2.0 * PI * (t - t1) / t0);
+    v = v * exp(-((t - t1) * (t - t1)) / (2.0 * (D.st * D.st)));
+    sT[e] = (float)(v * D.zv[e0 + e] * passes);
+    sN[e] = n;
+  }
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= D.nx || j >= D.ny) return;
+  const int blk = D.colx[i] + D.bx * D.coly[j] + D.bxy * D.colz[k];
+  float f = 0.f;
+  for (int e = 0; e < ne; ++e) {
+    const int n = sN[e];
+    if (!D.mask[(long long)n * D.nblocks + blk]) continue;
+    f = f + sT[e] * (D.px[(long long)n * D.nx + i] * D.py[(long long)n * D.ny + j]);
+  }
+  const long long g = ((long long)k * D.ny + j) * D.nx + i;
+  D.out[((long long)blockIdx.z * D.ny + j) * D.nx + i] = f * D.sd[g] * D.ssb[g];
+}
+
+int launch_psr32(Handle *h, cudaStream_t s) {
+  if (h->src.kind != SPARC_SRC_PSR || h->psr_khi <= h->psr_klo) return SPARC_OK;
+  Psr32 D;
+  D.nx = h->nx; D.ny = h->ny;
+  D.klo = h->psr_klo;
+  D.nblocks = h->nblocks;
+  D.bx = h->P.block_x;
+  D.bxy = h->P.block_x * h->P.block_y;
+  D.init = h->src.init;
+  D.timestep = h->P.timestep;
+  D.st = h->src.psr_st;
+  D.off = h->d_plane_off;
+  D.idx = h->d_plane_idx;
+  D.colx = h->d_colx;
+  D.coly = h->d_coly;
+  D.colz = h->d_colx + h->nx + h->ny;
+  D.zv = h->d_plane_z;
+  D.ptime = h->d_ptime;
+  D.px = h->f_px;
+  D.py = h->f_py;
+  D.sd = h->f_sd;
+  D.ssb = h->f_ssb;
+  D.mask = h->d_pmask;
+  D.out = h->f_psr;
+  D.iter = h->d_iter;
+  dim3 blk(32, 8);
+  dim3 grd((h->nx + 31) / 32, (h->ny + 7) / 8, h->psr_khi - h->psr_klo);
+  size_t smem = h->pulses.size() * (sizeof(float) + sizeof(int));
+  k_psr32<<<grd, blk, smem, s>>>(D);
+  ++h->launches;
+  return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
+}
+
+// ------------------------------------------------------ FP64 -> FP32 copy
+__global__ void k_d2f(long long n, const double *in, float *out) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x)
+    out[t] = (float)in[t];
+}
+
+int to_float(const double *in, float *out, long long n, cudaStream_t s) {
+  if (n <= 0) return SPARC_OK;
+  unsigned nb = (unsigned)std::min<long long>((n + 255) / 256, 148 * 32);
+  k_d2f<<<nb, 256, 0, s>>>(n, in, out);
+  return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
+}
+
+// ------------------------------------------------------------- launchers
+Sim32 make_sim32(Handle *h) {
+  Sim32 S{};
+  S.nx = h->nx; S.ny = h->ny; S.nz = h->nz; S.N = h->N;
+  S.periodic = h->periodic ? 1 : 0;
+  S.magnetic = h->magnetic ? 1 : 0;
+  S.bg1d = h->bg1d ? 1 : 0;
+  S.V = h->V;
+  S.stretchx = h->stretchx;
+  S.stretchy = h->stretchy;
+  S.stretch = h->f_stretch;
+  S.deltat = h->deltat;
+  S.dimc2rho = (h->dimc * h->dimc) * h->dimrho;
+  const float *const *b = h->f_bg;
+  S.rho0 = b[FB_RHO0]; S.p0 = b[FB_P0]; S.rhoinv = b[FB_RHOINV];
+  S.c2rho0 = b[FB_C2R]; S.grz = b[FB_GRZ]; S.gpz = b[FB_GPZ]; S.sponge = b[FB_SPONGE];
+  S.box = b[FB_BOX]; S.boy = b[FB_BOY]; S.boz = b[FB_BOZ];
+  S.cbx = b[FB_CBX]; S.cby = b[FB_CBY]; S.cbz = b[FB_CBZ];
+  S.grx = b[FB_GRX]; S.gry = b[FB_GRY]; S.gpx = b[FB_GPX]; S.gpy = b[FB_GPY];
+  S.red = b[FB_RED];
+  S.gblk = h->f_gblk;
+  S.colx = h->d_colx;
+  S.coly = h->d_coly;
+  S.bxdim = h->P.block_x;
+  S.zb = h->f_faces[0]; S.zt = h->f_faces[1];
+  S.xb = h->f_faces[2]; S.xt = h->f_faces[3];
+  S.yb = h->f_faces[4]; S.yt = h->f_faces[5];
+  ForcingT<float> &F = S.frc;
+  F.kind = h->src.kind;
+  F.dir = h->src.dir;
+  F.init = h->src.init;
+  F.fx = h->f_fx; F.fy = h->f_fy; F.fz = h->f_fz;
+  F.amp_c = h->src.amp / 0.56458272 / h->dimc;
+  F.t0 = h->src.t0; F.t1 = h->src.t1; F.st = h->src.st;
+  F.timestep = h->P.timestep;
+  F.psr = h->f_psr;
+  F.klo = h->psr_klo;
+  F.khi = h->psr_khi;
+  S.sc = h->f_sc;
+  S.isc = h->f_isc;
+  S.carry = h->f_carry;
+  S.iter = h->d_iter;
+  S.err = h->d_err;
+  S.partials = h->d_partials;
+  S.counter = h->d_counter;
+  S.diag = h->d_diag;
+  S.fail_iter = h->d_fail;
+  return S;
+}
+
+template <int TX, int TY>
+static void launch_quiet32(Handle *h, const Sim32 &S, int mode, const float *a,
+                           const float *tin, float *so, float beta, float bnext,
+                           cudaStream_t s) {
+  dim3 blk(TX, TY);
+  dim3 grd((h->nx + TX - 1) / TX, (h->ny + TY - 1) / TY, (h->nz + h->zchunk - 1) / h->zchunk);
+#define QL32(M, B) k_quiet32<TX, TY, M, B><<<grd, blk, 0, s>>>(S, a, tin, so, beta, bnext, h->zchunk)
+  if (S.bg1d) {
+    if (mode == F_FIRST) QL32(F_FIRST, true);
+    else if (mode == F_MID) QL32(F_MID, true);
+    else QL32(F_LAST, true);
+  } else {
+    if (mode == F_FIRST) QL32(F_FIRST, false);
+    else if (mode == F_MID) QL32(F_MID, false);
+    else QL32(F_LAST, false);
+  }
+#undef QL32
+}
+
+int launch_stage32(Handle *h, const Sim32 &S, int stage, const float *a,
+                   const float *tin, float *so, cudaStream_t s) {
+  const float beta = (float)h->betas[stage - 1];
+  const float bnext = (float)(stage < 5 ? h->betas[stage] : h->deltat);
+  const int mode = stage == 1 ? F_FIRST : (stage == 5 ? F_LAST : F_MID);
+  if (h->magnetic) {
+    using namespace t32;
+    int mt = -1, ma = -1;
+    for (int b = 0; b < 3; ++b) {
+      if (h->fbuf[b] == tin) mt = b;
+      if (h->fbuf[b] == a) ma = b;
+    }
+    if (mt < 0 || ma < 0) return SPARC_ERR_INVALID;
+    TmaSet32 T;
+    if (h->tma32)
+      for (int n = 0; n < 18; ++n) T.m[n] = h->tmaps32[n];
+    else
+      std::memset(&T, 0, sizeof(T));
+    dim3 blk(TX, TY, 2);
+    dim3 grd((h->nx + TX - 1) / TX, (h->ny + TY - 1) / TY, (h->nz + h->zchunk - 1) / h->zchunk);
+    const int sm = (int)SMEM;
+#define ML32(M, U)                                                                    \
+  do {                                                                                \
+    cudaFuncSetAttribute(k_mhd32<M, U>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); \
+    k_mhd32<M, U><<<grd, blk, SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt, ma); \
+  } while (0)
+    if (h->tma32) {
+      if (mode == F_FIRST) ML32(F_FIRST, true);
+      else if (mode == F_MID) ML32(F_MID, true);
+      else ML32(F_LAST, true);
+    } else {
+      if (mode == F_FIRST) ML32(F_FIRST, false);
+      else if (mode == F_MID) ML32(F_MID, false);
+      else ML32(F_LAST, false);
+    }
+#undef ML32
+  } else {
+    if (h->tx == 32) launch_quiet32<32, 8>(h, S, mode, a, tin, so, beta, bnext, s);
+    else launch_quiet32<16, 8>(h, S, mode, a, tin, so, beta, bnext, s);
+  }
+  ++h->launches;
+  return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
+}
+
+// FP32 tensor maps (32x8x1 boxes) of the own-point arrays of the MHD kernel
+// (needs 16-byte row strides: nx a multiple of 4).
+int encode_tensor_maps32(Handle *h) {
+  h->tma32 = false;
+  if (!h->magnetic || (h->nx & 3)) return SPARC_OK;
+  void *fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+          cudaSuccess || !fn || q != cudaDriverEntryPointSuccess) {
+    cudaGetLastError();
+    return SPARC_OK;
+  }
+  auto enc = (CUresult(*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                          const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                          const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                          CUtensorMapL2promotion, CUtensorMapFloatOOBfill))fn;
+  auto one = [&](CUtensorMap *m, const float *base, unsigned long long depth) {
+    cuuint64_t dims[3] = {(cuuint64_t)h->nx, (cuuint64_t)h->ny, (cuuint64_t)depth};
+    cuuint64_t strides[2] = {(cuuint64_t)h->nx * 4, (cuuint64_t)h->nx * h->ny * 4};
+    cuuint32_t box[3] = {32, 8, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)base, dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  };
+  bool ok = true;
+  for (int b = 0; b < 3; ++b)
+    ok = ok && one(&h->tmaps32[b], h->fbuf[b], (unsigned long long)h->nz * h->V);
+  const int order[15] = {FB_RED, FB_SPONGE, FB_RHO0, FB_GRX, FB_GRY, FB_GRZ, FB_C2R,
+                         FB_GPX, FB_GPY, FB_GPZ, FB_RHOINV, FB_CBX, FB_CBY, FB_CBZ, FB_P0};
+  for (int n = 0; n < 15; ++n)
+    ok = ok && h->f_bg[order[n]] && one(&h->tmaps32[3 + n], h->f_bg[order[n]], h->nz);
+  h->tma32 = ok;
+  return SPARC_OK;
+}
+
+// ------------------------------------------------------ precision-form setup
+// Runs after the FP64 setup (setup.cu): derives the depth scales from the
+// background column (1,1,:), converts the coefficients, CPML profiles and
+// tables to FP32 and releases the FP64 arrays that the FP32 path does not
+// read.
+static float *f_up(Handle *h, const double *src, long long n, cudaStream_t s) {
+  float *d = (float *)dev_alloc(h, (size_t)std::max<long long>(n, 1) * sizeof(float));
+  if (!d) return nullptr;
+  if (src && n > 0 && to_float(src, d, n, s)) return nullptr;
+  return d;
+}
+
+int setup32(Handle *h) {
+  cudaStream_t s = h->stream;
+  const int nz = h->nz, V = h->V;
+  const long long N = h->N, NXY = (long long)h->nx * h->ny;
+  // depth scales: rho 1/rho0, v sqrt(rho0), p 1/(rho0 c0^2), b 1
+  std::vector<double> r0(nz), c2r(nz);
+  if (cudaMemcpy2D(r0.data(), 8, h->rho0, NXY * 8, 8, nz, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy2D(c2r.data(), 8, h->c2rho0, NXY * 8, 8, nz, cudaMemcpyDeviceToHost) !=
+          cudaSuccess)
+    return SPARC_ERR_CUDA;
+  std::vector<float> sc((size_t)2 * V * nz);
+  for (int l = 0; l < V; ++l)
+    for (int k = 0; k < nz; ++k) {
+      double v = 1.0;
+      if (l == 0) v = 1.0 / r0[k];
+      else if (l <= 3) v = std::sqrt(r0[k]);
+      else if (l == 4) v = 1.0 / c2r[k];
+      sc[(size_t)l * nz + k] = (float)v;
+      sc[(size_t)(V + l) * nz + k] = (float)(1.0 / v);
+    }
+  h->f_sc = (float *)dev_alloc(h, sc.size() * sizeof(float));
+  if (!h->f_sc) return SPARC_ERR_NOMEM;
+  h->f_isc = h->f_sc + (size_t)V * nz;
+  if (cudaMemcpy(h->f_sc, sc.data(), sc.size() * sizeof(float), cudaMemcpyHostToDevice) !=
+      cudaSuccess)
+    return SPARC_ERR_CUDA;
+  // background
+  struct Src {
+    int fb;
+    double *d3, *d1;
+  } srcs[FB_COUNT] = {
+      {FB_RHO0, h->rho0, h->rho0_1},     {FB_P0, h->p0, h->p0_1},
+      {FB_RHOINV, h->rhoinv, h->rhoinv_1}, {FB_C2R, h->c2rho0, h->c2rho0_1},
+      {FB_GRZ, h->grz, h->grz_1},        {FB_GPZ, h->gpz, h->gpz_1},
+      {FB_SPONGE, h->sponge, h->sponge_1}, {FB_BOX, h->box, nullptr},
+      {FB_BOY, h->boy, nullptr},         {FB_BOZ, h->boz, nullptr},
+      {FB_CBX, h->cbx, nullptr},         {FB_CBY, h->cby, nullptr},
+      {FB_CBZ, h->cbz, nullptr},         {FB_GRX, h->grx, nullptr},
+      {FB_GRY, h->gry, nullptr},         {FB_GPX, h->gpx, nullptr},
+      {FB_GPY, h->gpy, nullptr},         {FB_RED, h->red, nullptr}};
+  for (const Src &q : srcs) {
+    const bool one = h->bg1d && q.d1;
+    const double *src = one ? q.d1 : q.d3;
+    if (!src) continue;
+    h->f_bg[q.fb] = f_up(h, src, one ? nz : N, s);
+    if (!h->f_bg[q.fb]) return SPARC_ERR_NOMEM;
+  }
+  h->f_stretch = f_up(h, h->d_stretch, nz, s);
+  h->f_gblk = f_up(h, h->d_gblk, (long long)h->g_blk.size(), s);
+  h->f_sd = f_up(h, h->source_damp, N, s);
+  h->f_ssb = f_up(h, h->ssb, N, s);
+  if (!h->f_stretch || !h->f_gblk || !h->f_sd || !h->f_ssb) return SPARC_ERR_NOMEM;
+  // CPML profiles (FP64 setup, FP32 storage)
+  for (int f = 0; f < 6; ++f) {
+    const FaceDev &D = h->faces[f];
+    FaceT<float> &F = h->f_faces[f];
+    if (!D.on) continue;
+    const long long n = D.uniform ? D.np : D.cnt;
+    float *pa = f_up(h, D.pa, n, s), *pb = f_up(h, D.pb, n, s), *pk = f_up(h, D.pk, n, s);
+    if (!pa || !pb || !pk) return SPARC_ERR_NOMEM;
+    F.pa = pa; F.pb = pb; F.pk = pk;
+    F.uniform = D.uniform;
+  }
+  if (cudaStreamSynchronize(s) != cudaSuccess) return SPARC_ERR_CUDA;
+  // release the FP64 arrays (geometry of the faces is kept)
+  double *rel[] = {h->rho0, h->p0, h->c2, h->rhoinv, h->c2rho0, h->grz, h->gpz,
+                   h->sponge, h->box, h->boy, h->boz, h->cbx, h->cby, h->cbz,
+                   h->grx, h->gry, h->gpx, h->gpy, h->red, h->source_damp, h->ssb,
+                   h->rho0_1, h->p0_1, h->rhoinv_1, h->c2rho0_1, h->grz_1, h->gpz_1,
+                   h->sponge_1};
+  for (double *p : rel)
+    if (p) dev_free(h, p);
+  h->rho0 = h->p0 = h->c2 = h->rhoinv = h->c2rho0 = h->grz = h->gpz = h->sponge = nullptr;
+  h->box = h->boy = h->boz = h->cbx = h->cby = h->cbz = nullptr;
+  h->grx = h->gry = h->gpx = h->gpy = h->red = h->source_damp = h->ssb = nullptr;
+  h->rho0_1 = h->p0_1 = h->rhoinv_1 = h->c2rho0_1 = h->grz_1 = h->gpz_1 = h->sponge_1 = nullptr;
+  for (int f = 0; f < 6; ++f) {
+    FaceDev &D = h->faces[f];
+    if (!D.on) continue;
+    dev_free(h, D.pa);
+    dev_free(h, D.pb);
+    dev_free(h, D.pk);
+    D.pa = D.pb = D.pk = nullptr;
+  }
+  return encode_tensor_maps32(h);
+}
+
+// FP32 copies of the forcing tables built by sparc_set_source.
+int source32(Handle *h) {
+  cudaStream_t s = h->stream;
+  if (h->src.kind == SPARC_SRC_PULSE) {
+    if (!h->f_fx) {
+      h->f_fx = f_up(h, nullptr, h->nx + h->ny + h->nz, s);
+      if (!h->f_fx) return SPARC_ERR_NOMEM;
+      h->f_fy = h->f_fx + h->nx;
+      h->f_fz = h->f_fy + h->ny;
+    }
+    if (to_float(h->d_fx, h->f_fx, h->nx + h->ny + h->nz, s)) return SPARC_ERR_CUDA;
+  } else if (h->src.kind == SPARC_SRC_PSR) {
+    const long long np = (long long)h->pulses.size();
+    h->f_px = f_up(h, h->d_px, np * h->nx, s);
+    h->f_py = f_up(h, h->d_py, np * h->ny, s);
+    h->f_psr = f_up(h, nullptr,
+                    std::max<long long>(1, (long long)(h->psr_khi - h->psr_klo) * h->nx * h->ny), s);
+    if (!h->f_px || !h->f_py || !h->f_psr) return SPARC_ERR_NOMEM;
+  }
+  return cudaStreamSynchronize(s) == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
+}
+
+}  // namespace sparc

@@ -97,3 +97,12 @@ def test_invalid_parameters_are_rejected_before_any_device_call(lib):
     p.block_z = 1
     assert lib.sparc_create(C.byref(p), 0, C.byref(h)) == abi.SPARC_ERR_INVALID
     assert b"block" in lib.sparc_last_error(None)
+    p.block_z = 2
+    p.precision = 7
+    assert lib.sparc_create(C.byref(p), 0, C.byref(h)) == abi.SPARC_ERR_INVALID
+    assert b"precision" in lib.sparc_last_error(None)
+    p.precision = abi.SPARC_FP32
+    p.nx = p.ny = 4096
+    p.nz = 4096
+    assert lib.sparc_create(C.byref(p), 0, C.byref(h)) == abi.SPARC_ERR_INVALID
+    assert b"precision form" in lib.sparc_last_error(None)

@@ -41,7 +41,18 @@ def parse():
     ap.add_argument("--steps", type=int, default=120)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
-    ap.add_argument("--workload", default="cfg1", choices=["cfg1", "cfg0"])
+    ap.add_argument("--workload", default="cfg1",
+                    choices=["cfg1", "cfg0", "ensemble"],
+                    help="cfg1: MHD flux tube 256x256x300; cfg0: quiet-Sun "
+                    "64x64x128; ensemble: 64 seeded FP32 members advanced by "
+                    "the batched engine")
+    ap.add_argument("--members", type=int, default=64,
+                    help="ensemble size (ensemble workload)")
+    ap.add_argument("--no-fp64-compare", action="store_true",
+                    help="ensemble: skip timing the FP64 plain cfg1 step")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
+                    help="fp64: plain form; fp32: precision form (depth-scaled "
+                    "FP32 state, compensated RK update)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--kernel-steps", type=int, default=10)
@@ -55,7 +66,8 @@ def parse():
 
 def algorithmic_bytes_per_point(p, with_filters=True):
     """Bytes per grid-point update of one RK step:
-    w*[14V + 5C + 14*sum_faces(P*phi) + 2V/n_z + 2V/n_xy]; w word size,
+    w*[14V + 5C + 14*sum_faces(P*phi) + 2V/n_z + 2V/n_xy] (+2V words of
+    the compensated-sum carry in the precision form); w word size,
     V state fields, C 3-D background inputs (quiet: 0, MHD: 6), P CPML
     fields per face, phi the fraction of points in that face's slab."""
     w = 8 if p.precision == abi.SPARC_FP64 else 4
@@ -69,6 +81,8 @@ def algorithmic_bytes_per_point(p, with_filters=True):
     if p.use_hpml:
         phi += (p.npml_xb + p.npml_xt) / p.nx + (p.npml_yb + p.npml_yt) / p.ny
     b = 14 * V + 5 * C + 14 * P * phi
+    if w == 4:
+        b += 2 * V  # compensated-sum carry, read and written by stage 5
     if with_filters:
         nz = int(np.floor(max(p.t_z, p.timestep) / p.timestep + 1e-5))
         nxy = int(np.floor(max(p.t_xy, p.timestep) / p.timestep + 1e-5))
@@ -77,18 +91,24 @@ def algorithmic_bytes_per_point(p, with_filters=True):
 
 
 def workload(name, precision=abi.SPARC_FP64, grid=None):
+    fp = "FP64" if precision == abi.SPARC_FP64 else "FP32 precision form"
     if name == "cfg0":
         p, bg, src = W.cfg0(precision=precision)
-        desc = ("plain quiet-Sun hydro 64x64x128 FP64 (50 Mm periodic, z -20..+1 "
-                "Mm, z-CPML 10, v_z pulse 3 mHz, dt 1 s)")
+        desc = ("plain quiet-Sun hydro 64x64x128 %s (50 Mm periodic, z -20..+1 "
+                "Mm, z-CPML 10, v_z pulse 3 mHz, dt 1 s)" % fp)
         return p, bg, src, desc
+    desc = WORKLOAD.replace("FP64", fp)
     if grid is None:
         p, bg, src = W.cfg1(precision=precision)
-        return p, bg, src, WORKLOAD
+        return p, bg, src, desc
     nx, ny, nz = grid
     p, bg, src = W.cfg1(nx=nx, ny=ny, nz=nz, precision=precision,
                         length_mm=100.0 * nx / 256)
-    return p, bg, src, WORKLOAD
+    return p, bg, src, desc
+
+
+def p_V(p):
+    return 8 if p.magnetic == 2 else 5
 
 
 def peaks():
@@ -227,7 +247,10 @@ def run_gpu(args, world, rank, local):
     dev = local
     torch.cuda.set_device(dev)
     rep = Replicas("nccl")
-    p, bg, src, desc = workload(args.workload, grid=args.grid)
+    fp32 = args.precision == "fp32"
+    prec = abi.SPARC_FP32 if fp32 else abi.SPARC_FP64
+    wsize = 4 if fp32 else 8
+    p, bg, src, desc = workload(args.workload, precision=prec, grid=args.grid)
     sim = Simulation(p, bg, src, device=dev)
     del bg
     pts = p.nx * p.ny * p.nz
@@ -287,7 +310,7 @@ def run_gpu(args, world, rank, local):
         try:
             with open(tfile) as f:
                 t = json.load(f)
-            if t.get("workload") == args.workload:
+            if t.get("workload") == args.workload + "_" + args.precision:
                 traffic = t.get("bytes_per_step")
         except Exception:
             traffic = None
@@ -319,9 +342,11 @@ def run_gpu(args, world, rank, local):
     x1.synchronize()
     ems = max_over_ranks(x0.elapsed_time(x1))
     e2e = world * pts * E / (ems / 1e3)
-    state_bytes = 8 * (a_host.size + psi_host.size)
-    h2d = (state_bytes + 8 * E) / E
-    d2h = (state_bytes + 40 * E) / E
+    # bytes that cross PCIe: the device state is FP32 in the precision form
+    # (its compensated-sum carry is read back with it)
+    h2d = (wsize * (a_host.size + psi_host.size) + 8 * E) / E
+    d2h = (wsize * (a_host.size * (2 if fp32 else 1) + psi_host.size)
+           + 40 * E) / E
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -335,13 +360,14 @@ def run_gpu(args, world, rank, local):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": K, "warmup": W_, "ms_per_step": ms_max / K,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic (seeded analytic background and "
+        "dtype": "f32" if fp32 else "f64",
+        "data": "synthetic (seeded analytic background and "
         "pulse table; no public dataset)",
         "config": {"workload": desc, "grid": [p.nx, p.ny, p.nz],
-                   "precision": "fp64 plain", "parallelism":
-                   "replicas" if world > 1 else "single GPU",
+                   "precision": "fp32 precision form" if fp32 else "fp64 plain",
+                   "parallelism": "replicas" if world > 1 else "single GPU",
                    "l2": "working set %.1f GB > 126 MB L2 (no flush needed)"
-                   % (3 * 8 * 8 * pts / 1e9)},
+                   % (3 * p_V(p) * wsize * pts / 1e9)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm,
                      "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": peak_kind, "traffic": traffic,
@@ -364,11 +390,184 @@ def run_gpu(args, world, rank, local):
     rep.close()
 
 
+def fp64_plain_rate(dev, steps=20, warmup=3):
+    """The FP64 plain form on the flux-tube configuration (256x256x300),
+    timed with CUDA events on its stream: the comparison point of the
+    batched precision form on the same GPU."""
+    import torch
+    from sparc2_b200 import Simulation
+    p, bg, src, _ = workload("cfg1")
+    sim = Simulation(p, bg, src, device=dev)
+    del bg
+    stream = torch.cuda.ExternalStream(sim.stream, device=dev)
+    sim.run(0, warmup)
+    sim.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.run(warmup, steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    sim.close()
+    return p.nx * p.ny * p.nz / (ms / 1e3), ms
+
+
+def run_ensemble(args, world, rank, local):
+    """Batched precision form: `members` seeded FP32 simulations of uneven
+    grids (quiet and flux-tube) advanced together by the batched engine,
+    one CUDA-graph launch per step; a step advances every member by one
+    driver iteration."""
+    import torch
+    from sparc2_b200 import Simulation
+    from sparc2_b200.batch import Batch
+    from sparc2_b200.replicas import Replicas
+    dev = local
+    torch.cuda.set_device(dev)
+    rep = Replicas("nccl")
+    draws = W.ensemble_draws(args.members)
+    W_, K, E = args.warmup, args.steps, args.e2e_steps
+    total_steps = 1000
+    sims, params = [], []
+    t_setup = time.perf_counter()
+    for nx, nz, b0, depth in draws:
+        p, bg, src = W.member(nx, nz, b0, depth)
+        sims.append(Simulation(p, bg, src, device=dev))
+        params.append(p)
+        del bg
+    t_setup = time.perf_counter() - t_setup
+    pts = sum(p.nx * p.ny * p.nz for p in params)
+    batch = Batch(len(sims), device=dev)
+    for s in sims:
+        batch.add(s, 0, total_steps)
+    stream = torch.cuda.ExternalStream(batch.stream, device=dev)
+    tiles = batch.tune(steps_per_trial=2)
+    tuned_steps = 1000 - int(batch.remaining()[0])
+    batch.run(W_)
+    batch.synchronize()
+    clocks = Clocks(dev)
+    n0 = batch.launch_count
+    rep.barrier()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    batch.run(K)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize(dev)
+    rep.barrier()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop() if clocks else None
+    launches = batch.launch_count - n0
+    ms_max = rep.max(ms)
+    value = world * pts * K / (ms_max / 1e3)
+    hbm, peak_kind = peaks()
+    step_bytes = sum(algorithmic_bytes_per_point(p) * p.nx * p.ny * p.nz
+                     for p in params)
+    achieved = step_bytes / (ms_max / K / 1e3) / 1e9
+    diags = [s.diagnostics() for s in sims]
+    unstable = sum(1 for _, r in diags if r != abi.SPARC_OK)
+
+    # end to end through the public API: every member restarts from a state
+    # uploaded from pinned host memory (set_state, outside the batch), E
+    # batched steps with every member's diagnostics read back each step,
+    # every member's state read back into pinned host memory at the end
+    for q in list(batch.members):
+        batch.remove(q)
+    sizes = [(s.n_state, s.n_psi) for s in sims]
+    big = max(n + m for n, m in sizes)
+    pin = torch.zeros(big, dtype=torch.float64, pin_memory=True).numpy()
+    first = int(diags[0][0].iteration) + 1
+    rep.barrier()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for s, (n, m) in zip(sims, sizes):
+        pin[:n + m] = 0.0
+        s.set_state(pin[:n], pin[n:n + m] if m else None)
+        batch.add(s, first, E)
+    for _ in range(E):
+        batch.run(1)
+        for s in sims:
+            s.diagnostics()
+    for q in list(batch.members):
+        batch.remove(q)
+    for s, (n, m) in zip(sims, sizes):
+        s.lib.sparc_get_state(s.h, abi.dptr(pin[:n]), abi.dptr(pin[n:n + m]))
+    torch.cuda.synchronize(dev)
+    et = rep.max(time.perf_counter() - t0)
+    e2e = world * pts * E / et
+    n_state = sum(n for n, _ in sizes)
+    n_psi = sum(m for _, m in sizes)
+    # the device state is FP32: 4 bytes per value up, state + carry down
+    h2d = 4 * (n_state + n_psi) / E
+    d2h = (4 * (2 * n_state + n_psi) + 40 * len(sims) * E) / E
+    batch.close()
+    for s in sims:
+        s.close()
+    sims = None
+    fp64 = None
+    if rank == 0 and not args.no_fp64_compare:
+        v64, ms64 = fp64_plain_rate(dev)
+        fp64 = {"value": v64, "unit": UNIT, "ms_per_step": ms64,
+                "workload": "plain MHD flux tube 256x256x300 FP64, one "
+                "simulation (sparc_run, CUDA graphs), same GPU"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline()
+    if rank != 0:
+        rep.close()
+        return
+    nq = sum(1 for d in draws if d[2] <= 0)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": K, "warmup": W_, "ms_per_step": ms_max / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded analytic backgrounds and "
+        "sources; no public dataset)",
+        "config": {"workload": "batched ensemble, FP32 precision form: %d "
+                   "members (%d quiet, %d flux tube), nx=ny in {96..256}, nz "
+                   "in [150, 300], one Gaussian source each, dt 0.5 s; a step "
+                   "advances every member one driver iteration"
+                   % (len(draws), nq, len(draws) - nq),
+                   "members": len(draws), "grid_points": pts,
+                   "tiles": {"zchunk_mhd": tiles[0], "zchunk_quiet": tiles[1],
+                             "autotuner_steps": tuned_steps},
+                   "setup_s": t_setup,
+                   "parallelism": "replicas" if world > 1 else "single GPU",
+                   "l2": "working set %.0f GB > 126 MB L2 (no flush needed)"
+                   % (step_bytes / 1e9)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_kind": peak_kind, "traffic": None,
+                     "kernel": "one batched step (forcing, 5 persistent RK "
+                     "stage launches, filter passes at cadence)",
+                     "algorithmic_bytes_per_launch": step_bytes,
+                     "ms_per_launch": ms_max / K},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "steps": E},
+        "gpu_launches": launches,
+        "diag": {"unstable_members": unstable},
+    }
+    if fp64:
+        line["fp64_plain"] = fp64
+        line["speedup_vs_fp64_plain"] = value / fp64["value"]
+    if clk:
+        line["clocks"] = clk
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    rep.close()
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.workload == "ensemble":
+        run_ensemble(args, world, rank, local)
         return
     run_gpu(args, world, rank, local)
 

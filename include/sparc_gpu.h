@@ -200,6 +200,57 @@ int sparc_get_scalars(sparc_handle *h, double *out12);
  * failed sparc_create when h is NULL). */
 const char *sparc_last_error(const sparc_handle *h);
 
+/* -------------------------------------------------------- batched engine
+ * No counterpart in the reference, which runs one simulation per MPI job.
+ * A batch advances many SPARC_FP32 handles of any grid sizes together: each
+ * step of all members is one CUDA-graph launch of persistent kernels (one
+ * per RK stage) over a device (simulation, tile, z-chunk) work-list.  While
+ * a handle is in a batch the batch owns its buffer roles, iteration and
+ * stream order: sparc_step/run/filter_vars/set_state/get_state/set_source/
+ * destroy on it return SPARC_ERR_ORDER; sparc_diagnostics works. */
+typedef struct sparc_batch sparc_batch;
+
+/* A batch of up to `capacity` simulations on CUDA device `device`. */
+int sparc_batch_create(int device, int capacity, sparc_batch **out);
+
+/* Removes the remaining members (they keep their state) and frees. */
+int sparc_batch_destroy(sparc_batch *b);
+
+/* Adds a SPARC_FP32 handle (background and source set) that will run
+ * driver iterations first .. first+count-1; *slot receives its slot. */
+int sparc_batch_add(sparc_batch *b, sparc_handle *h, int64_t first,
+                    int64_t count, int *slot);
+
+/* Takes a member out (after the queued steps); the handle is usable alone
+ * again with its state as the batch left it. */
+int sparc_batch_remove(sparc_batch *b, int slot);
+
+/* Enqueues `steps` batched steps.  Each step advances every member with
+ * iterations left by one driver iteration (forcing, five RK stages,
+ * diagnostics, FILTER_VARS at its own cadence).  Asynchronous. */
+int sparc_batch_run(sparc_batch *b, int64_t steps);
+
+/* Waits, then writes each slot's iterations left (-1: free slot),
+ * `capacity` entries. */
+int sparc_batch_remaining(sparc_batch *b, int64_t *remaining);
+
+/* z extent of the work items of MHD and quiet members (>= 11 layers);
+ * the autotuner's knob.  Results do not depend on it. */
+int sparc_batch_set_tiles(sparc_batch *b, int zchunk_mhd, int zchunk_quiet);
+int sparc_batch_get_tiles(const sparc_batch *b, int *zchunk_mhd,
+                          int *zchunk_quiet);
+
+/* Autotuner: times `steps_per_trial` batched steps per candidate z extent
+ * (one axis at a time, MHD then quiet) and keeps the fastest; returns the
+ * choice.  The trial steps advance the members like sparc_batch_run. */
+int sparc_batch_tune(sparc_batch *b, int steps_per_trial, int *best_mhd,
+                     int *best_quiet);
+
+int sparc_batch_synchronize(sparc_batch *b);
+int sparc_batch_stream(sparc_batch *b, void **stream);
+int sparc_batch_launch_count(const sparc_batch *b, int64_t *count);
+const char *sparc_batch_last_error(const sparc_batch *b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -107,6 +107,12 @@ EXPORTS = [
     "sparc_synchronize", "sparc_stream", "sparc_launch_count",
     "sparc_derivative", "sparc_filter_field", "sparc_get_coeff",
     "sparc_get_scalars", "sparc_last_error",
+    "sparc_batch_create", "sparc_batch_destroy", "sparc_batch_add",
+    "sparc_batch_remove", "sparc_batch_run", "sparc_batch_remaining",
+    "sparc_batch_set_tiles", "sparc_batch_get_tiles",
+    "sparc_batch_synchronize", "sparc_batch_stream",
+    "sparc_batch_launch_count", "sparc_batch_last_error",
+    "sparc_batch_tune",
 ]
 
 _lib = None
@@ -136,6 +142,20 @@ def _declare(lib):
         "sparc_get_coeff": (C.c_int, [h, C.c_char_p, d, P(C.c_int64)]),
         "sparc_get_scalars": (C.c_int, [h, d]),
         "sparc_last_error": (C.c_char_p, [h]),
+        "sparc_batch_create": (C.c_int, [C.c_int, C.c_int, P(C.c_void_p)]),
+        "sparc_batch_destroy": (C.c_int, [h]),
+        "sparc_batch_add": (C.c_int, [h, h, C.c_int64, C.c_int64,
+                                      P(C.c_int)]),
+        "sparc_batch_remove": (C.c_int, [h, C.c_int]),
+        "sparc_batch_run": (C.c_int, [h, C.c_int64]),
+        "sparc_batch_remaining": (C.c_int, [h, P(C.c_int64)]),
+        "sparc_batch_set_tiles": (C.c_int, [h, C.c_int, C.c_int]),
+        "sparc_batch_get_tiles": (C.c_int, [h, P(C.c_int), P(C.c_int)]),
+        "sparc_batch_synchronize": (C.c_int, [h]),
+        "sparc_batch_stream": (C.c_int, [h, P(C.c_void_p)]),
+        "sparc_batch_launch_count": (C.c_int, [h, P(C.c_int64)]),
+        "sparc_batch_last_error": (C.c_char_p, [h]),
+        "sparc_batch_tune": (C.c_int, [h, C.c_int, P(C.c_int), P(C.c_int)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -22,6 +22,7 @@ UNITS = {
     "step.cu": [],
     "step32.cu": [],
     "api.cu": [],
+    "batch.cu": [],
 }
 HEADERS = ["internal.h"]
 

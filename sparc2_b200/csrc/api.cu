@@ -48,6 +48,12 @@ static int fail(Handle *h, int code, const std::string &msg) {
   return code;
 }
 
+// a handle in a batch is advanced by the batch only
+#define NOT_IN_BATCH(h)                                                       \
+  do {                                                                        \
+    if ((h)->batch) return fail((h), SPARC_ERR_ORDER, "handle is in a batch"); \
+  } while (0)
+
 static void block_partition(int n, int B, std::vector<int> &start,
                             std::vector<int> &len) {
   // rank extents, initialize.f90:77-120 (remainder to the low ranks)
@@ -383,8 +389,8 @@ int sparc_create(const sparc_params *p, int device, sparc_handle **out) {
   if (!cuda_ok(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream")) {
     r = SPARC_ERR_CUDA;
   }
-  if (!r && (setup_constants() || step_constants() || filter_constants(h->gxy, h->gz) ||
-             step32_constants(h->gxy, h->gz)))
+  if (!r && (setup_constants() || step_constants() || filter_constants() ||
+             step32_constants()))
     r = fail(h, SPARC_ERR_CUDA, "constant upload failed");
   if (!r && stage_geometry(h))
     r = fail(h, SPARC_ERR_INVALID, "no tile shape fits this grid");
@@ -456,6 +462,7 @@ int sparc_create(const sparc_params *p, int device, sparc_handle **out) {
 
 int sparc_destroy(sparc_handle *h) {
   if (!h) return SPARC_ERR_INVALID;
+  NOT_IN_BATCH(h);
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   drop_graphs(h);
@@ -513,6 +520,7 @@ static bool psr_in_block(const Handle *h, const sparc_pulse &q, int b) {
 
 int sparc_set_source(sparc_handle *h, const sparc_source *s) {
   if (!h || !s) return SPARC_ERR_INVALID;
+  NOT_IN_BATCH(h);
   if (!h->bg_ready) return fail(h, SPARC_ERR_ORDER, "set the background first");
   if (s->kind < SPARC_SRC_NONE || s->kind > SPARC_SRC_PSR)
     return fail(h, SPARC_ERR_INVALID, "unknown source kind");
@@ -690,6 +698,7 @@ static int get_state32(Handle *h, double *a, double *psi) {
 
 int sparc_set_state(sparc_handle *h, const double *a, const double *psi) {
   if (!h) return SPARC_ERR_INVALID;
+  NOT_IN_BATCH(h);
   cudaSetDevice(h->device);
   if (h->fp32) {
     CK(h, cudaStreamSynchronize(h->stream));
@@ -713,6 +722,7 @@ int sparc_set_state(sparc_handle *h, const double *a, const double *psi) {
 
 int sparc_get_state(sparc_handle *h, double *a, double *psi) {
   if (!h) return SPARC_ERR_INVALID;
+  NOT_IN_BATCH(h);
   cudaSetDevice(h->device);
   if (h->fp32) return get_state32(h, a, psi);
   if (a)
@@ -733,6 +743,7 @@ int sparc_get_state(sparc_handle *h, double *a, double *psi) {
 
 int sparc_step(sparc_handle *h, int64_t nn) {
   if (!h) return SPARC_ERR_INVALID;
+  NOT_IN_BATCH(h);
   if (!h->bg_ready) return fail(h, SPARC_ERR_ORDER, "set the background first");
   cudaSetDevice(h->device);
   int r = set_iter(h, nn);
@@ -744,6 +755,7 @@ int sparc_step(sparc_handle *h, int64_t nn) {
 
 int sparc_filter_vars(sparc_handle *h, int64_t nn) {
   if (!h) return SPARC_ERR_INVALID;
+  NOT_IN_BATCH(h);
   if (!h->bg_ready) return fail(h, SPARC_ERR_ORDER, "set the background first");
   cudaSetDevice(h->device);
   int nk = 0;
@@ -752,6 +764,7 @@ int sparc_filter_vars(sparc_handle *h, int64_t nn) {
 
 int sparc_run(sparc_handle *h, int64_t first, int64_t count) {
   if (!h || count < 0) return SPARC_ERR_INVALID;
+  NOT_IN_BATCH(h);
   if (!h->bg_ready) return fail(h, SPARC_ERR_ORDER, "set the background first");
   cudaSetDevice(h->device);
   int r = set_iter(h, first);
@@ -776,10 +789,12 @@ int sparc_diagnostics(sparc_handle *h, sparc_diag *out) {
   double d[4];
   long long f;
   int e = 0;
-  CK(h, cudaMemcpyAsync(d, h->d_diag, 32, cudaMemcpyDeviceToHost, h->stream));
-  CK(h, cudaMemcpyAsync(&f, h->d_fail, 8, cudaMemcpyDeviceToHost, h->stream));
-  CK(h, cudaMemcpyAsync(&e, h->d_err, 4, cudaMemcpyDeviceToHost, h->stream));
-  CK(h, cudaStreamSynchronize(h->stream));
+  // in a batch, the batch stream orders the writes of these values
+  cudaStream_t st = h->batch ? h->batch_stream : h->stream;
+  CK(h, cudaMemcpyAsync(d, h->d_diag, 32, cudaMemcpyDeviceToHost, st));
+  CK(h, cudaMemcpyAsync(&f, h->d_fail, 8, cudaMemcpyDeviceToHost, st));
+  CK(h, cudaMemcpyAsync(&e, h->d_err, 4, cudaMemcpyDeviceToHost, st));
+  CK(h, cudaStreamSynchronize(st));
   if (e) return fail(h, SPARC_ERR_TIMEOUT, "a bounded device wait gave up");
   out->ke_norm = d[0];
   out->min_rho = d[1];

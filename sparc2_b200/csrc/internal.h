@@ -84,6 +84,51 @@ struct SimT {
 };
 using SimDev = SimT<double>;
 
+// PULSE = 2 forcing of the precision form: the per-layer pulse lists and
+// separable factors the forcing kernels read (all_modules.f90:521-663).
+struct Psr32 {
+  int nx, ny, klo, khi, nblocks, bx, bxy;
+  long long init;
+  double timestep, st;
+  const int *off, *idx, *colx, *coly, *colz;
+  const double *zv, *ptime;
+  const float *px, *py, *sd, *ssb;
+  const unsigned char *mask;
+  float *out;
+  const long long *iter;
+};
+
+// One simulation of a batch, as the batched kernels read it.  Buffer roles,
+// the steps left and the completion counter live here and are advanced on
+// the device, so a captured step stays valid while simulations come and go.
+struct Slot32 {
+  SimT<float> S;
+  Psr32 psr;
+  float *buf[3];
+  int role[3];                 // a, free1, free2
+  double betas[5];
+  long long remaining;         // driver iterations left
+  int active;                  // set at the start of each step
+  int has_psr;
+  int first_item, n_items;     // stage work-list range
+  int f_first, f_items;        // filter work-list range
+  int gxy, gz, xyfreq, zfreq;
+  float s_xy, s_z;
+  unsigned counter;            // items done in the current launch
+  double *partials;            // 3 per stage item (last stage)
+};
+
+// Device work-lists and launch shape of one batched step.
+struct BatchLaunch {
+  Slot32 *slots;
+  int nslots;
+  const int4 *items, *fitems, *pitems;  // stage, filter, forcing items
+  const int *counts;                    // [3] item counts
+  unsigned *wctr;                       // [9] work counters, zeroed per step
+  int grid;                             // persistent CTAs
+  size_t psr_smem;
+};
+
 // Background arrays of the precision form (FP32 copies of the FP64 setup).
 enum {
   FB_RHO0, FB_P0, FB_RHOINV, FB_C2R, FB_GRZ, FB_GPZ, FB_SPONGE, FB_BOX, FB_BOY,
@@ -180,6 +225,11 @@ struct Handle {
   bool tma32 = false;
   CUtensorMap tmaps32[18];
 
+  // member of a batch (sparc_batch_add): the batch owns the buffer roles,
+  // the iteration and the stream order until sparc_batch_remove
+  void *batch = nullptr;
+  cudaStream_t batch_stream = nullptr;
+
   // captured graphs keyed by (ra, rf1, rf2, filter kind)
   struct GraphEntry {
     int ra, rf1, rf2, fk;
@@ -205,7 +255,7 @@ int launch_filter_raw(Handle *h, int dir, const double *in, double *out,
 
 // step.cu
 int step_constants();
-int filter_constants(int gxy, int gz);
+int filter_constants();
 SimDev make_simdev(Handle *h);
 int launch_stage(Handle *h, const SimDev &S, int stage, const double *a,
                  const double *tin, double *tout, cudaStream_t s);
@@ -216,11 +266,14 @@ int stage_geometry(Handle *h);
 int encode_tensor_maps(Handle *h);
 
 // step32.cu (precision form)
-int step32_constants(int gxy, int gz);
+int step32_constants();
 SimT<float> make_sim32(Handle *h);
 int launch_stage32(Handle *h, const SimT<float> &S, int stage, const float *a,
                    const float *tin, float *so, cudaStream_t s);
 int launch_psr32(Handle *h, cudaStream_t s);
+Psr32 make_psr32(Handle *h);
+int launch_batch_step(const BatchLaunch &B, cudaStream_t s, int *nkernels);
+size_t batch_stage_smem();
 int launch_filter32(Handle *h, int dir, const float *in, float *out, cudaStream_t s);
 int encode_tensor_maps32(Handle *h);
 int setup32(Handle *h);

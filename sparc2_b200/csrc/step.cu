@@ -20,7 +20,7 @@
 namespace sparc {
 
 __constant__ double c_dp[6][11];   // derivative rows, initialize.f90:1959-2031
-__constant__ double c_df[2][11];   // filter stencils: [0] xy, [1] z
+__constant__ double c_df[2][11];   // filter stencils: [0] 11-point, [1] 7-point
 
 enum { FIRST = 0, MID = 1, LAST = 2 };
 
@@ -381,13 +381,8 @@ __global__ void __launch_bounds__(TX *TY)
 // computed.  Per buffer: 10 halo slots over the cross-shaped tile (stage
 // fields vx vy vz p bx by bz and B0; the B0 slots become flux1..3 in place
 // once the layer has landed) and 24 own-point slots (stage rho, a[0..7],
-// 14 background arrays, p0).  1 CTA of 32x8 threads per SM, 219 KB smem.
+// 14 background arrays, p0).
 namespace pipe {
-constexpr int TX = 32, TY = 8, NT = TX * TY;
-constexpr int HX = TX + 10, HY = TY + 10, HS = HX * HY;
-constexpr int NH = 10, NO = 24;
-constexpr int BUF = NH * HS + NO * TY * TX;  // doubles per buffer
-constexpr size_t SMEM = 2 * BUF * sizeof(double);
 // own slots
 constexpr int O_RHO = 0, O_A = 1, O_BG = 9, O_P0 = 23;
 // background order in the own slots (O_BG + n)
@@ -1377,7 +1372,7 @@ __global__ void k_filter_pass(FiltDev F, const double *__restrict__ in,
   const bool per = DIR != 2 && F.periodic;
   const bool avg = DIR == 2 || !F.periodic;
   const int g = F.g;
-  const double *c = c_df[DIR == 2 ? 1 : 0];
+  const double *c = c_df[g == 5 ? 0 : 1];
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
     const long long pnt = t % F.N;
@@ -1428,13 +1423,12 @@ int launch_filter_pass(Handle *h, int dir, const double *in, double *out,
   return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
 }
 
-int filter_constants(int gxy, int gz) {
+// Both stencils stay resident, so handles with different filter modes can
+// coexist; a pass picks its table by half-width.
+int filter_constants() {
   double t[2][11] = {};
-  for (int d = 0; d < 2; ++d) {
-    int g = d == 0 ? gxy : gz;
-    for (int m = 0; m < 11; ++m)
-      t[d][m] = g == 5 ? kFilter11[m] : (m < 7 ? kFilter7[m] : 0.0);
-  }
+  for (int m = 0; m < 11; ++m) t[0][m] = kFilter11[m];
+  for (int m = 0; m < 7; ++m) t[1][m] = kFilter7[m];
   return cudaMemcpyToSymbol(c_df, t, sizeof(t)) == cudaSuccess ? SPARC_OK
                                                                : SPARC_ERR_CUDA;
 }

@@ -32,17 +32,16 @@ __constant__ float f_df[2][11];
 
 enum { F_FIRST = 0, F_MID = 1, F_LAST = 2 };
 
-int step32_constants(int gxy, int gz) {
+// Derivative rows and both filter stencils ([0] 11-point, [1] 7-point) in
+// FP32; a filter pass picks its table by half-width.
+int step32_constants() {
   float t[6][11];
   for (int r = 0; r < 6; ++r)
     for (int m = 0; m < 11; ++m) t[r][m] = (float)kDerivRows[r][m];
   if (cudaMemcpyToSymbol(f_dp, t, sizeof(t)) != cudaSuccess) return SPARC_ERR_CUDA;
   float f[2][11] = {};
-  for (int d = 0; d < 2; ++d) {
-    int g = d == 0 ? gxy : gz;
-    for (int m = 0; m < 11; ++m)
-      f[d][m] = (float)(g == 5 ? kFilter11[m] : (m < 7 ? kFilter7[m] : 0.0));
-  }
+  for (int m = 0; m < 11; ++m) f[0][m] = (float)kFilter11[m];
+  for (int m = 0; m < 7; ++m) f[1][m] = (float)kFilter7[m];
   return cudaMemcpyToSymbol(f_df, f, sizeof(f)) == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
 }
 
@@ -219,20 +218,24 @@ __device__ void diag_reduce32(const Sim32 &S, double ke, double mr, double mp) {
 // ------------------------------------------ MP_QUIET_3D, precision form
 // RHS.f90:18-175 fused with one RK stage (as k_stage_quiet of step.cu),
 // FP32 with depth-scaled state.  Field scales: l = 0 rho, 1-3 v, 4 p.
+// The body covers the tile (x0, y0) of TX x TY columns over layers
+// [k0, k1); (tx, ty) is the calling thread's column in the tile.  Every
+// thread of the block calls it.  Diagnostics of the last stage accumulate
+// into ke, mr, mp.
 template <int TX, int TY, int MODE, bool BG1D>
-__global__ void __launch_bounds__(TX *TY)
-    k_quiet32(const Sim32 S, const float *__restrict__ a, const float *__restrict__ tin,
-              float *__restrict__ so, float beta, float bnext, int zchunk) {
+__device__ __forceinline__ void quiet_body(const Sim32 &S, const float *__restrict__ a,
+                                           const float *__restrict__ tin,
+                                           float *__restrict__ so, float beta, float bnext,
+                                           int x0, int y0, int k0, int k1, int tx, int ty,
+                                           double &ke, double &mr, double &mp) {
   constexpr int HX = TX + 10, HY = TY + 10;
   __shared__ float t_vx[HY][HX], t_vy[HY][HX], t_p[HY][HX];
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int tid = ty * TX + tx;
   const int nx = S.nx, ny = S.ny, nz = S.nz;
   const long long N = S.N, NXY = (long long)nx * ny;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   const int i = x0 + tx, j = y0 + ty;
   const bool act = i < nx && j < ny;
   const bool per = S.periodic;
-  const int k0 = blockIdx.z * zchunk, k1 = min(nz, k0 + zchunk);
   const long long col = (long long)j * nx + i;
   const long long it = *S.iter;
   const float Tp = pulse_time32(S, it);
@@ -252,7 +255,6 @@ __global__ void __launch_bounds__(TX *TY)
     wvz[m] = ok ? __ldg(tin + 3 * N + id) * isc[3 * nz + kk] : 0.f;
     wp[m] = ok ? __ldg(tin + 4 * N + id) * isc[4 * nz + kk] : 0.f;
   }
-  double ke = 0.0, mr = 1e300, mp = 1e300;
 
   for (int k = k0; k < k1; ++k) {
     if (k > k0 && k <= nz - 6) {
@@ -379,6 +381,17 @@ __global__ void __launch_bounds__(TX *TY)
         so[l * N + id] = zero ? av[l] : av[l] + bnext * (scv[l] * R[l]);
     }
   }
+}
+
+template <int TX, int TY, int MODE, bool BG1D>
+__global__ void __launch_bounds__(TX *TY)
+    k_quiet32(const Sim32 S, const float *__restrict__ a, const float *__restrict__ tin,
+              float *__restrict__ so, float beta, float bnext, int zchunk) {
+  double ke = 0.0, mr = 1e300, mp = 1e300;
+  const int k0 = blockIdx.z * zchunk;
+  quiet_body<TX, TY, MODE, BG1D>(S, a, tin, so, beta, bnext, blockIdx.x * TX, blockIdx.y * TY,
+                                 k0, min(S.nz, k0 + zchunk), threadIdx.x, threadIdx.y, ke, mr,
+                                 mp);
   if (MODE == F_LAST) diag_reduce32(S, ke, mr, mp);
 }
 
@@ -448,36 +461,32 @@ __device__ __forceinline__ bool mbar_wait32(unsigned long long *bar, unsigned pa
   return false;
 }
 
-// TMA = false: the own-point arrays are fetched by cp.async too (any nx).
+// The body covers the tile (x0, y0) over layers [k0, k1) with a block of
+// 32 x 8 x 2 threads (threadIdx.z is the role); smem is the 128-byte aligned
+// dynamic buffer.  TMA = false: the own-point arrays are fetched by
+// cp.async too (any nx).  Returns false when a bounded wait gave up.
 template <int MODE, bool TMA>
-__global__ void __launch_bounds__(t32::NT, 1)
-    k_mhd32(const Sim32 S, const __grid_constant__ TmaSet32 T,
-            const float *__restrict__ a, const float *__restrict__ tin,
-            float *__restrict__ so, float beta, float bnext, int zchunk, int mt,
-            int ma) {
+__device__ __forceinline__ bool mhd_body(const Sim32 &S, const TmaSet32 *T, float *smem,
+                                         const float *__restrict__ a,
+                                         const float *__restrict__ tin,
+                                         float *__restrict__ so, float beta, float bnext,
+                                         int x0, int y0, int k0, int k1, int mt, int ma,
+                                         double &ke, double &mr, double &mp) {
   using namespace t32;
-  extern __shared__ __align__(1024) float smem_raw32[];
   __shared__ unsigned long long bar[2];
   const int tx = threadIdx.x, ty = threadIdx.y, role = threadIdx.z;
   const int tid = (role * TY + ty) * TX + tx, cid = ty * TX + tx;
-  float *smem = (float *)(((size_t)smem_raw32 + 127) & ~(size_t)127);
-  if (sm_addr32(smem) & 127u) {
-    if (tid == 0) atomicExch(S.err, 2);
-    return;
-  }
   const int nx = S.nx, ny = S.ny, nz = S.nz;
   const int N = (int)S.N, NXY = nx * ny;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   const int i = x0 + tx, j = y0 + ty;
   const bool act = i < nx && j < ny;
   const bool per = S.periodic;
-  const int k0 = blockIdx.z * zchunk, k1 = min(nz, k0 + zchunk);
   const int col = j * nx + i;
   const int xo = origin32(x0, TX, nx, per), yo = origin32(y0, TY, ny, per);
   const int ry = y0 - yo + ty, rx = x0 - xo + tx;
   const int own = ry * HX + rx;
   const float *isc = S.isc, *sc = S.sc;
-  if (tid == 0) {
+  if (TMA && tid == 0) {
     mbar_init32(&bar[0]);
     mbar_init32(&bar[1]);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -550,13 +559,13 @@ __global__ void __launch_bounds__(t32::NT, 1)
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_tx32(&bar[b], own_bytes);
       float *ob = smem + b * BUF;
-      tma3d32(ob + O_RHO * NC, &T.m[mt], x0, y0, k, &bar[b]);
+      tma3d32(ob + O_RHO * NC, &T->m[mt], x0, y0, k, &bar[b]);
       if (MODE != F_FIRST)
         for (int l = 0; l < 8; ++l)
-          tma3d32(ob + (O_A + l) * NC, &T.m[ma], x0, y0, l * nz + k, &bar[b]);
+          tma3d32(ob + (O_A + l) * NC, &T->m[ma], x0, y0, l * nz + k, &bar[b]);
       for (int n = 0; n < 14; ++n)
-        tma3d32(ob + (O_BG + n) * NC, &T.m[3 + n], x0, y0, k, &bar[b]);
-      if (MODE == F_LAST) tma3d32(ob + O_P0 * NC, &T.m[17], x0, y0, k, &bar[b]);
+        tma3d32(ob + (O_BG + n) * NC, &T->m[3 + n], x0, y0, k, &bar[b]);
+      if (MODE == F_LAST) tma3d32(ob + O_P0 * NC, &T->m[17], x0, y0, k, &bar[b]);
     }
   };
   float w0[11], w1[11], w2[11];  // physical values
@@ -586,7 +595,6 @@ __global__ void __launch_bounds__(t32::NT, 1)
       else w0[m] = w1[m] = w2[m] = 0.f;
     }
   }
-  double ke = 0.0, mr = 1e300, mp = 1e300;
   unsigned phase = 0;
   bool ok = true;
   const float dt = (float)S.deltat;
@@ -781,8 +789,30 @@ __global__ void __launch_bounds__(t32::NT, 1)
       mbar_wait32(&bar[0], phase & 1u, S.err);
       mbar_wait32(&bar[1], (phase >> 1) & 1u, S.err);
     }
+    return false;
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  return true;
+}
+
+template <int MODE, bool TMA>
+__global__ void __launch_bounds__(t32::NT, 1)
+    k_mhd32(const Sim32 S, const __grid_constant__ TmaSet32 T,
+            const float *__restrict__ a, const float *__restrict__ tin,
+            float *__restrict__ so, float beta, float bnext, int zchunk, int mt,
+            int ma) {
+  extern __shared__ __align__(1024) float smem_raw32[];
+  float *smem = (float *)(((size_t)smem_raw32 + 127) & ~(size_t)127);
+  if (sm_addr32(smem) & 127u) {
+    if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) atomicExch(S.err, 2);
     return;
   }
+  double ke = 0.0, mr = 1e300, mp = 1e300;
+  const int k0 = blockIdx.z * zchunk;
+  if (!mhd_body<MODE, TMA>(S, &T, smem, a, tin, so, beta, bnext, blockIdx.x * t32::TX,
+                           blockIdx.y * t32::TY, k0, min(S.nz, k0 + zchunk), mt, ma, ke, mr,
+                           mp))
+    return;
   if (MODE == F_LAST) diag_reduce32(S, ke, mr, mp);
 }
 
@@ -798,51 +828,57 @@ struct Filt32 {
   const float *sc, *isc;
 };
 
+// Filtered value of element t (field-major over V x N).
 template <int DIR>
-__global__ void k_filter32(Filt32 F, const float *__restrict__ in, float *__restrict__ out) {
-  const long long total = F.N * F.V;
+__device__ __forceinline__ float filter_point32(const Filt32 &F, const float *__restrict__ in,
+                                                long long t) {
   const int n = DIR == 0 ? F.nx : (DIR == 1 ? F.ny : F.nz);
   const long long st = DIR == 0 ? 1 : (DIR == 1 ? F.nx : (long long)F.nx * F.ny);
   const bool per = DIR != 2 && F.periodic;
   const bool avg = DIR == 2 || !F.periodic;
   const int g = F.g;
-  const float *c = f_df[DIR == 2 ? 1 : 0];
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int l = (int)(t / F.N);
-    const long long pnt = t - (long long)l * F.N;
-    int q;
-    if (DIR == 0) q = (int)(pnt % F.nx);
-    else if (DIR == 1) q = (int)((pnt / F.nx) % F.ny);
-    else q = (int)(pnt / ((long long)F.nx * F.ny));
-    const long long base = t - (long long)q * st;
-    // physical (z) or stored (x, y) value at index qq
-    auto val = [&](int qq) -> float {
-      const float v = __ldg(in + base + (long long)qq * st);
-      return DIR == 2 ? v * F.isc[l * F.nz + qq] : v;
-    };
-    auto pre = [&](int qq) -> float {
-      if (avg && ((qq >= 1 && qq <= g - 1) || (qq >= n - g && qq <= n - 2)))
-        return (val(qq + 1) + val(qq - 1)) / 2.0f;
-      return val(qq);
-    };
-    const float pq = pre(q);
-    float filt;
-    if (!per && (q < g || q >= n - g)) {
-      filt = (DIR != 2 && g == 3) ? 0.f : pq;
-    } else {
-      float s = 0.f;
-      for (int m = 0; m < 2 * g + 1; ++m) {
-        int qq = q - g + m;
-        if (per) qq = wrap32(qq, n);
-        s += pre(qq) * c[m];
-      }
-      filt = s;
+  const float *c = f_df[g == 5 ? 0 : 1];
+  const int l = (int)(t / F.N);
+  const long long pnt = t - (long long)l * F.N;
+  int q;
+  if (DIR == 0) q = (int)(pnt % F.nx);
+  else if (DIR == 1) q = (int)((pnt / F.nx) % F.ny);
+  else q = (int)(pnt / ((long long)F.nx * F.ny));
+  const long long base = t - (long long)q * st;
+  // physical (z) or stored (x, y) value at index qq
+  auto val = [&](int qq) -> float {
+    const float v = __ldg(in + base + (long long)qq * st);
+    return DIR == 2 ? v * F.isc[l * F.nz + qq] : v;
+  };
+  auto pre = [&](int qq) -> float {
+    if (avg && ((qq >= 1 && qq <= g - 1) || (qq >= n - g && qq <= n - 2)))
+      return (val(qq + 1) + val(qq - 1)) / 2.0f;
+    return val(qq);
+  };
+  const float pq = pre(q);
+  float filt;
+  if (!per && (q < g || q >= n - g)) {
+    filt = (DIR != 2 && g == 3) ? 0.f : pq;
+  } else {
+    float sum = 0.f;
+    for (int m = 0; m < 2 * g + 1; ++m) {
+      int qq = q - g + m;
+      if (per) qq = wrap32(qq, n);
+      sum += pre(qq) * c[m];
     }
-    float r = F.mode2 ? pq - F.s * filt : filt;
-    if (DIR == 2) r = r * F.sc[l * F.nz + q];
-    out[t] = r;
+    filt = sum;
   }
+  float r = F.mode2 ? pq - F.s * filt : filt;
+  if (DIR == 2) r = r * F.sc[l * F.nz + q];
+  return r;
+}
+
+template <int DIR>
+__global__ void k_filter32(Filt32 F, const float *__restrict__ in, float *__restrict__ out) {
+  const long long total = F.N * F.V;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x)
+    out[t] = filter_point32<DIR>(F, in, t);
 }
 
 int launch_filter32(Handle *h, int dir, const float *in, float *out, cudaStream_t s) {
@@ -868,18 +904,6 @@ int launch_filter32(Handle *h, int dir, const float *in, float *out, cudaStream_
 // ------------------------------------------------ PULSE = 2, precision form
 // As k_psr of step.cu with an FP32 forcing buffer (the sum over pulses is
 // accumulated in FP32).
-struct Psr32 {
-  int nx, ny, klo, nblocks, bx, bxy;
-  long long init;
-  double timestep, st;
-  const int *off, *idx, *colx, *coly, *colz;
-  const double *zv, *ptime;
-  const float *px, *py, *sd, *ssb;
-  const unsigned char *mask;
-  float *out;
-  const long long *iter;
-};
-
 __global__ void k_psr32(Psr32 D) {
   extern __shared__ float shf[];
   const int k = D.klo + blockIdx.z;
@@ -913,11 +937,11 @@ __global__ void k_psr32(Psr32 D) {
   D.out[((long long)blockIdx.z * D.ny + j) * D.nx + i] = f * D.sd[g] * D.ssb[g];
 }
 
-int launch_psr32(Handle *h, cudaStream_t s) {
-  if (h->src.kind != SPARC_SRC_PSR || h->psr_khi <= h->psr_klo) return SPARC_OK;
-  Psr32 D;
+Psr32 make_psr32(Handle *h) {
+  Psr32 D{};
   D.nx = h->nx; D.ny = h->ny;
   D.klo = h->psr_klo;
+  D.khi = h->psr_khi;
   D.nblocks = h->nblocks;
   D.bx = h->P.block_x;
   D.bxy = h->P.block_x * h->P.block_y;
@@ -938,6 +962,12 @@ int launch_psr32(Handle *h, cudaStream_t s) {
   D.mask = h->d_pmask;
   D.out = h->f_psr;
   D.iter = h->d_iter;
+  return D;
+}
+
+int launch_psr32(Handle *h, cudaStream_t s) {
+  if (h->src.kind != SPARC_SRC_PSR || h->psr_khi <= h->psr_klo) return SPARC_OK;
+  Psr32 D = make_psr32(h);
   dim3 blk(32, 8);
   dim3 grd((h->nx + 31) / 32, (h->ny + 7) / 8, h->psr_khi - h->psr_klo);
   size_t smem = h->pulses.size() * (sizeof(float) + sizeof(int));
@@ -1108,6 +1138,275 @@ int encode_tensor_maps32(Handle *h) {
     ok = ok && h->f_bg[order[n]] && one(&h->tmaps32[3 + n], h->f_bg[order[n]], h->nz);
   h->tma32 = ok;
   return SPARC_OK;
+}
+
+// ------------------------------------------------------------ batched engine
+// Many simulations advance together: each RK stage is one persistent launch
+// whose blocks pull (sim, tile, z-chunk) items from a device work-list
+// (dynamic scheduling by an atomic counter).  MHD items are 32x8-column
+// tiles of the two-role body; quiet items are 32x16 tiles of the quiet body
+// on the same 512 threads.  The last item of a simulation to finish the
+// last stage reduces its diagnostics, advances its iteration, decrements
+// its steps left and rotates its buffer roles; filter passes check their
+// cadence per simulation on the device.
+
+constexpr int BT = t32::NT;  // threads of a batched block
+
+// block-wide sum / min / min of (ke, mr, mp); the result is valid in tid 0
+__device__ __forceinline__ void block_reduce3(double &ke, double &mr, double &mp, int tid) {
+  __shared__ double r[3][32];
+  const int lane = tid & 31, warp = tid >> 5, nw = BT / 32;
+  for (int o = 16; o > 0; o >>= 1) {
+    ke += __shfl_down_sync(0xffffffffu, ke, o);
+    mr = fmin(mr, __shfl_down_sync(0xffffffffu, mr, o));
+    mp = fmin(mp, __shfl_down_sync(0xffffffffu, mp, o));
+  }
+  __syncthreads();
+  if (lane == 0) { r[0][warp] = ke; r[1][warp] = mr; r[2][warp] = mp; }
+  __syncthreads();
+  if (tid == 0) {
+    ke = 0.0; mr = 1e300; mp = 1e300;
+    for (int w = 0; w < nw; ++w) {
+      ke += r[0][w]; mr = fmin(mr, r[1][w]); mp = fmin(mp, r[2][w]);
+    }
+  }
+}
+
+__device__ __forceinline__ void rotate_roles(Slot32 &L) {
+  const int a = L.role[0];
+  L.role[0] = L.role[1];
+  L.role[1] = L.role[2];
+  L.role[2] = a;
+}
+
+// Item `idx` of slot L finished the last stage: store its partial; the last
+// item of the slot ends the step (driver.f90:161-183 diagnostics).
+__device__ void batch_finish_step(Slot32 &L, const Sim32 &S, int idx, double ke, double mr,
+                                  double mp, int tid) {
+  __shared__ int am_last;
+  block_reduce3(ke, mr, mp, tid);
+  if (tid == 0) {
+    L.partials[3 * idx] = ke;
+    L.partials[3 * idx + 1] = mr;
+    L.partials[3 * idx + 2] = mp;
+    __threadfence();
+    const unsigned t = atomicAdd(&L.counter, 1u);
+    am_last = (t == (unsigned)(L.n_items - 1));
+  }
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+  ke = 0.0; mr = 1e300; mp = 1e300;
+  for (int b = tid; b < L.n_items; b += BT) {
+    ke += __ldcg(L.partials + 3 * b);
+    mr = fmin(mr, __ldcg(L.partials + 3 * b + 1));
+    mp = fmin(mp, __ldcg(L.partials + 3 * b + 2));
+  }
+  block_reduce3(ke, mr, mp, tid);
+  if (tid == 0) {
+    const long long it = *S.iter;
+    const double kev = sqrt(ke / ((double)S.nx * (double)S.ny * (double)S.nz)) * S.dimc2rho;
+    S.diag[0] = kev;
+    S.diag[1] = mr;
+    S.diag[2] = mp;
+    S.diag[3] = (double)it;
+    const bool fail = !(kev <= 1000.0) || !(mr > 0.0) || !(mp > 0.0);
+    if (fail && *S.fail_iter < 0) *S.fail_iter = it;
+    *S.iter = it + 1;
+    L.remaining -= 1;
+    rotate_roles(L);
+    L.counter = 0u;
+  }
+}
+
+__global__ void k_batch_begin(Slot32 *slots, int n) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+    slots[q].active = slots[q].remaining > 0 ? 1 : 0;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(BT, 1)
+    k_batch_stage(Slot32 *__restrict__ slots, const int4 *__restrict__ items,
+                  const int *__restrict__ counts, unsigned *wctr, int stage) {
+  extern __shared__ __align__(1024) float smem_raw32[];
+  __shared__ __align__(16) unsigned long long sS_raw[(sizeof(Sim32) + 7) / 8];
+  __shared__ int s_w;
+  float *smem = (float *)(((size_t)smem_raw32 + 127) & ~(size_t)127);
+  Sim32 &sS = *reinterpret_cast<Sim32 *>(sS_raw);
+  const int tid = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
+  const int total = counts[0];
+  int cur = -1;
+  for (;;) {
+    if (tid == 0) s_w = (int)atomicAdd(wctr, 1u);
+    __syncthreads();
+    const int w = s_w;
+    if (w >= total) break;
+    const int4 it = items[w];
+    Slot32 &L = slots[it.x];
+    if (!L.active) {
+      __syncthreads();
+      continue;
+    }
+    if (it.x != cur) {
+      const unsigned long long *src = reinterpret_cast<const unsigned long long *>(&L.S);
+      for (int q = tid; q < (int)(sizeof(Sim32) / 8); q += BT) sS_raw[q] = src[q];
+      cur = it.x;
+      __syncthreads();
+    }
+    const int ra = L.role[0], r1 = L.role[1], r2 = L.role[2];
+    const float *a = L.buf[ra];
+    const float *tin = stage == 1 ? a : L.buf[(stage == 2 || stage == 4) ? r1 : r2];
+    float *so = L.buf[(stage & 1) ? r1 : r2];
+    const float beta = (float)L.betas[stage - 1];
+    const float bnext = (float)(stage < 5 ? L.betas[stage] : sS.deltat);
+    const int x0 = it.y, y0 = it.z, k0 = it.w & 0xffff, k1 = it.w >> 16;
+    double ke = 0.0, mr = 1e300, mp = 1e300;
+    if (sS.magnetic)
+      mhd_body<MODE, false>(sS, nullptr, smem, a, tin, so, beta, bnext, x0, y0, k0, k1, 0, 0,
+                            ke, mr, mp);
+    else if (sS.bg1d)
+      quiet_body<32, 16, MODE, true>(sS, a, tin, so, beta, bnext, x0, y0, k0, k1, threadIdx.x,
+                                     threadIdx.y + 8 * threadIdx.z, ke, mr, mp);
+    else
+      quiet_body<32, 16, MODE, false>(sS, a, tin, so, beta, bnext, x0, y0, k0, k1, threadIdx.x,
+                                      threadIdx.y + 8 * threadIdx.z, ke, mr, mp);
+    if (MODE == F_LAST) batch_finish_step(L, sS, w - L.first_item, ke, mr, mp, tid);
+    __syncthreads();
+  }
+}
+
+// PULSE = 2 forcing of one layer of one simulation per item.
+__global__ void __launch_bounds__(BT)
+    k_batch_psr(Slot32 *__restrict__ slots, const int4 *__restrict__ items,
+                const int *__restrict__ counts, unsigned *wctr) {
+  extern __shared__ float shf[];
+  __shared__ int s_w;
+  const int tid = threadIdx.x;
+  const int total = counts[2];
+  for (;;) {
+    if (tid == 0) s_w = (int)atomicAdd(wctr, 1u);
+    __syncthreads();
+    const int w = s_w;
+    if (w >= total) break;
+    const int4 it = items[w];
+    const Slot32 &L = slots[it.x];
+    if (!L.active) {
+      __syncthreads();
+      continue;
+    }
+    const Psr32 &D = L.psr;
+    const int k = it.y;
+    const int e0 = D.off[k], e1 = D.off[k + 1], ne = e1 - e0;
+    float *sT = shf;
+    int *sN = (int *)(shf + ne);
+    const long long itn = *D.iter;
+    const double t = (double)itn * D.timestep;
+    const double passes = (itn == D.init) ? 2.0 : 1.0;
+    for (int e = tid; e < ne; e += BT) {
+      const int n = D.idx[e0 + e];
+      const double amp = D.ptime[3 * n], t0 = D.ptime[3 * n + 1], t1 = D.ptime[3 * n + 2];
+      double v = amp * sin(2.0 * PI * (t - t1) / t0);
+      v = v * exp(-((t - t1) * (t - t1)) / (2.0 * (D.st * D.st)));
+      sT[e] = (float)(v * D.zv[e0 + e] * passes);
+      sN[e] = n;
+    }
+    __syncthreads();
+    const int nx = D.nx, ny = D.ny;
+    const int bz = D.bxy * D.colz[k];
+    for (int q = tid; q < nx * ny; q += BT) {
+      const int j = q / nx, i = q - j * nx;
+      const int blk = D.colx[i] + D.bx * D.coly[j] + bz;
+      float f = 0.f;
+      for (int e = 0; e < ne; ++e) {
+        const int n = sN[e];
+        if (!D.mask[(long long)n * D.nblocks + blk]) continue;
+        f = f + sT[e] * (D.px[(long long)n * nx + i] * D.py[(long long)n * ny + j]);
+      }
+      const long long g = (long long)k * nx * ny + q;
+      D.out[(long long)(k - D.klo) * nx * ny + q] = f * D.sd[g] * D.ssb[g];
+    }
+    __syncthreads();
+  }
+}
+
+// One filter direction (y, x or z order as FILTER_VARS) over the simulations
+// whose cadence asks for it after the iteration just stepped.  The last
+// pass applied to a simulation starts a new compensated sum (carry 0).
+template <int DIR>
+__global__ void __launch_bounds__(BT)
+    k_batch_filter(Slot32 *__restrict__ slots, const int4 *__restrict__ items,
+                   const int *__restrict__ counts, unsigned *wctr) {
+  __shared__ int s_w;
+  const int tid = threadIdx.x;
+  const int total = counts[1];
+  for (;;) {
+    if (tid == 0) s_w = (int)atomicAdd(wctr, 1u);
+    __syncthreads();
+    const int w = s_w;
+    if (w >= total) break;
+    const int4 it = items[w];
+    Slot32 &L = slots[it.x];
+    bool need = false, need_z = false;
+    if (L.active) {
+      const long long nn = *L.S.iter - 1;
+      const bool need_xy = nn != 0 && nn % L.xyfreq == 0;
+      need_z = nn != 0 && nn % L.zfreq == 0;
+      need = DIR == 2 ? need_z : need_xy;
+    }
+    if (!need) {
+      __syncthreads();
+      continue;
+    }
+    Filt32 F;
+    F.nx = L.S.nx; F.ny = L.S.ny; F.nz = L.S.nz;
+    F.periodic = L.S.periodic;
+    F.g = DIR == 2 ? L.gz : L.gxy;
+    F.mode2 = F.g == 3;
+    F.V = L.S.V;
+    F.N = L.S.N;
+    F.s = DIR == 2 ? L.s_z : L.s_xy;
+    F.sc = L.S.sc;
+    F.isc = L.S.isc;
+    const float *in = L.buf[L.role[0]];
+    float *out = L.buf[L.role[1]];
+    float *carry = L.S.carry;
+    const bool zc = DIR == 2 || (DIR == 0 && !need_z);
+    const long long t0 = it.y, t1 = t0 + it.z;
+    for (long long t = t0 + tid; t < t1; t += BT) {
+      out[t] = filter_point32<DIR>(F, in, t);
+      if (zc) carry[t] = 0.f;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      const unsigned c = atomicAdd(&L.counter, 1u);
+      if (c == (unsigned)(L.f_items - 1)) {
+        rotate_roles(L);
+        L.counter = 0u;
+      }
+    }
+  }
+}
+
+size_t batch_stage_smem() { return t32::SMEM; }
+
+int launch_batch_step(const BatchLaunch &B, cudaStream_t s, int *nkernels) {
+  const int sm = (int)t32::SMEM;
+  cudaFuncSetAttribute(k_batch_stage<F_FIRST>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_batch_stage<F_MID>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_batch_stage<F_LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (cudaMemsetAsync(B.wctr, 0, 9 * sizeof(unsigned), s) != cudaSuccess) return SPARC_ERR_CUDA;
+  k_batch_begin<<<(B.nslots + 255) / 256, 256, 0, s>>>(B.slots, B.nslots);
+  k_batch_psr<<<B.grid, BT, B.psr_smem, s>>>(B.slots, B.pitems, B.counts, B.wctr + 0);
+  const dim3 blk(t32::TX, t32::TY, 2);
+  k_batch_stage<F_FIRST><<<B.grid, blk, t32::SMEM, s>>>(B.slots, B.items, B.counts, B.wctr + 1, 1);
+  for (int st = 2; st <= 4; ++st)
+    k_batch_stage<F_MID><<<B.grid, blk, t32::SMEM, s>>>(B.slots, B.items, B.counts, B.wctr + st, st);
+  k_batch_stage<F_LAST><<<B.grid, blk, t32::SMEM, s>>>(B.slots, B.items, B.counts, B.wctr + 5, 5);
+  k_batch_filter<1><<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 6);
+  k_batch_filter<0><<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 7);
+  k_batch_filter<2><<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 8);
+  *nkernels = 10;
+  return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
 }
 
 // ------------------------------------------------------ precision-form setup

@@ -19,6 +19,7 @@ MM = 1.0e8                    # cm per Mm
 
 SEED_CFG0 = 0x5A5C0000
 SEED_CFG1 = 0x5A5C0001
+SEED_CFG3 = 0x5A5C0003
 
 
 def base_params(nx, ny, nz, *, magnetic=0, periodic=True, hpml=False,
@@ -227,3 +228,47 @@ def cfg1(nx=256, ny=256, nz=300, npulses=200, seed=SEED_CFG1,
     tab = psr_table(p, npulses, seed)
     src = psr_source(tab)
     return p, bg, src
+
+
+# Grid spacing of the flux-tube configuration (256 points over 100 Mm,
+# 300 points over -25..+1 Mm), kept by the ensemble members.
+DX_MM = 100.0 / 256
+DZ_MM = 26.0 / 299
+
+
+def member(nx, nz, B0_gauss, depth_mm, precision=abi.SPARC_FP32,
+           blocks=(2, 2, 4)):
+    """One ensemble member: an nx x nx x nz box at the flux-tube spacing
+    whose top is at +1 Mm.  B0 = 0: quiet (periodic, z-CPML, the hydro
+    equations); B0 > 0: a flux tube (CPML on six faces, the MHD equations,
+    Alfven speed capped at 40 km/s).  One PULSE = 1 Gaussian source at the
+    horizontal centre at depth depth_mm; dt = 0.5 s, z filter every 10
+    steps, xy filter every 30."""
+    L = nx * DX_MM * MM
+    z_bot = 1.0 - (nz - 1) * DZ_MM
+    quiet = B0_gauss <= 0.0
+    p = base_params(nx, nx, nz, magnetic=0 if quiet else 2, periodic=quiet,
+                    hpml=not quiet, xlength=L, ylength=L, timestep=0.5,
+                    t_z=5.0, t_xy=15.0, blocks=blocks, maxva=4.0e6,
+                    precision=precision)
+    if quiet:
+        bg = quiet_background(nx, nx, nz, z_bot, 1.0)
+    else:
+        bg = fluxtube_background(nx, nx, nz, L, L, z_bot, 1.0, B0=B0_gauss)
+    src = pulse_source(px=0.5 * L, py=0.5 * L, pz=depth_mm * MM, t1=150.0,
+                       st=40.0)
+    return p, bg, src
+
+
+def ensemble_draws(n=64, seed=SEED_CFG3):
+    """The batched-ensemble members: nx = ny uniform in {96, 128, 160, 192,
+    256}, nz uniform in [150, 300], B0 uniform in {0, 0.5, ..., 3} kG (the
+    seeded B0 = 0 members are the quiet ones), source depth uniform in
+    [-2, 0] Mm.  Returns a list of (nx, nz, B0_gauss, depth_mm)."""
+    rng = np.random.Generator(np.random.Philox(key=seed))
+    nxs = rng.choice([96, 128, 160, 192, 256], size=n)
+    nzs = rng.integers(150, 301, size=n)
+    b0 = 500.0 * rng.integers(0, 7, size=n)
+    depth = -2.0 * rng.random(n)
+    return [(int(a), int(b), float(c), float(d))
+            for a, b, c, d in zip(nxs, nzs, b0, depth)]

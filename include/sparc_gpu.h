@@ -200,6 +200,20 @@ int sparc_get_scalars(sparc_handle *h, double *out12);
  * failed sparc_create when h is NULL). */
 const char *sparc_last_error(const sparc_handle *h);
 
+/* ------------------------------------------------ allocation-free path
+ * No counterpart in the reference.  The kinetic-energy norm of the handle's
+ * current state -- the quantity sparc_diagnostics reports as ke_norm
+ * (driver.f90:161, norm() of all_modules.f90:684-706) -- computed without
+ * allocating memory: the reduction's scratch is a static device array of
+ * 33,024 bytes, so grids above 67,108,864 points are rejected
+ * (SPARC_ERR_INVALID).  For callers that must not allocate, e.g. a monitor
+ * polling a simulation whose device memory is fully committed to the
+ * serving loop's budget.  The scratch is shared by every call on a device:
+ * calls that overlap in time race and must be serialised by the caller.
+ * The first call on a device looks up the scratch address; make it before
+ * any stream capture.  Waits for the handle's stream. */
+int sparc_ke_norm_noalloc(sparc_handle *h, double *ke_norm);
+
 /* -------------------------------------------------------- batched engine
  * No counterpart in the reference, which runs one simulation per MPI job.
  * A batch advances many SPARC_FP32 handles of any grid sizes together: each

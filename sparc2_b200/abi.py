@@ -112,7 +112,7 @@ EXPORTS = [
     "sparc_batch_set_tiles", "sparc_batch_get_tiles",
     "sparc_batch_synchronize", "sparc_batch_stream",
     "sparc_batch_launch_count", "sparc_batch_last_error",
-    "sparc_batch_tune",
+    "sparc_batch_tune", "sparc_ke_norm_noalloc",
 ]
 
 _lib = None
@@ -156,6 +156,7 @@ def _declare(lib):
         "sparc_batch_launch_count": (C.c_int, [h, P(C.c_int64)]),
         "sparc_batch_last_error": (C.c_char_p, [h]),
         "sparc_batch_tune": (C.c_int, [h, C.c_int, P(C.c_int), P(C.c_int)]),
+        "sparc_ke_norm_noalloc": (C.c_int, [h, d]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -23,6 +23,7 @@ UNITS = {
     "step32.cu": [],
     "api.cu": [],
     "batch.cu": [],
+    "noalloc.cu": [],
 }
 HEADERS = ["internal.h"]
 

@@ -42,12 +42,21 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--workload", default="cfg1",
-                    choices=["cfg1", "cfg0", "ensemble"],
+                    choices=["cfg1", "cfg0", "ensemble", "serve"],
                     help="cfg1: MHD flux tube 256x256x300; cfg0: quiet-Sun "
                     "64x64x128; ensemble: 64 seeded FP32 members advanced by "
                     "the batched engine")
     ap.add_argument("--members", type=int, default=64,
                     help="ensemble size (ensemble workload)")
+    ap.add_argument("--rate", type=float, default=5.0,
+                    help="serve: Poisson arrival rate (requests/s)")
+    ap.add_argument("--duration", type=float, default=60.0,
+                    help="serve: seconds of arrivals")
+    ap.add_argument("--steps-scale", type=float, default=0.05,
+                    help="serve: request durations (500-4000 iterations) "
+                    "scaled by this factor")
+    ap.add_argument("--budget-gb", type=float, default=150.0,
+                    help="serve: device-memory admission budget")
     ap.add_argument("--no-fp64-compare", action="store_true",
                     help="ensemble: skip timing the FP64 plain cfg1 step")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
@@ -560,6 +569,86 @@ def run_ensemble(args, world, rank, local):
     rep.close()
 
 
+def run_serve(args, world, rank, local):
+    """Served solves, FP32: Poisson arrivals (seeded) of requests with
+    random grid, background, source and duration, admitted by a device
+    memory budget into the running batch; latency percentiles beside the
+    served grid-point update rate."""
+    import torch
+    from sparc2_b200.serve import Server, drive
+    from sparc2_b200.replicas import Replicas
+    dev = local
+    torch.cuda.set_device(dev)
+    rep = Replicas("nccl")
+    draws = W.serve_draws(args.rate, args.duration,
+                          steps_scale=args.steps_scale)
+    reqs = []
+    for d in draws:
+        p = W.member_params(d["nx"], d["nz"], d["B0"])
+        reqs.append((d["arrival"], d["key"], p, 0, d["steps"]))
+    res = {}
+
+    def build(key):
+        _, bg, src = W.serve_request(draws[key])
+        return bg, src
+
+    def on_result(key, sim, state, times):
+        d, _ = sim.diagnostics()
+        res[key] = (state, times.copy(), d.ke_norm)
+
+    clocks = Clocks(dev)
+    srv = Server(capacity=64, budget_bytes=int(args.budget_gb * 1e9),
+                 quantum=10, device=dev)
+    wall = drive(srv, reqs, build, on_result, builders=3,
+                 deadline_s=20 * args.duration + 600)
+    st = srv.stats()
+    srv.close()
+    clk = clocks.stop() if clocks else None
+    lat = np.array([t[3] - t[0] for _, t, _ in res.values()])
+    wait = np.array([t[1] - t[0] for _, t, _ in res.values()])
+    setup = np.array([t[2] - t[1] for _, t, _ in res.values()])
+    serv = np.array([t[3] - t[2] for _, t, _ in res.values()])
+    pu = st["point_updates"]
+    offered = sum(d["nx"] * d["nx"] * d["nz"] * d["steps"] for d in draws)
+    value = pu / wall
+    pct = lambda a, q: float(np.percentile(a, q)) if a.size else None
+    if rank != 0:
+        rep.close()
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": int(st["batched_steps"]), "warmup": 0,
+        "ms_per_step": 1e3 * st["worker_gpu_wait_s"] / max(1, st["batched_steps"]),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded request stream)",
+        "config": {"workload": "served solves, FP32: Poisson arrivals at %g/s "
+                   "for %g s, nx=ny in [64,256], nz in [128,300], quiet or "
+                   "flux tube (B0 0.5-3 kG), one pulse or 50-500 PSR pulses, "
+                   "500-4000 iterations x %g" % (args.rate, args.duration,
+                                                  args.steps_scale),
+                   "requests": len(draws), "completed": len(res),
+                   "budget_gb": args.budget_gb, "slots": 64, "quantum": 10},
+        "serve": {"p50_latency_s": pct(lat, 50), "p99_latency_s": pct(lat, 99),
+                  "p50_queue_wait_s": pct(wait, 50),
+                  "p99_queue_wait_s": pct(wait, 99),
+                  "p50_setup_s": pct(setup, 50),
+                  "p50_service_s": pct(serv, 50), "p99_service_s": pct(serv, 99),
+                  "offered_point_updates_per_s": offered / args.duration,
+                  "served_point_updates": pu, "wall_s": wall,
+                  "max_concurrent": st["max_concurrent"],
+                  "worker_gpu_wait_s": st["worker_gpu_wait_s"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": None,
+                "d2h_bytes_per_step": None,
+                "note": "the served rate is end to end: host background "
+                "generation, set-up, admission and result read-back inside"},
+        "gpu_launches": None,
+    }
+    if clk:
+        line["clocks"] = clk
+    print(json.dumps(line), flush=True)
+    rep.close()
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
@@ -568,6 +657,9 @@ def main():
         return
     if args.workload == "ensemble":
         run_ensemble(args, world, rank, local)
+        return
+    if args.workload == "serve":
+        run_serve(args, world, rank, local)
         return
     run_gpu(args, world, rank, local)
 

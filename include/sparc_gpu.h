@@ -265,6 +265,72 @@ int sparc_batch_stream(sparc_batch *b, void **stream);
 int sparc_batch_launch_count(const sparc_batch *b, int64_t *count);
 const char *sparc_batch_last_error(const sparc_batch *b);
 
+/* ----------------------------------------------------------- serving
+ * No counterpart in the reference.  A server runs a worker thread over one
+ * batch: solve requests (SPARC_FP32 parameters and a duration) queue first
+ * in first out, are admitted by a device-memory budget and a slot count,
+ * built by the client once admitted, and run as batch members while later
+ * requests are admitted and set up.  Ticket states: */
+#define SPARC_REQ_QUEUED    0  /* submitted, nothing allocated             */
+#define SPARC_REQ_ADMITTED  1  /* budget reserved; client builds the handle */
+#define SPARC_REQ_RUNNING   2  /* attached; advancing in the batch          */
+#define SPARC_REQ_DONE      3  /* all iterations done; out of the batch     */
+#define SPARC_REQ_FAILED    4  /* the batch reported an error               */
+#define SPARC_REQ_COLLECTED 5  /* handle handed back by sparc_serve_result  */
+
+typedef struct sparc_server sparc_server;
+
+/* Device bytes of a SPARC_FP32 handle for `p`: resident while it runs, and
+ * at the peak of its set-up (FP64 setup arrays included). */
+int sparc_estimate_bytes(const sparc_params *p, int64_t *resident,
+                         int64_t *peak);
+
+/* A server on `device` with up to `capacity` concurrent requests, a device
+ * memory budget in bytes, and `quantum` batched steps per service round. */
+int sparc_server_create(int device, int capacity, int64_t budget_bytes,
+                        int quantum, sparc_server **out);
+
+/* Stops the worker; running requests end FAILED, their handles stay the
+ * client's. */
+int sparc_server_destroy(sparc_server *s);
+
+/* Queues a request for driver iterations first .. first+steps-1;
+ * SPARC_ERR_NOMEM if its peak size exceeds the whole budget. */
+int sparc_serve_submit(sparc_server *s, const sparc_params *p, int64_t first,
+                       int64_t steps, int64_t *ticket);
+
+/* Waits up to timeout_ms for a not yet taken ticket in `state`
+ * (SPARC_REQ_ADMITTED: to build; SPARC_REQ_DONE: to collect, FAILED ones
+ * included); SPARC_ERR_TIMEOUT if none. */
+int sparc_serve_next(sparc_server *s, int state, int64_t timeout_ms,
+                     int64_t *ticket);
+
+/* The parameters and iteration range a ticket was submitted with. */
+int sparc_serve_params(sparc_server *s, int64_t ticket, sparc_params *p,
+                       int64_t *first, int64_t *steps);
+
+/* Hands the built handle (background and source set) of an ADMITTED
+ * ticket to the server, which adds it to the batch. */
+int sparc_serve_attach(sparc_server *s, int64_t ticket, sparc_handle *h);
+
+/* The handle of a DONE or FAILED ticket and its timestamps (seconds since
+ * the server started: submit, admit, start, done). */
+int sparc_serve_result(sparc_server *s, int64_t ticket, sparc_handle **h,
+                       double *times4, int *state);
+
+/* Ends a ticket and returns its budget (after the client destroyed or
+ * took over the handle, or gave up building it). */
+int sparc_serve_release(sparc_server *s, int64_t ticket);
+
+int sparc_serve_state(sparc_server *s, int64_t ticket, int *state);
+
+/* stats[0..9]: queued, admitted, running, done, budget bytes in use, max
+ * concurrent requests, batched steps run, service rounds, grid-point
+ * updates, seconds the worker waited on batched steps. */
+int sparc_serve_stats(sparc_server *s, double *stats10);
+
+const char *sparc_server_last_error(const sparc_server *s);
+
 #ifdef __cplusplus
 }
 #endif

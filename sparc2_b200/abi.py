@@ -28,6 +28,13 @@ ERR_NAMES = {
 SPARC_FP64 = 0
 SPARC_FP32 = 1
 
+SPARC_REQ_QUEUED = 0
+SPARC_REQ_ADMITTED = 1
+SPARC_REQ_RUNNING = 2
+SPARC_REQ_DONE = 3
+SPARC_REQ_FAILED = 4
+SPARC_REQ_COLLECTED = 5
+
 SPARC_SRC_NONE = 0
 SPARC_SRC_PULSE = 1
 SPARC_SRC_PSR = 2
@@ -113,6 +120,10 @@ EXPORTS = [
     "sparc_batch_synchronize", "sparc_batch_stream",
     "sparc_batch_launch_count", "sparc_batch_last_error",
     "sparc_batch_tune", "sparc_ke_norm_noalloc",
+    "sparc_estimate_bytes", "sparc_server_create", "sparc_server_destroy",
+    "sparc_serve_submit", "sparc_serve_next", "sparc_serve_params",
+    "sparc_serve_attach", "sparc_serve_result", "sparc_serve_release",
+    "sparc_serve_state", "sparc_serve_stats", "sparc_server_last_error",
 ]
 
 _lib = None
@@ -157,6 +168,23 @@ def _declare(lib):
         "sparc_batch_last_error": (C.c_char_p, [h]),
         "sparc_batch_tune": (C.c_int, [h, C.c_int, P(C.c_int), P(C.c_int)]),
         "sparc_ke_norm_noalloc": (C.c_int, [h, d]),
+        "sparc_estimate_bytes": (C.c_int, [P(SparcParams), P(C.c_int64),
+                                           P(C.c_int64)]),
+        "sparc_server_create": (C.c_int, [C.c_int, C.c_int, C.c_int64,
+                                          C.c_int, P(C.c_void_p)]),
+        "sparc_server_destroy": (C.c_int, [h]),
+        "sparc_serve_submit": (C.c_int, [h, P(SparcParams), C.c_int64,
+                                         C.c_int64, P(C.c_int64)]),
+        "sparc_serve_next": (C.c_int, [h, C.c_int, C.c_int64, P(C.c_int64)]),
+        "sparc_serve_params": (C.c_int, [h, C.c_int64, P(SparcParams),
+                                         P(C.c_int64), P(C.c_int64)]),
+        "sparc_serve_attach": (C.c_int, [h, C.c_int64, h]),
+        "sparc_serve_result": (C.c_int, [h, C.c_int64, P(C.c_void_p), d,
+                                         P(C.c_int)]),
+        "sparc_serve_release": (C.c_int, [h, C.c_int64]),
+        "sparc_serve_state": (C.c_int, [h, C.c_int64, P(C.c_int)]),
+        "sparc_serve_stats": (C.c_int, [h, d]),
+        "sparc_server_last_error": (C.c_char_p, [h]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -24,6 +24,7 @@ UNITS = {
     "api.cu": [],
     "batch.cu": [],
     "noalloc.cu": [],
+    "serve.cu": [],
 }
 HEADERS = ["internal.h"]
 

@@ -1107,7 +1107,7 @@ int launch_stage32(Handle *h, const Sim32 &S, int stage, const float *a,
 // (needs 16-byte row strides: nx a multiple of 4).
 int encode_tensor_maps32(Handle *h) {
   h->tma32 = false;
-  if (!h->magnetic || (h->nx & 3)) return SPARC_OK;
+  if (!h->magnetic || (h->nx & 3) || !h->allow_tma32) return SPARC_OK;
   void *fn = nullptr;
   cudaDriverEntryPointQueryResult q;
   if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=

@@ -20,6 +20,7 @@ MM = 1.0e8                    # cm per Mm
 SEED_CFG0 = 0x5A5C0000
 SEED_CFG1 = 0x5A5C0001
 SEED_CFG3 = 0x5A5C0003
+SEED_CFG4 = 0x5A5C0004
 
 
 def base_params(nx, ny, nz, *, magnetic=0, periodic=True, hpml=False,
@@ -236,6 +237,17 @@ DX_MM = 100.0 / 256
 DZ_MM = 26.0 / 299
 
 
+def member_params(nx, nz, B0_gauss, precision=abi.SPARC_FP32,
+                  blocks=(2, 2, 4)):
+    """The run parameters of member() alone (no background arrays)."""
+    L = nx * DX_MM * MM
+    quiet = B0_gauss <= 0.0
+    return base_params(nx, nx, nz, magnetic=0 if quiet else 2, periodic=quiet,
+                       hpml=not quiet, xlength=L, ylength=L, timestep=0.5,
+                       t_z=5.0, t_xy=15.0, blocks=blocks, maxva=4.0e6,
+                       precision=precision)
+
+
 def member(nx, nz, B0_gauss, depth_mm, precision=abi.SPARC_FP32,
            blocks=(2, 2, 4)):
     """One ensemble member: an nx x nx x nz box at the flux-tube spacing
@@ -247,10 +259,7 @@ def member(nx, nz, B0_gauss, depth_mm, precision=abi.SPARC_FP32,
     L = nx * DX_MM * MM
     z_bot = 1.0 - (nz - 1) * DZ_MM
     quiet = B0_gauss <= 0.0
-    p = base_params(nx, nx, nz, magnetic=0 if quiet else 2, periodic=quiet,
-                    hpml=not quiet, xlength=L, ylength=L, timestep=0.5,
-                    t_z=5.0, t_xy=15.0, blocks=blocks, maxva=4.0e6,
-                    precision=precision)
+    p = member_params(nx, nz, B0_gauss, precision, blocks)
     if quiet:
         bg = quiet_background(nx, nx, nz, z_bot, 1.0)
     else:
@@ -272,3 +281,44 @@ def ensemble_draws(n=64, seed=SEED_CFG3):
     depth = -2.0 * rng.random(n)
     return [(int(a), int(b), float(c), float(d))
             for a, b, c, d in zip(nxs, nzs, b0, depth)]
+
+
+def serve_draws(rate, duration_s, seed=SEED_CFG4, steps_scale=1.0):
+    """Served-solve requests: Poisson arrivals at `rate` per second over
+    duration_s seconds.  Each request draws nx = ny uniform in [64, 256], nz
+    uniform in [128, 300], a background (quiet, or a flux tube with B0
+    uniform in [0.5, 3] kG, even odds), a source (one Gaussian pulse, or a
+    PULSE = 2 field of 50-500 pulses, even odds) and a duration of 500-4000
+    driver iterations (times steps_scale, at least 20).  Returns a list of
+    dicts sorted by arrival time."""
+    rng = np.random.Generator(np.random.Philox(key=seed + int(rate * 1000)))
+    out = []
+    t = 0.0
+    n = 0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > duration_s:
+            break
+        tube = rng.random() < 0.5
+        psr = rng.random() < 0.5
+        out.append(dict(
+            arrival=t, key=n,
+            nx=int(rng.integers(64, 257)), nz=int(rng.integers(128, 301)),
+            B0=float(rng.uniform(500.0, 3000.0)) if tube else 0.0,
+            npulses=int(rng.integers(50, 501)) if psr else 0,
+            depth=float(-2.0 * rng.random()),
+            steps=max(20, int(round(rng.integers(500, 4001) * steps_scale))),
+            seed=int(rng.integers(0, 2**62))))
+        n += 1
+    return out
+
+
+def serve_request(d, precision=abi.SPARC_FP32, blocks=(2, 2, 4)):
+    """(params, background, source) of a served request drawn by
+    serve_draws: the ensemble member geometry and numerics, with the PULSE
+    = 2 field when npulses > 0."""
+    p, bg, src = member(d["nx"], d["nz"], d["B0"], d["depth"],
+                        precision=precision, blocks=blocks)
+    if d["npulses"] > 0:
+        src = psr_source(psr_table(p, d["npulses"], d["seed"]))
+    return p, bg, src

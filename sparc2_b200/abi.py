@@ -201,7 +201,8 @@ def load(path=None):
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = path or LIB_PATH
+    # SPARC_GPU_LIB: another build of the same library (A/B timing)
+    p = path or os.environ.get("SPARC_GPU_LIB") or LIB_PATH
     if not os.path.exists(p):
         raise FileNotFoundError(
             f"{p} is missing; build it with `python -c 'import "

@@ -87,25 +87,48 @@ int rebuild(Batch *b) {
   std::vector<int4> items, fitems, pitems;
   size_t npart = 0;
   size_t maxp = 0;
-  // MHD items first: they cost most, dynamic scheduling then fills in
-  for (int pass = 0; pass < 2; ++pass)
+  // pass 0: interior MHD tiles (the list's prefix, run by the branch-free
+  // kernel); pass 1: MHD tiles at edges / CPML slabs; pass 2: quiet tiles.
+  // Costlier items first, dynamic scheduling then fills in.
+  int n_int = 0;
+  for (int pass = 0; pass < 3; ++pass) {
     for (int q = 0; q < b->cap; ++q) {
       Handle *h = b->members[q];
-      if (!h || (pass == 0) != h->magnetic) continue;
+      if (!h || (pass < 2) != h->magnetic) continue;
       Slot32 &L = b->slots[q];
       const int TY = h->magnetic ? 8 : 16;
       const int zc = std::max(11, h->magnetic ? b->zchunk_mhd : b->zchunk_quiet);
-      L.first_item = (int)items.size();
+      const int first = (int)items.size();
       for (int k0 = 0; k0 < h->nz; k0 += zc) {
         const int k1 = std::min(h->nz, k0 + zc);
         for (int y0 = 0; y0 < h->ny; y0 += TY)
-          for (int x0 = 0; x0 < h->nx; x0 += 32)
-            items.push_back(make_int4(q, x0, y0, k0 | (k1 << 16)));
+          for (int x0 = 0; x0 < h->nx; x0 += 32) {
+            bool in = false;
+            if (h->magnetic) {  // the kernels' interior test
+              const FaceT<float> *F = h->f_faces;
+              const int xm = std::max(5, F[2].on ? F[2].np : 0);
+              const int xM = std::max(5, F[3].on ? F[3].np : 0);
+              const int ym = std::max(5, F[4].on ? F[4].np : 0);
+              const int yM = std::max(5, F[5].on ? F[5].np : 0);
+              in = x0 >= xm && x0 + 32 <= h->nx - xM && y0 >= ym && y0 + 8 <= h->ny - yM;
+            }
+            if (in == (pass == 0)) items.push_back(make_int4(q, x0, y0, k0 | (k1 << 16)));
+          }
       }
-      L.n_items = (int)items.size() - L.first_item;
+      if (pass == 0) {
+        L.first_item = first;
+        L.n_items = (int)items.size() - first;
+      } else {
+        L.first_item2 = first;
+        L.n_items2 = (int)items.size() - first;
+      }
       L.partials = nullptr;  // set below
-      npart += (size_t)L.n_items;
     }
+    if (pass == 0) n_int = (int)items.size();
+  }
+  for (int q = 0; q < b->cap; ++q)
+    if (b->members[q] && !b->members[q]->magnetic) b->slots[q].first_item = b->slots[q].n_items = 0;
+  npart = items.size();
   for (int q = 0; q < b->cap; ++q) {
     Handle *h = b->members[q];
     if (!h) continue;
@@ -127,13 +150,13 @@ int rebuild(Batch *b) {
   r |= grow(b, b->d_partials, b->partials_cap, 3 * npart);
   if (r) return r;
   for (int q = 0; q < b->cap; ++q)
-    if (b->members[q]) b->slots[q].partials = b->d_partials + 3 * (size_t)b->slots[q].first_item;
+    if (b->members[q]) b->slots[q].partials = b->d_partials;
   const size_t smem = std::max<size_t>(maxp, 1) * (sizeof(float) + sizeof(int));
   if (smem != b->psr_smem) {
     b->psr_smem = smem;
     b->recapture = true;
   }
-  const int counts[3] = {(int)items.size(), (int)fitems.size(), (int)pitems.size()};
+  const int counts[4] = {(int)items.size(), (int)fitems.size(), (int)pitems.size(), n_int};
   BCK(b, cudaStreamSynchronize(b->stream));
   if (!items.empty())
     BCK(b, cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(int4),
@@ -220,10 +243,10 @@ int sparc_batch_create(int device, int capacity, sparc_batch **out) {
   b->grid = sms;
   bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
             cudaMalloc(&b->d_slots, capacity * sizeof(Slot32)) == cudaSuccess &&
-            cudaMalloc(&b->d_counts, 3 * sizeof(int)) == cudaSuccess &&
-            cudaMalloc(&b->d_wctr, 9 * sizeof(unsigned)) == cudaSuccess &&
+            cudaMalloc(&b->d_counts, 4 * sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&b->d_wctr, 14 * sizeof(unsigned)) == cudaSuccess &&
             cudaMemset(b->d_slots, 0, capacity * sizeof(Slot32)) == cudaSuccess &&
-            cudaMemset(b->d_counts, 0, 3 * sizeof(int)) == cudaSuccess;
+            cudaMemset(b->d_counts, 0, 4 * sizeof(int)) == cudaSuccess;
   if (!ok) {
     cudaGetLastError();
     sparc_batch_destroy(b);

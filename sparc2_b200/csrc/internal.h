@@ -30,6 +30,7 @@ struct FaceT {
   R *vars;              // RK state (zpmlvars...), cnt*P
   R *scr;               // stage right-hand side (scrzpml...), cnt*P
   const R *pa, *pb, *pk;
+  const R *pki;         // 1/kappa (precision form)
 };
 using FaceDev = FaceT<double>;
 
@@ -110,12 +111,13 @@ struct Slot32 {
   long long remaining;         // driver iterations left
   int active;                  // set at the start of each step
   int has_psr;
-  int first_item, n_items;     // stage work-list range
+  int first_item, n_items;     // stage items of the interior part (MHD only)
+  int first_item2, n_items2;   // stage items of the general part
   int f_first, f_items;        // filter work-list range
   int gxy, gz, xyfreq, zfreq;
   float s_xy, s_z;
   unsigned counter;            // items done in the current launch
-  double *partials;            // 3 per stage item (last stage)
+  double *partials;            // 3 per stage item of the work-list (last stage)
 };
 
 // Device work-lists and launch shape of one batched step.
@@ -123,8 +125,9 @@ struct BatchLaunch {
   Slot32 *slots;
   int nslots;
   const int4 *items, *fitems, *pitems;  // stage, filter, forcing items
-  const int *counts;                    // [3] item counts
-  unsigned *wctr;                       // [9] work counters, zeroed per step
+  const int *counts;                    // [4] stage, filter, forcing items,
+                                        // interior stage items (a prefix)
+  unsigned *wctr;                       // [14] work counters, zeroed per step
   int grid;                             // persistent CTAs
   size_t psr_smem;
 };

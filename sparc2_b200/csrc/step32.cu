@@ -63,15 +63,48 @@ template <int MODE>
 __device__ __forceinline__ void cpml32(const Face32 &F, long long f, int layer, int slot,
                                        float beta, float dt, float &d) {
   const long long pf = F.uniform ? (long long)layer : f;
-  const float pa = __ldg(F.pa + pf), pb = __ldg(F.pb + pf), pk = __ldg(F.pk + pf);
+  const float pa = __ldg(F.pa + pf), pb = __ldg(F.pb + pf), pki = __ldg(F.pki + pf);
   const long long o = (long long)slot * F.cnt + f;
   const float v = F.vars[o];
   float psi = v;
   if (MODE != F_FIRST) psi = v + beta * F.scr[o];
   const float rhs = pa * d + pb * psi;
-  d = d / pk + psi;
+  d = d * pki + psi;
   if (MODE == F_LAST) F.vars[o] = v + dt * rhs;
   else F.scr[o] = rhs;
+}
+
+// Three CPML fields of one face at one point: every load is issued before
+// any store (one memory round trip instead of three), the profile once.
+template <int MODE>
+__device__ __forceinline__ void cpml3_32(const Face32 &F, long long f, int layer, int s0, int s1,
+                                         int s2, float beta, float dt, float &d0, float &d1,
+                                         float &d2) {
+  const long long pf = F.uniform ? (long long)layer : f;
+  const float pa = __ldg(F.pa + pf), pb = __ldg(F.pb + pf), pki = __ldg(F.pki + pf);
+  const long long o0 = (long long)s0 * F.cnt + f, o1 = (long long)s1 * F.cnt + f,
+                  o2 = (long long)s2 * F.cnt + f;
+  const float v0 = F.vars[o0], v1 = F.vars[o1], v2 = F.vars[o2];
+  float p0 = v0, p1 = v1, p2 = v2;
+  if (MODE != F_FIRST) {
+    const float c0 = F.scr[o0], c1 = F.scr[o1], c2 = F.scr[o2];
+    p0 = v0 + beta * c0;
+    p1 = v1 + beta * c1;
+    p2 = v2 + beta * c2;
+  }
+  const float r0 = pa * d0 + pb * p0, r1 = pa * d1 + pb * p1, r2 = pa * d2 + pb * p2;
+  d0 = d0 * pki + p0;
+  d1 = d1 * pki + p1;
+  d2 = d2 * pki + p2;
+  if (MODE == F_LAST) {
+    F.vars[o0] = v0 + dt * r0;
+    F.vars[o1] = v1 + dt * r1;
+    F.vars[o2] = v2 + dt * r2;
+  } else {
+    F.scr[o0] = r0;
+    F.scr[o1] = r1;
+    F.scr[o2] = r2;
+  }
 }
 
 __device__ __forceinline__ float pulse_time32(const Sim32 &S, long long it) {
@@ -113,9 +146,11 @@ __device__ __forceinline__ float dxy32(int q, int n, bool per, float sc, Get t) 
 __device__ __forceinline__ float dz32(const float (&w)[11], int k, int nz, float sc) {
   float s = 0.f;
   if (k < nz - 5) {
-#pragma unroll
-    for (int m = 0; m < 11; ++m) s += w[m] * f_dp[5][m];
-    return sc * s;
+    const float d1 = w[6] - w[4], d2 = w[7] - w[3], d3 = w[8] - w[2], d4 = w[9] - w[1],
+                d5 = w[10] - w[0];
+    const float a = fmaf(f_dp[5][8], d3, fmaf(f_dp[5][10], d5, f_dp[5][6] * d1));
+    const float b = fmaf(f_dp[5][9], d4, f_dp[5][7] * d2);
+    return sc * (a + b);
   }
   const int row = nz - 1 - k;
 #pragma unroll
@@ -129,7 +164,19 @@ __device__ __forceinline__ void shift32(float (&w)[11], float v) {
   w[10] = v;
 }
 
+// Centred 11-point sum at p[5*st]; the centred row is antisymmetric
+// (c[5+m] = -c[5-m], c[5] = 0), so it is sum_m c[5+m] (f[+m] - f[-m]),
+// evaluated as two short independent chains.
 __device__ __forceinline__ float csum32(const float *p, int st) {
+  // (the general tiles use csumf32: the plain 11-term sum needs fewer live values)
+  const float d1 = p[6 * st] - p[4 * st], d2 = p[7 * st] - p[3 * st],
+              d3 = p[8 * st] - p[2 * st], d4 = p[9 * st] - p[st], d5 = p[10 * st] - p[0];
+  const float a = fmaf(f_dp[5][8], d3, fmaf(f_dp[5][10], d5, f_dp[5][6] * d1));
+  const float b = fmaf(f_dp[5][9], d4, f_dp[5][7] * d2);
+  return a + b;
+}
+
+__device__ __forceinline__ float csumf32(const float *p, int st) {
   float s = 0.f;
 #pragma unroll
   for (int m = 0; m < 11; ++m) s += p[m * st] * f_dp[5][m];
@@ -146,14 +193,15 @@ __device__ __forceinline__ float kahan(float a, float inc, float &c) {
 
 // Per-CTA partial of the KE norm and minima (FP64) and the last-CTA
 // reduction with the fail criterion of driver.f90:175-183.
-__device__ void diag_reduce32(const Sim32 &S, double ke, double mr, double mp) {
+// bid/nb: this block's index and the block count of the logical grid (a
+// stage split over several launches shares one logical grid).
+__device__ void diag_reduce32(const Sim32 &S, double ke, double mr, double mp, long long bid,
+                              long long nb) {
   __shared__ double r[3][32];
   __shared__ int am_last;
   const int nt = blockDim.x * blockDim.y * blockDim.z;
   const int tid = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5, nw = (nt + 31) >> 5;
-  const long long nb = (long long)gridDim.x * gridDim.y * gridDim.z;
-  const long long bid = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
   for (int o = 16; o > 0; o >>= 1) {
     ke += __shfl_down_sync(0xffffffffu, ke, o);
     mr = fmin(mr, __shfl_down_sync(0xffffffffu, mr, o));
@@ -392,7 +440,10 @@ __global__ void __launch_bounds__(TX *TY)
   quiet_body<TX, TY, MODE, BG1D>(S, a, tin, so, beta, bnext, blockIdx.x * TX, blockIdx.y * TY,
                                  k0, min(S.nz, k0 + zchunk), threadIdx.x, threadIdx.y, ke, mr,
                                  mp);
-  if (MODE == F_LAST) diag_reduce32(S, ke, mr, mp);
+  if (MODE == F_LAST)
+    diag_reduce32(S, ke, mr, mp,
+                  blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z),
+                  (long long)gridDim.x * gridDim.y * gridDim.z);
 }
 
 // -------------------------------------------- MP_MHD_3D, precision form
@@ -464,8 +515,17 @@ __device__ __forceinline__ bool mbar_wait32(unsigned long long *bar, unsigned pa
 // The body covers the tile (x0, y0) over layers [k0, k1) with a block of
 // 32 x 8 x 2 threads (threadIdx.z is the role); smem is the 128-byte aligned
 // dynamic buffer.  TMA = false: the own-point arrays are fetched by
-// cp.async too (any nx).  Returns false when a bounded wait gave up.
-template <int MODE, bool TMA>
+// cp.async too (any nx).  INT: the tile's stencil footprint touches no
+// non-periodic edge, no x/y CPML slab and needs no periodic wrap, so its
+// x/y derivatives are the centred stencil with no branch.  Returns false
+// when a bounded wait gave up.
+//
+// Per layer: every thread waits for its own halo copies, turns the B0 halo
+// values it copied into the fluxes v x B0 in place, then one barrier makes
+// the layer visible; the copies of the next layer are issued after that
+// barrier (the buffer they overwrite was last read before it).  A second
+// barrier exchanges d(vz)/dz and d(by)/dz between the roles.
+template <int MODE, bool TMA, bool INT>
 __device__ __forceinline__ bool mhd_body(const Sim32 &S, const TmaSet32 *T, float *smem,
                                          const float *__restrict__ a,
                                          const float *__restrict__ tin,
@@ -479,13 +539,40 @@ __device__ __forceinline__ bool mhd_body(const Sim32 &S, const TmaSet32 *T, floa
   const int nx = S.nx, ny = S.ny, nz = S.nz;
   const int N = (int)S.N, NXY = nx * ny;
   const int i = x0 + tx, j = y0 + ty;
-  const bool act = i < nx && j < ny;
+  const bool act = INT || (i < nx && j < ny);
   const bool per = S.periodic;
   const int col = j * nx + i;
-  const int xo = origin32(x0, TX, nx, per), yo = origin32(y0, TY, ny, per);
+  const int xo = INT ? x0 - 5 : origin32(x0, TX, nx, per);
+  const int yo = INT ? y0 - 5 : origin32(y0, TY, ny, per);
   const int ry = y0 - yo + ty, rx = x0 - xo + tx;
   const int own = ry * HX + rx;
   const float *isc = S.isc, *sc = S.sc;
+  // General tiles: each lane (x) and row (y) gets its own 11 coefficients and
+  // window start in the tile, so every x/y derivative is one branch-free
+  // sum: the centred row; one-sided row q at the low edge (q = i); at the
+  // high edge -row q reversed over f(n-11..n-1) (derivatives.f90:72, 98).
+  __shared__ float cxs[INT ? 1 : TX * 11], cys[INT ? 1 : TY * 11];
+  __shared__ int cxb[INT ? 1 : TX], cyb[INT ? 1 : TY];
+  if (!INT && tid < TX + TY) {
+    const bool isx = tid < TX;
+    const int q0 = isx ? tid : tid - TX;                 // lane or row
+    const int g = isx ? x0 + q0 : y0 + q0, n = isx ? nx : ny, o = isx ? xo : yo;
+    float *c = isx ? cxs + q0 * 11 : cys + q0 * 11;
+    int base;
+    if (per || (g >= 5 && g < n - 5) || g >= n) {
+      for (int m = 0; m < 11; ++m) c[m] = f_dp[5][m];
+      base = g - 5 - o;
+    } else if (g < 5) {
+      for (int m = 0; m < 11; ++m) c[m] = f_dp[g][m];
+      base = -o;
+    } else {
+      const int q = n - 1 - g;
+      for (int m = 0; m < 11; ++m) c[m] = -f_dp[q][10 - m];
+      base = n - 11 - o;
+    }
+    if (isx) cxb[q0] = base;
+    else cyb[q0] = base;
+  }
   if (TMA && tid == 0) {
     mbar_init32(&bar[0]);
     mbar_init32(&bar[1]);
@@ -568,6 +655,16 @@ __device__ __forceinline__ bool mhd_body(const Sim32 &S, const TmaSet32 *T, floa
       if (MODE == F_LAST) tma3d32(ob + O_P0 * NC, &T->m[17], x0, y0, k, &bar[b]);
     }
   };
+  // fluxes v x B0 (stored velocity units) in place of the B0 halo values,
+  // at the halo positions this thread copied
+  auto flux = [&](int b, int t) {
+    float *H = Hp(b, 0) + t;
+    const float vx_ = H[0], vy_ = H[HS], vz_ = H[2 * HS];
+    const float bx0 = H[7 * HS], by0 = H[8 * HS], bz0 = H[9 * HS];
+    H[7 * HS] = -vz_ * by0 + vy_ * bz0;
+    H[8 * HS] = -vx_ * bz0 + vz_ * bx0;
+    H[9 * HS] = -vy_ * bx0 + vx_ * by0;
+  };
   float w0[11], w1[11], w2[11];  // physical values
   auto head = [&](int kk, float &v0, float &v1, float &v2) {
     const int id = kk * NXY + col;
@@ -598,72 +695,65 @@ __device__ __forceinline__ bool mhd_body(const Sim32 &S, const TmaSet32 *T, floa
   unsigned phase = 0;
   bool ok = true;
   const float dt = (float)S.deltat;
+  const float sx = (float)S.stretchx, sy = (float)S.stretchy;
+  const float *gcol = S.gblk + (act ? S.colx[i] + S.bxdim * S.coly[j] : 0) * nz;
 
   for (int k = k0; k < k1; ++k) {
     const int b = (k - k0) & 1;
+    const int id = k * NXY + col;
     float h0 = 0, h1 = 0, h2 = 0;
     const bool sh = k > k0 && k <= nz - 6;
     if (sh && act) head(k + 5, h0, h1, h2);
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    if (hs0 >= 0) flux(b, hs0);
+    if (hs1 >= 0) flux(b, hs1);
+    bool mine = true;
+    if (TMA && tid == 0) mine = mbar_wait32(&bar[b], (phase >> b) & 1u, S.err);
+    phase ^= 1u << b;
+    if (!__syncthreads_and(mine)) { ok = false; break; }
     if (k + 1 < k1) issue(k + 1, b ^ 1);
-    else cp_commit32();
-    cp_wait1_32();
-    if (TMA) {
-      ok = mbar_wait32(&bar[b], (phase >> b) & 1u, S.err);
-      phase ^= 1u << b;
-    }
-    if (!__syncthreads_and(ok)) { ok = false; break; }
     if (sh) { shift32(w0, h0); shift32(w1, h1); shift32(w2, h2); }
-    float *H7 = Hp(b, 7), *H8 = Hp(b, 8), *H9 = Hp(b, 9);
-    const float ox = H7[own], oy = H8[own], oz = H9[own];
-    __syncthreads();
-    {
-      const float *H0 = Hp(b, 0), *H1 = Hp(b, 1), *H2 = Hp(b, 2);
-      const int cx0 = x0 - xo, cy0 = y0 - yo;
-      for (int t = tid; t < HS; t += NT) {
-        const int ly = t / HX, lx = t - ly * HX;
-        const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
-        if (!inx && !iny) continue;
-        const float vx_ = H0[t], vy_ = H1[t], vz_ = H2[t];
-        const float bx0 = H7[t], by0 = H8[t], bz0 = H9[t];
-        H7[t] = -vz_ * by0 + vy_ * bz0;  // fluxes in stored velocity units
-        H8[t] = -vx_ * bz0 + vz_ * bx0;
-        H9[t] = -vy_ * bx0 + vx_ * by0;
-      }
-    }
-    __syncthreads();
-    const int id = k * NXY + col;
     const float szk = __ldg(S.stretch + k);
-    const float sx = (float)S.stretchx, sy = (float)S.stretchy;
     auto DX = [&](int slot) {
       const float *row = Hp(b, slot) + ry * HX;
-      if (per || (i >= 5 && i < nx - 5)) return sx * csum32(row + (i - 5 - xo), 1);
-      return dxy32(i, nx, per, sx, [&](int g) { return row[g - xo]; });
+      if (INT) return sx * csum32(row + tx, 1);
+      const float *r = row + cxb[tx], *c = cxs + tx * 11;
+      float sum = 0.f;
+#pragma unroll
+      for (int m = 0; m < 11; ++m) sum += r[m] * c[m];
+      return sx * sum;
     };
     auto DY = [&](int slot) {
       const float *colp = Hp(b, slot) + rx;
-      if (per || (j >= 5 && j < ny - 5)) return sy * csum32(colp + (j - 5 - yo) * HX, HX);
-      return dxy32(j, ny, per, sy, [&](int g) { return colp[(g - yo) * HX]; });
+      if (INT) return sy * csum32(colp + ty * HX, HX);
+      const float *r = colp + cyb[ty] * HX, *c = cys + ty * 11;
+      float sum = 0.f;
+#pragma unroll
+      for (int m = 0; m < 11; ++m) sum += r[m * HX] * c[m];
+      return sy * sum;
     };
     const bool zpml = S.zb.on && (k < S.zb.np || k >= nz - S.zt.np);
-    const bool xpml = S.xb.on && act && (i < S.xb.np || i >= nx - S.xt.np);
-    const bool ypml = S.xb.on && act && (j < S.yb.np || j >= ny - S.yt.np);
-    auto pz = [&](int slot, float &d) {
+    const bool xpml = !INT && S.xb.on && act && (i < S.xb.np || i >= nx - S.xt.np);
+    const bool ypml = !INT && S.yb.on && act && (j < S.yb.np || j >= ny - S.yt.np);
+    auto pz = [&](int s0, int s1, int s2, float &da, float &db, float &dc) {
       const bool bot = k < S.zb.np;
       const Face32 &F = bot ? S.zb : S.zt;
       const int kl = bot ? k : k - (nz - S.zt.np);
-      cpml32<MODE>(F, (long long)kl * NXY + col, kl, slot, beta, dt, d);
+      cpml3_32<MODE>(F, (long long)kl * NXY + col, kl, s0, s1, s2, beta, dt, da, db, dc);
     };
-    auto px = [&](int slot, float &d) {
+    auto px = [&](int s0, int s1, int s2, float &da, float &db, float &dc) {
       const bool bot = i < S.xb.np;
       const Face32 &F = bot ? S.xb : S.xt;
       const int il = bot ? i : i - (nx - S.xt.np);
-      cpml32<MODE>(F, il + (long long)F.np * (j + (long long)ny * k), il, slot, beta, dt, d);
+      cpml3_32<MODE>(F, il + (long long)F.np * (j + (long long)ny * k), il, s0, s1, s2, beta,
+                     dt, da, db, dc);
     };
-    auto py = [&](int slot, float &d) {
+    auto py = [&](int s0, int s1, int s2, float &da, float &db, float &dc) {
       const bool bot = j < S.yb.np;
       const Face32 &F = bot ? S.yb : S.yt;
       const int jl = bot ? j : j - (ny - S.yt.np);
-      cpml32<MODE>(F, i + (long long)nx * (jl + (long long)F.np * k), jl, slot, beta, dt, d);
+      cpml3_32<MODE>(F, i + (long long)nx * (jl + (long long)F.np * k), jl, s0, s1, s2, beta,
+                     dt, da, db, dc);
     };
     auto Hv = [&](int slot) { return Hp(b, slot)[own]; };
     const float iv = isc[nz + k];  // velocity (and flux) scale of this layer
@@ -674,17 +764,17 @@ __device__ __forceinline__ bool mhd_body(const Sim32 &S, const TmaSet32 *T, floa
         d0 = ip * DX(3); d5 = ib * DX(6); d7 = ib * DX(5);
         d1 = ip * DY(3); d4 = ib * DY(6); d8 = ib * DY(4);
         d3 = dz32(w0, k, nz, szk); d2 = dz32(w1, k, nz, szk); d6 = dz32(w2, k, nz, szk);
-        if (zpml) { pz(1, d2); pz(0, d3); pz(2, d6); }
-        if (xpml) { px(1, d0); px(3, d5); px(2, d7); }
-        if (ypml) { py(1, d1); py(3, d4); py(2, d8); }
+        if (zpml) pz(1, 0, 2, d2, d3, d6);
+        if (xpml) px(1, 3, 2, d0, d5, d7);
+        if (ypml) py(1, 3, 2, d1, d4, d8);
         X[cid] = d3;
       } else {
         d0 = iv * DX(0); d2 = iv * DX(9); d3 = iv * DX(8);
         d1 = iv * DY(1); d4 = iv * DY(9); d5 = iv * DY(7);
         d6 = dz32(w0, k, nz, szk); d7 = dz32(w1, k, nz, szk); d8 = dz32(w2, k, nz, szk);
-        if (zpml) { pz(4, d7); pz(5, d6); pz(3, d8); }
-        if (xpml) { px(0, d0); px(4, d2); px(5, d3); }
-        if (ypml) { py(0, d1); py(4, d4); py(5, d5); }
+        if (zpml) pz(4, 5, 3, d7, d6, d8);
+        if (xpml) px(0, 4, 5, d0, d2, d3);
+        if (ypml) py(0, 4, 5, d1, d4, d5);
         X[NC + cid] = d8;
       }
     }
@@ -692,12 +782,14 @@ __device__ __forceinline__ bool mhd_body(const Sim32 &S, const TmaSet32 *T, floa
     double an_rho = 0.0;
     if (act) {
       const bool zero = k == 0 || k == nz - 1 ||
-                        (!per && (i == 0 || i == nx - 1 || j == 0 || j == ny - 1));
+                        (!INT && !per && (i == 0 || i == nx - 1 || j == 0 || j == ny - 1));
       const float fac = MODE == F_LAST ? dt : bnext;
       const float rho = O(b, O_RHO) * isc[k], vx = Hv(0) * iv, vy = Hv(1) * iv,
                   vz = Hv(2) * iv;
       const float red = O(b, O_BG + B_RED), sg = O(b, O_BG + B_SPONGE);
       if (role == 0) {
+        // B0 at the own point (its halo slots now hold the fluxes)
+        const float ox = __ldg(S.box + id), oy = __ldg(S.boy + id), oz = __ldg(S.boz + id);
         const float ib = isc[5 * nz + k];
         const float dzby = X[NC + cid];
         const float cbx = d4 - dzby, cby = -d5 + d6, cbz = d7 - d8;
@@ -712,8 +804,7 @@ __device__ __forceinline__ bool mhd_body(const Sim32 &S, const TmaSet32 *T, floa
         vxr = vxr + ri * e1 * red;
         vyr = vyr + ri * e2 * red;
         vzr = vzr + ri * e3 * red;
-        const int gc = S.colx[i] + S.bxdim * S.coly[j];
-        vzr = vzr - ri * rho * __ldg(S.gblk + gc * nz + k);
+        vzr = vzr - ri * rho * __ldg(gcol + k);
         if (S.frc.kind != SPARC_SRC_NONE) {
           const long long it = *S.iter;
           const float frc = forcing32(S, pulse_time32(S, it), i, j, k);
@@ -781,7 +872,6 @@ __device__ __forceinline__ bool mhd_body(const Sim32 &S, const TmaSet32 *T, floa
         ke += m * m;
       }
     }
-    __syncthreads();
   }
   if (!ok) {
     asm volatile("cp.async.wait_all;\n" ::: "memory");
@@ -795,25 +885,45 @@ __device__ __forceinline__ bool mhd_body(const Sim32 &S, const TmaSet32 *T, floa
   return true;
 }
 
-template <int MODE, bool TMA>
+
+// Tiles away from every edge, CPML slab and periodic wrap: their x/y
+// derivatives are the centred stencil with no branch.
+__device__ __forceinline__ bool mhd_interior(const Sim32 &S, int x0, int y0) {
+  const int xm = max(5, S.xb.on ? S.xb.np : 0), xM = max(5, S.xt.on ? S.xt.np : 0);
+  const int ym = max(5, S.yb.on ? S.yb.np : 0), yM = max(5, S.yt.on ? S.yt.np : 0);
+  return x0 >= xm && x0 + t32::TX <= S.nx - xM && y0 >= ym && y0 + t32::TY <= S.ny - yM;
+}
+
+// One RK stage of the MHD equations.  A stage is two launches over one
+// logical grid of (x tile, y tile, z chunk) blocks: INT = true covers the
+// interior tile rectangle [ix0, ix0 + gridDim.x) x [iy0, iy0 + gridDim.y)
+// with the branch-free body; INT = false covers the whole grid and returns at
+// once on interior tiles.  Each kernel is compiled with one body only, so
+// neither pays the other's registers.
+template <int MODE, bool TMA, bool INT>
 __global__ void __launch_bounds__(t32::NT, 1)
     k_mhd32(const Sim32 S, const __grid_constant__ TmaSet32 T,
             const float *__restrict__ a, const float *__restrict__ tin,
             float *__restrict__ so, float beta, float bnext, int zchunk, int mt,
-            int ma) {
+            int ma, int ix0, int iy0, int gx, int gy) {
   extern __shared__ __align__(1024) float smem_raw32[];
   float *smem = (float *)(((size_t)smem_raw32 + 127) & ~(size_t)127);
+  const int tx_ = INT ? blockIdx.x + ix0 : blockIdx.x;
+  const int ty_ = INT ? blockIdx.y + iy0 : blockIdx.y;
+  const int x0 = tx_ * t32::TX, y0 = ty_ * t32::TY;
+  if (!INT && mhd_interior(S, x0, y0)) return;
   if (sm_addr32(smem) & 127u) {
     if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) atomicExch(S.err, 2);
     return;
   }
   double ke = 0.0, mr = 1e300, mp = 1e300;
   const int k0 = blockIdx.z * zchunk;
-  if (!mhd_body<MODE, TMA>(S, &T, smem, a, tin, so, beta, bnext, blockIdx.x * t32::TX,
-                           blockIdx.y * t32::TY, k0, min(S.nz, k0 + zchunk), mt, ma, ke, mr,
-                           mp))
+  if (!mhd_body<MODE, TMA, INT>(S, &T, smem, a, tin, so, beta, bnext, x0, y0, k0,
+                                min(S.nz, k0 + zchunk), mt, ma, ke, mr, mp))
     return;
-  if (MODE == F_LAST) diag_reduce32(S, ke, mr, mp);
+  if (MODE == F_LAST)
+    diag_reduce32(S, ke, mr, mp, tx_ + (long long)gx * (ty_ + (long long)gy * blockIdx.z),
+                  (long long)gx * gy * gridDim.z);
 }
 
 // ---------------------------------------------- FILTER_VARS, precision form
@@ -983,6 +1093,20 @@ __global__ void k_d2f(long long n, const double *in, float *out) {
     out[t] = (float)in[t];
 }
 
+__global__ void k_d2f_inv(long long n, const double *in, float *out) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x)
+    out[t] = (float)(1.0 / in[t]);
+}
+
+// 1/x in FP64, stored FP32 (the CPML 1/kappa profile)
+int to_float_inv(const double *in, float *out, long long n, cudaStream_t s) {
+  if (n <= 0) return SPARC_OK;
+  unsigned nb = (unsigned)std::min<long long>((n + 255) / 256, 148 * 32);
+  k_d2f_inv<<<nb, 256, 0, s>>>(n, in, out);
+  return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
+}
+
 int to_float(const double *in, float *out, long long n, cudaStream_t s) {
   if (n <= 0) return SPARC_OK;
   unsigned nb = (unsigned)std::min<long long>((n + 255) / 256, 148 * 32);
@@ -1080,10 +1204,24 @@ int launch_stage32(Handle *h, const Sim32 &S, int stage, const float *a,
     dim3 blk(TX, TY, 2);
     dim3 grd((h->nx + TX - 1) / TX, (h->ny + TY - 1) / TY, (h->nz + h->zchunk - 1) / h->zchunk);
     const int sm = (int)SMEM;
-#define ML32(M, U)                                                                    \
-  do {                                                                                \
-    cudaFuncSetAttribute(k_mhd32<M, U>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); \
-    k_mhd32<M, U><<<grd, blk, SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt, ma); \
+// interior tile rectangle (see mhd_interior), in tile units
+    const int gx = (h->nx + TX - 1) / TX, gy = (h->ny + TY - 1) / TY;
+    const FaceT<float> *F = h->f_faces;
+    const int xm = std::max(5, F[2].on ? F[2].np : 0), xM = std::max(5, F[3].on ? F[3].np : 0);
+    const int ym = std::max(5, F[4].on ? F[4].np : 0), yM = std::max(5, F[5].on ? F[5].np : 0);
+    const int ix0 = (xm + TX - 1) / TX, ix1 = (h->nx - xM - TX) / TX + 1;
+    const int iy0 = (ym + TY - 1) / TY, iy1 = (h->ny - yM - TY) / TY + 1;
+    const bool has_int = h->nx - xM - TX >= 0 && h->ny - yM - TY >= 0 && ix1 > ix0 && iy1 > iy0;
+    dim3 gint(has_int ? ix1 - ix0 : 1, has_int ? iy1 - iy0 : 1, grd.z);
+#define ML32(M, U)                                                                          \
+  do {                                                                                      \
+    cudaFuncSetAttribute(k_mhd32<M, U, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); \
+    cudaFuncSetAttribute(k_mhd32<M, U, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); \
+    if (has_int)                                                                            \
+      k_mhd32<M, U, true><<<gint, blk, SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, \
+                                                  mt, ma, ix0, iy0, gx, gy);                \
+    k_mhd32<M, U, false><<<grd, blk, SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk,   \
+                                                mt, ma, 0, 0, gx, gy);                      \
   } while (0)
     if (h->tma32) {
       if (mode == F_FIRST) ML32(F_FIRST, true);
@@ -1179,25 +1317,26 @@ __device__ __forceinline__ void rotate_roles(Slot32 &L) {
   L.role[2] = a;
 }
 
-// Item `idx` of slot L finished the last stage: store its partial; the last
+// Item w (of slot L) finished the last stage: store its partial; the last
 // item of the slot ends the step (driver.f90:161-183 diagnostics).
-__device__ void batch_finish_step(Slot32 &L, const Sim32 &S, int idx, double ke, double mr,
+__device__ void batch_finish_step(Slot32 &L, const Sim32 &S, int w, double ke, double mr,
                                   double mp, int tid) {
   __shared__ int am_last;
   block_reduce3(ke, mr, mp, tid);
   if (tid == 0) {
-    L.partials[3 * idx] = ke;
-    L.partials[3 * idx + 1] = mr;
-    L.partials[3 * idx + 2] = mp;
+    L.partials[3 * w] = ke;
+    L.partials[3 * w + 1] = mr;
+    L.partials[3 * w + 2] = mp;
     __threadfence();
     const unsigned t = atomicAdd(&L.counter, 1u);
-    am_last = (t == (unsigned)(L.n_items - 1));
+    am_last = (t == (unsigned)(L.n_items + L.n_items2 - 1));
   }
   __syncthreads();
   if (!am_last) return;
   __threadfence();
   ke = 0.0; mr = 1e300; mp = 1e300;
-  for (int b = tid; b < L.n_items; b += BT) {
+  for (int q = tid; q < L.n_items + L.n_items2; q += BT) {
+    const int b = q < L.n_items ? L.first_item + q : L.first_item2 + (q - L.n_items);
     ke += __ldcg(L.partials + 3 * b);
     mr = fmin(mr, __ldcg(L.partials + 3 * b + 1));
     mp = fmin(mp, __ldcg(L.partials + 3 * b + 2));
@@ -1224,7 +1363,10 @@ __global__ void k_batch_begin(Slot32 *slots, int n) {
     slots[q].active = slots[q].remaining > 0 ? 1 : 0;
 }
 
-template <int MODE>
+// PART 0: the interior MHD items (a prefix of the list, branch-free body);
+// PART 1: the rest (MHD tiles at edges/CPML, quiet tiles).  Two launches per
+// stage so that each kernel carries only its own bodies' registers.
+template <int MODE, int PART>
 __global__ void __launch_bounds__(BT, 1)
     k_batch_stage(Slot32 *__restrict__ slots, const int4 *__restrict__ items,
                   const int *__restrict__ counts, unsigned *wctr, int stage) {
@@ -1234,13 +1376,13 @@ __global__ void __launch_bounds__(BT, 1)
   float *smem = (float *)(((size_t)smem_raw32 + 127) & ~(size_t)127);
   Sim32 &sS = *reinterpret_cast<Sim32 *>(sS_raw);
   const int tid = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
-  const int total = counts[0];
+  const int lo = PART == 0 ? 0 : counts[3], hi = PART == 0 ? counts[3] : counts[0];
   int cur = -1;
   for (;;) {
-    if (tid == 0) s_w = (int)atomicAdd(wctr, 1u);
+    if (tid == 0) s_w = lo + (int)atomicAdd(wctr, 1u);
     __syncthreads();
     const int w = s_w;
-    if (w >= total) break;
+    if (w >= hi) break;
     const int4 it = items[w];
     Slot32 &L = slots[it.x];
     if (!L.active) {
@@ -1261,16 +1403,19 @@ __global__ void __launch_bounds__(BT, 1)
     const float bnext = (float)(stage < 5 ? L.betas[stage] : sS.deltat);
     const int x0 = it.y, y0 = it.z, k0 = it.w & 0xffff, k1 = it.w >> 16;
     double ke = 0.0, mr = 1e300, mp = 1e300;
-    if (sS.magnetic)
-      mhd_body<MODE, false>(sS, nullptr, smem, a, tin, so, beta, bnext, x0, y0, k0, k1, 0, 0,
-                            ke, mr, mp);
+    if (PART == 0)
+      mhd_body<MODE, false, true>(sS, nullptr, smem, a, tin, so, beta, bnext, x0, y0, k0, k1,
+                                  0, 0, ke, mr, mp);
+    else if (sS.magnetic)
+      mhd_body<MODE, false, false>(sS, nullptr, smem, a, tin, so, beta, bnext, x0, y0, k0, k1,
+                                   0, 0, ke, mr, mp);
     else if (sS.bg1d)
       quiet_body<32, 16, MODE, true>(sS, a, tin, so, beta, bnext, x0, y0, k0, k1, threadIdx.x,
                                      threadIdx.y + 8 * threadIdx.z, ke, mr, mp);
     else
       quiet_body<32, 16, MODE, false>(sS, a, tin, so, beta, bnext, x0, y0, k0, k1, threadIdx.x,
                                       threadIdx.y + 8 * threadIdx.z, ke, mr, mp);
-    if (MODE == F_LAST) batch_finish_step(L, sS, w - L.first_item, ke, mr, mp, tid);
+    if (MODE == F_LAST) batch_finish_step(L, sS, w, ke, mr, mp, tid);
     __syncthreads();
   }
 }
@@ -1391,21 +1536,34 @@ size_t batch_stage_smem() { return t32::SMEM; }
 
 int launch_batch_step(const BatchLaunch &B, cudaStream_t s, int *nkernels) {
   const int sm = (int)t32::SMEM;
-  cudaFuncSetAttribute(k_batch_stage<F_FIRST>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  cudaFuncSetAttribute(k_batch_stage<F_MID>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  cudaFuncSetAttribute(k_batch_stage<F_LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  if (cudaMemsetAsync(B.wctr, 0, 9 * sizeof(unsigned), s) != cudaSuccess) return SPARC_ERR_CUDA;
+  cudaFuncSetAttribute(k_batch_stage<F_FIRST, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_batch_stage<F_MID, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_batch_stage<F_LAST, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_batch_stage<F_FIRST, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_batch_stage<F_MID, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_batch_stage<F_LAST, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (cudaMemsetAsync(B.wctr, 0, 14 * sizeof(unsigned), s) != cudaSuccess) return SPARC_ERR_CUDA;
   k_batch_begin<<<(B.nslots + 255) / 256, 256, 0, s>>>(B.slots, B.nslots);
   k_batch_psr<<<B.grid, BT, B.psr_smem, s>>>(B.slots, B.pitems, B.counts, B.wctr + 0);
   const dim3 blk(t32::TX, t32::TY, 2);
-  k_batch_stage<F_FIRST><<<B.grid, blk, t32::SMEM, s>>>(B.slots, B.items, B.counts, B.wctr + 1, 1);
-  for (int st = 2; st <= 4; ++st)
-    k_batch_stage<F_MID><<<B.grid, blk, t32::SMEM, s>>>(B.slots, B.items, B.counts, B.wctr + st, st);
-  k_batch_stage<F_LAST><<<B.grid, blk, t32::SMEM, s>>>(B.slots, B.items, B.counts, B.wctr + 5, 5);
+  // per stage: interior part (counter 1..5), then general part (9..13)
+  for (int st = 1; st <= 5; ++st) {
+    unsigned *c0 = B.wctr + st, *c1 = B.wctr + 8 + st;
+    if (st == 1) {
+      k_batch_stage<F_FIRST, 0><<<B.grid, blk, t32::SMEM, s>>>(B.slots, B.items, B.counts, c0, st);
+      k_batch_stage<F_FIRST, 1><<<B.grid, blk, t32::SMEM, s>>>(B.slots, B.items, B.counts, c1, st);
+    } else if (st < 5) {
+      k_batch_stage<F_MID, 0><<<B.grid, blk, t32::SMEM, s>>>(B.slots, B.items, B.counts, c0, st);
+      k_batch_stage<F_MID, 1><<<B.grid, blk, t32::SMEM, s>>>(B.slots, B.items, B.counts, c1, st);
+    } else {
+      k_batch_stage<F_LAST, 0><<<B.grid, blk, t32::SMEM, s>>>(B.slots, B.items, B.counts, c0, st);
+      k_batch_stage<F_LAST, 1><<<B.grid, blk, t32::SMEM, s>>>(B.slots, B.items, B.counts, c1, st);
+    }
+  }
   k_batch_filter<1><<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 6);
   k_batch_filter<0><<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 7);
   k_batch_filter<2><<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 8);
-  *nkernels = 10;
+  *nkernels = 15;
   return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
 }
 
@@ -1480,8 +1638,10 @@ int setup32(Handle *h) {
     if (!D.on) continue;
     const long long n = D.uniform ? D.np : D.cnt;
     float *pa = f_up(h, D.pa, n, s), *pb = f_up(h, D.pb, n, s), *pk = f_up(h, D.pk, n, s);
-    if (!pa || !pb || !pk) return SPARC_ERR_NOMEM;
-    F.pa = pa; F.pb = pb; F.pk = pk;
+    float *pki = f_up(h, nullptr, n, s);
+    if (!pa || !pb || !pk || !pki) return SPARC_ERR_NOMEM;
+    if (to_float_inv(D.pk, pki, n, s)) return SPARC_ERR_CUDA;
+    F.pa = pa; F.pb = pb; F.pk = pk; F.pki = pki;
     F.uniform = D.uniform;
   }
   if (cudaStreamSynchronize(s) != cudaSuccess) return SPARC_ERR_CUDA;

@@ -80,6 +80,8 @@ static std::string validate(const sparc_params &P) {
     return "precision must be SPARC_FP64 or SPARC_FP32";
   if (P.precision == SPARC_FP32 && (long long)P.nx * P.ny * P.nz * 8 >= (1LL << 31))
     return "the precision form takes grids below 2^28 points";
+  if (P.magnetic == 2 && (long long)P.nx * P.ny * P.nz * 8 >= (1LL << 31))
+    return "MHD grids are limited to 2^28 points (32-bit indexing of 8 fields)";
   std::vector<int> s, l;
   const int dims[3] = {P.nx, P.ny, P.nz}, B[3] = {P.block_x, P.block_y, P.block_z};
   for (int a = 0; a < 3; ++a) {
@@ -380,7 +382,7 @@ int sparc_create(const sparc_params *p, int device, sparc_handle **out) {
     cols[h->nx + h->ny + k] = b;
   }
   if (const char *kv = std::getenv("SPARC_MHD_KERNEL"))  // A/B timing only
-    h->mhd_kernel = std::atoi(kv) == 4 ? 4 : 3;
+    h->mhd_kernel = std::atoi(kv) == 4 ? 4 : (std::atoi(kv) == 3 ? 3 : 5);
   if (const char *kv = std::getenv("SPARC_TMA_TY")) {  // A/B timing only
     int t = std::atoi(kv);
     if (t == 6 || t == 8) h->tma_ty = t;

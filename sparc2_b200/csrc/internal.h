@@ -205,10 +205,11 @@ struct Handle {
   unsigned int *d_counter = nullptr;
   int max_stage_blocks = 0;
 
-  // stage launch geometry; mhd_kernel 3: two-role cp.async-pipelined MHD
-  // kernel (default), 4: its variant with TMA own-point loads (even nx)
+  // stage launch geometry; mhd_kernel 5: the shared-body interior/general
+  // kernel pair (default); 3: the earlier two-role kernel, 4: its TMA
+  // variant (even nx) -- kept for A/B timing
   int tx = 32, ty = 8, zchunk = 32;
-  int mhd_kernel = 3;
+  int mhd_kernel = 5;
 
   // precision form (SPARC_FP32): FP32 state in fbuf (roles ra/rf1/rf2 as
   // for buf), the compensated-sum carry of the state, depth scales

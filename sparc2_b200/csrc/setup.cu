@@ -683,6 +683,17 @@ int setup_background(Handle *h, const double *rho0_in, const double *pre0_in,
     }
     F.uniform = 1;
   }
+  // 1/kappa of every face (the stage kernels multiply by it)
+  for (int f = 0; f < 6; ++f) {
+    FaceDev &F = h->faces[f];
+    if (!F.on) continue;
+    const long long n = F.uniform ? F.np : F.cnt;
+    double *ki = up(h, nullptr, n);
+    if (!ki) return SPARC_ERR_NOMEM;
+    const double *pk = F.pk;
+    each(n, s, [=] __device__(long long t) { ki[t] = 1.0 / pk[t]; });
+    F.pki = ki;
+  }
   CK(cudaStreamSynchronize(s));
   return SPARC_OK;
 }

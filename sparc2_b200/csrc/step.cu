@@ -15,7 +15,7 @@
 
 #include <cmath>
 
-#include "internal.h"
+#include "mhd_body.cuh"
 
 namespace sparc {
 
@@ -23,6 +23,11 @@ __constant__ double c_dp[6][11];   // derivative rows, initialize.f90:1959-2031
 __constant__ double c_df[2][11];   // filter stencils: [0] 11-point, [1] 7-point
 
 enum { FIRST = 0, MID = 1, LAST = 2 };
+
+template <>
+__device__ __forceinline__ double dcoef<double>(int r, int m) {
+  return c_dp[r][m];
+}
 
 int step_constants() {
   if (cudaMemcpyToSymbol(c_dp, kDerivRows, sizeof(double) * 66) != cudaSuccess)
@@ -1267,9 +1272,73 @@ int encode_tensor_maps(Handle *h) {
   return SPARC_OK;
 }
 
+// ------------------------- MP_MHD_3D, shared-body stage kernels (default)
+// One RK stage as two launches over one logical grid of (x tile, y tile, z
+// chunk) blocks: INT = true over the interior tile rectangle with the
+// branch-free body of mhd_body.cuh, INT = false over the whole grid,
+// returning at once on interior tiles (edge and CPML tiles).
+template <int MODE, bool INT>
+__global__ void __launch_bounds__(mg::NT, 1)
+    k_mhd64(const SimDev S, const double *__restrict__ a, const double *__restrict__ tin,
+            double *__restrict__ so, double beta, double bnext, int zchunk, int ix0, int iy0,
+            int gx, int gy) {
+  extern __shared__ __align__(1024) double smem_raw64[];
+  double *smem = (double *)(((size_t)smem_raw64 + 127) & ~(size_t)127);
+  const int tx_ = INT ? blockIdx.x + ix0 : blockIdx.x;
+  const int ty_ = INT ? blockIdx.y + iy0 : blockIdx.y;
+  const int x0 = tx_ * mg::TX, y0 = ty_ * mg::TY;
+  if (!INT && mhd_interior(S, x0, y0)) return;
+  double ke = 0.0, mr = 1e300, mp = 1e300;
+  const int k0 = blockIdx.z * zchunk;
+  mhd_body<double, MODE, false, INT>(S, nullptr, smem, a, tin, so, beta, bnext, x0, y0, k0,
+                                     min(S.nz, k0 + zchunk), 0, 0, ke, mr, mp);
+  if (MODE == F_LAST)
+    diag_reduce_t(S, ke, mr, mp, tx_ + (long long)gx * (ty_ + (long long)gy * blockIdx.z),
+                  (long long)gx * gy * gridDim.z);
+}
+
+static int launch_mhd64(Handle *h, const SimDev &S, int stage, const double *a,
+                        const double *tin, double *so, cudaStream_t s) {
+  const double beta = h->betas[stage - 1];
+  const double bnext = stage < 5 ? h->betas[stage] : h->deltat;
+  const int mode = stage == 1 ? FIRST : (stage == 5 ? LAST : MID);
+  dim3 blk(mg::TX, mg::TY, 2);
+  dim3 grd((h->nx + mg::TX - 1) / mg::TX, (h->ny + mg::TY - 1) / mg::TY,
+           (h->nz + h->zchunk - 1) / h->zchunk);
+  const int np[4] = {h->faces[2].on ? h->faces[2].np : 0, h->faces[3].on ? h->faces[3].np : 0,
+                     h->faces[4].on ? h->faces[4].np : 0, h->faces[5].on ? h->faces[5].np : 0};
+  int ix0, ix1, iy0, iy1;
+  mhd_interior_rect(h->nx, h->ny, np, ix0, ix1, iy0, iy1);
+  const bool has_int = ix1 > ix0 && iy1 > iy0;
+  dim3 gint(has_int ? ix1 - ix0 : 1, has_int ? iy1 - iy0 : 1, grd.z);
+  const size_t sm = MhdBuf<double>::SMEM;
+#define ML64(M)                                                                              \
+  do {                                                                                       \
+    cudaFuncSetAttribute(k_mhd64<M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
+    cudaFuncSetAttribute(k_mhd64<M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
+    if (has_int)                                                                             \
+      k_mhd64<M, true><<<gint, blk, sm, s>>>(S, a, tin, so, beta, bnext, h->zchunk, ix0, iy0, \
+                                             grd.x, grd.y);                                  \
+    k_mhd64<M, false><<<grd, blk, sm, s>>>(S, a, tin, so, beta, bnext, h->zchunk, 0, 0, grd.x, \
+                                           grd.y);                                           \
+  } while (0)
+  if (mode == FIRST) ML64(F_FIRST);
+  else if (mode == MID) ML64(F_MID);
+  else ML64(F_LAST);
+#undef ML64
+  return SPARC_OK;
+}
+
 int launch_stage(Handle *h, const SimDev &S, int stage, const double *a,
                  const double *tin, double *so, cudaStream_t s) {
   int r = SPARC_ERR_INVALID;
+  if (h->magnetic && h->mhd_kernel == 5) {
+    if (h->tx != 32 || h->ty != 8) return SPARC_ERR_INVALID;
+    r = launch_mhd64(h, S, stage, a, tin, so, s);
+    ++h->launches;
+    if (r == SPARC_OK && cudaGetLastError() != cudaSuccess) r = SPARC_ERR_CUDA;
+    return r;
+  }
   if (h->magnetic && h->mhd_kernel == 4 && h->tma && h->tx == 32 &&
       (long long)h->V * h->N < (1LL << 31)) {
     r = launch_mhd_tma(h, S, stage, a, tin, so, s);

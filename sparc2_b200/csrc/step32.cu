@@ -23,14 +23,13 @@
 #include <cstring>
 #include <vector>
 
-#include "internal.h"
+#include "mhd_body.cuh"
 
 namespace sparc {
 
 __constant__ float f_dp[6][11];
 __constant__ float f_df[2][11];
 
-enum { F_FIRST = 0, F_MID = 1, F_LAST = 2 };
 
 // Derivative rows and both filter stencils ([0] 11-point, [1] 7-point) in
 // FP32; a filter pass picks its table by half-width.
@@ -43,6 +42,11 @@ int step32_constants() {
   for (int m = 0; m < 11; ++m) f[0][m] = (float)kFilter11[m];
   for (int m = 0; m < 7; ++m) f[1][m] = (float)kFilter7[m];
   return cudaMemcpyToSymbol(f_df, f, sizeof(f)) == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
+}
+
+template <>
+__device__ __forceinline__ float dcoef<float>(int r, int m) {
+  return f_dp[r][m];
 }
 
 using Sim32 = SimT<float>;
@@ -72,39 +76,6 @@ __device__ __forceinline__ void cpml32(const Face32 &F, long long f, int layer, 
   d = d * pki + psi;
   if (MODE == F_LAST) F.vars[o] = v + dt * rhs;
   else F.scr[o] = rhs;
-}
-
-// Three CPML fields of one face at one point: every load is issued before
-// any store (one memory round trip instead of three), the profile once.
-template <int MODE>
-__device__ __forceinline__ void cpml3_32(const Face32 &F, long long f, int layer, int s0, int s1,
-                                         int s2, float beta, float dt, float &d0, float &d1,
-                                         float &d2) {
-  const long long pf = F.uniform ? (long long)layer : f;
-  const float pa = __ldg(F.pa + pf), pb = __ldg(F.pb + pf), pki = __ldg(F.pki + pf);
-  const long long o0 = (long long)s0 * F.cnt + f, o1 = (long long)s1 * F.cnt + f,
-                  o2 = (long long)s2 * F.cnt + f;
-  const float v0 = F.vars[o0], v1 = F.vars[o1], v2 = F.vars[o2];
-  float p0 = v0, p1 = v1, p2 = v2;
-  if (MODE != F_FIRST) {
-    const float c0 = F.scr[o0], c1 = F.scr[o1], c2 = F.scr[o2];
-    p0 = v0 + beta * c0;
-    p1 = v1 + beta * c1;
-    p2 = v2 + beta * c2;
-  }
-  const float r0 = pa * d0 + pb * p0, r1 = pa * d1 + pb * p1, r2 = pa * d2 + pb * p2;
-  d0 = d0 * pki + p0;
-  d1 = d1 * pki + p1;
-  d2 = d2 * pki + p2;
-  if (MODE == F_LAST) {
-    F.vars[o0] = v0 + dt * r0;
-    F.vars[o1] = v1 + dt * r1;
-    F.vars[o2] = v2 + dt * r2;
-  } else {
-    F.scr[o0] = r0;
-    F.scr[o1] = r1;
-    F.scr[o2] = r2;
-  }
 }
 
 __device__ __forceinline__ float pulse_time32(const Sim32 &S, long long it) {
@@ -162,33 +133,6 @@ __device__ __forceinline__ void shift32(float (&w)[11], float v) {
 #pragma unroll
   for (int m = 0; m < 10; ++m) w[m] = w[m + 1];
   w[10] = v;
-}
-
-// Centred 11-point sum at p[5*st]; the centred row is antisymmetric
-// (c[5+m] = -c[5-m], c[5] = 0), so it is sum_m c[5+m] (f[+m] - f[-m]),
-// evaluated as two short independent chains.
-__device__ __forceinline__ float csum32(const float *p, int st) {
-  // (the general tiles use csumf32: the plain 11-term sum needs fewer live values)
-  const float d1 = p[6 * st] - p[4 * st], d2 = p[7 * st] - p[3 * st],
-              d3 = p[8 * st] - p[2 * st], d4 = p[9 * st] - p[st], d5 = p[10 * st] - p[0];
-  const float a = fmaf(f_dp[5][8], d3, fmaf(f_dp[5][10], d5, f_dp[5][6] * d1));
-  const float b = fmaf(f_dp[5][9], d4, f_dp[5][7] * d2);
-  return a + b;
-}
-
-__device__ __forceinline__ float csumf32(const float *p, int st) {
-  float s = 0.f;
-#pragma unroll
-  for (int m = 0; m < 11; ++m) s += p[m * st] * f_dp[5][m];
-  return s;
-}
-
-// Compensated final update (step.f90:58): a + dt*F with a Kahan carry c.
-__device__ __forceinline__ float kahan(float a, float inc, float &c) {
-  const float y = inc - c;
-  const float t = a + y;
-  c = (t - a) - y;
-  return t;
 }
 
 // Per-CTA partial of the KE norm and minima (FP64) and the last-CTA
@@ -450,449 +394,13 @@ __global__ void __launch_bounds__(TX *TY)
 // The two-role TMA kernel of step.cu in FP32 with depth scaling (field
 // scales: 0 rho, 1-3 v, 4 p, 5-7 b).  Own-point arrays of a layer arrive by
 // TMA (32x8 FP32 boxes), halos by cp.async; one CTA of 512 threads per SM.
-struct TmaSet32 {
-  CUtensorMap m[18];
-};
 
 namespace t32 {
-constexpr int TX = 32, TY = 8, NC = TX * TY, NT = 2 * NC;
-constexpr int HX = TX + 10, HY = TY + 10, HS = HX * HY;
-constexpr int NH = 10, NO = 24;
-constexpr int BUF = ((NO * NC + NH * HS) + 31) / 32 * 32;  // 128-B multiple
-constexpr int XCH = 4 * NC;  // dvzdz, dzby (float) and |v_new|^2 (double)
-constexpr size_t SMEM = (2 * (size_t)BUF + XCH) * sizeof(float) + 128;
-constexpr long long WAIT_LIMIT = 1LL << 26;
-constexpr int O_RHO = 0, O_A = 1, O_BG = 9, O_P0 = 23;
-enum { B_RED, B_SPONGE, B_RHO0, B_GRX, B_GRY, B_GRZ, B_C2R, B_GPX, B_GPY,
-       B_GPZ, B_RHOINV, B_CBX, B_CBY, B_CBZ };
+using namespace mg;
+constexpr int BUF = MhdBuf<float>::BUF;
+constexpr int XCH = MhdBuf<float>::XCH;
+constexpr size_t SMEM = MhdBuf<float>::SMEM;
 }  // namespace t32
-
-__device__ __forceinline__ unsigned sm_addr32(const void *p) {
-  return (unsigned)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void cp4(float *dst, const float *src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sm_addr32(dst)), "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cp_commit32() {
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-__device__ __forceinline__ void cp_wait1_32() {
-  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-}
-__device__ __forceinline__ void mbar_init32(unsigned long long *bar) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sm_addr32(bar)) : "memory");
-}
-__device__ __forceinline__ void mbar_tx32(unsigned long long *bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sm_addr32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void tma3d32(float *dst, const CUtensorMap *map, int x, int y,
-                                        int z, unsigned long long *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(sm_addr32(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(z), "r"(sm_addr32(bar))
-      : "memory");
-}
-__device__ __forceinline__ bool mbar_wait32(unsigned long long *bar, unsigned parity,
-                                            int *err) {
-  for (long long n = 0; n < t32::WAIT_LIMIT; ++n) {
-    unsigned ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(sm_addr32(bar)), "r"(parity)
-        : "memory");
-    if (ok) return true;
-  }
-  atomicExch(err, 1);
-  return false;
-}
-
-// The body covers the tile (x0, y0) over layers [k0, k1) with a block of
-// 32 x 8 x 2 threads (threadIdx.z is the role); smem is the 128-byte aligned
-// dynamic buffer.  TMA = false: the own-point arrays are fetched by
-// cp.async too (any nx).  INT: the tile's stencil footprint touches no
-// non-periodic edge, no x/y CPML slab and needs no periodic wrap, so its
-// x/y derivatives are the centred stencil with no branch.  Returns false
-// when a bounded wait gave up.
-//
-// Per layer: every thread waits for its own halo copies, turns the B0 halo
-// values it copied into the fluxes v x B0 in place, then one barrier makes
-// the layer visible; the copies of the next layer are issued after that
-// barrier (the buffer they overwrite was last read before it).  A second
-// barrier exchanges d(vz)/dz and d(by)/dz between the roles.
-template <int MODE, bool TMA, bool INT>
-__device__ __forceinline__ bool mhd_body(const Sim32 &S, const TmaSet32 *T, float *smem,
-                                         const float *__restrict__ a,
-                                         const float *__restrict__ tin,
-                                         float *__restrict__ so, float beta, float bnext,
-                                         int x0, int y0, int k0, int k1, int mt, int ma,
-                                         double &ke, double &mr, double &mp) {
-  using namespace t32;
-  __shared__ unsigned long long bar[2];
-  const int tx = threadIdx.x, ty = threadIdx.y, role = threadIdx.z;
-  const int tid = (role * TY + ty) * TX + tx, cid = ty * TX + tx;
-  const int nx = S.nx, ny = S.ny, nz = S.nz;
-  const int N = (int)S.N, NXY = nx * ny;
-  const int i = x0 + tx, j = y0 + ty;
-  const bool act = INT || (i < nx && j < ny);
-  const bool per = S.periodic;
-  const int col = j * nx + i;
-  const int xo = INT ? x0 - 5 : origin32(x0, TX, nx, per);
-  const int yo = INT ? y0 - 5 : origin32(y0, TY, ny, per);
-  const int ry = y0 - yo + ty, rx = x0 - xo + tx;
-  const int own = ry * HX + rx;
-  const float *isc = S.isc, *sc = S.sc;
-  // General tiles: each lane (x) and row (y) gets its own 11 coefficients and
-  // window start in the tile, so every x/y derivative is one branch-free
-  // sum: the centred row; one-sided row q at the low edge (q = i); at the
-  // high edge -row q reversed over f(n-11..n-1) (derivatives.f90:72, 98).
-  __shared__ float cxs[INT ? 1 : TX * 11], cys[INT ? 1 : TY * 11];
-  __shared__ int cxb[INT ? 1 : TX], cyb[INT ? 1 : TY];
-  if (!INT && tid < TX + TY) {
-    const bool isx = tid < TX;
-    const int q0 = isx ? tid : tid - TX;                 // lane or row
-    const int g = isx ? x0 + q0 : y0 + q0, n = isx ? nx : ny, o = isx ? xo : yo;
-    float *c = isx ? cxs + q0 * 11 : cys + q0 * 11;
-    int base;
-    if (per || (g >= 5 && g < n - 5) || g >= n) {
-      for (int m = 0; m < 11; ++m) c[m] = f_dp[5][m];
-      base = g - 5 - o;
-    } else if (g < 5) {
-      for (int m = 0; m < 11; ++m) c[m] = f_dp[g][m];
-      base = -o;
-    } else {
-      const int q = n - 1 - g;
-      for (int m = 0; m < 11; ++m) c[m] = -f_dp[q][10 - m];
-      base = n - 11 - o;
-    }
-    if (isx) cxb[q0] = base;
-    else cyb[q0] = base;
-  }
-  if (TMA && tid == 0) {
-    mbar_init32(&bar[0]);
-    mbar_init32(&bar[1]);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  auto O = [&](int b, int slot) -> float { return smem[b * BUF + slot * NC + cid]; };
-  auto Hp = [&](int b, int slot) -> float * { return smem + b * BUF + NO * NC + slot * HS; };
-  float *X = smem + 2 * BUF;
-  int hs0 = -1, hs1 = -1, ho0 = 0, ho1 = 0;
-  {
-    const int cx0 = x0 - xo, cy0 = y0 - yo;
-    auto pos = [&](int t, int &hs, int &ho) {
-      if (t >= HS) return;
-      const int ly = t / HX, lx = t - ly * HX;
-      const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
-      if (!inx && !iny) return;
-      int gx = xo + lx, gy = yo + ly;
-      if (per) {
-        gx = wrap32(gx, nx);
-        gy = wrap32(gy, ny);
-      } else if (gx < 0 || gx >= nx || gy < 0 || gy >= ny) {
-        return;
-      }
-      hs = t;
-      ho = gy * nx + gx;
-    };
-    pos(tid, hs0, ho0);
-    pos(tid + NT, hs1, ho1);
-  }
-  const unsigned own_bytes =
-      (MODE == F_FIRST ? 15u : (MODE == F_MID ? 23u : 24u)) * NC * (unsigned)sizeof(float);
-  auto issue = [&](int k, int b) {
-    const int kb = k * NXY;
-    if (hs0 >= 0) {
-      float *h = Hp(b, 0) + hs0;
-      const int id = kb + ho0;
-#pragma unroll
-      for (int sl = 0; sl < 7; ++sl) cp4(h + sl * HS, tin + (sl + 1) * N + id);
-      cp4(h + 7 * HS, S.box + id);
-      cp4(h + 8 * HS, S.boy + id);
-      cp4(h + 9 * HS, S.boz + id);
-    }
-    if (hs1 >= 0) {
-      float *h = Hp(b, 0) + hs1;
-      const int id = kb + ho1;
-#pragma unroll
-      for (int sl = 0; sl < 7; ++sl) cp4(h + sl * HS, tin + (sl + 1) * N + id);
-      cp4(h + 7 * HS, S.box + id);
-      cp4(h + 8 * HS, S.boy + id);
-      cp4(h + 9 * HS, S.boz + id);
-    }
-    if (!TMA && act) {
-      float *ob = smem + b * BUF + cid;
-      const int id = kb + col;
-      if (role == 0) {
-        cp4(ob + O_RHO * NC, tin + id);
-        if (MODE != F_FIRST)
-#pragma unroll
-          for (int l = 0; l < 8; ++l) cp4(ob + (O_A + l) * NC, a + l * N + id);
-      } else {
-        const float *bg[14] = {S.red, S.sponge, S.rho0, S.grx, S.gry, S.grz,
-                               S.c2rho0, S.gpx, S.gpy, S.gpz, S.rhoinv, S.cbx, S.cby, S.cbz};
-#pragma unroll
-        for (int n = 0; n < 14; ++n) cp4(ob + (O_BG + n) * NC, bg[n] + id);
-        if (MODE == F_LAST) cp4(ob + O_P0 * NC, S.p0 + id);
-      }
-    }
-    cp_commit32();
-    if (TMA && tid == 0) {
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_tx32(&bar[b], own_bytes);
-      float *ob = smem + b * BUF;
-      tma3d32(ob + O_RHO * NC, &T->m[mt], x0, y0, k, &bar[b]);
-      if (MODE != F_FIRST)
-        for (int l = 0; l < 8; ++l)
-          tma3d32(ob + (O_A + l) * NC, &T->m[ma], x0, y0, l * nz + k, &bar[b]);
-      for (int n = 0; n < 14; ++n)
-        tma3d32(ob + (O_BG + n) * NC, &T->m[3 + n], x0, y0, k, &bar[b]);
-      if (MODE == F_LAST) tma3d32(ob + O_P0 * NC, &T->m[17], x0, y0, k, &bar[b]);
-    }
-  };
-  // fluxes v x B0 (stored velocity units) in place of the B0 halo values,
-  // at the halo positions this thread copied
-  auto flux = [&](int b, int t) {
-    float *H = Hp(b, 0) + t;
-    const float vx_ = H[0], vy_ = H[HS], vz_ = H[2 * HS];
-    const float bx0 = H[7 * HS], by0 = H[8 * HS], bz0 = H[9 * HS];
-    H[7 * HS] = -vz_ * by0 + vy_ * bz0;
-    H[8 * HS] = -vx_ * bz0 + vz_ * bx0;
-    H[9 * HS] = -vy_ * bx0 + vx_ * by0;
-  };
-  float w0[11], w1[11], w2[11];  // physical values
-  auto head = [&](int kk, float &v0, float &v1, float &v2) {
-    const int id = kk * NXY + col;
-    if (role == 0) {
-      v0 = __ldg(tin + 3 * N + id) * isc[3 * nz + kk];
-      v1 = __ldg(tin + 4 * N + id) * isc[4 * nz + kk];
-      v2 = __ldg(tin + 5 * N + id) * isc[5 * nz + kk];
-    } else {
-      const float iv = isc[nz + kk];
-      const float vx_ = __ldg(tin + N + id) * iv, vy_ = __ldg(tin + 2 * N + id) * iv,
-                  vz_ = __ldg(tin + 3 * N + id) * iv;
-      const float ox = __ldg(S.box + id), oy = __ldg(S.boy + id), oz = __ldg(S.boz + id);
-      v0 = -vz_ * oy + vy_ * oz;
-      v1 = -vx_ * oz + vz_ * ox;
-      v2 = __ldg(tin + 6 * N + id) * isc[6 * nz + kk];
-    }
-  };
-  issue(k0, 0);
-  {
-    const int b0 = min(k0 - 5, nz - 11);
-#pragma unroll
-    for (int m = 0; m < 11; ++m) {
-      const int kk = b0 + m;
-      if (act && kk >= 0) head(kk, w0[m], w1[m], w2[m]);
-      else w0[m] = w1[m] = w2[m] = 0.f;
-    }
-  }
-  unsigned phase = 0;
-  bool ok = true;
-  const float dt = (float)S.deltat;
-  const float sx = (float)S.stretchx, sy = (float)S.stretchy;
-  const float *gcol = S.gblk + (act ? S.colx[i] + S.bxdim * S.coly[j] : 0) * nz;
-
-  for (int k = k0; k < k1; ++k) {
-    const int b = (k - k0) & 1;
-    const int id = k * NXY + col;
-    float h0 = 0, h1 = 0, h2 = 0;
-    const bool sh = k > k0 && k <= nz - 6;
-    if (sh && act) head(k + 5, h0, h1, h2);
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-    if (hs0 >= 0) flux(b, hs0);
-    if (hs1 >= 0) flux(b, hs1);
-    bool mine = true;
-    if (TMA && tid == 0) mine = mbar_wait32(&bar[b], (phase >> b) & 1u, S.err);
-    phase ^= 1u << b;
-    if (!__syncthreads_and(mine)) { ok = false; break; }
-    if (k + 1 < k1) issue(k + 1, b ^ 1);
-    if (sh) { shift32(w0, h0); shift32(w1, h1); shift32(w2, h2); }
-    const float szk = __ldg(S.stretch + k);
-    auto DX = [&](int slot) {
-      const float *row = Hp(b, slot) + ry * HX;
-      if (INT) return sx * csum32(row + tx, 1);
-      const float *r = row + cxb[tx], *c = cxs + tx * 11;
-      float sum = 0.f;
-#pragma unroll
-      for (int m = 0; m < 11; ++m) sum += r[m] * c[m];
-      return sx * sum;
-    };
-    auto DY = [&](int slot) {
-      const float *colp = Hp(b, slot) + rx;
-      if (INT) return sy * csum32(colp + ty * HX, HX);
-      const float *r = colp + cyb[ty] * HX, *c = cys + ty * 11;
-      float sum = 0.f;
-#pragma unroll
-      for (int m = 0; m < 11; ++m) sum += r[m * HX] * c[m];
-      return sy * sum;
-    };
-    const bool zpml = S.zb.on && (k < S.zb.np || k >= nz - S.zt.np);
-    const bool xpml = !INT && S.xb.on && act && (i < S.xb.np || i >= nx - S.xt.np);
-    const bool ypml = !INT && S.yb.on && act && (j < S.yb.np || j >= ny - S.yt.np);
-    auto pz = [&](int s0, int s1, int s2, float &da, float &db, float &dc) {
-      const bool bot = k < S.zb.np;
-      const Face32 &F = bot ? S.zb : S.zt;
-      const int kl = bot ? k : k - (nz - S.zt.np);
-      cpml3_32<MODE>(F, (long long)kl * NXY + col, kl, s0, s1, s2, beta, dt, da, db, dc);
-    };
-    auto px = [&](int s0, int s1, int s2, float &da, float &db, float &dc) {
-      const bool bot = i < S.xb.np;
-      const Face32 &F = bot ? S.xb : S.xt;
-      const int il = bot ? i : i - (nx - S.xt.np);
-      cpml3_32<MODE>(F, il + (long long)F.np * (j + (long long)ny * k), il, s0, s1, s2, beta,
-                     dt, da, db, dc);
-    };
-    auto py = [&](int s0, int s1, int s2, float &da, float &db, float &dc) {
-      const bool bot = j < S.yb.np;
-      const Face32 &F = bot ? S.yb : S.yt;
-      const int jl = bot ? j : j - (ny - S.yt.np);
-      cpml3_32<MODE>(F, i + (long long)nx * (jl + (long long)F.np * k), jl, s0, s1, s2, beta,
-                     dt, da, db, dc);
-    };
-    auto Hv = [&](int slot) { return Hp(b, slot)[own]; };
-    const float iv = isc[nz + k];  // velocity (and flux) scale of this layer
-    float d0 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0, d6 = 0, d7 = 0, d8 = 0;
-    if (act) {
-      const float ip = isc[4 * nz + k], ib = isc[5 * nz + k];
-      if (role == 0) {
-        d0 = ip * DX(3); d5 = ib * DX(6); d7 = ib * DX(5);
-        d1 = ip * DY(3); d4 = ib * DY(6); d8 = ib * DY(4);
-        d3 = dz32(w0, k, nz, szk); d2 = dz32(w1, k, nz, szk); d6 = dz32(w2, k, nz, szk);
-        if (zpml) pz(1, 0, 2, d2, d3, d6);
-        if (xpml) px(1, 3, 2, d0, d5, d7);
-        if (ypml) py(1, 3, 2, d1, d4, d8);
-        X[cid] = d3;
-      } else {
-        d0 = iv * DX(0); d2 = iv * DX(9); d3 = iv * DX(8);
-        d1 = iv * DY(1); d4 = iv * DY(9); d5 = iv * DY(7);
-        d6 = dz32(w0, k, nz, szk); d7 = dz32(w1, k, nz, szk); d8 = dz32(w2, k, nz, szk);
-        if (zpml) pz(4, 5, 3, d7, d6, d8);
-        if (xpml) px(0, 4, 5, d0, d2, d3);
-        if (ypml) py(0, 4, 5, d1, d4, d5);
-        X[NC + cid] = d8;
-      }
-    }
-    __syncthreads();
-    double an_rho = 0.0;
-    if (act) {
-      const bool zero = k == 0 || k == nz - 1 ||
-                        (!INT && !per && (i == 0 || i == nx - 1 || j == 0 || j == ny - 1));
-      const float fac = MODE == F_LAST ? dt : bnext;
-      const float rho = O(b, O_RHO) * isc[k], vx = Hv(0) * iv, vy = Hv(1) * iv,
-                  vz = Hv(2) * iv;
-      const float red = O(b, O_BG + B_RED), sg = O(b, O_BG + B_SPONGE);
-      if (role == 0) {
-        // B0 at the own point (its halo slots now hold the fluxes)
-        const float ox = __ldg(S.box + id), oy = __ldg(S.boy + id), oz = __ldg(S.boz + id);
-        const float ib = isc[5 * nz + k];
-        const float dzby = X[NC + cid];
-        const float cbx = d4 - dzby, cby = -d5 + d6, cbz = d7 - d8;
-        const float c1 = cby * oz - cbz * oy, c2 = ox * cbz - cbx * oz, c3 = cbx * oy - cby * ox;
-        const float ri = O(b, O_BG + B_RHOINV);
-        float vxr = -ri * (d0 - (c1 * red)) - sg * vx;
-        float vyr = -ri * (d1 - (c2 * red)) - sg * vy;
-        float vzr = -ri * (d2 - (c3 * red)) - sg * vz;
-        const float bx = Hv(4) * ib, by = Hv(5) * ib, bz = Hv(6) * ib;
-        const float qx = O(b, O_BG + B_CBX), qy = O(b, O_BG + B_CBY), qz = O(b, O_BG + B_CBZ);
-        const float e1 = qy * bz - qz * by, e2 = bx * qz - qx * bz, e3 = qx * by - qy * bx;
-        vxr = vxr + ri * e1 * red;
-        vyr = vyr + ri * e2 * red;
-        vzr = vzr + ri * e3 * red;
-        vzr = vzr - ri * rho * __ldg(gcol + k);
-        if (S.frc.kind != SPARC_SRC_NONE) {
-          const long long it = *S.iter;
-          const float frc = forcing32(S, pulse_time32(S, it), i, j, k);
-          if (S.frc.dir == 1) vxr = vxr + frc;
-          else if (S.frc.dir == 2) vyr = vyr + frc;
-          else vzr = vzr + frc;
-        }
-        const float sv = sc[nz + k];
-        const float R[3] = {vxr, vyr, vzr};
-        double vsq = 0.0;
-#pragma unroll
-        for (int l = 1; l < 4; ++l) {
-          const float av = MODE == F_FIRST ? Hv(l - 1) : O(b, O_A + l);
-          float an;
-          if (MODE == F_LAST) {
-            float c = S.carry[l * N + id];
-            an = zero ? av : kahan(av, fac * (sv * R[l - 1]), c);
-            S.carry[l * N + id] = c;
-            const double ph = ((double)an - (double)c) * (double)iv;
-            vsq += ph * ph;
-          } else {
-            an = zero ? av : av + fac * (sv * R[l - 1]);
-          }
-          so[l * N + id] = an;
-        }
-        if (MODE == F_LAST) ((double *)(X + 2 * NC))[cid] = vsq;
-      } else {
-        const float p = Hv(3) * isc[4 * nz + k];
-        const float dvzdz = X[cid];
-        const float div = d0 + d1 + dvzdz;
-        const float r0 = O(b, O_BG + B_RHO0);
-        const float Rr = -O(b, O_BG + B_GRX) * vx - O(b, O_BG + B_GRY) * vy -
-                         O(b, O_BG + B_GRZ) * vz - r0 * div - sg * rho;
-        const float Rp = -O(b, O_BG + B_C2R) * div - vx * O(b, O_BG + B_GPX) -
-                         vy * O(b, O_BG + B_GPY) - vz * O(b, O_BG + B_GPZ) - sg * p;
-        const float Rb[3] = {red * (d4 - d7), red * (d6 - d2), red * (d3 - d5)};
-        const float Rs[5] = {Rr, Rp, Rb[0], Rb[1], Rb[2]};
-#pragma unroll
-        for (int q = 0; q < 5; ++q) {
-          const int l = q == 0 ? 0 : (q == 1 ? 4 : q + 3);
-          const float av = MODE == F_FIRST ? (l == 0 ? O(b, O_RHO) : Hv(l - 1)) : O(b, O_A + l);
-          const float s = sc[l * nz + k];
-          float an;
-          if (MODE == F_LAST) {
-            float c = S.carry[l * N + id];
-            an = zero ? av : kahan(av, fac * (s * Rs[q]), c);
-            S.carry[l * N + id] = c;
-            if (q == 0) an_rho = ((double)an - (double)c) * (double)isc[k];
-          } else {
-            an = zero ? av : av + fac * (s * Rs[q]);
-          }
-          so[l * N + id] = an;
-        }
-        if (MODE == F_LAST) {
-          mr = fmin(mr, (double)rho + (double)r0);
-          mp = fmin(mp, (double)p + (double)O(b, O_P0));
-        }
-      }
-    }
-    if (MODE == F_LAST) {
-      __syncthreads();
-      if (act && role == 1) {
-        const double m = ((double)O(b, O_BG + B_RHO0) + an_rho) *
-                         ((double *)(X + 2 * NC))[cid] / 2.0;
-        ke += m * m;
-      }
-    }
-  }
-  if (!ok) {
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-    if (TMA && tid == 0) {
-      mbar_wait32(&bar[0], phase & 1u, S.err);
-      mbar_wait32(&bar[1], (phase >> 1) & 1u, S.err);
-    }
-    return false;
-  }
-  asm volatile("cp.async.wait_all;\n" ::: "memory");
-  return true;
-}
-
-
-// Tiles away from every edge, CPML slab and periodic wrap: their x/y
-// derivatives are the centred stencil with no branch.
-__device__ __forceinline__ bool mhd_interior(const Sim32 &S, int x0, int y0) {
-  const int xm = max(5, S.xb.on ? S.xb.np : 0), xM = max(5, S.xt.on ? S.xt.np : 0);
-  const int ym = max(5, S.yb.on ? S.yb.np : 0), yM = max(5, S.yt.on ? S.yt.np : 0);
-  return x0 >= xm && x0 + t32::TX <= S.nx - xM && y0 >= ym && y0 + t32::TY <= S.ny - yM;
-}
 
 // One RK stage of the MHD equations.  A stage is two launches over one
 // logical grid of (x tile, y tile, z chunk) blocks: INT = true covers the
@@ -912,17 +420,17 @@ __global__ void __launch_bounds__(t32::NT, 1)
   const int ty_ = INT ? blockIdx.y + iy0 : blockIdx.y;
   const int x0 = tx_ * t32::TX, y0 = ty_ * t32::TY;
   if (!INT && mhd_interior(S, x0, y0)) return;
-  if (sm_addr32(smem) & 127u) {
+  if (sm_addr_t(smem) & 127u) {
     if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) atomicExch(S.err, 2);
     return;
   }
   double ke = 0.0, mr = 1e300, mp = 1e300;
   const int k0 = blockIdx.z * zchunk;
-  if (!mhd_body<MODE, TMA, INT>(S, &T, smem, a, tin, so, beta, bnext, x0, y0, k0,
+  if (!mhd_body<float, MODE, TMA, INT>(S, &T, smem, a, tin, so, beta, bnext, x0, y0, k0,
                                 min(S.nz, k0 + zchunk), mt, ma, ke, mr, mp))
     return;
   if (MODE == F_LAST)
-    diag_reduce32(S, ke, mr, mp, tx_ + (long long)gx * (ty_ + (long long)gy * blockIdx.z),
+    diag_reduce_t(S, ke, mr, mp, tx_ + (long long)gx * (ty_ + (long long)gy * blockIdx.z),
                   (long long)gx * gy * gridDim.z);
 }
 
@@ -1404,10 +912,10 @@ __global__ void __launch_bounds__(BT, 1)
     const int x0 = it.y, y0 = it.z, k0 = it.w & 0xffff, k1 = it.w >> 16;
     double ke = 0.0, mr = 1e300, mp = 1e300;
     if (PART == 0)
-      mhd_body<MODE, false, true>(sS, nullptr, smem, a, tin, so, beta, bnext, x0, y0, k0, k1,
+      mhd_body<float, MODE, false, true>(sS, nullptr, smem, a, tin, so, beta, bnext, x0, y0, k0, k1,
                                   0, 0, ke, mr, mp);
     else if (sS.magnetic)
-      mhd_body<MODE, false, false>(sS, nullptr, smem, a, tin, so, beta, bnext, x0, y0, k0, k1,
+      mhd_body<float, MODE, false, false>(sS, nullptr, smem, a, tin, so, beta, bnext, x0, y0, k0, k1,
                                    0, 0, ke, mr, mp);
     else if (sS.bg1d)
       quiet_body<32, 16, MODE, true>(sS, a, tin, so, beta, bnext, x0, y0, k0, k1, threadIdx.x,
@@ -1663,7 +1171,8 @@ int setup32(Handle *h) {
     dev_free(h, D.pa);
     dev_free(h, D.pb);
     dev_free(h, D.pk);
-    D.pa = D.pb = D.pk = nullptr;
+    dev_free(h, D.pki);
+    D.pa = D.pb = D.pk = D.pki = nullptr;
   }
   return encode_tensor_maps32(h);
 }

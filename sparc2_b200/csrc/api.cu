@@ -389,6 +389,8 @@ int sparc_create(const sparc_params *p, int device, sparc_handle **out) {
   }
   if (const char *kv = std::getenv("SPARC_TMA32"))  // A/B timing only
     h->allow_tma32 = std::atoi(kv) != 0;
+  if (const char *kv = std::getenv("SPARC_TMA64"))  // A/B timing only
+    h->allow_tma64 = std::atoi(kv) != 0;
   int r = SPARC_OK;
   if (!cuda_ok(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream")) {
     r = SPARC_ERR_CUDA;

@@ -228,6 +228,7 @@ struct Handle {
   float *f_sd = nullptr, *f_ssb = nullptr;
   bool tma32 = false;
   bool allow_tma32 = true;   // FP32 MHD own-point loads by TMA (nx % 4 == 0)
+  bool allow_tma64 = true;   // FP64 MHD own-point loads by TMA (nx even)
   CUtensorMap tmaps32[18];
 
   // member of a batch (sparc_batch_add): the batch owns the buffer roles,

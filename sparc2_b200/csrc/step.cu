@@ -14,6 +14,7 @@
 // step) and the values are bitwise those of forming a + beta*F on load.
 
 #include <cmath>
+#include <cstring>
 
 #include "mhd_body.cuh"
 
@@ -1277,11 +1278,12 @@ int encode_tensor_maps(Handle *h) {
 // chunk) blocks: INT = true over the interior tile rectangle with the
 // branch-free body of mhd_body.cuh, INT = false over the whole grid,
 // returning at once on interior tiles (edge and CPML tiles).
-template <int MODE, bool INT>
+// TMA: the 24 own-point arrays of a layer arrive as 32x8x1 TMA boxes.
+template <int MODE, bool TMA, bool INT>
 __global__ void __launch_bounds__(mg::NT, 1)
-    k_mhd64(const SimDev S, const double *__restrict__ a, const double *__restrict__ tin,
-            double *__restrict__ so, double beta, double bnext, int zchunk, int ix0, int iy0,
-            int gx, int gy) {
+    k_mhd64(const SimDev S, const __grid_constant__ TmaSet32 T, const double *__restrict__ a,
+            const double *__restrict__ tin, double *__restrict__ so, double beta, double bnext,
+            int zchunk, int mt, int ma, int ix0, int iy0, int gx, int gy) {
   extern __shared__ __align__(1024) double smem_raw64[];
   double *smem = (double *)(((size_t)smem_raw64 + 127) & ~(size_t)127);
   const int tx_ = INT ? blockIdx.x + ix0 : blockIdx.x;
@@ -1290,8 +1292,9 @@ __global__ void __launch_bounds__(mg::NT, 1)
   if (!INT && mhd_interior(S, x0, y0)) return;
   double ke = 0.0, mr = 1e300, mp = 1e300;
   const int k0 = blockIdx.z * zchunk;
-  mhd_body<double, MODE, false, INT>(S, nullptr, smem, a, tin, so, beta, bnext, x0, y0, k0,
-                                     min(S.nz, k0 + zchunk), 0, 0, ke, mr, mp);
+  if (!mhd_body<double, MODE, TMA, INT>(S, &T, smem, a, tin, so, beta, bnext, x0, y0, k0,
+                                         min(S.nz, k0 + zchunk), mt, ma, ke, mr, mp))
+    return;
   if (MODE == F_LAST)
     diag_reduce_t(S, ke, mr, mp, tx_ + (long long)gx * (ty_ + (long long)gy * blockIdx.z),
                   (long long)gx * gy * gridDim.z);
@@ -1312,19 +1315,37 @@ static int launch_mhd64(Handle *h, const SimDev &S, int stage, const double *a,
   const bool has_int = ix1 > ix0 && iy1 > iy0;
   dim3 gint(has_int ? ix1 - ix0 : 1, has_int ? iy1 - iy0 : 1, grd.z);
   const size_t sm = MhdBuf<double>::SMEM;
-#define ML64(M)                                                                              \
-  do {                                                                                       \
-    cudaFuncSetAttribute(k_mhd64<M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
-    cudaFuncSetAttribute(k_mhd64<M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
-    if (has_int)                                                                             \
-      k_mhd64<M, true><<<gint, blk, sm, s>>>(S, a, tin, so, beta, bnext, h->zchunk, ix0, iy0, \
-                                             grd.x, grd.y);                                  \
-    k_mhd64<M, false><<<grd, blk, sm, s>>>(S, a, tin, so, beta, bnext, h->zchunk, 0, 0, grd.x, \
-                                           grd.y);                                           \
+  const bool tma = h->tma && h->tma_ty == mg::TY && h->allow_tma64;
+  int mt = -1, ma = -1;
+  for (int b = 0; b < 3; ++b) {
+    if (h->buf[b] == tin) mt = b;
+    if (h->buf[b] == a) ma = b;
+  }
+  if (mt < 0 || ma < 0) return SPARC_ERR_INVALID;
+  TmaSet32 T;
+  if (tma)
+    for (int n = 0; n < 18; ++n) T.m[n] = h->tmaps_ty[n];
+  else
+    std::memset(&T, 0, sizeof(T));
+#define ML64(M, U)                                                                            \
+  do {                                                                                        \
+    cudaFuncSetAttribute(k_mhd64<M, U, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
+    cudaFuncSetAttribute(k_mhd64<M, U, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
+    if (has_int)                                                                              \
+      k_mhd64<M, U, true><<<gint, blk, sm, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt,  \
+                                                ma, ix0, iy0, grd.x, grd.y);                  \
+    k_mhd64<M, U, false><<<grd, blk, sm, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt, ma, \
+                                              0, 0, grd.x, grd.y);                            \
   } while (0)
-  if (mode == FIRST) ML64(F_FIRST);
-  else if (mode == MID) ML64(F_MID);
-  else ML64(F_LAST);
+  if (tma) {
+    if (mode == FIRST) ML64(F_FIRST, true);
+    else if (mode == MID) ML64(F_MID, true);
+    else ML64(F_LAST, true);
+  } else {
+    if (mode == FIRST) ML64(F_FIRST, false);
+    else if (mode == MID) ML64(F_MID, false);
+    else ML64(F_LAST, false);
+  }
 #undef ML64
   return SPARC_OK;
 }

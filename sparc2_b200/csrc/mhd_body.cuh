@@ -499,6 +499,8 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet32 *T, R 
   const R dt = (R)S.deltat;
   const R sx = (R)S.stretchx, sy = (R)S.stretchy;
   const R *gcol = S.gblk + (act ? S.colx[i] + S.bxdim * S.coly[j] : 0) * nz;
+  // PULSE = 1 time factor: the iteration is fixed during a stage
+  const R Tp = S.frc.kind == SPARC_SRC_PULSE ? pulse_time_t(S, *S.iter) : R(0);
 
   for (int k = k0; k < k1; ++k) {
     const int b = (k - k0) & 1;
@@ -506,6 +508,16 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet32 *T, R 
     R h0 = 0, h1 = 0, h2 = 0;
     const bool sh = k > k0 && k <= nz - 6;
     if (sh && act) head(k + 5, h0, h1, h2);
+    // momentum role: own-point B0 (its halo slots will hold the fluxes),
+    // gravity and forcing, loaded early
+    R ox = 0, oy = 0, oz = 0, gk = 0, frc = 0;
+    if (role == 0 && act) {
+      ox = __ldg(S.box + id);
+      oy = __ldg(S.boy + id);
+      oz = __ldg(S.boz + id);
+      gk = __ldg(gcol + k);
+      if (S.frc.kind != SPARC_SRC_NONE) frc = forcing_t(S, Tp, i, j, k);
+    }
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     if (hs0 >= 0) flux(b, hs0);
     if (hs1 >= 0) flux(b, hs1);
@@ -590,8 +602,6 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet32 *T, R 
                   vz = Hv(2) * iv;
       const R red = O(b, O_BG + B_RED), sg = O(b, O_BG + B_SPONGE);
       if (role == 0) {
-        // B0 at the own point (its halo slots now hold the fluxes)
-        const R ox = __ldg(S.box + id), oy = __ldg(S.boy + id), oz = __ldg(S.boz + id);
         const R ib = IS(5, k);
         const R dzby = X[NC + cid];
         const R cbx = d4 - dzby, cby = -d5 + d6, cbz = d7 - d8;
@@ -606,10 +616,8 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet32 *T, R 
         vxr = vxr + ri * e1 * red;
         vyr = vyr + ri * e2 * red;
         vzr = vzr + ri * e3 * red;
-        vzr = vzr - ri * rho * __ldg(gcol + k);
+        vzr = vzr - ri * rho * gk;
         if (S.frc.kind != SPARC_SRC_NONE) {
-          const long long it = *S.iter;
-          const R frc = forcing_t(S, pulse_time_t(S, it), i, j, k);
           if (S.frc.dir == 1) vxr = vxr + frc;
           else if (S.frc.dir == 2) vyr = vyr + frc;
           else vzr = vzr + frc;

@@ -57,6 +57,9 @@ def parse():
                     "scaled by this factor")
     ap.add_argument("--budget-gb", type=float, default=150.0,
                     help="serve: device-memory admission budget")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="cfg1: skip the FP32 precision-form and batched-ensemble "
+                    "lines that the default run adds beside the FP64 number")
     ap.add_argument("--no-fp64-compare", action="store_true",
                     help="ensemble: skip timing the FP64 plain cfg1 step")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
@@ -361,8 +364,21 @@ def run_gpu(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline()
 
-    if rank != 0:
+    # the north star's comparison: the FP32 precision form and the FP32
+    # batched ensemble on the same GPU, beside this FP64 plain number
+    extras = {}
+    if (world == 1 and not args.no_extras and args.workload == "cfg1"
+            and not fp32 and args.grid is None):
         sim.close()
+        sim = None
+        extras["fp32_precision_form"] = measure_fp32_cfg2(dev)
+        extras["fp32_batched"] = measure_ensemble(dev, members=args.members)
+        extras["fp32_batched"]["ratio_vs_fp64_plain"] = \
+            extras["fp32_batched"]["value"] / value
+
+    if rank != 0:
+        if sim is not None:
+            sim.close()
         rep.close()
         return
     line = {
@@ -394,8 +410,10 @@ def run_gpu(args, world, rank, local):
         line["clocks"] = clk
     if cpu:
         line["cpu_baseline"] = cpu
+    line.update(extras)
     print(json.dumps(line), flush=True)
-    sim.close()
+    if sim is not None:
+        sim.close()
     rep.close()
 
 
@@ -420,6 +438,72 @@ def fp64_plain_rate(dev, steps=20, warmup=3):
     ms = e0.elapsed_time(e1) / steps
     sim.close()
     return p.nx * p.ny * p.nz / (ms / 1e3), ms
+
+
+def measure_fp32_cfg2(dev, steps=40, warmup=3):
+    """The precision form on the flux-tube configuration (cfg2), timed like
+    the headline: graph-launched iterations, CUDA events on its stream."""
+    import torch
+    from sparc2_b200 import Simulation
+    p, bg, src, desc = workload("cfg1", precision=abi.SPARC_FP32)
+    sim = Simulation(p, bg, src, device=dev)
+    del bg
+    stream = torch.cuda.ExternalStream(sim.stream, device=dev)
+    sim.run(0, warmup)
+    sim.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.run(warmup, steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    sim.close()
+    pts = p.nx * p.ny * p.nz
+    return {"value": pts / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "steps": steps,
+            "dtype": "f32", "workload": desc}
+
+
+def measure_ensemble(dev, members=64, steps=10, warmup=2):
+    """The batched precision form: `members` seeded FP32 simulations through
+    the batched engine (autotuned tiles), one graph launch per step."""
+    import torch
+    from sparc2_b200 import Simulation
+    from sparc2_b200.batch import Batch
+    draws = W.ensemble_draws(members)
+    sims, pts = [], 0
+    t0 = time.perf_counter()
+    for nx, nz, b0, depth in draws:
+        p, bg, src = W.member(nx, nz, b0, depth)
+        sims.append(Simulation(p, bg, src, device=dev))
+        pts += p.nx * p.ny * p.nz
+        del bg
+    setup = time.perf_counter() - t0
+    batch = Batch(len(sims), device=dev)
+    for sm in sims:
+        batch.add(sm, 0, 1000)
+    stream = torch.cuda.ExternalStream(batch.stream, device=dev)
+    tiles = batch.tune(steps_per_trial=1)
+    batch.run(warmup)
+    batch.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    batch.run(steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    batch.close()
+    for sm in sims:
+        sm.close()
+    nq = sum(1 for d in draws if d[2] <= 0)
+    return {"value": pts / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "steps": steps,
+            "dtype": "f32", "members": len(draws), "quiet_members": nq,
+            "grid_points": pts, "tiles": {"zchunk_mhd": tiles[0], "zchunk_quiet": tiles[1]},
+            "setup_s": setup,
+            "workload": "batched ensemble: %d seeded members (nx=ny in {96..256}, nz in "
+                        "[150, 300], quiet or flux tube, one pulse each), a step advances "
+                        "every member one driver iteration" % len(draws)}
 
 
 def run_ensemble(args, world, rank, local):

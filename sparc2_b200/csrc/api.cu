@@ -177,16 +177,14 @@ static int enqueue_step32(Handle *h, cudaStream_t s, int *nk) {
   SimT<float> S = make_sim32(h);
   float *a = h->fbuf[h->ra], *f1 = h->fbuf[h->rf1], *f2 = h->fbuf[h->rf2];
   int r = SPARC_OK;
-  if (h->src.kind == SPARC_SRC_PSR && h->psr_khi > h->psr_klo) {
-    r |= launch_psr32(h, s);
-    ++*nk;
-  }
+  const long long l0 = h->launches;
+  if (h->src.kind == SPARC_SRC_PSR && h->psr_khi > h->psr_klo) r |= launch_psr32(h, s);
   r |= launch_stage32(h, S, 1, a, a, f1, s);
   r |= launch_stage32(h, S, 2, a, f1, f2, s);
   r |= launch_stage32(h, S, 3, a, f2, f1, s);
   r |= launch_stage32(h, S, 4, a, f1, f2, s);
   r |= launch_stage32(h, S, 5, a, f2, f1, s);
-  *nk += 5;
+  *nk += (int)(h->launches - l0);
   rotate(h);
   return r ? SPARC_ERR_CUDA : SPARC_OK;
 }
@@ -197,17 +195,15 @@ static int enqueue_step(Handle *h, cudaStream_t s, int *nk) {
   SimDev S = make_simdev(h);
   double *a = h->buf[h->ra], *f1 = h->buf[h->rf1], *f2 = h->buf[h->rf2];
   int r = SPARC_OK;
-  if (h->src.kind == SPARC_SRC_PSR && h->psr_khi > h->psr_klo) {
-    r |= launch_psr_forcing(h, S, s);
-    ++*nk;
-  }
+  const long long l0 = h->launches;
+  if (h->src.kind == SPARC_SRC_PSR && h->psr_khi > h->psr_klo) r |= launch_psr_forcing(h, S, s);
   // stage k reads temp_k and writes temp_{k+1}; stage 5 writes a_new
   r |= launch_stage(h, S, 1, a, a, f1, s);
   r |= launch_stage(h, S, 2, a, f1, f2, s);
   r |= launch_stage(h, S, 3, a, f2, f1, s);
   r |= launch_stage(h, S, 4, a, f1, f2, s);
   r |= launch_stage(h, S, 5, a, f2, f1, s);
-  *nk += 5;
+  *nk += (int)(h->launches - l0);
   rotate(h);
   return r ? SPARC_ERR_CUDA : SPARC_OK;
 }

@@ -1337,6 +1337,7 @@ static int launch_mhd64(Handle *h, const SimDev &S, int stage, const double *a,
     k_mhd64<M, U, false><<<grd, blk, sm, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt, ma, \
                                               0, 0, grd.x, grd.y);                            \
   } while (0)
+  if (has_int) ++h->launches;  // the interior launch (launch_stage counts the other)
   if (tma) {
     if (mode == FIRST) ML64(F_FIRST, true);
     else if (mode == MID) ML64(F_MID, true);

@@ -731,6 +731,7 @@ int launch_stage32(Handle *h, const Sim32 &S, int stage, const float *a,
     k_mhd32<M, U, false><<<grd, blk, SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk,   \
                                                 mt, ma, 0, 0, gx, gy);                      \
   } while (0)
+    if (has_int) ++h->launches;  // the interior launch (counted below: the other)
     if (h->tma32) {
       if (mode == F_FIRST) ML32(F_FIRST, true);
       else if (mode == F_MID) ML32(F_MID, true);

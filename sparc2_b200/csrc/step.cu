@@ -14,6 +14,7 @@
 // step) and the values are bitwise those of forming a + beta*F on load.
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "mhd_body.cuh"
@@ -1142,9 +1143,15 @@ int stage_geometry(Handle *h) {
     h->tx = 16;
     tiles = (long long)((h->nx + 15) / 16) * ((h->ny + 7) / 8);
   }
-  // z chunk: aim for >= 4 CTAs per SM on 148 SMs
-  int zc = h->nz;
-  while (zc > 16 && tiles * ((h->nz + zc - 1) / zc) < 148 * 4) zc = (zc + 1) / 2;
+  // z chunk: about seven CTAs per SM on 148 SMs (one MHD CTA is resident per
+  // SM: shorter tails; each chunk pays 10 window warm-up layers)
+  const long long chunks = std::max<long long>(1, (148LL * 7 + tiles - 1) / tiles);
+  int zc = (int)std::max<long long>(16, (h->nz + chunks - 1) / chunks);
+  zc = std::min(zc, h->nz);
+  if (const char *kv = std::getenv("SPARC_ZCHUNK")) {  // A/B timing only
+    const int v = std::atoi(kv);
+    if (v >= 11) zc = std::min(v, h->nz);
+  }
   h->zchunk = zc;
   h->max_stage_blocks = (int)(tiles * ((h->nz + zc - 1) / zc));
   return SPARC_OK;

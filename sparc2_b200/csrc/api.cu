@@ -388,7 +388,10 @@ int sparc_create(const sparc_params *p, int device, sparc_handle **out) {
   if (const char *kv = std::getenv("SPARC_TMA64"))  // A/B timing only
     h->allow_tma64 = std::atoi(kv) != 0;
   int r = SPARC_OK;
-  if (!cuda_ok(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream")) {
+  if (!cuda_ok(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream") ||
+      !cuda_ok(h, cudaStreamCreateWithFlags(&h->aux, cudaStreamNonBlocking), "stream") ||
+      !cuda_ok(h, cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming), "event") ||
+      !cuda_ok(h, cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming), "event")) {
     r = SPARC_ERR_CUDA;
   }
   if (!r && (setup_constants() || step_constants() || filter_constants() ||
@@ -469,6 +472,10 @@ int sparc_destroy(sparc_handle *h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   drop_graphs(h);
   for (void *p : h->allocs) cudaFree(p);
+  if (h->aux) cudaStreamSynchronize(h->aux);
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
+  if (h->aux) cudaStreamDestroy(h->aux);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return SPARC_OK;

@@ -148,6 +148,10 @@ struct Handle {
   int gxy = 5, gz = 5, xyfreq = 1, zfreq = 1;
   bool bg_ready = false;
   cudaStream_t stream = nullptr;
+  // MHD stages: the edge/CPML launch runs on `aux`, forked from and joined
+  // back to `stream` by the two events, beside the interior launch
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::string err;
   long long launches = 0;
 

@@ -1338,11 +1338,19 @@ static int launch_mhd64(Handle *h, const SimDev &S, int stage, const double *a,
   do {                                                                                        \
     cudaFuncSetAttribute(k_mhd64<M, U, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
     cudaFuncSetAttribute(k_mhd64<M, U, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
-    if (has_int)                                                                              \
+    if (has_int) {                                                                            \
+      cudaEventRecord(h->ev_fork, s);                                                         \
+      cudaStreamWaitEvent(h->aux, h->ev_fork, 0);                                             \
+      k_mhd64<M, U, false><<<grd, blk, sm, h->aux>>>(S, T, a, tin, so, beta, bnext, h->zchunk, \
+                                                     mt, ma, 0, 0, grd.x, grd.y);             \
+      cudaEventRecord(h->ev_join, h->aux);                                                    \
       k_mhd64<M, U, true><<<gint, blk, sm, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt,  \
                                                 ma, ix0, iy0, grd.x, grd.y);                  \
-    k_mhd64<M, U, false><<<grd, blk, sm, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt, ma, \
-                                              0, 0, grd.x, grd.y);                            \
+      cudaStreamWaitEvent(s, h->ev_join, 0);                                                  \
+    } else {                                                                                  \
+      k_mhd64<M, U, false><<<grd, blk, sm, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt,  \
+                                                ma, 0, 0, grd.x, grd.y);                      \
+    }                                                                                         \
   } while (0)
   if (has_int) ++h->launches;  // the interior launch (launch_stage counts the other)
   if (tma) {

@@ -725,11 +725,19 @@ int launch_stage32(Handle *h, const Sim32 &S, int stage, const float *a,
   do {                                                                                      \
     cudaFuncSetAttribute(k_mhd32<M, U, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); \
     cudaFuncSetAttribute(k_mhd32<M, U, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); \
-    if (has_int)                                                                            \
+    if (has_int) {                                                                          \
+      cudaEventRecord(h->ev_fork, s);                                                       \
+      cudaStreamWaitEvent(h->aux, h->ev_fork, 0);                                           \
+      k_mhd32<M, U, false><<<grd, blk, SMEM, h->aux>>>(S, T, a, tin, so, beta, bnext,       \
+                                                       h->zchunk, mt, ma, 0, 0, gx, gy);    \
+      cudaEventRecord(h->ev_join, h->aux);                                                  \
       k_mhd32<M, U, true><<<gint, blk, SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, \
                                                   mt, ma, ix0, iy0, gx, gy);                \
-    k_mhd32<M, U, false><<<grd, blk, SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk,   \
-                                                mt, ma, 0, 0, gx, gy);                      \
+      cudaStreamWaitEvent(s, h->ev_join, 0);                                                \
+    } else {                                                                                \
+      k_mhd32<M, U, false><<<grd, blk, SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, \
+                                                  mt, ma, 0, 0, gx, gy);                    \
+    }                                                                                       \
   } while (0)
     if (has_int) ++h->launches;  // the interior launch (counted below: the other)
     if (h->tma32) {

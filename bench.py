@@ -683,7 +683,7 @@ def run_serve(args, world, rank, local):
     clocks = Clocks(dev)
     srv = Server(capacity=64, budget_bytes=int(args.budget_gb * 1e9),
                  quantum=10, device=dev)
-    wall = drive(srv, reqs, build, on_result, builders=3,
+    wall = drive(srv, reqs, build, on_result, builders=4,
                  deadline_s=20 * args.duration + 600)
     st = srv.stats()
     srv.close()

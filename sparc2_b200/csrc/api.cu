@@ -9,6 +9,8 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "internal.h"
 
@@ -296,6 +298,20 @@ static Handle::GraphEntry *graph_for(Handle *h, int fk) {
   e.nkernels = nk;
   h->graphs.push_back(e);
   return &h->graphs.back();
+}
+
+// f(i) for i in [0, n) on the host's cores (state conversion of the
+// precision form: one (field, layer) plane per index)
+template <class F>
+static void parallel_for(long long n, F f) {
+  const long long nt = std::max<long long>(
+      1, std::min<long long>(n, std::min(16u, std::max(1u, std::thread::hardware_concurrency()))));
+  std::vector<std::thread> th;
+  for (long long w = 0; w < nt; ++w)
+    th.emplace_back([=, &f] {
+      for (long long i = w; i < n; i += nt) f(i);
+    });
+  for (auto &t : th) t.join();
 }
 
 }  // namespace sparc
@@ -654,11 +670,11 @@ static int set_state32(Handle *h, const double *a, const double *psi) {
   if (a && h->h_scale.empty()) return fail(h, SPARC_ERR_ORDER, "set the background first");
   if (a) {
     std::vector<float> t((size_t)h->V * N);
-    for (int l = 0; l < h->V; ++l)
-      for (long long n = 0; n < N; ++n) {
-        const double sc = h->h_scale[(size_t)l * nz + n / NXY];
-        t[(size_t)l * N + n] = (float)(sc * a[(size_t)l * N + n]);
-      }
+    parallel_for((long long)h->V * nz, [&](long long lk) {
+      const double sc = h->h_scale[(size_t)lk];  // field l = lk / nz, layer lk % nz
+      const size_t o = (size_t)lk * NXY;
+      for (long long n = 0; n < NXY; ++n) t[o + n] = (float)(sc * a[o + n]);
+    });
     CK(h, cudaMemcpy(h->fbuf[h->ra], t.data(), t.size() * 4, cudaMemcpyHostToDevice));
     CK(h, cudaMemset(h->f_carry, 0, t.size() * 4));
   }
@@ -685,12 +701,11 @@ static int get_state32(Handle *h, double *a, double *psi) {
     std::vector<float> t((size_t)V * N), c((size_t)V * N);
     CK(h, cudaMemcpy(t.data(), h->fbuf[h->ra], t.size() * 4, cudaMemcpyDeviceToHost));
     CK(h, cudaMemcpy(c.data(), h->f_carry, c.size() * 4, cudaMemcpyDeviceToHost));
-    for (int l = 0; l < V; ++l)
-      for (long long n = 0; n < N; ++n) {
-        const size_t q = (size_t)l * N + n;
-        const double isc = h->h_scale[(size_t)(V + l) * nz + n / NXY];
-        a[q] = ((double)t[q] - (double)c[q]) * isc;
-      }
+    parallel_for((long long)V * nz, [&](long long lk) {
+      const double isc = h->h_scale[(size_t)V * nz + (size_t)lk];
+      const size_t o = (size_t)lk * NXY;
+      for (long long n = 0; n < NXY; ++n) a[o + n] = ((double)t[o + n] - (double)c[o + n]) * isc;
+    });
   }
   if (psi) {
     size_t off = 0;

@@ -115,14 +115,16 @@ def fluxtube_background(nx, ny, nz, xlength, ylength, z_bot=-25.0,
     X = xs[None, None, :] - 0.5 * xlength
     Y = ys[None, :, None] - 0.5 * ylength
     R3 = R[:, None, None]
-    E = np.exp(-(X * X + Y * Y) / (R3 * R3))
+    E = np.exp((-(X * X + Y * Y)) / (R3 * R3))   # negate the 2-D plane, not the cube
     bz = Ba[:, None, None] * E
     bx = Ba[:, None, None] * Rp_over_R[:, None, None] * X * E
     by = Ba[:, None, None] * Rp_over_R[:, None, None] * Y * E
     pm = (bx * bx + by * by + bz * bz) / (8.0 * np.pi)
     q = 1.0 - pm / pre[:, None, None]
     lo = 2.0 * p_floor
-    fac = np.where(q >= lo, q, p_floor + p_floor * np.exp((q - lo) / p_floor))
+    fac = q.copy()                                # the floor only where it applies
+    low = q < lo
+    fac[low] = p_floor + p_floor * np.exp((q[low] - lo) / p_floor)
     pre3 = pre[:, None, None] * fac
     rho3 = rho[:, None, None] * fac
     cs3 = np.sqrt(gamma * pre3 / rho3)

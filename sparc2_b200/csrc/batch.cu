@@ -190,6 +190,7 @@ int capture(Batch *b) {
   L.counts = b->d_counts;
   L.wctr = b->d_wctr;
   L.grid = b->grid;
+  L.zmax = std::max(11, std::max(b->zchunk_mhd, b->zchunk_quiet));
   L.psr_smem = b->psr_smem;
   cudaGraph_t g;
   BCK(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
@@ -371,6 +372,7 @@ int sparc_batch_set_tiles(sparc_batch *b, int zchunk_mhd, int zchunk_quiet) {
   b->zchunk_mhd = zchunk_mhd;
   b->zchunk_quiet = zchunk_quiet;
   b->dirty = true;
+  b->recapture = true;  // the stage launches' shared memory depends on it
   return SPARC_OK;
 }
 

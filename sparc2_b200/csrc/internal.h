@@ -129,6 +129,7 @@ struct BatchLaunch {
                                         // interior stage items (a prefix)
   unsigned *wctr;                       // [14] work counters, zeroed per step
   int grid;                             // persistent CTAs
+  int zmax;                             // largest z extent of a stage item
   size_t psr_smem;
 };
 

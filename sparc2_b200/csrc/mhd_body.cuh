@@ -44,6 +44,11 @@ struct MhdBuf {
   static constexpr int BUF = ((mg::NO * mg::NC + mg::NH * mg::HS) + ALIGN - 1) / ALIGN * ALIGN;
   static constexpr int XCH = (2 * mg::NC * (int)sizeof(R) + mg::NC * 8) / (int)sizeof(R);
   static constexpr size_t SMEM = (2 * (size_t)BUF + XCH) * sizeof(R) + 128;
+  // precision form: the depth scales (8 inverse, 8 forward per layer) of a
+  // chunk of at most zext layers follow the exchange area
+  static constexpr size_t smem_bytes(int zext) {
+    return SMEM + (sizeof(R) == 4 ? (size_t)(zext + 16) * 16 * sizeof(R) : 0);
+  }
 };
 
 struct TmaSet32 {
@@ -340,13 +345,23 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet32 *T, R 
   const int ry = y0 - yo + ty, rx = x0 - xo + tx;
   const int own = ry * HX + rx;
   const R *isc = S.isc, *sc = S.sc;
-  // depth scales of the precision form; 1 (folded away) in the plain form
+  // depth scales of the precision form, staged in shared memory for the
+  // layers this chunk touches; 1 (folded away) in the plain form
+  R *ZT = smem + 2 * BUF + MhdBuf<R>::XCH;
+  const int zb = max(0, min(k0 - 5, nz - 11));
+  if constexpr (SCALED) {
+    const int ze = min(nz, max(k1 + 5, zb + 11));
+    for (int t = tid; t < (ze - zb) * 16; t += NT) {
+      const int kk = zb + (t >> 4), l = t & 15;
+      ZT[t] = l < 8 ? isc[l * nz + kk] : sc[(l - 8) * nz + kk];
+    }
+  }
   auto IS = [&](int l, int kk) -> R {
-    if constexpr (SCALED) return isc[l * nz + kk];
+    if constexpr (SCALED) return ZT[(kk - zb) * 16 + l];
     else return R(1);
   };
   auto SS = [&](int l, int kk) -> R {
-    if constexpr (SCALED) return sc[l * nz + kk];
+    if constexpr (SCALED) return ZT[(kk - zb) * 16 + 8 + l];
     else return R(1);
   };
   // General tiles: each lane (x) and row (y) gets its own 11 coefficients and

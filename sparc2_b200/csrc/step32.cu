@@ -397,9 +397,6 @@ __global__ void __launch_bounds__(TX *TY)
 
 namespace t32 {
 using namespace mg;
-constexpr int BUF = MhdBuf<float>::BUF;
-constexpr int XCH = MhdBuf<float>::XCH;
-constexpr size_t SMEM = MhdBuf<float>::SMEM;
 }  // namespace t32
 
 // One RK stage of the MHD equations.  A stage is two launches over one
@@ -711,8 +708,7 @@ int launch_stage32(Handle *h, const Sim32 &S, int stage, const float *a,
       std::memset(&T, 0, sizeof(T));
     dim3 blk(TX, TY, 2);
     dim3 grd((h->nx + TX - 1) / TX, (h->ny + TY - 1) / TY, (h->nz + h->zchunk - 1) / h->zchunk);
-    const int sm = (int)SMEM;
-// interior tile rectangle (see mhd_interior), in tile units
+    // interior tile rectangle (see mhd_interior), in tile units
     const int gx = (h->nx + TX - 1) / TX, gy = (h->ny + TY - 1) / TY;
     const FaceT<float> *F = h->f_faces;
     const int xm = std::max(5, F[2].on ? F[2].np : 0), xM = std::max(5, F[3].on ? F[3].np : 0);
@@ -721,21 +717,22 @@ int launch_stage32(Handle *h, const Sim32 &S, int stage, const float *a,
     const int iy0 = (ym + TY - 1) / TY, iy1 = (h->ny - yM - TY) / TY + 1;
     const bool has_int = h->nx - xM - TX >= 0 && h->ny - yM - TY >= 0 && ix1 > ix0 && iy1 > iy0;
     dim3 gint(has_int ? ix1 - ix0 : 1, has_int ? iy1 - iy0 : 1, grd.z);
+const int smz = (int)MhdBuf<float>::smem_bytes(h->zchunk);
 #define ML32(M, U)                                                                          \
   do {                                                                                      \
-    cudaFuncSetAttribute(k_mhd32<M, U, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); \
-    cudaFuncSetAttribute(k_mhd32<M, U, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); \
+    cudaFuncSetAttribute(k_mhd32<M, U, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smz); \
+    cudaFuncSetAttribute(k_mhd32<M, U, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smz); \
     if (has_int) {                                                                          \
       cudaEventRecord(h->ev_fork, s);                                                       \
       cudaStreamWaitEvent(h->aux, h->ev_fork, 0);                                           \
-      k_mhd32<M, U, false><<<grd, blk, SMEM, h->aux>>>(S, T, a, tin, so, beta, bnext,       \
+      k_mhd32<M, U, false><<<grd, blk, smz, h->aux>>>(S, T, a, tin, so, beta, bnext,       \
                                                        h->zchunk, mt, ma, 0, 0, gx, gy);    \
       cudaEventRecord(h->ev_join, h->aux);                                                  \
-      k_mhd32<M, U, true><<<gint, blk, SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, \
+      k_mhd32<M, U, true><<<gint, blk, smz, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, \
                                                   mt, ma, ix0, iy0, gx, gy);                \
       cudaStreamWaitEvent(s, h->ev_join, 0);                                                \
     } else {                                                                                \
-      k_mhd32<M, U, false><<<grd, blk, SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, \
+      k_mhd32<M, U, false><<<grd, blk, smz, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, \
                                                   mt, ma, 0, 0, gx, gy);                    \
     }                                                                                       \
   } while (0)
@@ -1049,10 +1046,10 @@ __global__ void __launch_bounds__(BT)
   }
 }
 
-size_t batch_stage_smem() { return t32::SMEM; }
+size_t batch_stage_smem() { return MhdBuf<float>::SMEM; }
 
 int launch_batch_step(const BatchLaunch &B, cudaStream_t s, int *nkernels) {
-  const int sm = (int)t32::SMEM;
+  const int sm = (int)MhdBuf<float>::smem_bytes(B.zmax);
   cudaFuncSetAttribute(k_batch_stage<F_FIRST, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   cudaFuncSetAttribute(k_batch_stage<F_MID, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   cudaFuncSetAttribute(k_batch_stage<F_LAST, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
@@ -1067,14 +1064,14 @@ int launch_batch_step(const BatchLaunch &B, cudaStream_t s, int *nkernels) {
   for (int st = 1; st <= 5; ++st) {
     unsigned *c0 = B.wctr + st, *c1 = B.wctr + 8 + st;
     if (st == 1) {
-      k_batch_stage<F_FIRST, 0><<<B.grid, blk, t32::SMEM, s>>>(B.slots, B.items, B.counts, c0, st);
-      k_batch_stage<F_FIRST, 1><<<B.grid, blk, t32::SMEM, s>>>(B.slots, B.items, B.counts, c1, st);
+      k_batch_stage<F_FIRST, 0><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c0, st);
+      k_batch_stage<F_FIRST, 1><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c1, st);
     } else if (st < 5) {
-      k_batch_stage<F_MID, 0><<<B.grid, blk, t32::SMEM, s>>>(B.slots, B.items, B.counts, c0, st);
-      k_batch_stage<F_MID, 1><<<B.grid, blk, t32::SMEM, s>>>(B.slots, B.items, B.counts, c1, st);
+      k_batch_stage<F_MID, 0><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c0, st);
+      k_batch_stage<F_MID, 1><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c1, st);
     } else {
-      k_batch_stage<F_LAST, 0><<<B.grid, blk, t32::SMEM, s>>>(B.slots, B.items, B.counts, c0, st);
-      k_batch_stage<F_LAST, 1><<<B.grid, blk, t32::SMEM, s>>>(B.slots, B.items, B.counts, c1, st);
+      k_batch_stage<F_LAST, 0><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c0, st);
+      k_batch_stage<F_LAST, 1><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c1, st);
     }
   }
   k_batch_filter<1><<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 6);

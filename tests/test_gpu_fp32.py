@@ -146,3 +146,32 @@ def test_cfg0_fp32_errors_at_100_500_1000():
         print(f"iteration {mark}: rel L2 {errs} max-norm {mx}")
         assert max(errs) <= LONG_TOL32, (mark, errs)
     assert np.max(np.abs(oa[3])) > 0
+
+
+def test_cfg2_fp32_errors_at_100_500_1000():
+    """The precision form on the flux-tube configuration at full size
+    (256x256x300, 200 PSR pulses): relative L2 and max-norm error per field
+    against the FP64 plain form (itself within 1e-11 of the oracle) at
+    iterations 100, 500 and 1000, each within 1e-4 relative L2."""
+    p64, bg, src = W.cfg1()
+    s64 = Simulation(p64, bg, src)
+    p32, _, _ = W.cfg1(precision=abi.SPARC_FP32)
+    s32 = Simulation(p32, bg, src)
+    del bg
+    done = 0
+    for mark in (100, 500, 1000):
+        for s in (s64, s32):
+            s.run(done, mark + 1 - done)
+        done = mark + 1
+        ga, _ = s32.get_state()
+        oa, _ = s64.get_state()
+        errs = [rel_l2(ga[l], oa[l]) for l in range(s32.V)]
+        mx = [max_norm(ga[l], oa[l]) for l in range(s32.V)]
+        print(f"cfg2 iteration {mark}: rel L2 {[f'{e:.2e}' for e in errs]} "
+              f"max-norm {[f'{e:.2e}' for e in mx]}")
+        assert max(errs) <= LONG_TOL32, (mark, errs)
+        del ga, oa
+    d32, r32 = s32.diagnostics()
+    d64, r64 = s64.diagnostics()
+    assert r32 == r64 == abi.SPARC_OK
+    assert d32.ke_norm == pytest.approx(d64.ke_norm, rel=1e-4)

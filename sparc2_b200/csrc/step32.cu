@@ -219,7 +219,7 @@ __device__ __forceinline__ void quiet_body(const Sim32 &S, const float *__restri
                                            const float *__restrict__ tin,
                                            float *__restrict__ so, float beta, float bnext,
                                            int x0, int y0, int k0, int k1, int tx, int ty,
-                                           double &ke, double &mr, double &mp) {
+                                           float *zt, double &ke, double &mr, double &mp) {
   constexpr int HX = TX + 10, HY = TY + 10;
   __shared__ float t_vx[HY][HX], t_vy[HY][HX], t_p[HY][HX];
   const int tid = ty * TX + tx;
@@ -235,7 +235,19 @@ __device__ __forceinline__ void quiet_body(const Sim32 &S, const float *__restri
   const int gc = act ? S.colx[i] + S.bxdim * S.coly[j] : 0;
   const int xo = origin32(x0, TX, nx, per), yo = origin32(y0, TY, ny, per);
   const int cx0 = x0 - xo, cy0 = y0 - yo;
-  const float *isc = S.isc, *sc = S.sc;
+  // depth scales of the layers this chunk touches, staged in shared memory
+  // (zt: 16 floats per layer, 1/sc of the 5 fields then sc)
+  const int zb = max(0, min(k0 - 5, nz - 11));
+  {
+    const int ze = min(nz, max(k1 + 5, zb + 11));
+    for (int t = tid; t < (ze - zb) * 16; t += TX * TY) {
+      const int kk = zb + (t >> 4), l = t & 15;
+      zt[t] = l < 5 ? S.isc[l * nz + kk] : (l >= 8 && l < 13 ? S.sc[(l - 8) * nz + kk] : 0.f);
+    }
+  }
+  __syncthreads();
+  auto isc_ = [&](int l, int kk) { return zt[(kk - zb) * 16 + l]; };
+  auto sc_ = [&](int l, int kk) { return zt[(kk - zb) * 16 + 8 + l]; };
 
   float wvz[11], wp[11];  // physical values
   const int b0 = min(k0 - 5, nz - 11);
@@ -244,15 +256,15 @@ __device__ __forceinline__ void quiet_body(const Sim32 &S, const float *__restri
     const int kk = b0 + m;
     const bool ok = act && kk >= 0;
     const long long id = (long long)kk * NXY + col;
-    wvz[m] = ok ? __ldg(tin + 3 * N + id) * isc[3 * nz + kk] : 0.f;
-    wp[m] = ok ? __ldg(tin + 4 * N + id) * isc[4 * nz + kk] : 0.f;
+    wvz[m] = ok ? __ldg(tin + 3 * N + id) * isc_(3, kk) : 0.f;
+    wp[m] = ok ? __ldg(tin + 4 * N + id) * isc_(4, kk) : 0.f;
   }
 
   for (int k = k0; k < k1; ++k) {
     if (k > k0 && k <= nz - 6) {
       const long long id = (long long)(k + 5) * NXY + col;
-      shift32(wvz, act ? __ldg(tin + 3 * N + id) * isc[3 * nz + k + 5] : 0.f);
-      shift32(wp, act ? __ldg(tin + 4 * N + id) * isc[4 * nz + k + 5] : 0.f);
+      shift32(wvz, act ? __ldg(tin + 3 * N + id) * isc_(3, k + 5) : 0.f);
+      shift32(wp, act ? __ldg(tin + 4 * N + id) * isc_(4, k + 5) : 0.f);
     }
     const long long kb = (long long)k * NXY;
     __syncthreads();
@@ -280,8 +292,8 @@ __device__ __forceinline__ void quiet_body(const Sim32 &S, const float *__restri
     float isv[5], scv[5];
 #pragma unroll
     for (int l = 0; l < 5; ++l) {
-      isv[l] = isc[l * nz + k];
-      scv[l] = sc[l * nz + k];
+      isv[l] = isc_(l, k);
+      scv[l] = sc_(l, k);
     }
     float av[5], tv[5];
 #pragma unroll
@@ -379,11 +391,12 @@ template <int TX, int TY, int MODE, bool BG1D>
 __global__ void __launch_bounds__(TX *TY)
     k_quiet32(const Sim32 S, const float *__restrict__ a, const float *__restrict__ tin,
               float *__restrict__ so, float beta, float bnext, int zchunk) {
+  extern __shared__ __align__(1024) float smem_raw32[];  // the depth-scale table
   double ke = 0.0, mr = 1e300, mp = 1e300;
   const int k0 = blockIdx.z * zchunk;
   quiet_body<TX, TY, MODE, BG1D>(S, a, tin, so, beta, bnext, blockIdx.x * TX, blockIdx.y * TY,
-                                 k0, min(S.nz, k0 + zchunk), threadIdx.x, threadIdx.y, ke, mr,
-                                 mp);
+                                 k0, min(S.nz, k0 + zchunk), threadIdx.x, threadIdx.y, smem_raw32,
+                                 ke, mr, mp);
   if (MODE == F_LAST)
     diag_reduce32(S, ke, mr, mp,
                   blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z),
@@ -675,7 +688,12 @@ static void launch_quiet32(Handle *h, const Sim32 &S, int mode, const float *a,
                            cudaStream_t s) {
   dim3 blk(TX, TY);
   dim3 grd((h->nx + TX - 1) / TX, (h->ny + TY - 1) / TY, (h->nz + h->zchunk - 1) / h->zchunk);
-#define QL32(M, B) k_quiet32<TX, TY, M, B><<<grd, blk, 0, s>>>(S, a, tin, so, beta, bnext, h->zchunk)
+  const int zsm = (h->zchunk + 16) * 16 * (int)sizeof(float);
+#define QL32(M, B)                                                                     \
+  do {                                                                                 \
+    cudaFuncSetAttribute(k_quiet32<TX, TY, M, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, zsm); \
+    k_quiet32<TX, TY, M, B><<<grd, blk, zsm, s>>>(S, a, tin, so, beta, bnext, h->zchunk); \
+  } while (0)
   if (S.bg1d) {
     if (mode == F_FIRST) QL32(F_FIRST, true);
     else if (mode == F_MID) QL32(F_MID, true);
@@ -888,6 +906,7 @@ __global__ void __launch_bounds__(BT, 1)
   __shared__ __align__(16) unsigned long long sS_raw[(sizeof(Sim32) + 7) / 8];
   __shared__ int s_w;
   float *smem = (float *)(((size_t)smem_raw32 + 127) & ~(size_t)127);
+  float *qzt = smem + 2 * MhdBuf<float>::BUF + MhdBuf<float>::XCH;  // quiet items' scale table
   Sim32 &sS = *reinterpret_cast<Sim32 *>(sS_raw);
   const int tid = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
   const int lo = PART == 0 ? 0 : counts[3], hi = PART == 0 ? counts[3] : counts[0];
@@ -925,10 +944,10 @@ __global__ void __launch_bounds__(BT, 1)
                                    0, 0, ke, mr, mp);
     else if (sS.bg1d)
       quiet_body<32, 16, MODE, true>(sS, a, tin, so, beta, bnext, x0, y0, k0, k1, threadIdx.x,
-                                     threadIdx.y + 8 * threadIdx.z, ke, mr, mp);
+                                     threadIdx.y + 8 * threadIdx.z, qzt, ke, mr, mp);
     else
       quiet_body<32, 16, MODE, false>(sS, a, tin, so, beta, bnext, x0, y0, k0, k1, threadIdx.x,
-                                      threadIdx.y + 8 * threadIdx.z, ke, mr, mp);
+                                      threadIdx.y + 8 * threadIdx.z, qzt, ke, mr, mp);
     if (MODE == F_LAST) batch_finish_step(L, sS, w, ke, mr, mp, tid);
     __syncthreads();
   }

@@ -393,12 +393,6 @@ int sparc_create(const sparc_params *p, int device, sparc_handle **out) {
     while (b + 1 < p->block_z && k >= h->bzs[b + 1]) ++b;
     cols[h->nx + h->ny + k] = b;
   }
-  if (const char *kv = std::getenv("SPARC_MHD_KERNEL"))  // A/B timing only
-    h->mhd_kernel = std::atoi(kv) == 4 ? 4 : (std::atoi(kv) == 3 ? 3 : 5);
-  if (const char *kv = std::getenv("SPARC_TMA_TY")) {  // A/B timing only
-    int t = std::atoi(kv);
-    if (t == 6 || t == 8) h->tma_ty = t;
-  }
   if (const char *kv = std::getenv("SPARC_TMA32"))  // A/B timing only
     h->allow_tma32 = std::atoi(kv) != 0;
   if (const char *kv = std::getenv("SPARC_TMA64"))  // A/B timing only

@@ -198,10 +198,9 @@ struct Handle {
   double *d_damp2 = nullptr;                // source_damp(i,j) (N/nz)
   int nblocks = 1;
 
-  // TMA tensor maps of the own-point arrays: [0..2] the state buffers
-  // (nx, ny, nz*V), [3..17] the background arrays read per layer
+  // TMA tensor maps (32x8x1 boxes) of the MHD own-point arrays: [0..2] the
+  // state buffers (nx, ny, nz*V), [3..17] the background arrays per layer
   bool tma = false;
-  int tma_ty = 8;           // tile height of the TMA kernel (8 or 6)
   CUtensorMap tmaps_ty[18];
   // device bookkeeping
   int *d_err = nullptr;
@@ -210,11 +209,8 @@ struct Handle {
   unsigned int *d_counter = nullptr;
   int max_stage_blocks = 0;
 
-  // stage launch geometry; mhd_kernel 5: the shared-body interior/general
-  // kernel pair (default); 3: the earlier two-role kernel, 4: its TMA
-  // variant (even nx) -- kept for A/B timing
+  // stage launch geometry (quiet tiles tx x ty; MHD tiles 32 x 8)
   int tx = 32, ty = 8, zchunk = 32;
-  int mhd_kernel = 5;
 
   // precision form (SPARC_FP32): FP32 state in fbuf (roles ra/rf1/rf2 as
   // for buf), the compensated-sum carry of the state, depth scales

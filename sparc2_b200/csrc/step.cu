@@ -215,15 +215,6 @@ __device__ __forceinline__ void shift(double (&w)[11], double v) {
   w[10] = v;
 }
 
-// value of layer k held in a window whose base is b
-__device__ __forceinline__ double wsel(const double (&w)[11], int off) {
-  double v = w[5];
-#pragma unroll
-  for (int m = 0; m < 11; ++m)
-    if (m == off) v = w[m];
-  return v;
-}
-
 // ------------------------------------------------ MP_QUIET_3D stage kernel
 // RHS.f90:18-175 fused with one RK stage of step.f90:26-61.
 template <int TX, int TY, int MODE, bool BG1D>
@@ -381,762 +372,11 @@ __global__ void __launch_bounds__(TX *TY)
   if (MODE == LAST) diag_reduce(S, ke, mr, mp);
 }
 
-// ------------------------------------ MP_MHD_3D, pipelined stage kernel
-// Shared-memory layout of the pipelined MHD kernels: every
-// array a layer needs is copied into shared memory with cp.async one layer
-// ahead (double buffer), so the loads of layer k+1 stream while layer k is
-// computed.  Per buffer: 10 halo slots over the cross-shaped tile (stage
-// fields vx vy vz p bx by bz and B0; the B0 slots become flux1..3 in place
-// once the layer has landed) and 24 own-point slots (stage rho, a[0..7],
-// 14 background arrays, p0).
-namespace pipe {
-// own slots
-constexpr int O_RHO = 0, O_A = 1, O_BG = 9, O_P0 = 23;
-// background order in the own slots (O_BG + n)
-enum { B_RED, B_SPONGE, B_RHO0, B_GRX, B_GRY, B_GRZ, B_C2R, B_GPX, B_GPY,
-       B_GPZ, B_RHOINV, B_CBX, B_CBY, B_CBZ, NBG };
-}  // namespace pipe
-
-__device__ __forceinline__ void cp_async8(double *dst, const double *src) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async16(double *dst, const double *src) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cp_commit() {
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-__device__ __forceinline__ void cp_wait1() {
-  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-}
-
-// ------------------------- MP_MHD_3D, two-role pipelined stage kernel
-// The pipelined layer tiles of k_stage_mhd_pipe, with each column served by
-// two warps-groups (threadIdx.z = role) so that a thread holds only three
-// z windows (66 FP64 registers) and the CTA keeps 16 warps resident:
-//   role 0: momentum (RHS.f90:570-580, 630-645); windows vz, p, bx;
-//           derivatives gpx gpy gpz dvzdz dybz dxbz dzbx dxby dybx
-//   role 1: continuity, pressure, induction (RHS.f90:548-568); windows
-//           flux1, flux2, by; derivatives dvxdx dvydy dxflux3 dxflux2
-//           dyflux3 dyflux1 dzflux1 dzflux2 dzby
-// dvzdz and dzby cross over through shared memory after their CPML
-// corrections.  Arithmetic and summation order follow RHS.f90 as in the
-// oracle (11-tap sums from the first tap, operand order of each term).
-namespace duo {
-constexpr int TX = 32, TY = 8, NC = TX * TY, NT = 2 * NC;
-constexpr int HX = TX + 10, HY = TY + 10, HS = HX * HY;
-constexpr int NH = 10, NO = 24;
-constexpr int BUF = NH * HS + NO * NC;
-constexpr int XCH = 3 * NC;                       // exchange slots
-constexpr size_t SMEM = (2 * BUF + XCH) * sizeof(double);
-}  // namespace duo
-
-template <int MODE>
-__global__ void __launch_bounds__(duo::NT, 1)
-    k_stage_mhd_duo(const SimDev S, const double *__restrict__ a,
-                    const double *__restrict__ tin, double *__restrict__ so,
-                    double beta, double bnext, int zchunk) {
-  using namespace duo;
-  using pipe::O_RHO;
-  using pipe::O_A;
-  using pipe::O_BG;
-  using pipe::O_P0;
-  extern __shared__ double smem[];
-  __shared__ const double *optr[NO];
-  const int tx = threadIdx.x, ty = threadIdx.y, role = threadIdx.z;
-  const int tid = (role * TY + ty) * TX + tx, cid = ty * TX + tx;
-  const int nx = S.nx, ny = S.ny, nz = S.nz;
-  const long long N = S.N, NXY = (long long)nx * ny;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-  const int i = x0 + tx, j = y0 + ty;
-  const bool act = i < nx && j < ny;
-  const bool per = S.periodic;
-  const int k0 = blockIdx.z * zchunk, k1 = min(nz, k0 + zchunk);
-  const long long col = (long long)j * nx + i;
-  const long long it = *S.iter;
-  const double dt = S.deltat;
-  const int xo = tile_origin(x0, TX, nx, per), yo = tile_origin(y0, TY, ny, per);
-  const int cx0 = x0 - xo, cy0 = y0 - yo;
-  const int ry = cy0 + ty, rx = cx0 + tx;
-  const bool vec2 = (nx & 1) == 0;
-  if (tid == 0) {
-    optr[O_RHO] = tin;
-    for (int l = 0; l < 8; ++l) optr[O_A + l] = a + l * N;
-    optr[O_BG + pipe::B_RED] = S.red;    optr[O_BG + pipe::B_SPONGE] = S.sponge;
-    optr[O_BG + pipe::B_RHO0] = S.rho0;  optr[O_BG + pipe::B_GRX] = S.grx;
-    optr[O_BG + pipe::B_GRY] = S.gry;    optr[O_BG + pipe::B_GRZ] = S.grz;
-    optr[O_BG + pipe::B_C2R] = S.c2rho0; optr[O_BG + pipe::B_GPX] = S.gpx;
-    optr[O_BG + pipe::B_GPY] = S.gpy;    optr[O_BG + pipe::B_GPZ] = S.gpz;
-    optr[O_BG + pipe::B_RHOINV] = S.rhoinv;
-    optr[O_BG + pipe::B_CBX] = S.cbx;    optr[O_BG + pipe::B_CBY] = S.cby;
-    optr[O_BG + pipe::B_CBZ] = S.cbz;
-    optr[O_P0] = S.p0;
-  }
-  __syncthreads();
-  auto H = [&](int b, int slot, int ly, int lx) -> double & {
-    return smem[b * BUF + (slot * HY + ly) * HX + lx];
-  };
-  auto O = [&](int b, int slot) -> double & {
-    return smem[b * BUF + NH * HS + slot * NC + cid];
-  };
-  double *X = smem + 2 * BUF;  // [0] dvzdz, [1] dzby, [2] |v_new|^2
-  auto own_active = [&](int slot) -> bool {
-    if (slot >= O_A && slot < O_BG) return MODE != FIRST;
-    if (slot == O_P0) return MODE == LAST;
-    return true;
-  };
-  auto issue = [&](int k, int b) {
-    const long long kb = (long long)k * NXY;
-    for (int t = tid; t < HS; t += NT) {
-      const int ly = t / HX, lx = t - ly * HX;
-      const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
-      if (!inx && !iny) continue;
-      int gx = xo + lx, gy = yo + ly;
-      if (per) {
-        gx = wrapi(gx, nx);
-        gy = wrapi(gy, ny);
-      } else if (gx < 0 || gx >= nx || gy < 0 || gy >= ny) {
-        continue;
-      }
-      const long long id = kb + (long long)gy * nx + gx;
-#pragma unroll
-      for (int sl = 0; sl < 7; ++sl) cp_async8(&H(b, sl, ly, lx), tin + (sl + 1) * N + id);
-      cp_async8(&H(b, 7, ly, lx), S.box + id);
-      cp_async8(&H(b, 8, ly, lx), S.boy + id);
-      cp_async8(&H(b, 9, ly, lx), S.boz + id);
-    }
-    double *ob = smem + b * BUF + NH * HS;
-    if (vec2) {
-      constexpr int PAIRS = NC / 2;
-      for (int t = tid; t < NO * PAIRS; t += NT) {
-        const int slot = t / PAIRS, rem = t - slot * PAIRS;
-        if (!own_active(slot)) continue;
-        const int r = rem / (TX / 2), c = 2 * (rem - r * (TX / 2));
-        const int gx = x0 + c, gy = y0 + r;
-        if (gx >= nx || gy >= ny) continue;
-        cp_async16(ob + slot * NC + r * TX + c, optr[slot] + kb + (long long)gy * nx + gx);
-      }
-    } else {
-      for (int t = tid; t < NO * NC; t += NT) {
-        const int slot = t / NC, rem = t - slot * NC;
-        if (!own_active(slot)) continue;
-        const int r = rem / TX, c = rem - r * TX;
-        const int gx = x0 + c, gy = y0 + r;
-        if (gx >= nx || gy >= ny) continue;
-        cp_async8(ob + slot * NC + r * TX + c, optr[slot] + kb + (long long)gy * nx + gx);
-      }
-    }
-    cp_commit();
-  };
-
-  // role 0 windows: vz, p, bx ; role 1 windows: flux1, flux2, by
-  double w0[11], w1[11], w2[11];
-  auto head = [&](int kk, double &v0, double &v1, double &v2) {
-    const long long id = (long long)kk * NXY + col;
-    if (role == 0) {
-      v0 = __ldg(tin + 3 * N + id);
-      v1 = __ldg(tin + 4 * N + id);
-      v2 = __ldg(tin + 5 * N + id);
-    } else {
-      const double vx_ = __ldg(tin + N + id), vy_ = __ldg(tin + 2 * N + id),
-                   vz_ = __ldg(tin + 3 * N + id);
-      const double ox = __ldg(S.box + id), oy = __ldg(S.boy + id),
-                   oz = __ldg(S.boz + id);
-      v0 = -vz_ * oy + vy_ * oz;       // flux1
-      v1 = -vx_ * oz + vz_ * ox;       // flux2
-      v2 = __ldg(tin + 6 * N + id);    // by
-    }
-  };
-  issue(k0, 0);
-  const int b0 = min(k0 - 5, nz - 11);
-#pragma unroll
-  for (int m = 0; m < 11; ++m) {
-    const int kk = b0 + m;
-    if (act && kk >= 0) head(kk, w0[m], w1[m], w2[m]);
-    else w0[m] = w1[m] = w2[m] = 0.0;
-  }
-  double h0 = 0, h1 = 0, h2 = 0;
-  double ke = 0.0, mr = 1e300, mp = 1e300;
-
-  for (int k = k0; k < k1; ++k) {
-    const int b = (k - k0) & 1;
-    if (k > k0 && k <= nz - 6) {
-      shift(w0, h0); shift(w1, h1); shift(w2, h2);
-    }
-    if (k + 1 < k1) issue(k + 1, b ^ 1);
-    else cp_commit();
-    cp_wait1();
-    __syncthreads();
-    const double ox = H(b, 7, ry, rx), oy = H(b, 8, ry, rx), oz = H(b, 9, ry, rx);
-    __syncthreads();
-    for (int t = tid; t < HS; t += NT) {
-      const int ly = t / HX, lx = t - ly * HX;
-      const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
-      if (!inx && !iny) continue;
-      const double vx_ = H(b, 0, ly, lx), vy_ = H(b, 1, ly, lx), vz_ = H(b, 2, ly, lx);
-      const double bx0 = H(b, 7, ly, lx), by0 = H(b, 8, ly, lx), bz0 = H(b, 9, ly, lx);
-      H(b, 7, ly, lx) = -vz_ * by0 + vy_ * bz0;
-      H(b, 8, ly, lx) = -vx_ * bz0 + vz_ * bx0;
-      H(b, 9, ly, lx) = -vy_ * bx0 + vx_ * by0;
-    }
-    __syncthreads();
-    const long long id = (long long)k * NXY + col;
-    const double szk = __ldg(S.stretch + k);
-    auto DX = [&](int slot) {
-      return dxy(i, nx, per, S.stretchx, [&](int g) { return H(b, slot, ry, g - xo); });
-    };
-    auto DY = [&](int slot) {
-      return dxy(j, ny, per, S.stretchy, [&](int g) { return H(b, slot, g - yo, rx); });
-    };
-    const bool zpml = S.zb.on && (k < S.zb.np || k >= nz - S.zt.np);
-    const bool zbot = k < S.zb.np;
-    const FaceDev &FZ = zbot ? S.zb : S.zt;
-    const int kl = zbot ? k : k - (nz - S.zt.np);
-    const long long fz = (long long)kl * NXY + col;
-    const bool xpml = S.xb.on && act && (i < S.xb.np || i >= nx - S.xt.np);
-    const bool xbot = i < S.xb.np;
-    const FaceDev &FX = xbot ? S.xb : S.xt;
-    const int il = xbot ? i : i - (nx - S.xt.np);
-    const long long fx = il + (long long)FX.np * (j + (long long)ny * k);
-    const bool ypml = S.xb.on && act && (j < S.yb.np || j >= ny - S.yt.np);
-    const bool ybot = j < S.yb.np;
-    const FaceDev &FY = ybot ? S.yb : S.yt;
-    const int jl = ybot ? j : j - (ny - S.yt.np);
-    const long long fy = i + (long long)nx * (jl + (long long)FY.np * k);
-    const bool zero = k == 0 || k == nz - 1 ||
-                      (!per && (i == 0 || i == nx - 1 || j == 0 || j == ny - 1));
-    // halo slots: 0 vx, 1 vy, 2 vz, 3 p, 4 bx, 5 by, 6 bz, 7-9 flux1..3
-    // phase A: the role's nine derivatives with their CPML corrections.
-    // role 0: d0 gpx d1 gpy d2 gpz d3 dvzdz d4 dybz d5 dxbz d6 dzbx d7 dxby d8 dybx
-    // role 1: d0 dvxdx d1 dvydy d2 dxflux3 d3 dxflux2 d4 dyflux3 d5 dyflux1
-    //         d6 dzflux1 d7 dzflux2 d8 dzby
-    double d0 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0, d6 = 0, d7 = 0, d8 = 0;
-    if (act) {
-      if (role == 0) {
-        d0 = DX(3); d5 = DX(6); d7 = DX(5);
-        d1 = DY(3); d4 = DY(6); d8 = DY(4);
-        d3 = dz(w0, k, nz, szk); d2 = dz(w1, k, nz, szk); d6 = dz(w2, k, nz, szk);
-        if (zpml) {
-          cpml<MODE>(FZ, fz, kl, 1, beta, dt, d2);
-          cpml<MODE>(FZ, fz, kl, 0, beta, dt, d3);
-          cpml<MODE>(FZ, fz, kl, 2, beta, dt, d6);
-        }
-        if (xpml) {
-          cpml<MODE>(FX, fx, il, 1, beta, dt, d0);
-          cpml<MODE>(FX, fx, il, 3, beta, dt, d5);
-          cpml<MODE>(FX, fx, il, 2, beta, dt, d7);
-        }
-        if (ypml) {
-          cpml<MODE>(FY, fy, jl, 1, beta, dt, d1);
-          cpml<MODE>(FY, fy, jl, 3, beta, dt, d4);
-          cpml<MODE>(FY, fy, jl, 2, beta, dt, d8);
-        }
-        X[cid] = d3;          // dvzdz for role 1
-      } else {
-        d0 = DX(0); d2 = DX(9); d3 = DX(8);
-        d1 = DY(1); d4 = DY(9); d5 = DY(7);
-        d6 = dz(w0, k, nz, szk); d7 = dz(w1, k, nz, szk); d8 = dz(w2, k, nz, szk);
-        if (zpml) {
-          cpml<MODE>(FZ, fz, kl, 4, beta, dt, d7);
-          cpml<MODE>(FZ, fz, kl, 5, beta, dt, d6);
-          cpml<MODE>(FZ, fz, kl, 3, beta, dt, d8);
-        }
-        if (xpml) {
-          cpml<MODE>(FX, fx, il, 0, beta, dt, d0);
-          cpml<MODE>(FX, fx, il, 4, beta, dt, d2);
-          cpml<MODE>(FX, fx, il, 5, beta, dt, d3);
-        }
-        if (ypml) {
-          cpml<MODE>(FY, fy, jl, 0, beta, dt, d1);
-          cpml<MODE>(FY, fy, jl, 4, beta, dt, d4);
-          cpml<MODE>(FY, fy, jl, 5, beta, dt, d5);
-        }
-        X[NC + cid] = d8;     // dzby for role 0
-      }
-    }
-    __syncthreads();
-    // phase B: right-hand sides and the stage (or final) update
-    double an_rho = 0.0;
-    if (act) {
-      const double rho = O(b, O_RHO), vx = H(b, 0, ry, rx), vy = H(b, 1, ry, rx),
-                   vz = H(b, 2, ry, rx);
-      const double red = O(b, O_BG + pipe::B_RED), sg = O(b, O_BG + pipe::B_SPONGE);
-      if (role == 0) {
-        const double bx = H(b, 4, ry, rx), by = H(b, 5, ry, rx), bz = H(b, 6, ry, rx);
-        const double dzby = X[NC + cid];
-        const double cbx = d4 - dzby, cby = -d5 + d6, cbz = d7 - d8;
-        const double c1 = cby * oz - cbz * oy, c2 = ox * cbz - cbx * oz,
-                     c3 = cbx * oy - cby * ox;
-        const double ri = O(b, O_BG + pipe::B_RHOINV);
-        double vxr = -ri * (d0 - (c1 * red)) - sg * vx;
-        double vyr = -ri * (d1 - (c2 * red)) - sg * vy;
-        double vzr = -ri * (d2 - (c3 * red)) - sg * vz;
-        const double qx = O(b, O_BG + pipe::B_CBX), qy = O(b, O_BG + pipe::B_CBY),
-                     qz = O(b, O_BG + pipe::B_CBZ);
-        const double e1 = qy * bz - qz * by, e2 = bx * qz - qx * bz,
-                     e3 = qx * by - qy * bx;
-        vxr = vxr + ri * e1 * red;
-        vyr = vyr + ri * e2 * red;
-        vzr = vzr + ri * e3 * red;
-        const int gc = S.colx[i] + S.bxdim * S.coly[j];
-        vzr = vzr - ri * rho * __ldg(S.gblk + (long long)gc * nz + k);
-        if (S.frc.kind != SPARC_SRC_NONE) {
-          const double frc = forcing_at(S, it, pulse_time(S, it), i, j, k);
-          if (S.frc.dir == 1) vxr = vxr + frc;
-          else if (S.frc.dir == 2) vyr = vyr + frc;
-          else vzr = vzr + frc;
-        }
-        const double R[3] = {vxr, vyr, vzr};
-        double vsq = 0.0;
-#pragma unroll
-        for (int l = 1; l < 4; ++l) {
-          const double av = MODE == FIRST ? H(b, l - 1, ry, rx) : O(b, O_A + l);
-          const double an = zero ? av : av + (MODE == LAST ? dt : bnext) * R[l - 1];
-          so[l * N + id] = an;
-          vsq = l == 1 ? an * an : vsq + an * an;
-        }
-        if (MODE == LAST) X[2 * NC + cid] = vsq;
-      } else {
-        const double p = H(b, 3, ry, rx);
-        const double dvzdz = X[cid];
-        double R[5];  // rho, p, bx, by, bz
-        R[2] = red * (d4 - d7);
-        R[3] = red * (d6 - d2);
-        R[4] = red * (d3 - d5);
-        const double div = d0 + d1 + dvzdz;
-        const double r0 = O(b, O_BG + pipe::B_RHO0);
-        R[0] = -O(b, O_BG + pipe::B_GRX) * vx - O(b, O_BG + pipe::B_GRY) * vy -
-               O(b, O_BG + pipe::B_GRZ) * vz - r0 * div - sg * rho;
-        R[1] = -O(b, O_BG + pipe::B_C2R) * div - vx * O(b, O_BG + pipe::B_GPX) -
-               vy * O(b, O_BG + pipe::B_GPY) - vz * O(b, O_BG + pipe::B_GPZ) - sg * p;
-#pragma unroll
-        for (int q = 0; q < 5; ++q) {
-          const int l = q == 0 ? 0 : q + 3;   // fields rho, p(4), bx(5), by(6), bz(7)
-          const int ls = q == 1 ? 4 : l;
-          const double av = MODE == FIRST ? (ls == 0 ? rho : H(b, ls - 1, ry, rx))
-                                          : O(b, O_A + ls);
-          const double an = zero ? av : av + (MODE == LAST ? dt : bnext) * R[q];
-          so[ls * N + id] = an;
-          if (q == 0) an_rho = an;
-        }
-        if (MODE == LAST) {
-          mr = fmin(mr, rho + r0);
-          mp = fmin(mp, p + O(b, O_P0));
-        }
-      }
-    }
-    if (MODE == LAST) {
-      __syncthreads();
-      if (act && role == 1) {  // KE density of driver.f90:161 on a_new
-        const double r0 = O(b, O_BG + pipe::B_RHO0);
-        const double m = (r0 + an_rho) * X[2 * NC + cid] / 2.0;
-        ke += m * m;
-      }
-    }
-    if (act && k + 1 < k1 && k + 1 <= nz - 6) head(k + 6, h0, h1, h2);
-    __syncthreads();
-  }
-  if (MODE == LAST) diag_reduce(S, ke, mr, mp);
-}
-
-// --------------------- MP_MHD_3D, two-role stage kernel with TMA loads
-// k_stage_mhd_duo with the 24 own-point arrays of a layer fetched by TMA
-// (one elected thread, 3-D tensor maps, 32x8 boxes, one mbarrier per
-// buffer) instead of per-thread copies, halo copy addresses computed once
-// per CTA, and branch-free centred x/y stencils for interior columns.
-// Shared memory per buffer: 24 own slots (2 KB each, 128-B aligned) then
-// the 10 halo slots.  Needs an even nx (16-B row strides).
-struct TmaSet {
-  CUtensorMap m[18];
-};
-
-namespace tmak {
-constexpr long long WAIT_LIMIT = 1LL << 26;
-}  // namespace tmak
-// geometry of the TMA kernel for a tile height TY (tile 32 x TY columns,
-// two roles -> 64*TY threads)
-template <int TY_>
-struct TmaGeo {
-  static constexpr int TX = 32, TY = TY_, NC = TX * TY, NT = 2 * NC;
-  static constexpr int HX = TX + 10, HY = TY + 10, HS = HX * HY;
-  static constexpr int NH = 10, NO = 24;
-  static constexpr int BUF = ((NO * NC + NH * HS) + 15) / 16 * 16;  // 128-B multiple
-  static constexpr int XCH = 3 * NC;
-  static constexpr size_t SMEM = (2 * (size_t)BUF + XCH) * sizeof(double) + 128;
-};
-
-__device__ __forceinline__ unsigned sm_addr(const void *p) {
-  return (unsigned)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sm_addr(bar)), "r"(count)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sm_addr(bar)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void tma_load_3d(double *dst, const CUtensorMap *map, int x,
-                                            int y, int z, unsigned long long *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(sm_addr(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(z), "r"(sm_addr(bar))
-      : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(sm_addr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// bounded wait: false (and the error flag set) if the copies never land
-__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity,
-                                          int *err) {
-  for (long long n = 0; n < tmak::WAIT_LIMIT; ++n)
-    if (mbar_try_wait(bar, parity)) return true;
-  atomicExch(err, 1);
-  return false;
-}
-
-// centred 11-point sum along a shared-memory line with element stride st
-__device__ __forceinline__ double csum(const double *p, int st) {
-  double s = 0.0;
-#pragma unroll
-  for (int m = 0; m < 11; ++m) s += p[m * st] * c_dp[5][m];
-  return s;
-}
-
-template <int MODE, int TYV>
-__global__ void __launch_bounds__(TmaGeo<TYV>::NT, 1)
-    k_stage_mhd_tma(const SimDev S, const __grid_constant__ TmaSet T,
-                    const double *__restrict__ a, const double *__restrict__ tin,
-                    double *__restrict__ so, double beta, double bnext,
-                    int zchunk, int mt, int ma) {
-  // 32-bit indexing throughout (the launcher checks V*N < 2^31)
-  using G = TmaGeo<TYV>;
-  constexpr int TX = G::TX, TY = G::TY, NC = G::NC, NT = G::NT, HX = G::HX,
-                HS = G::HS, NO = G::NO, BUF = G::BUF;
-  using pipe::O_RHO;
-  using pipe::O_A;
-  using pipe::O_BG;
-  using pipe::O_P0;
-  extern __shared__ __align__(1024) double smem_raw[];
-  __shared__ unsigned long long bar[2];
-  const int tx = threadIdx.x, ty = threadIdx.y, role = threadIdx.z;
-  const int tid = (role * TY + ty) * TX + tx, cid = ty * TX + tx;
-  double *smem = (double *)(((size_t)smem_raw + 127) & ~(size_t)127);
-  if (sm_addr(smem) & 127u) {
-    if (tid == 0) atomicExch(S.err, 2);
-    return;
-  }
-  const int nx = S.nx, ny = S.ny, nz = S.nz;
-  const int N = (int)S.N, NXY = nx * ny;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-  const int i = x0 + tx, j = y0 + ty;
-  const bool act = i < nx && j < ny;
-  const bool per = S.periodic;
-  const int k0 = blockIdx.z * zchunk, k1 = min(nz, k0 + zchunk);
-  const int col = j * nx + i;
-  const int xo = tile_origin(x0, TX, nx, per), yo = tile_origin(y0, TY, ny, per);
-  const int ry = y0 - yo + ty, rx = x0 - xo + tx;
-  const int own = ry * HX + rx;
-  if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  auto O = [&](int b, int slot) -> double { return smem[b * BUF + slot * NC + cid]; };
-  auto Hp = [&](int b, int slot) -> double * { return smem + b * BUF + NO * NC + slot * HS; };
-  double *X = smem + 2 * BUF;
-  // this thread's halo positions (smem index, global xy offset), or -1
-  int hs0 = -1, hs1 = -1, ho0 = 0, ho1 = 0;
-  {
-    const int cx0 = x0 - xo, cy0 = y0 - yo;
-    auto pos = [&](int t, int &hs, int &ho) {
-      if (t >= HS) return;
-      const int ly = t / HX, lx = t - ly * HX;
-      const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
-      if (!inx && !iny) return;
-      int gx = xo + lx, gy = yo + ly;
-      if (per) {
-        gx = wrapi(gx, nx);
-        gy = wrapi(gy, ny);
-      } else if (gx < 0 || gx >= nx || gy < 0 || gy >= ny) {
-        return;
-      }
-      hs = t;
-      ho = gy * nx + gx;
-    };
-    pos(tid, hs0, ho0);
-    pos(tid + NT, hs1, ho1);
-  }
-  const unsigned own_bytes =
-      (MODE == FIRST ? 15u : (MODE == MID ? 23u : 24u)) * NC * (unsigned)sizeof(double);
-  auto issue = [&](int k, int b) {
-    const int kb = k * NXY;
-    if (hs0 >= 0) {
-      double *h = Hp(b, 0) + hs0;
-      const int id = kb + ho0;
-#pragma unroll
-      for (int sl = 0; sl < 7; ++sl) cp_async8(h + sl * HS, tin + (sl + 1) * N + id);
-      cp_async8(h + 7 * HS, S.box + id);
-      cp_async8(h + 8 * HS, S.boy + id);
-      cp_async8(h + 9 * HS, S.boz + id);
-    }
-    if (hs1 >= 0) {
-      double *h = Hp(b, 0) + hs1;
-      const int id = kb + ho1;
-#pragma unroll
-      for (int sl = 0; sl < 7; ++sl) cp_async8(h + sl * HS, tin + (sl + 1) * N + id);
-      cp_async8(h + 7 * HS, S.box + id);
-      cp_async8(h + 8 * HS, S.boy + id);
-      cp_async8(h + 9 * HS, S.boz + id);
-    }
-    cp_commit();
-    if (tid == 0) {
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_expect_tx(&bar[b], own_bytes);
-      double *ob = smem + b * BUF;
-      tma_load_3d(ob + O_RHO * NC, &T.m[mt], x0, y0, k, &bar[b]);
-      if (MODE != FIRST)
-        for (int l = 0; l < 8; ++l)
-          tma_load_3d(ob + (O_A + l) * NC, &T.m[ma], x0, y0, l * nz + k, &bar[b]);
-      for (int n = 0; n < 14; ++n)
-        tma_load_3d(ob + (O_BG + n) * NC, &T.m[3 + n], x0, y0, k, &bar[b]);
-      if (MODE == LAST) tma_load_3d(ob + O_P0 * NC, &T.m[17], x0, y0, k, &bar[b]);
-    }
-  };
-  // role 0 windows vz, p, bx; role 1 windows flux1, flux2, by
-  double w0[11], w1[11], w2[11];
-  auto head = [&](int kk, double &v0, double &v1, double &v2) {
-    const int id = kk * NXY + col;
-    if (role == 0) {
-      v0 = __ldg(tin + 3 * N + id);
-      v1 = __ldg(tin + 4 * N + id);
-      v2 = __ldg(tin + 5 * N + id);
-    } else {
-      const double vx_ = __ldg(tin + N + id), vy_ = __ldg(tin + 2 * N + id),
-                   vz_ = __ldg(tin + 3 * N + id);
-      const double ox = __ldg(S.box + id), oy = __ldg(S.boy + id),
-                   oz = __ldg(S.boz + id);
-      v0 = -vz_ * oy + vy_ * oz;
-      v1 = -vx_ * oz + vz_ * ox;
-      v2 = __ldg(tin + 6 * N + id);
-    }
-  };
-  issue(k0, 0);
-  {
-    const int b0 = min(k0 - 5, nz - 11);
-#pragma unroll
-    for (int m = 0; m < 11; ++m) {
-      const int kk = b0 + m;
-      if (act && kk >= 0) head(kk, w0[m], w1[m], w2[m]);
-      else w0[m] = w1[m] = w2[m] = 0.0;
-    }
-  }
-  double ke = 0.0, mr = 1e300, mp = 1e300;
-  unsigned phase = 0;
-  bool ok = true;
-
-  for (int k = k0; k < k1; ++k) {
-    const int b = (k - k0) & 1;
-    double h0 = 0, h1 = 0, h2 = 0;
-    const bool sh = k > k0 && k <= nz - 6;
-    if (sh && act) head(k + 5, h0, h1, h2);   // in flight during the waits
-    if (k + 1 < k1) issue(k + 1, b ^ 1);
-    else cp_commit();
-    cp_wait1();
-    ok = mbar_wait(&bar[b], (phase >> b) & 1u, S.err);
-    phase ^= 1u << b;
-    if (!__syncthreads_and(ok)) { ok = false; break; }
-    if (sh) { shift(w0, h0); shift(w1, h1); shift(w2, h2); }
-    double *H7 = Hp(b, 7), *H8 = Hp(b, 8), *H9 = Hp(b, 9);
-    const double ox = H7[own], oy = H8[own], oz = H9[own];
-    __syncthreads();
-    {
-      const double *H0 = Hp(b, 0), *H1 = Hp(b, 1), *H2 = Hp(b, 2);
-      const int cx0 = x0 - xo, cy0 = y0 - yo;
-      for (int t = tid; t < HS; t += NT) {
-        const int ly = t / HX, lx = t - ly * HX;
-        const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
-        if (!inx && !iny) continue;
-        const double vx_ = H0[t], vy_ = H1[t], vz_ = H2[t];
-        const double bx0 = H7[t], by0 = H8[t], bz0 = H9[t];
-        H7[t] = -vz_ * by0 + vy_ * bz0;
-        H8[t] = -vx_ * bz0 + vz_ * bx0;
-        H9[t] = -vy_ * bx0 + vx_ * by0;
-      }
-    }
-    __syncthreads();
-    const int id = k * NXY + col;
-    const double szk = __ldg(S.stretch + k);
-    const double dt = S.deltat;
-    auto DX = [&](int slot) {
-      const double *row = Hp(b, slot) + ry * HX;
-      if (per || (i >= 5 && i < nx - 5)) return S.stretchx * csum(row + (i - 5 - xo), 1);
-      return dxy(i, nx, per, S.stretchx, [&](int g) { return row[g - xo]; });
-    };
-    auto DY = [&](int slot) {
-      const double *colp = Hp(b, slot) + rx;
-      if (per || (j >= 5 && j < ny - 5)) return S.stretchy * csum(colp + (j - 5 - yo) * HX, HX);
-      return dxy(j, ny, per, S.stretchy, [&](int g) { return colp[(g - yo) * HX]; });
-    };
-    const bool zpml = S.zb.on && (k < S.zb.np || k >= nz - S.zt.np);
-    const bool xpml = S.xb.on && act && (i < S.xb.np || i >= nx - S.xt.np);
-    const bool ypml = S.xb.on && act && (j < S.yb.np || j >= ny - S.yt.np);
-    // CPML correction of derivative d with auxiliary slot `slot` on the
-    // z, x or y face this point lies in (RHS.f90:424-546)
-    auto pz = [&](int slot, double &d) {
-      const bool bot = k < S.zb.np;
-      const FaceDev &F = bot ? S.zb : S.zt;
-      const int kl = bot ? k : k - (nz - S.zt.np);
-      cpml<MODE>(F, (long long)kl * NXY + col, kl, slot, beta, dt, d);
-    };
-    auto px = [&](int slot, double &d) {
-      const bool bot = i < S.xb.np;
-      const FaceDev &F = bot ? S.xb : S.xt;
-      const int il = bot ? i : i - (nx - S.xt.np);
-      cpml<MODE>(F, il + (long long)F.np * (j + (long long)ny * k), il, slot, beta, dt, d);
-    };
-    auto py = [&](int slot, double &d) {
-      const bool bot = j < S.yb.np;
-      const FaceDev &F = bot ? S.yb : S.yt;
-      const int jl = bot ? j : j - (ny - S.yt.np);
-      cpml<MODE>(F, i + (long long)nx * (jl + (long long)F.np * k), jl, slot, beta, dt, d);
-    };
-    auto Hv = [&](int slot) { return Hp(b, slot)[own]; };
-    double d0 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0, d6 = 0, d7 = 0, d8 = 0;
-    if (act) {
-      if (role == 0) {
-        d0 = DX(3); d5 = DX(6); d7 = DX(5);
-        d1 = DY(3); d4 = DY(6); d8 = DY(4);
-        d3 = dz(w0, k, nz, szk); d2 = dz(w1, k, nz, szk); d6 = dz(w2, k, nz, szk);
-        if (zpml) { pz(1, d2); pz(0, d3); pz(2, d6); }
-        if (xpml) { px(1, d0); px(3, d5); px(2, d7); }
-        if (ypml) { py(1, d1); py(3, d4); py(2, d8); }
-        X[cid] = d3;
-      } else {
-        d0 = DX(0); d2 = DX(9); d3 = DX(8);
-        d1 = DY(1); d4 = DY(9); d5 = DY(7);
-        d6 = dz(w0, k, nz, szk); d7 = dz(w1, k, nz, szk); d8 = dz(w2, k, nz, szk);
-        if (zpml) { pz(4, d7); pz(5, d6); pz(3, d8); }
-        if (xpml) { px(0, d0); px(4, d2); px(5, d3); }
-        if (ypml) { py(0, d1); py(4, d4); py(5, d5); }
-        X[NC + cid] = d8;
-      }
-    }
-    __syncthreads();
-    double an_rho = 0.0;
-    if (act) {
-      const bool zero = k == 0 || k == nz - 1 ||
-                        (!per && (i == 0 || i == nx - 1 || j == 0 || j == ny - 1));
-      const double fac = MODE == LAST ? dt : bnext;
-      const double rho = O(b, O_RHO), vx = Hv(0), vy = Hv(1), vz = Hv(2);
-      const double red = O(b, O_BG + pipe::B_RED), sg = O(b, O_BG + pipe::B_SPONGE);
-      if (role == 0) {
-        const double dzby = X[NC + cid];
-        const double cbx = d4 - dzby, cby = -d5 + d6, cbz = d7 - d8;
-        const double c1 = cby * oz - cbz * oy, c2 = ox * cbz - cbx * oz,
-                     c3 = cbx * oy - cby * ox;
-        const double ri = O(b, O_BG + pipe::B_RHOINV);
-        double vxr = -ri * (d0 - (c1 * red)) - sg * vx;
-        double vyr = -ri * (d1 - (c2 * red)) - sg * vy;
-        double vzr = -ri * (d2 - (c3 * red)) - sg * vz;
-        const double bx = Hv(4), by = Hv(5), bz = Hv(6);
-        const double qx = O(b, O_BG + pipe::B_CBX), qy = O(b, O_BG + pipe::B_CBY),
-                     qz = O(b, O_BG + pipe::B_CBZ);
-        const double e1 = qy * bz - qz * by, e2 = bx * qz - qx * bz,
-                     e3 = qx * by - qy * bx;
-        vxr = vxr + ri * e1 * red;
-        vyr = vyr + ri * e2 * red;
-        vzr = vzr + ri * e3 * red;
-        const int gc = S.colx[i] + S.bxdim * S.coly[j];
-        vzr = vzr - ri * rho * __ldg(S.gblk + gc * nz + k);
-        if (S.frc.kind != SPARC_SRC_NONE) {
-          const long long it = *S.iter;
-          const double frc = forcing_at(S, it, pulse_time(S, it), i, j, k);
-          if (S.frc.dir == 1) vxr = vxr + frc;
-          else if (S.frc.dir == 2) vyr = vyr + frc;
-          else vzr = vzr + frc;
-        }
-        const double a1 = MODE == FIRST ? vx : O(b, O_A + 1);
-        const double a2 = MODE == FIRST ? vy : O(b, O_A + 2);
-        const double a3 = MODE == FIRST ? vz : O(b, O_A + 3);
-        const double n1 = zero ? a1 : a1 + fac * vxr;
-        const double n2 = zero ? a2 : a2 + fac * vyr;
-        const double n3 = zero ? a3 : a3 + fac * vzr;
-        so[N + id] = n1;
-        so[2 * N + id] = n2;
-        so[3 * N + id] = n3;
-        if (MODE == LAST) X[2 * NC + cid] = n1 * n1 + n2 * n2 + n3 * n3;
-      } else {
-        const double p = Hv(3);
-        const double dvzdz = X[cid];
-        const double div = d0 + d1 + dvzdz;
-        const double r0 = O(b, O_BG + pipe::B_RHO0);
-        const double Rr = -O(b, O_BG + pipe::B_GRX) * vx - O(b, O_BG + pipe::B_GRY) * vy -
-                          O(b, O_BG + pipe::B_GRZ) * vz - r0 * div - sg * rho;
-        const double Rp = -O(b, O_BG + pipe::B_C2R) * div - vx * O(b, O_BG + pipe::B_GPX) -
-                          vy * O(b, O_BG + pipe::B_GPY) - vz * O(b, O_BG + pipe::B_GPZ) -
-                          sg * p;
-        const double Rbx = red * (d4 - d7), Rby = red * (d6 - d2), Rbz = red * (d3 - d5);
-        const double ar = MODE == FIRST ? rho : O(b, O_A + 0);
-        const double ap = MODE == FIRST ? p : O(b, O_A + 4);
-        const double abx = MODE == FIRST ? Hv(4) : O(b, O_A + 5);
-        const double aby = MODE == FIRST ? Hv(5) : O(b, O_A + 6);
-        const double abz = MODE == FIRST ? Hv(6) : O(b, O_A + 7);
-        an_rho = zero ? ar : ar + fac * Rr;
-        so[id] = an_rho;
-        so[4 * N + id] = zero ? ap : ap + fac * Rp;
-        so[5 * N + id] = zero ? abx : abx + fac * Rbx;
-        so[6 * N + id] = zero ? aby : aby + fac * Rby;
-        so[7 * N + id] = zero ? abz : abz + fac * Rbz;
-        if (MODE == LAST) {
-          mr = fmin(mr, rho + r0);
-          mp = fmin(mp, p + O(b, O_P0));
-        }
-      }
-    }
-    if (MODE == LAST) {
-      __syncthreads();
-      if (act && role == 1) {  // KE density of driver.f90:161 on a_new
-        const double m = (O(b, O_BG + pipe::B_RHO0) + an_rho) * X[2 * NC + cid] / 2.0;
-        ke += m * m;
-      }
-    }
-    __syncthreads();
-  }
-  if (!ok) {
-    // a bounded wait gave up: drain (again bounded) what this CTA issued
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-    if (tid == 0) {
-      mbar_wait(&bar[0], phase & 1u, S.err);
-      mbar_wait(&bar[1], (phase >> 1) & 1u, S.err);
-    }
-    return;
-  }
-  if (MODE == LAST) diag_reduce(S, ke, mr, mp);
-}
-
-// ------------------------------------------------------- stage dispatch
 int stage_geometry(Handle *h) {
   // tile shape: (32, 8); the quiet kernel drops to (16, 8) on grids too
   // small to fill the GPU.  The MHD kernels always use (32, 8).
   h->tx = 32;
   h->ty = 8;
-  if (h->magnetic && !h->fp32 && h->mhd_kernel == 4 && (h->nx % 2) == 0)
-    h->ty = h->tma_ty;  // TMA tiles: 32 x tma_ty
   long long tiles = (long long)((h->nx + h->tx - 1) / h->tx) *
                     ((h->ny + h->ty - 1) / h->ty);
   if (tiles < 64 && !h->magnetic) {
@@ -1181,72 +421,6 @@ static int launch_quiet(Handle *h, const SimDev &S, int stage,
   return SPARC_OK;
 }
 
-static int launch_mhd_duo(Handle *h, const SimDev &S, int stage,
-                          const double *a, const double *tin, double *so,
-                          cudaStream_t s) {
-  using namespace duo;
-  dim3 blk(TX, TY, 2);
-  dim3 grd((h->nx + TX - 1) / TX, (h->ny + TY - 1) / TY,
-           (h->nz + h->zchunk - 1) / h->zchunk);
-  const double beta = h->betas[stage - 1];
-  const double bnext = stage < 5 ? h->betas[stage] : h->deltat;
-  const int mode = stage == 1 ? FIRST : (stage == 5 ? LAST : MID);
-  if (mode == FIRST) {
-    cudaFuncSetAttribute(k_stage_mhd_duo<FIRST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
-    k_stage_mhd_duo<FIRST><<<grd, blk, SMEM, s>>>(S, a, tin, so, beta, bnext, h->zchunk);
-  } else if (mode == MID) {
-    cudaFuncSetAttribute(k_stage_mhd_duo<MID>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
-    k_stage_mhd_duo<MID><<<grd, blk, SMEM, s>>>(S, a, tin, so, beta, bnext, h->zchunk);
-  } else {
-    cudaFuncSetAttribute(k_stage_mhd_duo<LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
-    k_stage_mhd_duo<LAST><<<grd, blk, SMEM, s>>>(S, a, tin, so, beta, bnext, h->zchunk);
-  }
-  return SPARC_OK;
-}
-
-template <int TYV>
-static int launch_mhd_tma_ty(Handle *h, const SimDev &S, int stage, const double *a,
-                             const double *tin, double *so, cudaStream_t s, int mt,
-                             int ma) {
-  using G = TmaGeo<TYV>;
-  TmaSet T;
-  for (int n = 0; n < 18; ++n) T.m[n] = h->tmaps_ty[n];
-  dim3 blk(G::TX, G::TY, 2);
-  dim3 grd((h->nx + G::TX - 1) / G::TX, (h->ny + G::TY - 1) / G::TY,
-           (h->nz + h->zchunk - 1) / h->zchunk);
-  const double beta = h->betas[stage - 1];
-  const double bnext = stage < 5 ? h->betas[stage] : h->deltat;
-  const int mode = stage == 1 ? FIRST : (stage == 5 ? LAST : MID);
-  const int sm = (int)G::SMEM;
-  if (mode == FIRST) {
-    cudaFuncSetAttribute(k_stage_mhd_tma<FIRST, TYV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    k_stage_mhd_tma<FIRST, TYV><<<grd, blk, G::SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt, ma);
-  } else if (mode == MID) {
-    cudaFuncSetAttribute(k_stage_mhd_tma<MID, TYV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    k_stage_mhd_tma<MID, TYV><<<grd, blk, G::SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt, ma);
-  } else {
-    cudaFuncSetAttribute(k_stage_mhd_tma<LAST, TYV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    k_stage_mhd_tma<LAST, TYV><<<grd, blk, G::SMEM, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt, ma);
-  }
-  return SPARC_OK;
-}
-
-static int launch_mhd_tma(Handle *h, const SimDev &S, int stage,
-                          const double *a, const double *tin, double *so,
-                          cudaStream_t s) {
-  int mt = -1, ma = -1;
-  for (int b = 0; b < 3; ++b) {
-    if (h->buf[b] == tin) mt = b;
-    if (h->buf[b] == a) ma = b;
-  }
-  if (mt < 0 || ma < 0) return SPARC_ERR_INVALID;
-  if ((long long)h->V * h->N >= (1LL << 31)) return SPARC_ERR_INVALID;
-  if (h->tma_ty == 6) return launch_mhd_tma_ty<6>(h, S, stage, a, tin, so, s, mt, ma);
-  return launch_mhd_tma_ty<8>(h, S, stage, a, tin, so, s, mt, ma);
-}
-
-// Tensor maps (3-D, FP64, 32x8x1 boxes) of the arrays the TMA kernel loads
-// per layer; needs 16-byte row strides, i.e. an even nx.
 int encode_tensor_maps(Handle *h) {
   h->tma = false;
   if (!h->magnetic || (h->nx & 1)) return SPARC_OK;
@@ -1264,7 +438,7 @@ int encode_tensor_maps(Handle *h) {
   auto one = [&](CUtensorMap *m, const double *base, unsigned long long depth) {
     cuuint64_t dims[3] = {(cuuint64_t)h->nx, (cuuint64_t)h->ny, (cuuint64_t)depth};
     cuuint64_t strides[2] = {(cuuint64_t)h->nx * 8, (cuuint64_t)h->nx * h->ny * 8};
-    cuuint32_t box[3] = {32, (cuuint32_t)h->tma_ty, 1};
+    cuuint32_t box[3] = {(cuuint32_t)mg::TX, (cuuint32_t)mg::TY, 1};
     cuuint32_t es[3] = {1, 1, 1};
     return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void *)base, dims, strides, box, es,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -1322,7 +496,7 @@ static int launch_mhd64(Handle *h, const SimDev &S, int stage, const double *a,
   const bool has_int = ix1 > ix0 && iy1 > iy0;
   dim3 gint(has_int ? ix1 - ix0 : 1, has_int ? iy1 - iy0 : 1, grd.z);
   const size_t sm = MhdBuf<double>::SMEM;
-  const bool tma = h->tma && h->tma_ty == mg::TY && h->allow_tma64;
+  const bool tma = h->tma && h->allow_tma64;
   int mt = -1, ma = -1;
   for (int b = 0; b < 3; ++b) {
     if (h->buf[b] == tin) mt = b;
@@ -1369,23 +543,9 @@ static int launch_mhd64(Handle *h, const SimDev &S, int stage, const double *a,
 int launch_stage(Handle *h, const SimDev &S, int stage, const double *a,
                  const double *tin, double *so, cudaStream_t s) {
   int r = SPARC_ERR_INVALID;
-  if (h->magnetic && h->mhd_kernel == 5) {
-    if (h->tx != 32 || h->ty != 8) return SPARC_ERR_INVALID;
-    r = launch_mhd64(h, S, stage, a, tin, so, s);
-    ++h->launches;
-    if (r == SPARC_OK && cudaGetLastError() != cudaSuccess) r = SPARC_ERR_CUDA;
-    return r;
-  }
-  if (h->magnetic && h->mhd_kernel == 4 && h->tma && h->tx == 32 &&
-      (long long)h->V * h->N < (1LL << 31)) {
-    r = launch_mhd_tma(h, S, stage, a, tin, so, s);
-    ++h->launches;
-    if (r == SPARC_OK && cudaGetLastError() != cudaSuccess) r = SPARC_ERR_CUDA;
-    return r;
-  }
   if (h->magnetic) {
     if (h->tx != 32 || h->ty != 8) return SPARC_ERR_INVALID;
-    r = launch_mhd_duo(h, S, stage, a, tin, so, s);
+    r = launch_mhd64(h, S, stage, a, tin, so, s);
     ++h->launches;
     if (r == SPARC_OK && cudaGetLastError() != cudaSuccess) r = SPARC_ERR_CUDA;
     return r;

@@ -26,7 +26,7 @@ UNITS = {
     "noalloc.cu": [],
     "serve.cu": [],
 }
-HEADERS = ["internal.h"]
+HEADERS = ["internal.h", "mhd_body.cuh"]
 
 
 def nvcc():

@@ -201,7 +201,7 @@ struct Handle {
   // TMA tensor maps (32x8x1 boxes) of the MHD own-point arrays: [0..2] the
   // state buffers (nx, ny, nz*V), [3..17] the background arrays per layer
   bool tma = false;
-  CUtensorMap tmaps_ty[18];
+  CUtensorMap tmaps_ty[24];
   // device bookkeeping
   int *d_err = nullptr;
   long long *d_iter = nullptr, *d_fail = nullptr;

@@ -435,10 +435,11 @@ int encode_tensor_maps(Handle *h) {
                           const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
                           const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
                           CUtensorMapL2promotion, CUtensorMapFloatOOBfill))fn;
-  auto one = [&](CUtensorMap *m, const double *base, unsigned long long depth) {
+  auto one = [&](CUtensorMap *m, const double *base, unsigned long long depth, bool halo = false) {
     cuuint64_t dims[3] = {(cuuint64_t)h->nx, (cuuint64_t)h->ny, (cuuint64_t)depth};
     cuuint64_t strides[2] = {(cuuint64_t)h->nx * 8, (cuuint64_t)h->nx * h->ny * 8};
-    cuuint32_t box[3] = {(cuuint32_t)mg::TX, (cuuint32_t)mg::TY, 1};
+    cuuint32_t box[3] = {(cuuint32_t)(halo ? MhdBuf<double, true>::HXL : mg::TX),
+                         (cuuint32_t)(halo ? mg::HY : mg::TY), 1};
     cuuint32_t es[3] = {1, 1, 1};
     return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void *)base, dims, strides, box, es,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -450,6 +451,10 @@ int encode_tensor_maps(Handle *h) {
   const double *bg[15] = {h->red, h->sponge, h->rho0, h->grx, h->gry, h->grz, h->c2rho0,
                           h->gpx, h->gpy, h->gpz, h->rhoinv, h->cbx, h->cby, h->cbz, h->p0};
   for (int n = 0; n < 15; ++n) ok = ok && bg[n] && one(&h->tmaps_ty[3 + n], bg[n], h->nz);
+  for (int b = 0; b < 3; ++b)
+    ok = ok && one(&h->tmaps_ty[18 + b], h->buf[b], (unsigned long long)h->nz * h->V, true);
+  const double *b0[3] = {h->box, h->boy, h->boz};
+  for (int n = 0; n < 3; ++n) ok = ok && b0[n] && one(&h->tmaps_ty[21 + n], b0[n], h->nz, true);
   h->tma = ok;
   return SPARC_OK;
 }
@@ -495,8 +500,10 @@ static int launch_mhd64(Handle *h, const SimDev &S, int stage, const double *a,
   mhd_interior_rect(h->nx, h->ny, np, ix0, ix1, iy0, iy1);
   const bool has_int = ix1 > ix0 && iy1 > iy0;
   dim3 gint(has_int ? ix1 - ix0 : 1, has_int ? iy1 - iy0 : 1, grd.z);
-  const size_t sm = MhdBuf<double>::SMEM;
   const bool tma = h->tma && h->allow_tma64;
+  // the interior kernel's layout holds TMA halo boxes when TMA is on
+  const size_t smg = MhdBuf<double>::SMEM;
+  const size_t smi = tma ? MhdBuf<double, true>::SMEM : smg;
   int mt = -1, ma = -1;
   for (int b = 0; b < 3; ++b) {
     if (h->buf[b] == tin) mt = b;
@@ -505,24 +512,24 @@ static int launch_mhd64(Handle *h, const SimDev &S, int stage, const double *a,
   if (mt < 0 || ma < 0) return SPARC_ERR_INVALID;
   TmaSet32 T;
   if (tma)
-    for (int n = 0; n < 18; ++n) T.m[n] = h->tmaps_ty[n];
+    for (int n = 0; n < 24; ++n) T.m[n] = h->tmaps_ty[n];
   else
     std::memset(&T, 0, sizeof(T));
 #define ML64(M, U)                                                                            \
   do {                                                                                        \
-    cudaFuncSetAttribute(k_mhd64<M, U, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
-    cudaFuncSetAttribute(k_mhd64<M, U, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
+    cudaFuncSetAttribute(k_mhd64<M, U, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smi); \
+    cudaFuncSetAttribute(k_mhd64<M, U, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smg); \
     if (has_int) {                                                                            \
       cudaEventRecord(h->ev_fork, s);                                                         \
       cudaStreamWaitEvent(h->aux, h->ev_fork, 0);                                             \
-      k_mhd64<M, U, false><<<grd, blk, sm, h->aux>>>(S, T, a, tin, so, beta, bnext, h->zchunk, \
+      k_mhd64<M, U, false><<<grd, blk, smg, h->aux>>>(S, T, a, tin, so, beta, bnext, h->zchunk, \
                                                      mt, ma, 0, 0, grd.x, grd.y);             \
       cudaEventRecord(h->ev_join, h->aux);                                                    \
-      k_mhd64<M, U, true><<<gint, blk, sm, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt,  \
+      k_mhd64<M, U, true><<<gint, blk, smi, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt, \
                                                 ma, ix0, iy0, grd.x, grd.y);                  \
       cudaStreamWaitEvent(s, h->ev_join, 0);                                                  \
     } else {                                                                                  \
-      k_mhd64<M, U, false><<<grd, blk, sm, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt,  \
+      k_mhd64<M, U, false><<<grd, blk, smg, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt, \
                                                 ma, 0, 0, grd.x, grd.y);                      \
     }                                                                                         \
   } while (0)

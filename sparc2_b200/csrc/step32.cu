@@ -720,10 +720,9 @@ int launch_stage32(Handle *h, const Sim32 &S, int stage, const float *a,
     }
     if (mt < 0 || ma < 0) return SPARC_ERR_INVALID;
     TmaSet32 T;
+    std::memset(&T, 0, sizeof(T));  // [18..23]: the plain form's halo maps
     if (h->tma32)
       for (int n = 0; n < 18; ++n) T.m[n] = h->tmaps32[n];
-    else
-      std::memset(&T, 0, sizeof(T));
     dim3 blk(TX, TY, 2);
     dim3 grd((h->nx + TX - 1) / TX, (h->ny + TY - 1) / TY, (h->nz + h->zchunk - 1) / h->zchunk);
     // interior tile rectangle (see mhd_interior), in tile units
@@ -735,7 +734,7 @@ int launch_stage32(Handle *h, const Sim32 &S, int stage, const float *a,
     const int iy0 = (ym + TY - 1) / TY, iy1 = (h->ny - yM - TY) / TY + 1;
     const bool has_int = h->nx - xM - TX >= 0 && h->ny - yM - TY >= 0 && ix1 > ix0 && iy1 > iy0;
     dim3 gint(has_int ? ix1 - ix0 : 1, has_int ? iy1 - iy0 : 1, grd.z);
-const int smz = (int)MhdBuf<float>::smem_bytes(h->zchunk);
+    const int smz = (int)MhdBuf<float>::smem_bytes(h->zchunk);
 #define ML32(M, U)                                                                          \
   do {                                                                                      \
     cudaFuncSetAttribute(k_mhd32<M, U, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smz); \

@@ -118,6 +118,10 @@ __device__ __forceinline__ bool mbar_wait_t(unsigned long long *bar, unsigned pa
 __device__ __forceinline__ void pf_l2(const void *p) {
   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
+// brings the line holding p into L1
+__device__ __forceinline__ void pf_l1(const void *p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
 
 __device__ __forceinline__ int wrap_t(int q, int n) {
   q = q < 0 ? q + n : q;
@@ -595,14 +599,25 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet32 *T, R 
     if (sh && act) head(k + 5, h0, h1, h2);
     prefetch(k + 7);
     // momentum role: own-point B0 (its halo slots will hold the fluxes),
-    // gravity and forcing, loaded early
+    // gravity and forcing.  The precision form loads them here; the plain
+    // form, short of registers, prefetches them into L1 here and loads them
+    // after the exchange barrier.
     R ox = 0, oy = 0, oz = 0, gk = 0, frc = 0;
-    if (role == 0 && act) {
+    auto own_loads = [&] {
       ox = __ldg(S.box + id);
       oy = __ldg(S.boy + id);
       oz = __ldg(S.boz + id);
       gk = __ldg(gcol + k);
       if (S.frc.kind != SPARC_SRC_NONE) frc = forcing_t(S, Tp, i, j, k);
+    };
+    if (role == 0 && act) {
+      if (SCALED) {
+        own_loads();
+      } else {
+        pf_l1(S.box + id);
+        pf_l1(S.boy + id);
+        pf_l1(S.boz + id);
+      }
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     bool mine = true;
@@ -701,6 +716,7 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet32 *T, R 
                   vz = Hv(2) * iv;
       const R red = O(b, O_BG + B_RED), sg = O(b, O_BG + B_SPONGE);
       if (role == 0) {
+        if (!SCALED) own_loads();
         const R ib = IS(5, k);
         const R dzby = X[NC + cid];
         const R cbx = d4 - dzby, cby = d5, cbz = d7;

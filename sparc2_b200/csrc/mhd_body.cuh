@@ -551,11 +551,10 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet32 *T, R 
     }
   };
   // the z-window head of layer kk is read from DRAM a layer before it is
-  // needed; in the precision form an L2 prefetch two layers earlier takes
-  // that latency off the layer loop (measured: 4 % faster in FP32, 2 %
-  // slower in FP64)
+  // needed; an L2 prefetch two layers earlier takes that latency off the
+  // layer loop
   auto prefetch = [&](int kk) {
-    if (!SCALED || !act || kk >= nz) return;
+    if (!act || kk >= nz) return;
     const int id = kk * NXY + col;
     if (role == 0) {
       pf_l2(tin + 3 * N + id);
@@ -599,9 +598,8 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet32 *T, R 
     if (sh && act) head(k + 5, h0, h1, h2);
     prefetch(k + 7);
     // momentum role: own-point B0 (its halo slots will hold the fluxes),
-    // gravity and forcing.  The precision form loads them here; the plain
-    // form, short of registers, prefetches them into L1 here and loads them
-    // after the exchange barrier.
+    // gravity and forcing, prefetched into L1 here and loaded after the
+    // exchange barrier (not live across the derivatives: fewer registers)
     R ox = 0, oy = 0, oz = 0, gk = 0, frc = 0;
     auto own_loads = [&] {
       ox = __ldg(S.box + id);
@@ -611,13 +609,9 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet32 *T, R 
       if (S.frc.kind != SPARC_SRC_NONE) frc = forcing_t(S, Tp, i, j, k);
     };
     if (role == 0 && act) {
-      if (SCALED) {
-        own_loads();
-      } else {
-        pf_l1(S.box + id);
-        pf_l1(S.boy + id);
-        pf_l1(S.boz + id);
-      }
+      pf_l1(S.box + id);
+      pf_l1(S.boy + id);
+      pf_l1(S.boz + id);
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     bool mine = true;
@@ -716,7 +710,7 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet32 *T, R 
                   vz = Hv(2) * iv;
       const R red = O(b, O_BG + B_RED), sg = O(b, O_BG + B_SPONGE);
       if (role == 0) {
-        if (!SCALED) own_loads();
+        own_loads();
         const R ib = IS(5, k);
         const R dzby = X[NC + cid];
         const R cbx = d4 - dzby, cby = d5, cbz = d7;

@@ -123,6 +123,11 @@ __device__ __forceinline__ void pf_l1(const void *p) {
   asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
 
+// named barrier of two warps (64 threads)
+__device__ __forceinline__ void bar_pair_t(int id) {
+  asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory");
+}
+
 __device__ __forceinline__ int wrap_t(int q, int n) {
   q = q < 0 ? q + n : q;
   return q >= n ? q - n : q;
@@ -340,8 +345,10 @@ inline void mhd_interior_rect(int nx, int ny, const int np[4], int &ix0, int &ix
 // Per layer: every thread waits for its own halo copies, turns the B0 halo
 // values it copied into the fluxes v x B0 in place, then one barrier makes
 // the layer visible; the copies of the next layer are issued after that
-// barrier (the buffer they overwrite was last read before it).  A second
-// barrier exchanges d(vz)/dz and d(by)/dz between the roles.
+// barrier (the buffer they overwrite was last read before it).  A named
+// barrier of the two warps that share rows ty (role 0 warp ty, role 1 warp
+// 8 + ty) exchanges d(vz)/dz and d(by)/dz: nothing else crosses warps
+// until the next layer's barrier.
 template <class R, int MODE, bool TMA, bool INT>
 __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet32 *T, R *smem,
                                          const R *__restrict__ a,
@@ -447,8 +454,10 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet32 *T, R 
       hs = t;
       ho = gy * nx + gx;
     };
+    // halo positions 0..511 one per thread, 512..755 on role 1 (role 0
+    // carries the TMA issue and the heavier momentum update)
     pos(tid, hs0, ho0);
-    pos(tid + NT, hs1, ho1);
+    if (role == 1) pos(tid + NC, hs1, ho1);
   }
   const unsigned own_bytes =
       (MODE == F_FIRST ? 15u : (MODE == F_MID ? 23u : 24u)) * NC * (unsigned)sizeof(R) +
@@ -700,7 +709,8 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet32 *T, R 
         d0 = d0 + d1;
       }
     }
-    __syncthreads();
+    // the exchange involves only the role-0 and role-1 warps of rows ty
+    bar_pair_t(1 + ty);
     double an_rho = 0.0;
     if (act) {
       const bool zero = k == 0 || k == nz - 1 ||
@@ -794,7 +804,7 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet32 *T, R 
       }
     }
     if (MODE == F_LAST) {
-      __syncthreads();
+      bar_pair_t(1 + ty);
       if (act && role == 1) {
         const double m = ((double)O(b, O_BG + B_RHO0) + an_rho) * VSQ[cid] / 2.0;
         ke += m * m;

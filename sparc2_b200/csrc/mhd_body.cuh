@@ -401,6 +401,12 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet32 *T, R 
   // window start in the tile, so every x/y derivative is one branch-free
   // sum: the centred row; one-sided row q at the low edge (q = i); at the
   // high edge -row q reversed over f(n-11..n-1) (derivatives.f90:72, 98).
+  // CTA-uniform: every lane's (row's) stencil is the centred one (periodic
+  // axis, or no lane within 5 points of an edge); then the centred sum
+  // from the window start cxo (cyo) of lane (row) 0 serves
+  const bool cen_x = per || (x0 >= 5 && x0 + TX <= nx - 5);
+  const bool cen_y = per || (y0 >= 5 && y0 + TY <= ny - 5);
+  const int cxo = x0 - 5 - xo, cyo = y0 - 5 - yo;
   __shared__ R cxs[INT ? 1 : TX * 11], cys[INT ? 1 : TY * 11];
   __shared__ int cxb[INT ? 1 : TX], cyb[INT ? 1 : TY];
   if (!INT && tid < TX + TY) {
@@ -638,6 +644,7 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet32 *T, R 
     auto DX = [&](int slot) {
       const R *row = Hp(b, slot) + ry * HXL + XOFF;
       if (INT) return sx * csum_t(row + tx, 1);
+      if (cen_x) return sx * csum_t(row + cxo + tx, 1);
       const R *r = row + cxb[tx], *c = cxs + tx * 11;
       R sum = R(0);
 #pragma unroll
@@ -647,6 +654,7 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet32 *T, R 
     auto DY = [&](int slot) {
       const R *colp = Hp(b, slot) + rx + XOFF;
       if (INT) return sy * csum_t(colp + ty * HXL, HXL);
+      if (cen_y) return sy * csum_t(colp + (cyo + ty) * HXL, HXL);
       const R *r = colp + cyb[ty] * HXL, *c = cys + ty * 11;
       R sum = R(0);
 #pragma unroll

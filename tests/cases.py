@@ -78,6 +78,11 @@ CASES = {
     "thermal_hpml": thermal_hpml,
     "mhd_hpml": mhd_hpml,
     "mhd_periodic": mhd_periodic,
+    # 96x96 columns: 32x8 MHD tiles away from every edge and CPML slab
+    # exist (x tile 32..63, y tiles 8..87), so the interior stage kernel
+    # (and in FP64 its TMA halo planes) runs, not only the edge kernel
+    "mhd_hpml_96": lambda: mhd_hpml(nx=96, ny=96, nz=48),
+    "mhd_periodic_96": lambda: mhd_periodic(nx=96, ny=96, nz=48),
 }
 
 

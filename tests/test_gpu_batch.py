@@ -26,6 +26,7 @@ MEMBERS = {
     "mhd_hpml": cases.mhd_hpml,
     "mhd_hpml_nx42": lambda: cases.mhd_hpml(nx=42, ny=40),
     "mhd_periodic": cases.mhd_periodic,
+    "mhd_hpml_96": cases.CASES["mhd_hpml_96"],   # interior tiles: the batch's first part
 }
 
 

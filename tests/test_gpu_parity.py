@@ -130,7 +130,8 @@ def test_graph_run_equals_call_sequence(name):
 @pytest.mark.parametrize("name,steps", [("quiet_periodic", 300),
                                         ("mhd_hpml", 200),
                                         ("thermal_hpml", 120),
-                                        ("mhd_periodic", 120)])
+                                        ("mhd_periodic", 120),
+                                        ("mhd_hpml_96", 40)])
 def test_many_iterations_from_rest(name, steps):
     """Driver loop from rest with the configured source, filters at cadence."""
     sim, orc = pair(name)

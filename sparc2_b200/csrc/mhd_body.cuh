@@ -612,6 +612,22 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet32 *T, R 
     const bool sh = k > k0 && k <= nz - 6;
     if (sh && act) head(k + 5, h0, h1, h2);
     prefetch(k + 7);
+    // precision form, last stage: the compensation carries of layer k + 2
+    // into L2 (they are read just before their use)
+    if (SCALED && MODE == F_LAST && act && k + 2 < k1) {
+      const int id2 = (k + 2) * NXY + col;
+      if (role == 0) {
+        pf_l2(S.carry + N + id2);
+        pf_l2(S.carry + 2 * N + id2);
+        pf_l2(S.carry + 3 * N + id2);
+      } else {
+        pf_l2(S.carry + id2);
+        pf_l2(S.carry + 4 * N + id2);
+        pf_l2(S.carry + 5 * N + id2);
+        pf_l2(S.carry + 6 * N + id2);
+        pf_l2(S.carry + 7 * N + id2);
+      }
+    }
     // momentum role: own-point B0 (its halo slots will hold the fluxes),
     // gravity and forcing, prefetched into L1 here and loaded after the
     // exchange barrier (not live across the derivatives: fewer registers)

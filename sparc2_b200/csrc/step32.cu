@@ -404,7 +404,7 @@ __global__ void __launch_bounds__(TX *TY)
 }
 
 // -------------------------------------------- MP_MHD_3D, precision form
-// The two-role TMA kernel of step.cu in FP32 with depth scaling (field
+// The two-role body of mhd_body.cuh in FP32 with depth scaling (field
 // scales: 0 rho, 1-3 v, 4 p, 5-7 b).  Own-point arrays of a layer arrive by
 // TMA (32x8 FP32 boxes), halos by cp.async; one CTA of 512 threads per SM.
 

@@ -41,6 +41,8 @@ extern "C" {
 #define SPARC_SRC_NONE  0
 #define SPARC_SRC_PULSE 1  /* PULSE = 1: one analytic pulse                   */
 #define SPARC_SRC_PSR   2  /* PULSE = 2: table of "random-ish" pulses         */
+#define SPARC_SRC_RANDOM 3 /* PULSE = 0: forcing series vr(x, y, t), 7-point
+                              Lagrange in time (all_modules.f90:1892-1950)   */
 
 /*
  * Run parameters: the subset of the .trol keys (initialize.f90:1385-1924)
@@ -91,6 +93,16 @@ typedef struct sparc_source {
     int32_t npulses;
     int32_t pad;
     const sparc_pulse *pulses;
+    /* SPARC_SRC_RANDOM (driver.f90:73-81, 130-132): the series replaces the
+     * forcingfunc FITS cube; it is copied, times rnd_ampl / dimc.  The
+     * forcing acts on v_z (dir is ignored). */
+    double  cadforcing;  /* s between two samples of the series              */
+    double  rnd_ampl;    /* randomexciteampl, cm/s                           */
+    double  rnd_depth;   /* randomexcitedepth, cm (centre of source_dep)     */
+    double  rnd_sigma;   /* randomexcitesigma, cm                            */
+    int32_t nseries;     /* num_steps: samples in the series (>= 1)          */
+    int32_t pad2;
+    const double *series; /* nx*ny*nseries, x fastest, then y, then sample   */
 } sparc_source;
 
 typedef struct sparc_handle sparc_handle;

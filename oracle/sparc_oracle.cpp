@@ -83,6 +83,8 @@ struct orc_handle {
   std::vector<double> a, temp, scr, forcing;
   std::vector<double> w[16];
   sparc_source src;
+  std::vector<double> vr;          // PULSE = 0: the scaled forcing series
+  std::vector<double> source_dep;  // PULSE = 0: depth profile (all_modules.f90:300)
   std::vector<sparc_pulse> pulses;
   std::vector<unsigned char> pulse_in_block;  // npulses * nblocks
   int64_t forcing_iter = -1;
@@ -380,10 +382,60 @@ struct orc_handle {
       }
   }
 
+  // PULSE = 0, LAGRANGE_INTERP (all_modules.f90:1892-1950) then
+  // forcing * source_damp(:,:,1) (driver.f90:131-132), spread over the
+  // layers by source_dep (RHS.f90:147, 641).  Samples the reference would
+  // read past the end of the series count as absent (zero weight).
+  void forcing_random(int64_t nn) {
+    const double cad = src.cadforcing;
+    const int ns = src.nseries;
+    double xt = (double)nn * P.timestep / cad;
+    const long long time1 = (long long)std::floor(xt) + 1;
+    xt = (double)nn * P.timestep;
+    double x[7];
+    for (int j = 0; j < 7; ++j) x[j] = (double)(time1 - 4 + j) * cad;
+    bool use[7];
+    for (int j = 0; j < 4; ++j) use[j] = x[j] >= 0.0;
+    use[4] = true;
+    use[5] = time1 < ns;
+    use[6] = time1 < ns - 1;
+    for (int j = 0; j < 7; ++j) {
+      const long long m = time1 - 4 + j;  // 0-based sample of vr(:,:,time1-3+j)
+      use[j] = use[j] && m >= 0 && m < ns;
+    }
+    double den[7];  // (x_j - x_a) * (x_j - x_b) ... left to right
+    for (int j = 0; j < 7; ++j) {
+      double d = 1.0;
+      bool first = true;
+      for (int m = 0; m < 7; ++m) {
+        if (m == j) continue;
+        d = first ? x[j] - x[m] : d * (x[j] - x[m]);
+        first = false;
+      }
+      den[j] = d;
+    }
+    const size_t NXY = (size_t)nx * ny;
+#pragma omp parallel for schedule(static)
+    for (size_t q = 0; q < NXY; ++q) {
+      double f = 0.0;
+      for (int j = 0; j < 7; ++j) {
+        double lc = use[j] ? vr[q + NXY * (size_t)(time1 - 4 + j)] / den[j] : 0.0;
+        // LC_j * (xt - x_a) * (xt - x_b) ... left to right, as the reference
+        double t = lc;
+        for (int m = 0; m < 7; ++m)
+          if (m != j) t = t * (xt - x[m]);
+        f = j == 0 ? t : f + t;
+      }
+      f = f * source_damp[q];  // source_damp(:,:,1)
+      for (int k = 0; k < nz; ++k) forcing[q + NXY * (size_t)k] = f * source_dep[k];
+    }
+  }
+
   void build_forcing(int64_t nn) {
     if (forcing_iter == nn) return;
     if (src.kind == SPARC_SRC_PULSE) forcing_pulse(nn);
     else if (src.kind == SPARC_SRC_PSR) forcing_psr(nn);
+    else if (src.kind == SPARC_SRC_RANDOM) forcing_random(nn);
     else std::fill(forcing.begin(), forcing.end(), 0.0);
     forcing_iter = nn;
   }
@@ -417,7 +469,8 @@ struct orc_handle {
 
   void add_forcing(double *RVx, double *RVy, double *RVz) const {
     if (src.kind == SPARC_SRC_NONE) return;
-    double *R = src.dir == 1 ? RVx : (src.dir == 2 ? RVy : RVz);
+    const int dir = src.kind == SPARC_SRC_RANDOM ? 3 : src.dir;
+    double *R = dir == 1 ? RVx : (dir == 2 ? RVy : RVz);
 #pragma omp parallel for schedule(static)
     for (size_t n = 0; n < N; ++n) R[n] = R[n] + forcing[n];
   }
@@ -1221,10 +1274,39 @@ void orc_destroy(orc_handle *h) { delete h; }
 
 int orc_set_source(orc_handle *h, const sparc_source *s) {
   if (!s) return SPARC_ERR_INVALID;
-  if (s->kind != SPARC_SRC_NONE && (s->dir < 1 || s->dir > 3)) return SPARC_ERR_INVALID;
+  if (s->kind < SPARC_SRC_NONE || s->kind > SPARC_SRC_RANDOM) return SPARC_ERR_INVALID;
+  if (s->kind != SPARC_SRC_NONE && s->kind != SPARC_SRC_RANDOM && (s->dir < 1 || s->dir > 3))
+    return SPARC_ERR_INVALID;
+  if (s->kind == SPARC_SRC_RANDOM && (s->nseries < 1 || !s->series || !(s->cadforcing > 0.0)))
+    return SPARC_ERR_INVALID;
   h->src = *s;
   h->pulses.clear();
   h->pulse_in_block.clear();
+  h->vr.clear();
+  h->source_dep.clear();
+  if (s->kind == SPARC_SRC_RANDOM) {
+    // driver.f90:80: vr = (randomexciteampl/dimc)*vr
+    const double f = s->rnd_ampl / h->dimc;
+    const size_t n = (size_t)h->nx * h->ny * s->nseries;
+    h->vr.resize(n);
+    for (size_t q = 0; q < n; ++q) h->vr[q] = f * s->series[q];
+    // e_rad and source_dep (all_modules.f90:289-301)
+    const double temp2 = 1.0 + s->rnd_depth / RSUN;
+    double temp = 1.0;
+    int e_rad = 0;
+    for (int k = 0; k < h->nz; ++k)
+      if (std::fabs(h->zaxis[k] - temp2) <= temp) {
+        temp = std::fabs(h->zaxis[k] - temp2);
+        e_rad = k;
+      }
+    h->source_dep.resize(h->nz);
+    const double sg = s->rnd_sigma / RSUN;
+    for (int k = 0; k < h->nz; ++k) {
+      const double d = h->zaxis[k] - h->zaxis[e_rad];
+      h->source_dep[k] = std::exp(-0.5 * (d * d) / 2.0 / (sg * sg));
+    }
+  }
+  h->src.series = nullptr;
   if (s->kind == SPARC_SRC_PSR) {
     if (s->npulses < 0 || (s->npulses > 0 && !s->pulses)) return SPARC_ERR_INVALID;
     h->pulses.assign(s->pulses, s->pulses + s->npulses);
@@ -1339,6 +1421,7 @@ int orc_get_coeff(orc_handle *h, const char *name, double *out, int64_t *count) 
   else if (s == "gblk") v = &h->gblk;
   else if (s == "invrho0q") v = &h->invrho0q;
   else if (s == "cq") v = &h->cq;
+  else if (s == "source_dep") v = &h->source_dep;
   else {
     static const char *fn[6] = {"z_bot", "z_top", "x_bot", "x_top", "y_bot", "y_top"};
     for (int f = 0; f < 6; ++f) {

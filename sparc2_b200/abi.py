@@ -38,6 +38,7 @@ SPARC_REQ_COLLECTED = 5
 SPARC_SRC_NONE = 0
 SPARC_SRC_PULSE = 1
 SPARC_SRC_PSR = 2
+SPARC_SRC_RANDOM = 3
 
 
 class SparcParams(C.Structure):
@@ -80,6 +81,10 @@ class SparcSource(C.Structure):
         ("psr_st", C.c_double),
         ("npulses", C.c_int32), ("pad", C.c_int32),
         ("pulses", C.POINTER(SparcPulse)),
+        ("cadforcing", C.c_double), ("rnd_ampl", C.c_double),
+        ("rnd_depth", C.c_double), ("rnd_sigma", C.c_double),
+        ("nseries", C.c_int32), ("pad2", C.c_int32),
+        ("series", C.POINTER(C.c_double)),
     ]
 
 

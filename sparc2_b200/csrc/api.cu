@@ -181,6 +181,7 @@ static int enqueue_step32(Handle *h, cudaStream_t s, int *nk) {
   int r = SPARC_OK;
   const long long l0 = h->launches;
   if (h->src.kind == SPARC_SRC_PSR && h->psr_khi > h->psr_klo) r |= launch_psr32(h, s);
+  if (h->src.kind == SPARC_SRC_RANDOM) r |= launch_random_forcing(h, s);
   r |= launch_stage32(h, S, 1, a, a, f1, s);
   r |= launch_stage32(h, S, 2, a, f1, f2, s);
   r |= launch_stage32(h, S, 3, a, f2, f1, s);
@@ -199,6 +200,7 @@ static int enqueue_step(Handle *h, cudaStream_t s, int *nk) {
   int r = SPARC_OK;
   const long long l0 = h->launches;
   if (h->src.kind == SPARC_SRC_PSR && h->psr_khi > h->psr_klo) r |= launch_psr_forcing(h, S, s);
+  if (h->src.kind == SPARC_SRC_RANDOM) r |= launch_random_forcing(h, s);
   // stage k reads temp_k and writes temp_{k+1}; stage 5 writes a_new
   r |= launch_stage(h, S, 1, a, a, f1, s);
   r |= launch_stage(h, S, 2, a, f1, f2, s);
@@ -541,10 +543,12 @@ int sparc_set_source(sparc_handle *h, const sparc_source *s) {
   if (!h || !s) return SPARC_ERR_INVALID;
   NOT_IN_BATCH(h);
   if (!h->bg_ready) return fail(h, SPARC_ERR_ORDER, "set the background first");
-  if (s->kind < SPARC_SRC_NONE || s->kind > SPARC_SRC_PSR)
+  if (s->kind < SPARC_SRC_NONE || s->kind > SPARC_SRC_RANDOM)
     return fail(h, SPARC_ERR_INVALID, "unknown source kind");
-  if (s->kind != SPARC_SRC_NONE && (s->dir < 1 || s->dir > 3))
+  if (s->kind != SPARC_SRC_NONE && s->kind != SPARC_SRC_RANDOM && (s->dir < 1 || s->dir > 3))
     return fail(h, SPARC_ERR_INVALID, "pulse_dir must be 1, 2 or 3");
+  if (s->kind == SPARC_SRC_RANDOM && (s->nseries < 1 || !s->series || !(s->cadforcing > 0.0)))
+    return fail(h, SPARC_ERR_INVALID, "forcing series (nseries >= 1, cadforcing > 0)");
   if (s->kind == SPARC_SRC_PSR && (s->npulses < 0 || (s->npulses > 0 && !s->pulses)))
     return fail(h, SPARC_ERR_INVALID, "pulse table");
   cudaSetDevice(h->device);
@@ -552,8 +556,39 @@ int sparc_set_source(sparc_handle *h, const sparc_source *s) {
   drop_graphs(h);
   h->src = *s;
   h->src.pulses = nullptr;
+  h->src.series = nullptr;
   const int nx = h->nx, ny = h->ny, nz = h->nz;
   const double diml = h->diml;
+  if (s->kind == SPARC_SRC_RANDOM) {
+    // driver.f90:80: vr = (randomexciteampl/dimc)*vr; the forcing acts on v_z
+    h->src.dir = 3;
+    const double f = s->rnd_ampl / h->dimc;
+    const size_t n = (size_t)nx * ny * s->nseries;
+    std::vector<double> vr(n);
+    for (size_t q = 0; q < n; ++q) vr[q] = f * s->series[q];
+    // e_rad and source_dep (all_modules.f90:289-301)
+    const double temp2 = 1.0 + s->rnd_depth / RSUN;
+    double temp = 1.0;
+    int e_rad = 0;
+    for (int k = 0; k < nz; ++k)
+      if (std::fabs(h->zaxis[k] - temp2) <= temp) {
+        temp = std::fabs(h->zaxis[k] - temp2);
+        e_rad = k;
+      }
+    std::vector<double> dep(nz);
+    const double sg = s->rnd_sigma / RSUN;
+    for (int k = 0; k < nz; ++k) {
+      const double d = h->zaxis[k] - h->zaxis[e_rad];
+      dep[k] = std::exp(-0.5 * (d * d) / 2.0 / (sg * sg));
+    }
+    dev_free(h, h->d_series);
+    h->d_series = (double *)dev_alloc(h, n * 8);
+    if (!h->d_sdep) h->d_sdep = (double *)dev_alloc(h, (size_t)nz * 8);
+    if (!h->d_f2d) h->d_f2d = (double *)dev_alloc(h, (size_t)nx * ny * 8);
+    if (!h->d_series || !h->d_sdep || !h->d_f2d) return SPARC_ERR_NOMEM;
+    CK(h, cudaMemcpy(h->d_series, vr.data(), n * 8, cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->d_sdep, dep.data(), (size_t)nz * 8, cudaMemcpyHostToDevice));
+  }
   if (s->kind == SPARC_SRC_PULSE) {
     // driver.f90:140-145, split into x, y, z factors
     std::vector<double> t(nx + ny + nz);

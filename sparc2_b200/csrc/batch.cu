@@ -281,6 +281,8 @@ int sparc_batch_add(sparc_batch *b, sparc_handle *hh, int64_t first, int64_t cou
   if (!b || !hh || count < 0) return SPARC_ERR_INVALID;
   Handle *h = reinterpret_cast<Handle *>(hh);
   if (!h->fp32) return bfail(b, SPARC_ERR_INVALID, "batched simulations use SPARC_FP32");
+  if (h->src.kind == SPARC_SRC_RANDOM)
+    return bfail(b, SPARC_ERR_INVALID, "a random-source (PULSE = 0) simulation runs alone");
   if (!h->bg_ready) return bfail(b, SPARC_ERR_ORDER, "set the background first");
   if (h->batch) return bfail(b, SPARC_ERR_ORDER, "handle is already in a batch");
   if (h->device != b->device) return bfail(b, SPARC_ERR_INVALID, "handle on another device");

@@ -46,6 +46,8 @@ struct ForcingT {
   // PULSE = 2: precomputed per iteration for layers [klo, khi)
   const R *psr;          // (khi-klo)*nx*ny
   int klo, khi;
+  // PULSE = 0: f = f2d[j*nx + i] * sdep[k], f2d rebuilt per iteration
+  const R *f2d, *sdep;
 };
 using ForcingDev = ForcingT<double>;
 
@@ -195,7 +197,10 @@ struct Handle {
   double *d_plane_z = nullptr;              // Z_n(k) per CSR entry
   unsigned char *d_pmask = nullptr;         // npulses * nblocks
   double *d_ptime = nullptr;                // amp, t0, t1 per pulse
-  double *d_damp2 = nullptr;                // source_damp(i,j) (N/nz)
+  // PULSE = 0: the scaled forcing series (nx*ny*nseries), source_dep and
+  // the per-iteration forcing plane
+  double *d_series = nullptr, *d_sdep = nullptr, *d_f2d = nullptr;
+  float *f_f2d = nullptr, *f_sdep = nullptr;
   int nblocks = 1;
 
   // TMA tensor maps (32x8x1 boxes) of the MHD own-point arrays: [0..2] the
@@ -267,6 +272,7 @@ SimDev make_simdev(Handle *h);
 int launch_stage(Handle *h, const SimDev &S, int stage, const double *a,
                  const double *tin, double *tout, cudaStream_t s);
 int launch_psr_forcing(Handle *h, const SimDev &S, cudaStream_t s);
+int launch_random_forcing(Handle *h, cudaStream_t s);
 int launch_filter_pass(Handle *h, int dir, const double *in, double *out,
                        cudaStream_t s);
 int stage_geometry(Handle *h);

@@ -236,6 +236,7 @@ __device__ __forceinline__ R forcing_t(const SimT<R> &S, R T, int i, int j, int 
   if (F.kind == SPARC_SRC_PULSE) return T * __ldg(F.fz + k) * (__ldg(F.fy + j) * __ldg(F.fx + i));
   if (F.kind == SPARC_SRC_PSR && k >= F.klo && k < F.khi)
     return F.psr[((long long)(k - F.klo) * S.ny + j) * S.nx + i];
+  if (F.kind == SPARC_SRC_RANDOM) return F.f2d[(long long)j * S.nx + i] * __ldg(F.sdep + k);
   return R(0);
 }
 

@@ -66,6 +66,7 @@ __device__ __forceinline__ double forcing_at(const SimDev &S, long long it,
     return T * __ldg(F.fz + k) * (__ldg(F.fy + j) * __ldg(F.fx + i));
   if (F.kind == SPARC_SRC_PSR && k >= F.klo && k < F.khi)
     return F.psr[((long long)(k - F.klo) * S.ny + j) * S.nx + i];
+  if (F.kind == SPARC_SRC_RANDOM) return F.f2d[(long long)j * S.nx + i] * __ldg(F.sdep + k);
   return 0.0;
 }
 
@@ -709,6 +710,70 @@ int filter_constants() {
                                                                : SPARC_ERR_CUDA;
 }
 
+// PULSE = 0: LAGRANGE_INTERP (all_modules.f90:1892-1950) of the forcing
+// series at the device's iteration, times source_damp(:,:,1)
+// (driver.f90:131-132), one value per column; the stage kernels add
+// f2d(i,j) * source_dep(k) to RHSv_z (RHS.f90:147, 641).  FP64 in the
+// reference's operation order, without contraction; samples the reference
+// would read past the end of the series count as absent.
+template <class D, class T>
+__global__ void k_random(const double *__restrict__ vr, const D *__restrict__ damp, int nxy,
+                         int ns, double timestep, double cad, const long long *iter,
+                         T *__restrict__ out) {
+  const long long nn = *iter;
+  double xt = __ddiv_rn(__dmul_rn((double)nn, timestep), cad);
+  const long long time1 = (long long)floor(xt) + 1;
+  xt = __dmul_rn((double)nn, timestep);
+  double x[7], den[7];
+  bool use[7];
+#pragma unroll
+  for (int j = 0; j < 7; ++j) x[j] = __dmul_rn((double)(time1 - 4 + j), cad);
+#pragma unroll
+  for (int j = 0; j < 7; ++j) {
+    const long long m = time1 - 4 + j;
+    use[j] = (j < 4 ? x[j] >= 0.0 : (j == 4 ? true : (j == 5 ? time1 < ns : time1 < ns - 1))) &&
+             m >= 0 && m < ns;
+    double d = 0.0;
+    bool first = true;
+#pragma unroll
+    for (int q = 0; q < 7; ++q) {
+      if (q == j) continue;
+      const double e = __dsub_rn(x[j], x[q]);
+      d = first ? e : __dmul_rn(d, e);
+      first = false;
+    }
+    den[j] = d;
+  }
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nxy; q += gridDim.x * blockDim.x) {
+    double f = 0.0;
+#pragma unroll
+    for (int j = 0; j < 7; ++j) {
+      double t = use[j] ? __ddiv_rn(vr[q + (long long)nxy * (time1 - 4 + j)], den[j]) : 0.0;
+#pragma unroll
+      for (int m = 0; m < 7; ++m)
+        if (m != j) t = __dmul_rn(t, __dsub_rn(xt, x[m]));
+      f = j == 0 ? t : __dadd_rn(f, t);
+    }
+    out[q] = (T)__dmul_rn(f, (double)damp[q]);
+  }
+}
+
+int launch_random_forcing(Handle *h, cudaStream_t s) {
+  if (h->src.kind != SPARC_SRC_RANDOM) return SPARC_OK;
+  const int nxy = h->nx * h->ny;
+  const int grid = std::min((nxy + 255) / 256, 4 * 148);
+  if (h->fp32)
+    k_random<float, float><<<grid, 256, 0, s>>>(h->d_series, h->f_sd, nxy, h->src.nseries,
+                                               h->P.timestep, h->src.cadforcing, h->d_iter,
+                                               h->f_f2d);
+  else
+    k_random<double, double><<<grid, 256, 0, s>>>(h->d_series, h->source_damp, nxy,
+                                                 h->src.nseries, h->P.timestep,
+                                                 h->src.cadforcing, h->d_iter, h->d_f2d);
+  ++h->launches;
+  return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
+}
+
 int launch_psr_forcing(Handle *h, const SimDev &S, cudaStream_t s) {
   (void)S;
   if (h->src.kind != SPARC_SRC_PSR || h->psr_khi <= h->psr_klo) return SPARC_OK;
@@ -787,6 +852,8 @@ SimDev make_simdev(Handle *h) {
   F.psr = h->d_psr;
   F.klo = h->psr_klo;
   F.khi = h->psr_khi;
+  F.f2d = h->d_f2d;
+  F.sdep = h->d_sdep;
   S.iter = h->d_iter;
   S.err = h->d_err;
   S.partials = h->d_partials;

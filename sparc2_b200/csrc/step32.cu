@@ -92,6 +92,7 @@ __device__ __forceinline__ float forcing32(const Sim32 &S, float T, int i, int j
     return T * __ldg(F.fz + k) * (__ldg(F.fy + j) * __ldg(F.fx + i));
   if (F.kind == SPARC_SRC_PSR && k >= F.klo && k < F.khi)
     return F.psr[((long long)(k - F.klo) * S.ny + j) * S.nx + i];
+  if (F.kind == SPARC_SRC_RANDOM) return F.f2d[(long long)j * S.nx + i] * __ldg(F.sdep + k);
   return 0.f;
 }
 
@@ -670,6 +671,8 @@ Sim32 make_sim32(Handle *h) {
   F.psr = h->f_psr;
   F.klo = h->psr_klo;
   F.khi = h->psr_khi;
+  F.f2d = h->f_f2d;
+  F.sdep = h->f_sdep;
   S.sc = h->f_sc;
   S.isc = h->f_isc;
   S.carry = h->f_carry;
@@ -1219,6 +1222,10 @@ int source32(Handle *h) {
     h->f_psr = f_up(h, nullptr,
                     std::max<long long>(1, (long long)(h->psr_khi - h->psr_klo) * h->nx * h->ny), s);
     if (!h->f_px || !h->f_py || !h->f_psr) return SPARC_ERR_NOMEM;
+  } else if (h->src.kind == SPARC_SRC_RANDOM) {
+    h->f_sdep = f_up(h, h->d_sdep, h->nz, s);
+    h->f_f2d = f_up(h, nullptr, (long long)h->nx * h->ny, s);
+    if (!h->f_sdep || !h->f_f2d) return SPARC_ERR_NOMEM;
   }
   return cudaStreamSynchronize(s) == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
 }

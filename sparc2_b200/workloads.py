@@ -9,6 +9,8 @@ see identical inputs.
 Array convention: numpy C-order shape (nz, ny, nx), which is the Fortran
 (nx, ny, nz) layout of the reference (x fastest).
 """
+import ctypes as C
+
 import numpy as np
 
 from . import abi
@@ -184,6 +186,36 @@ def psr_table(params, npulses, seed, init=0):
     tab["sr"], tab["sz"], tab["amp"] = sr, sz, amp
     tab["t0"], tab["t1"] = t0, t1
     return tab
+
+
+def random_series(params, maxtime, cadforcing, seed):
+    """A seeded stand-in for the forcingfunc cube of PULSE = 0 (the
+    reference reads it from a FITS file): nx*ny*num_steps unit-variance
+    samples, x fastest, with num_steps as driver.f90:38-39 sizes it for a
+    run of `maxtime` iterations."""
+    ns = int(np.floor(maxtime * params.timestep / cadforcing)) + 2
+    ns = 2 * (ns // 2) + 2
+    rng = np.random.Generator(np.random.Philox(key=seed))
+    return np.ascontiguousarray(rng.standard_normal((ns, params.ny, params.nx)))
+
+
+def random_source(series, *, cadforcing=30.0, ampl=1.0e3, depth=-0.15 * MM,
+                  sigma=0.1 * MM, init=0):
+    """A PULSE = 0 source (driver.f90:73-81, 130-132) over a forcing series of
+    shape (num_steps, ny, nx); keeps the series alive on the returned object
+    (attribute _keep).  ampl, depth, sigma: randomexciteampl (cm/s),
+    randomexcitedepth and randomexcitesigma (cm)."""
+    arr = np.ascontiguousarray(series, dtype=np.float64)
+    s = abi.SparcSource()
+    s.kind = abi.SPARC_SRC_RANDOM
+    s.dir = 3
+    s.init = init
+    s.cadforcing, s.rnd_ampl = cadforcing, ampl
+    s.rnd_depth, s.rnd_sigma = depth, sigma
+    s.nseries = arr.shape[0]
+    s.series = arr.ctypes.data_as(C.POINTER(C.c_double))
+    s._keep = arr
+    return s
 
 
 def psr_source(table, direction=3, init=0, psr_st=120.0):

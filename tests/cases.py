@@ -72,6 +72,26 @@ def thermal_hpml(nx=40, ny=40, nz=48, npml=8, npulses=12, seed=5):
     return p, bg, W.psr_source(tab)
 
 
+def _random(p, seed, cad):
+    """PULSE = 0 source: a seeded forcing series sampled every `cad` s."""
+    series = W.random_series(p, 400, cad, seed)
+    return W.random_source(series, cadforcing=cad, ampl=3.0e3, depth=-0.5 * MM,
+                           sigma=0.3 * MM)
+
+
+def quiet_random(nx=40, ny=36, nz=48):
+    """Quiet background with side CPML, driven by the random source."""
+    p, bg, _ = quiet_hpml(nx, ny, nz)
+    return p, bg, _random(p, 21, 8.0)
+
+
+def mhd_random(nx=96, ny=96, nz=48):
+    """Flux tube with CPML on six faces (interior tiles too), driven by the
+    random source."""
+    p, bg, _ = mhd_hpml(nx, ny, nz)
+    return p, bg, _random(p, 23, 4.0)
+
+
 CASES = {
     "quiet_periodic": quiet_periodic,
     "quiet_hpml": quiet_hpml,
@@ -83,6 +103,8 @@ CASES = {
     # (and in FP64 its TMA halo planes) runs, not only the edge kernel
     "mhd_hpml_96": lambda: mhd_hpml(nx=96, ny=96, nz=48),
     "mhd_periodic_96": lambda: mhd_periodic(nx=96, ny=96, nz=48),
+    "quiet_random": quiet_random,
+    "mhd_random": mhd_random,
 }
 
 

@@ -119,6 +119,18 @@ def test_tile_extent_does_not_change_results():
     assert np.array_equal(res[0][1], res[1][1])
 
 
+def test_random_source_member_is_refused():
+    """PULSE = 0 simulations run alone (sparc_run); a batch refuses them."""
+    p, bg, src = cases.quiet_random()
+    p.precision = abi.SPARC_FP32
+    s = Simulation(p, bg, src)
+    with Batch(2) as b:
+        with pytest.raises(abi.SparcError) as e:
+            b.add(s, 0, 10)
+        assert e.value.code == abi.SPARC_ERR_INVALID
+    s.close()
+
+
 def test_tuner_and_membership_rules():
     s = Simulation(*fp32("mhd_hpml"))
     q = Simulation(*fp32("quiet_periodic"))

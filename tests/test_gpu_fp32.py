@@ -108,7 +108,9 @@ def test_graph_run_equals_call_sequence_fp32(name):
                                         ("mhd_hpml", 200),
                                         ("mhd_hpml_nx42", 100),
                                         ("thermal_hpml", 120),
-                                        ("mhd_periodic", 120)])
+                                        ("mhd_periodic", 120),
+                                        ("quiet_random", 120),
+                                        ("mhd_random", 80)])
 def test_many_iterations_fp32(name, steps):
     s64, s32 = twins(name)
     s64.run(0, steps)

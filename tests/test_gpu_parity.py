@@ -131,7 +131,9 @@ def test_graph_run_equals_call_sequence(name):
                                         ("mhd_hpml", 200),
                                         ("thermal_hpml", 120),
                                         ("mhd_periodic", 120),
-                                        ("mhd_hpml_96", 40)])
+                                        ("mhd_hpml_96", 40),
+                                        ("quiet_random", 120),
+                                        ("mhd_random", 60)])
 def test_many_iterations_from_rest(name, steps):
     """Driver loop from rest with the configured source, filters at cadence."""
     sim, orc = pair(name)

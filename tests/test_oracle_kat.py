@@ -155,3 +155,84 @@ def test_stabilise_clamp(quiet):
     sel = (z <= np.float32(0.9998)) & (np.arange(len(z)) >= p.npml_zb) & \
         (np.arange(len(z)) < len(z) - p.npml_zt)
     assert np.all(gp[sel] >= -rho0[sel] * g[sel] - 1e-300)
+
+
+# ------------------------------------------------ PULSE = 0 random source
+def _lagrange_point(vr, nn, dt, cad, ns):
+    """LAGRANGE_INTERP (all_modules.f90:1892-1950) for one column's series
+    vr[m] (0-based samples), the reference's operation order."""
+    xt = nn * dt / cad
+    time1 = int(np.floor(xt)) + 1
+    xt = nn * dt
+    x = [(time1 - 4 + j) * cad for j in range(7)]
+    use = [x[j] >= 0 for j in range(4)] + [True, time1 < ns, time1 < ns - 1]
+    f = 0.0
+    for j in range(7):
+        m = time1 - 4 + j
+        lc = 0.0
+        if use[j] and 0 <= m < ns:
+            den = None
+            for q in range(7):
+                if q != j:
+                    den = x[j] - x[q] if den is None else den * (x[j] - x[q])
+            lc = vr[m] / den
+        t = lc
+        for q in range(7):
+            if q != j:
+                t = t * (xt - x[q])
+        f = t if j == 0 else f + t
+    return f
+
+
+def _random_case(series_fn, nn_list, cad=10.0):
+    p, bg, _ = cases.quiet_hpml(nx=24, ny=22, nz=24)
+    ns = 2 * ((int(np.floor(400 * p.timestep / cad)) + 2) // 2) + 2
+    tm = np.arange(ns) * cad
+    series = series_fn(tm)[:, None, None] * (1.0 + 0.1 * np.arange(p.nx))[None, None, :] * \
+        np.ones((1, p.ny, 1))
+    src = W.random_source(series, cadforcing=cad, ampl=2.0e3, depth=-0.6 * W.MM,
+                          sigma=0.4 * W.MM)
+    o = oracle.Oracle(p, bg, src)
+    dimc = o.scalars()["dimc"]
+    out = [o.forcing(nn) for nn in nn_list]
+    sd = o.coeff("source_damp").reshape(p.nz, p.ny, p.nx)[0]
+    dep = o.coeff("source_dep")
+    # e_rad and source_dep as all_modules.f90:289-301 state them
+    z = o.coeff("zaxis")
+    temp2, temp, e_rad = 1.0 + (-0.6 * W.MM) / W.RSUN, 1.0, 0
+    for k in range(p.nz):
+        if abs(z[k] - temp2) <= temp:
+            temp, e_rad = abs(z[k] - temp2), k
+    sg = 0.4 * W.MM / W.RSUN
+    want = np.exp(-0.5 * (z - z[e_rad]) ** 2 / 2.0 / sg ** 2)
+    assert np.array_equal(dep, want)
+    return p, series, dimc, sd, dep, out, ns
+
+
+def test_random_source_follows_the_reference_formula():
+    """Early iterations drop the samples before t = 0 (x_j < 0), late ones
+    those past the series; every value follows LAGRANGE_INTERP, times
+    source_damp(:,:,1) and source_dep(k) (driver.f90:131-132, RHS.f90:147)."""
+    nn_list = [0, 1, 7, 25, 41, 399]
+    p, series, dimc, sd, dep, out, ns = _random_case(
+        lambda t: np.sin(t / 37.0) + 0.2 * np.cos(t / 11.0), nn_list)
+    vr = (2.0e3 / dimc) * series
+    for nn, f in zip(nn_list, out):
+        for (j, i) in [(0, 0), (3, 7), (21, 23)]:
+            g = _lagrange_point(vr[:, j, i], nn, p.timestep, 10.0, ns) * sd[j, i]
+            assert np.allclose(f[:, j, i], g * dep, rtol=1e-14, atol=0.0), (nn, j, i)
+    assert dep.max() == 1.0 and dep.min() > 0.0
+
+
+def test_random_source_reproduces_a_cubic_in_time():
+    """With all seven samples in range, 7-point Lagrange interpolation is
+    exact on a cubic in time (KAT of the restatement)."""
+    T = 200.0
+    P = lambda t: 1.0 + 0.3 * (t / T) - 0.2 * (t / T) ** 2 + 0.05 * (t / T) ** 3
+    nn_list = [90, 133, 250]          # time1 in [4, ns - 2]
+    p, series, dimc, sd, dep, out, ns = _random_case(P, nn_list)
+    for nn, f in zip(nn_list, out):
+        t = nn * p.timestep
+        want = (2.0e3 / dimc) * P(t) * (1.0 + 0.1 * np.arange(p.nx))[None, :] * sd
+        got = f / dep[:, None, None]
+        assert np.allclose(got, want[None], rtol=1e-11, atol=0.0), nn

@@ -658,6 +658,12 @@ int sparc_set_source(sparc_handle *h, const sparc_source *s) {
     if (khi <= klo) { klo = 0; khi = 0; }
     h->psr_klo = klo;
     h->psr_khi = khi;
+    // a later call replaces the tables of an earlier one
+    for (const void *p : {(const void *)h->d_px, (const void *)h->d_py, (const void *)h->d_ptime,
+                          (const void *)h->d_pmask, (const void *)h->d_plane_off,
+                          (const void *)h->d_plane_idx, (const void *)h->d_plane_z,
+                          (const void *)h->d_psr})
+      dev_free(h, p);
     auto upd = [&](void *&dst, const void *src, size_t bytes) -> int {
       dst = dev_alloc(h, bytes);
       if (!dst) return SPARC_ERR_NOMEM;

@@ -1217,12 +1217,17 @@ int source32(Handle *h) {
     if (to_float(h->d_fx, h->f_fx, h->nx + h->ny + h->nz, s)) return SPARC_ERR_CUDA;
   } else if (h->src.kind == SPARC_SRC_PSR) {
     const long long np = (long long)h->pulses.size();
+    dev_free(h, h->f_px);  // a later call replaces the tables of an earlier one
+    dev_free(h, h->f_py);
+    dev_free(h, h->f_psr);
     h->f_px = f_up(h, h->d_px, np * h->nx, s);
     h->f_py = f_up(h, h->d_py, np * h->ny, s);
     h->f_psr = f_up(h, nullptr,
                     std::max<long long>(1, (long long)(h->psr_khi - h->psr_klo) * h->nx * h->ny), s);
     if (!h->f_px || !h->f_py || !h->f_psr) return SPARC_ERR_NOMEM;
   } else if (h->src.kind == SPARC_SRC_RANDOM) {
+    dev_free(h, h->f_sdep);
+    dev_free(h, h->f_f2d);
     h->f_sdep = f_up(h, h->d_sdep, h->nz, s);
     h->f_f2d = f_up(h, nullptr, (long long)h->nx * h->ny, s);
     if (!h->f_sdep || !h->f_f2d) return SPARC_ERR_NOMEM;

@@ -199,3 +199,25 @@ def test_errors_cross_the_abi():
     bad.dir = 7
     with pytest.raises(abi.SparcError):
         sim.set_source(bad)
+
+
+@pytest.mark.parametrize("precision", [abi.SPARC_FP64, abi.SPARC_FP32])
+def test_set_source_again_replaces_the_source(precision):
+    """A later sparc_set_source replaces an earlier one (the earlier tables
+    are freed): after PSR, random, then PSR again the run is bitwise the run
+    of a handle that only ever had the PSR source."""
+    p, bg, psr = cases.mhd_hpml()
+    _, _, rnd = cases.mhd_random(nx=p.nx, ny=p.ny, nz=p.nz)
+    p.precision = precision
+    a = Simulation(p, bg, psr)
+    a.set_source(rnd)
+    a.set_source(psr)
+    b = Simulation(p, bg, psr)
+    for s in (a, b):
+        s.run(0, 12)
+    ga, gpsi = a.get_state()
+    ba, bpsi = b.get_state()
+    assert np.array_equal(ga, ba) and np.array_equal(gpsi, bpsi)
+    assert a.diagnostics()[0].ke_norm == b.diagnostics()[0].ke_norm
+    a.close()
+    b.close()

@@ -106,3 +106,22 @@ def test_invalid_parameters_are_rejected_before_any_device_call(lib):
     p.nz = 4096
     assert lib.sparc_create(C.byref(p), 0, C.byref(h)) == abi.SPARC_ERR_INVALID
     assert b"precision form" in lib.sparc_last_error(None)
+
+
+def test_c_driver_builds_and_reports_the_missing_device(tmp_path):
+    """The C caller of the ABI (the driver.f90 loop) compiles against the
+    header and the library; without a device it stops at sparc_create with
+    its documented exit status 3."""
+    import torch
+    from sparc2_b200 import workloads as W
+    from tests import c_driver, cases
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    exe = c_driver.build(tmp_path)
+    p, bg, src = cases.quiet_periodic()
+    c_driver.write_inputs(tmp_path, p, bg, src)
+    r = c_driver.run(exe, tmp_path, 0, 3)
+    assert r.returncode == 3, (r.returncode, r.stderr)
+    assert "sparc_create" in r.stderr
+    (tmp_path / "params.bin").write_bytes(b"short")
+    assert c_driver.run(exe, tmp_path, 0, 3).returncode == 1

@@ -364,7 +364,7 @@ def run_gpu(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline()
 
-    # the north star's comparison: the FP32 precision form and the FP32
+    # the precision comparison: the FP32 precision form and the FP32
     # batched ensemble on the same GPU, beside this FP64 plain number
     extras = {}
     if (world == 1 and not args.no_extras and args.workload == "cfg1"

@@ -6,7 +6,7 @@ cfg0-sized test also compares with the oracle directly.
 
 Tolerances: one iteration from a random state agrees to 1e-5 relative L2
 per field (FP32 rounding of the stencils and RHS, ~1e-7 per operation); the
-north-star bar for the precision form is 1e-4 relative L2 per field after
+required bar for the precision form is 1e-4 relative L2 per field after
 1000 steps.
 """
 import numpy as np

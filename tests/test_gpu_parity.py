@@ -3,7 +3,7 @@
 Tolerances: the setup kernels are compiled without FMA contraction and
 reproduce the oracle to a few ulp (1e-13 relative; exp/pow/sin may differ
 by an ulp between CUDA and glibc).  The fused stage kernels contract to FMA,
-so one step agrees to ~1e-14 relative L2 per field; the north-star bar for
+so one step agrees to ~1e-14 relative L2 per field; the required bar for
 the FP64 plain form is 1e-11 relative L2 per field after 1000 steps.
 """
 import numpy as np
@@ -17,7 +17,7 @@ from tests.cases import rel_l2
 pytestmark = pytest.mark.gpu
 
 STEP_TOL = 1e-12       # one driver iteration from a random state
-LONG_TOL = 1e-11       # after many iterations (north-star FP64 bar)
+LONG_TOL = 1e-11       # after many iterations (the FP64 plain-form bar)
 COEF_TOL = 1e-13
 
 

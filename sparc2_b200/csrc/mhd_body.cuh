@@ -63,7 +63,7 @@ struct MhdBuf {
 // tensor maps: [0..2] the state buffers (nx, ny, nz*V) and [3..17] the
 // background arrays in 32x8x1 boxes (own points); plain form: [18..20] the
 // state buffers and [21..23] B0 x, y, z in 44x18x1 halo boxes
-struct TmaSet32 {
+struct TmaSet {
   CUtensorMap m[24];
 };
 
@@ -351,7 +351,7 @@ inline void mhd_interior_rect(int nx, int ny, const int np[4], int &ix0, int &ix
 // 8 + ty) exchanges d(vz)/dz and d(by)/dz: nothing else crosses warps
 // until the next layer's barrier.
 template <class R, int MODE, bool TMA, bool INT>
-__device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet32 *T, R *smem,
+__device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *smem,
                                          const R *__restrict__ a,
                                          const R *__restrict__ tin,
                                          R *__restrict__ so, R beta, R bnext,

@@ -471,7 +471,7 @@ int encode_tensor_maps(Handle *h) {
 // TMA: the 24 own-point arrays of a layer arrive as 32x8x1 TMA boxes.
 template <int MODE, bool TMA, bool INT>
 __global__ void __launch_bounds__(mg::NT, 1)
-    k_mhd64(const SimDev S, const __grid_constant__ TmaSet32 T, const double *__restrict__ a,
+    k_mhd64(const SimDev S, const __grid_constant__ TmaSet T, const double *__restrict__ a,
             const double *__restrict__ tin, double *__restrict__ so, double beta, double bnext,
             int zchunk, int mt, int ma, int ix0, int iy0, int gx, int gy) {
   extern __shared__ __align__(1024) double smem_raw64[];
@@ -514,7 +514,7 @@ static int launch_mhd64(Handle *h, const SimDev &S, int stage, const double *a,
     if (h->buf[b] == a) ma = b;
   }
   if (mt < 0 || ma < 0) return SPARC_ERR_INVALID;
-  TmaSet32 T;
+  TmaSet T;
   if (tma)
     for (int n = 0; n < 24; ++n) T.m[n] = h->tmaps_ty[n];
   else

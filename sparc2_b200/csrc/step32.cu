@@ -421,7 +421,7 @@ using namespace mg;
 // neither pays the other's registers.
 template <int MODE, bool TMA, bool INT>
 __global__ void __launch_bounds__(t32::NT, 1)
-    k_mhd32(const Sim32 S, const __grid_constant__ TmaSet32 T,
+    k_mhd32(const Sim32 S, const __grid_constant__ TmaSet T,
             const float *__restrict__ a, const float *__restrict__ tin,
             float *__restrict__ so, float beta, float bnext, int zchunk, int mt,
             int ma, int ix0, int iy0, int gx, int gy) {
@@ -722,7 +722,7 @@ int launch_stage32(Handle *h, const Sim32 &S, int stage, const float *a,
       if (h->fbuf[b] == a) ma = b;
     }
     if (mt < 0 || ma < 0) return SPARC_ERR_INVALID;
-    TmaSet32 T;
+    TmaSet T;
     std::memset(&T, 0, sizeof(T));  // [18..23]: the plain form's halo maps
     if (h->tma32)
       for (int n = 0; n < 18; ++n) T.m[n] = h->tmaps32[n];

@@ -506,9 +506,10 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
       }
     }
     cp_commit_t();
-    // TMA copies of the layer, one per lane of warp 0: copy c < 24 is own
-    // slot c (stage rho, a[0..7], 14 background arrays, p0); with TH, copy
-    // 24 + s is halo plane s (state fields 1..7, then B0 x, y, z)
+    // TMA copies of the layer, spread over warp 0 (lane l issues copies l
+    // and l + 32): copy c < 24 is own slot c (stage rho, a[0..7], 14
+    // background arrays, p0); with TH, copy 24 + s is halo plane s (state
+    // fields 1..7, then B0 x, y, z)
     if (TMA && tid < 32) {
       if (tid == 0) mbar_tx_t(&bar[b], own_bytes);
       __syncwarp();

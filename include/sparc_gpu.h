@@ -226,6 +226,16 @@ const char *sparc_last_error(const sparc_handle *h);
  * any stream capture.  Waits for the handle's stream. */
 int sparc_ke_norm_noalloc(sparc_handle *h, double *ke_norm);
 
+/* ---------------------------------------------------- failure injection
+ * No counterpart in the reference.  For failure-detection tests: launches on
+ * the handle's stream a kernel whose bounded wait on an mbarrier that nothing
+ * completes gives up after `polls` polls (1 <= polls <= 2^26) and raises the
+ * handle's device error flag, as a stage kernel's gave-up wait does.  The
+ * GPU neither hangs nor faults.  The next sparc_diagnostics returns
+ * SPARC_ERR_TIMEOUT; sparc_set_state (a restart from saved state) clears
+ * the flag. */
+int sparc_inject_wait_timeout(sparc_handle *h, int64_t polls);
+
 /* -------------------------------------------------------- batched engine
  * No counterpart in the reference, which runs one simulation per MPI job.
  * A batch advances many SPARC_FP32 handles of any grid sizes together: each

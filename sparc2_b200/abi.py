@@ -124,7 +124,7 @@ EXPORTS = [
     "sparc_batch_set_tiles", "sparc_batch_get_tiles",
     "sparc_batch_synchronize", "sparc_batch_stream",
     "sparc_batch_launch_count", "sparc_batch_last_error",
-    "sparc_batch_tune", "sparc_ke_norm_noalloc",
+    "sparc_batch_tune", "sparc_ke_norm_noalloc", "sparc_inject_wait_timeout",
     "sparc_estimate_bytes", "sparc_server_create", "sparc_server_destroy",
     "sparc_serve_submit", "sparc_serve_next", "sparc_serve_params",
     "sparc_serve_attach", "sparc_serve_result", "sparc_serve_release",
@@ -173,6 +173,7 @@ def _declare(lib):
         "sparc_batch_last_error": (C.c_char_p, [h]),
         "sparc_batch_tune": (C.c_int, [h, C.c_int, P(C.c_int), P(C.c_int)]),
         "sparc_ke_norm_noalloc": (C.c_int, [h, d]),
+        "sparc_inject_wait_timeout": (C.c_int, [h, C.c_int64]),
         "sparc_estimate_bytes": (C.c_int, [P(SparcParams), P(C.c_int64),
                                            P(C.c_int64)]),
         "sparc_server_create": (C.c_int, [C.c_int, C.c_int, C.c_int64,

@@ -316,6 +316,28 @@ static void parallel_for(long long n, F f) {
   for (auto &t : th) t.join();
 }
 
+// Failure injection: one thread waits on an mbarrier that expects one
+// arrival which never comes; the bounded wait gives up after `polls` polls
+// and raises the error flag, as a stage kernel's gave-up wait does.
+__global__ void k_wait_probe(int *err, long long polls) {
+  __shared__ unsigned long long bar;
+  if (threadIdx.x != 0) return;
+  const unsigned a = (unsigned)__cvta_generic_to_shared(&bar);
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  for (long long n = 0; n < polls; ++n) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(0u)
+        : "memory");
+    if (ok) return;
+  }
+  atomicExch(err, 1);
+}
+
 }  // namespace sparc
 
 using namespace sparc;
@@ -759,9 +781,12 @@ int sparc_set_state(sparc_handle *h, const double *a, const double *psi) {
   if (!h) return SPARC_ERR_INVALID;
   NOT_IN_BATCH(h);
   cudaSetDevice(h->device);
+  // a restart from saved state clears the device error flag
   if (h->fp32) {
     CK(h, cudaStreamSynchronize(h->stream));
-    return set_state32(h, a, psi);
+    const int r = set_state32(h, a, psi);
+    if (r == SPARC_OK) CK(h, cudaMemset(h->d_err, 0, 4));
+    return r;
   }
   if (a)
     CK(h, cudaMemcpyAsync(h->buf[h->ra], a, (size_t)h->V * h->N * 8,
@@ -776,6 +801,19 @@ int sparc_set_state(sparc_handle *h, const double *a, const double *psi) {
       }
   }
   CK(h, cudaStreamSynchronize(h->stream));
+  CK(h, cudaMemset(h->d_err, 0, 4));
+  return SPARC_OK;
+}
+
+int sparc_inject_wait_timeout(sparc_handle *h, int64_t polls) {
+  if (!h) return SPARC_ERR_INVALID;
+  NOT_IN_BATCH(h);
+  if (polls < 1 || polls > (1LL << 26))
+    return fail(h, SPARC_ERR_INVALID, "polls must be in [1, 2^26]");
+  cudaSetDevice(h->device);
+  k_wait_probe<<<1, 32, 0, h->stream>>>(h->d_err, (long long)polls);
+  ++h->launches;
+  CK(h, cudaGetLastError());
   return SPARC_OK;
 }
 

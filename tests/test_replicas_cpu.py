@@ -52,6 +52,39 @@ def test_max_over_ranks_and_whole_job_rate():
     assert [r[2] for r in res] == [2000.0, 2000.0]    # 2 ranks * 1000 / 1 s
 
 
+def _failing_worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port),
+                      RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    sys.path.insert(0, ROOT)
+    from sparc2_b200.replicas import Replicas
+    rep = Replicas("gloo", timeout_s=10)
+    if rank == 1:
+        raise SystemExit(3)        # leaves between steps, before the barrier
+    try:
+        rep.barrier()
+        q.put((rank, "passed"))
+    except Exception:
+        q.put((rank, "error"))
+
+
+def test_a_rank_that_leaves_ends_the_others_barrier_with_an_error():
+    """Failure on the host: a rank exits between steps; the surviving rank's
+    next collective ends with an error (peer gone or the short process-group
+    timeout) instead of waiting for good."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_failing_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    assert q.get(timeout=120) == (0, "error")
+    for p in procs:
+        p.join(timeout=60)
+    assert procs[1].exitcode == 3
+    assert procs[0].exitcode == 0
+
+
 def test_reference_arm_under_torchrun_prints_one_line():
     port = _free_port()
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",

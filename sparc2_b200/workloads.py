@@ -114,21 +114,29 @@ def fluxtube_background(nx, ny, nz, xlength, ylength, z_bot=-25.0,
     else:
         xs = np.arange(nx) / (nx - 1) * xlength
         ys = np.arange(ny) / (ny - 1) * ylength
-    X = xs[None, None, :] - 0.5 * xlength
-    Y = ys[None, :, None] - 0.5 * ylength
-    R3 = R[:, None, None]
-    E = np.exp((-(X * X + Y * Y)) / (R3 * R3))   # negate the 2-D plane, not the cube
-    bz = Ba[:, None, None] * E
-    bx = Ba[:, None, None] * Rp_over_R[:, None, None] * X * E
-    by = Ba[:, None, None] * Rp_over_R[:, None, None] * Y * E
-    pm = (bx * bx + by * by + bz * bz) / (8.0 * np.pi)
-    q = 1.0 - pm / pre[:, None, None]
+    x = xs - 0.5 * xlength
+    y = ys - 0.5 * ylength
+    # exp(-r^2/R^2) = exp(-x^2/R^2) exp(-y^2/R^2): nz*(nx + ny) exponentials
+    # instead of one per point; the cube is built by products, in place
+    iR2 = 1.0 / (R * R)
+    ex = np.exp(-(x * x)[None, :] * iR2[:, None])          # (nz, nx)
+    ey = np.exp(-(y * y)[None, :] * iR2[:, None])          # (nz, ny)
+    bz = (Ba[:, None] * ey)[:, :, None] * ex[:, None, :]
+    bx = bz * (Rp_over_R[:, None, None] * x[None, None, :])
+    by = bz * (Rp_over_R[:, None, None] * y[None, :, None])
+    pm = bx * bx
+    pm += by * by
+    pm += bz * bz
+    pm /= 8.0 * np.pi
+    fac = pm                                      # q = 1 - pm/p, in place
+    fac /= -pre[:, None, None]
+    fac += 1.0
     lo = 2.0 * p_floor
-    fac = q.copy()                                # the floor only where it applies
-    low = q < lo
-    fac[low] = p_floor + p_floor * np.exp((q[low] - lo) / p_floor)
-    pre3 = pre[:, None, None] * fac
-    rho3 = rho[:, None, None] * fac
+    low = fac < lo                                # the floor only where it applies
+    fac[low] = p_floor + p_floor * np.exp((fac[low] - lo) / p_floor)
+    pre3 = fac * pre[:, None, None]
+    rho3 = fac
+    rho3 *= rho[:, None, None]
     cs3 = np.sqrt(gamma * pre3 / rho3)
     c = np.ascontiguousarray
     return dict(rho0=c(rho3), pre0=c(pre3), cs0=c(cs3), bx0=c(bx),

@@ -1,6 +1,7 @@
 """Regenerates the golden fixtures of the oracle (tests/golden/*.npz).
 
-Run from the repository root:  python tests/golden/make_golden.py
+Run from the repository root:  python tests/golden/make_golden.py [NAME...]
+(all fixtures without names).
 The fixtures freeze the oracle's output on tiny seeded cases so that any
 change of the restatement is deliberate.  Each fixture keeps, per state
 field, the L2 norm, sum, max |.| and the x-y slice at the middle layer, plus
@@ -25,6 +26,9 @@ FIXTURES = {
     "mhd_rest_12": ("mhd_hpml", dict(nx=24, ny=24, nz=32, npml=6, npulses=8), None, 0, 12),
     "quiet_random_it30": ("quiet_periodic", dict(nx=24, ny=24, nz=32, npml=6), 21, 30, 1),
     "mhd_random_it30": ("mhd_hpml", dict(nx=24, ny=24, nz=32, npml=6, npulses=8), 22, 30, 1),
+    # PULSE = 0 random-series source from rest (the series' first samples
+    # are dropped at early times, as LAGRANGE_INTERP does)
+    "quiet_rndsrc_40": ("quiet_random", dict(nx=24, ny=24, nz=32), None, 0, 40),
 }
 
 
@@ -55,12 +59,12 @@ def run(name):
     return summarize(o)
 
 
-def main():
+def main(names=None):
     oracle.build()
-    for name in FIXTURES:
+    for name in names or FIXTURES:
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **run(name))
         print("wrote", name)
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

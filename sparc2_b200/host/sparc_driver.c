@@ -10,7 +10,9 @@
  *   rho0.bin pre0.bin cs0.bin               nx*ny*nz doubles each
  *   bx0.bin by0.bin bz0.bin                 (MAGNETIC = 2 only)
  *   zaxis.bin (Mm) grav.bin (cm/s^2)        nz doubles each
- * source.bin is optional; its pointer fields are ignored (pulse sources).
+ *   pulses.bin  npulses sparc_pulse         (source.bin kind PULSE = 2)
+ *   series.bin  nx*ny*nseries doubles       (source.bin kind PULSE = 0)
+ * source.bin is optional; its pointer fields are replaced by the tables.
  *
  * Output: one line per iteration, "nn ke_norm min_rho min_p status".
  * Exit status: 0 done, 1 bad input, 2 library error, 3 no usable device,
@@ -18,7 +20,9 @@
  *
  * Build: cc -O2 -I include sparc2_b200/host/sparc_driver.c \
  *           -L sparc2_b200/_lib -lsparc_gpu -Wl,-rpath,sparc2_b200/_lib
- * Run:   sparc_driver DIR FIRST COUNT [DEVICE]
+ * Run:   sparc_driver DIR FIRST COUNT [DEVICE | --dry-run]
+ * --dry-run reads and checks the inputs, prints one summary line and exits
+ * without touching a device.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -57,12 +61,13 @@ static double *field(const char *dir, const char *name, size_t count) {
 
 int main(int argc, char **argv) {
   if (argc < 4) {
-    fprintf(stderr, "usage: %s DIR FIRST COUNT [DEVICE]\n", argv[0]);
+    fprintf(stderr, "usage: %s DIR FIRST COUNT [DEVICE | --dry-run]\n", argv[0]);
     return 1;
   }
   const char *dir = argv[1];
   const long long first = atoll(argv[2]), count = atoll(argv[3]);
-  const int device = argc > 4 ? atoi(argv[4]) : 0;
+  const int dry = argc > 4 && strcmp(argv[4], "--dry-run") == 0;
+  const int device = argc > 4 && !dry ? atoi(argv[4]) : 0;
   size_t n = 0;
   sparc_params *p = (sparc_params *)slurp(dir, "params.bin", &n);
   if (!p || n != sizeof *p) {
@@ -89,6 +94,44 @@ int main(int argc, char **argv) {
     fprintf(stderr, "source.bin: want %zu bytes\n", sizeof *src);
     return 1;
   }
+  sparc_pulse *pulses = NULL;
+  double *series = NULL;
+  if (src) {
+    src->pulses = NULL;
+    src->series = NULL;
+    if (src->kind == SPARC_SRC_PSR) {
+      pulses = (sparc_pulse *)slurp(dir, "pulses.bin", &n);
+      if (!pulses || n % sizeof(sparc_pulse) != 0) {
+        fprintf(stderr, "pulses.bin: whole sparc_pulse records wanted\n");
+        return 1;
+      }
+      src->npulses = (int32_t)(n / sizeof(sparc_pulse));
+      src->pulses = pulses;
+    } else if (src->kind == SPARC_SRC_RANDOM) {
+      if (src->nseries < 1) {
+        fprintf(stderr, "source.bin: nseries must be >= 1\n");
+        return 1;
+      }
+      series = field(dir, "series.bin", (size_t)p->nx * p->ny * (size_t)src->nseries);
+      if (!series) {
+        fprintf(stderr, "series.bin missing or of the wrong size\n");
+        return 1;
+      }
+      src->series = series;
+    } else {
+      src->npulses = 0;
+    }
+  }
+  if (dry) {
+    double ssum = 0.0;
+    if (series)
+      for (size_t q = 0; q < (size_t)p->nx * p->ny * (size_t)src->nseries; ++q) ssum += series[q];
+    printf("inputs ok: %d x %d x %d, magnetic %d, source %d, pulses %d, series %d (sum %.17g)\n",
+           p->nx, p->ny, p->nz, p->magnetic, src ? src->kind : -1,
+           src && src->kind == SPARC_SRC_PSR ? src->npulses : 0,
+           src && src->kind == SPARC_SRC_RANDOM ? src->nseries : 0, ssum);
+    return 0;
+  }
 
   sparc_handle *h = NULL;
   int r = sparc_create(p, device, &h);
@@ -97,12 +140,7 @@ int main(int argc, char **argv) {
     return r == SPARC_ERR_NODEVICE ? 3 : 2;
   }
   r = sparc_set_background(h, rho0, pre0, cs0, bx0, by0, bz0, zaxis, grav);
-  if (r == SPARC_OK && src) {
-    src->pulses = NULL;  /* raw files carry no pulse table or series */
-    src->npulses = 0;
-    src->series = NULL;
-    r = sparc_set_source(h, src);
-  }
+  if (r == SPARC_OK && src) r = sparc_set_source(h, src);
   int status = 0;
   for (long long nn = first; r == SPARC_OK && nn < first + count; ++nn) {
     r = sparc_step(h, nn);
@@ -127,6 +165,8 @@ int main(int argc, char **argv) {
   sparc_destroy(h);
   free(p);
   free(src);
+  free(pulses);
+  free(series);
   free(rho0); free(pre0); free(cs0); free(zaxis); free(grav);
   free(bx0); free(by0); free(bz0);
   return status;

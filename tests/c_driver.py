@@ -6,6 +6,8 @@ import subprocess
 
 import numpy as np
 
+from sparc2_b200 import abi
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 SRC = os.path.join(ROOT, "sparc2_b200", "host", "sparc_driver.c")
 LIBDIR = os.path.join(ROOT, "sparc2_b200", "_lib")
@@ -29,6 +31,12 @@ def write_inputs(d, params, bg, source=None):
     if source is not None:
         with open(os.path.join(d, "source.bin"), "wb") as f:
             f.write(C.string_at(C.addressof(source), C.sizeof(source)))
+        keep = getattr(source, "_keep", None)
+        if source.kind == abi.SPARC_SRC_PSR:
+            with open(os.path.join(d, "pulses.bin"), "wb") as f:
+                f.write(C.string_at(C.addressof(keep), C.sizeof(keep)))
+        elif source.kind == abi.SPARC_SRC_RANDOM:
+            np.ascontiguousarray(keep, dtype="<f8").tofile(os.path.join(d, "series.bin"))
     names = ["rho0", "pre0", "cs0", "zaxis", "grav"]
     if params.magnetic == 2:
         names += ["bx0", "by0", "bz0"]
@@ -36,6 +44,6 @@ def write_inputs(d, params, bg, source=None):
         np.ascontiguousarray(bg[n], dtype="<f8").tofile(os.path.join(d, n + ".bin"))
 
 
-def run(exe, d, first, count):
-    return subprocess.run([exe, str(d), str(first), str(count)], capture_output=True,
-                          text=True, timeout=600)
+def run(exe, d, first, count, *extra):
+    return subprocess.run([exe, str(d), str(first), str(count), *extra],
+                          capture_output=True, text=True, timeout=600)

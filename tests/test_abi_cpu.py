@@ -125,3 +125,30 @@ def test_c_driver_builds_and_reports_the_missing_device(tmp_path):
     assert "sparc_create" in r.stderr
     (tmp_path / "params.bin").write_bytes(b"short")
     assert c_driver.run(exe, tmp_path, 0, 3).returncode == 1
+
+
+@pytest.mark.parametrize("name", ["quiet_periodic", "mhd_hpml", "quiet_random"])
+def test_c_driver_reads_every_source_kind(tmp_path, name):
+    """The C caller's input files for the pulse, PULSE = 2 and PULSE = 0
+    sources read back as written (its --dry-run needs no device)."""
+    import numpy as np
+    from tests import c_driver, cases
+    exe = c_driver.build(tmp_path)
+    p, bg, src = cases.CASES[name]()
+    c_driver.write_inputs(tmp_path, p, bg, src)
+    r = c_driver.run(exe, tmp_path, 0, 1, "--dry-run")
+    assert r.returncode == 0, r.stderr
+    words = r.stdout.replace(",", "").replace("(", "").replace(")", "").split()
+    assert words[:2] == ["inputs", "ok:"]
+    assert int(words[words.index("source") + 1]) == src.kind
+    npl = int(words[words.index("pulses") + 1])
+    nser = int(words[words.index("series") + 1])
+    if src.kind == abi.SPARC_SRC_PSR:
+        assert npl == len(src._keep) == src.npulses
+    elif src.kind == abi.SPARC_SRC_RANDOM:
+        assert nser == src.nseries
+        assert float(words[words.index("sum") + 1]) == pytest.approx(float(np.sum(src._keep)),
+                                                                    rel=1e-12, abs=1e-9)
+    if src.kind == abi.SPARC_SRC_RANDOM:
+        (tmp_path / "series.bin").write_bytes(b"\0" * 16)
+        assert c_driver.run(exe, tmp_path, 0, 1, "--dry-run").returncode == 1

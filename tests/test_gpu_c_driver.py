@@ -1,7 +1,7 @@
 """The C caller of the ABI (sparc2_b200/host/sparc_driver.c, the driver.f90
-loop: step, diagnostics, filter) on the device: its per-iteration
-diagnostics equal those of the Python host loop over the same library
-calls, bit for bit."""
+loop: step, diagnostics, filter) on the device, with pulse, PULSE = 2 and
+PULSE = 0 sources: its per-iteration diagnostics equal those of the Python
+host loop over the same library calls, bit for bit."""
 import pytest
 
 from sparc2_b200 import Simulation
@@ -10,7 +10,7 @@ from tests import c_driver, cases
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("name", ["quiet_periodic", "mhd_periodic"])
+@pytest.mark.parametrize("name", ["quiet_periodic", "mhd_periodic", "mhd_hpml", "quiet_random"])
 def test_c_driver_matches_the_python_loop(tmp_path, name):
     exe = c_driver.build(tmp_path)
     p, bg, src = cases.CASES[name]()

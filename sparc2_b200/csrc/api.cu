@@ -438,8 +438,8 @@ int sparc_create(const sparc_params *p, int device, sparc_handle **out) {
     if (!h->d_colx) r = SPARC_ERR_NOMEM;
     else {
       h->d_coly = h->d_colx + h->nx;
-      if (cudaMemcpy(h->d_colx, cols.data(), cols.size() * sizeof(int),
-                     cudaMemcpyHostToDevice) != cudaSuccess)
+      if (cudaMemcpyAsync(h->d_colx, cols.data(), cols.size() * sizeof(int),
+                          cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
         r = SPARC_ERR_CUDA;
     }
   }
@@ -482,10 +482,12 @@ int sparc_create(const sparc_params *p, int device, sparc_handle **out) {
   if (!r) {
     long long m1 = -1;
     double d4[4] = {0, 0, 0, -1};
-    if (cudaMemcpy(h->d_fail, &m1, 8, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(h->d_iter, &m1, 8, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(h->d_diag, d4, 32, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemset(h->d_counter, 0, 4) != cudaSuccess)
+    // ordered on the handle's stream; synchronised before m1 and d4 go
+    if (cudaMemcpyAsync(h->d_fail, &m1, 8, cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+        cudaMemcpyAsync(h->d_iter, &m1, 8, cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+        cudaMemcpyAsync(h->d_diag, d4, 32, cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+        cudaMemsetAsync(h->d_counter, 0, 4, h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess)
       r = SPARC_ERR_CUDA;
   }
   if (!r) r = zero_state(h);
@@ -608,8 +610,9 @@ int sparc_set_source(sparc_handle *h, const sparc_source *s) {
     if (!h->d_sdep) h->d_sdep = (double *)dev_alloc(h, (size_t)nz * 8);
     if (!h->d_f2d) h->d_f2d = (double *)dev_alloc(h, (size_t)nx * ny * 8);
     if (!h->d_series || !h->d_sdep || !h->d_f2d) return SPARC_ERR_NOMEM;
-    CK(h, cudaMemcpy(h->d_series, vr.data(), n * 8, cudaMemcpyHostToDevice));
-    CK(h, cudaMemcpy(h->d_sdep, dep.data(), (size_t)nz * 8, cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpyAsync(h->d_series, vr.data(), n * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(h->d_sdep, dep.data(), (size_t)nz * 8, cudaMemcpyHostToDevice,
+                          h->stream));
   }
   if (s->kind == SPARC_SRC_PULSE) {
     // driver.f90:140-145, split into x, y, z factors
@@ -633,7 +636,7 @@ int sparc_set_source(sparc_handle *h, const sparc_source *s) {
       h->d_fy = h->d_fx + nx;
       h->d_fz = h->d_fx + nx + ny;
     }
-    CK(h, cudaMemcpy(h->d_fx, t.data(), t.size() * 8, cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpyAsync(h->d_fx, t.data(), t.size() * 8, cudaMemcpyHostToDevice, h->stream));
   } else if (s->kind == SPARC_SRC_PSR) {
     const int np = s->npulses;
     h->pulses.assign(s->pulses, s->pulses + np);
@@ -689,7 +692,8 @@ int sparc_set_source(sparc_handle *h, const sparc_source *s) {
     auto upd = [&](void *&dst, const void *src, size_t bytes) -> int {
       dst = dev_alloc(h, bytes);
       if (!dst) return SPARC_ERR_NOMEM;
-      if (bytes && cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+      if (bytes && cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream) !=
+                       cudaSuccess)
         return SPARC_ERR_CUDA;
       return SPARC_OK;
     };
@@ -705,7 +709,9 @@ int sparc_set_source(sparc_handle *h, const sparc_source *s) {
     h->d_psr = (double *)dev_alloc(h, std::max<size_t>(8, (size_t)(khi - klo) * nx * ny * 8));
     if (r || !h->d_psr) return r ? r : SPARC_ERR_NOMEM;
   }
+  // the uploads above are ordered on the handle's stream
   if (h->fp32) return source32(h);
+  CK(h, cudaStreamSynchronize(h->stream));
   return SPARC_OK;
 }
 
@@ -732,8 +738,11 @@ static int set_state32(Handle *h, const double *a, const double *psi) {
       const size_t o = (size_t)lk * NXY;
       for (long long n = 0; n < NXY; ++n) t[o + n] = (float)(sc * a[o + n]);
     });
-    CK(h, cudaMemcpy(h->fbuf[h->ra], t.data(), t.size() * 4, cudaMemcpyHostToDevice));
-    CK(h, cudaMemset(h->f_carry, 0, t.size() * 4));
+    // ordered on the handle's (non-blocking) stream, done before t goes
+    CK(h, cudaMemcpyAsync(h->fbuf[h->ra], t.data(), t.size() * 4, cudaMemcpyHostToDevice,
+                          h->stream));
+    CK(h, cudaMemsetAsync(h->f_carry, 0, t.size() * 4, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
   }
   if (psi) {
     size_t off = 0;
@@ -741,7 +750,9 @@ static int set_state32(Handle *h, const double *a, const double *psi) {
       if (F.on) {
         std::vector<float> t(F.cnt * F.P);
         for (size_t n = 0; n < t.size(); ++n) t[n] = (float)psi[off + n];
-        CK(h, cudaMemcpy(F.vars, t.data(), t.size() * 4, cudaMemcpyHostToDevice));
+        CK(h, cudaMemcpyAsync(F.vars, t.data(), t.size() * 4, cudaMemcpyHostToDevice,
+                              h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
         off += t.size();
       }
   }
@@ -785,8 +796,10 @@ int sparc_set_state(sparc_handle *h, const double *a, const double *psi) {
   if (h->fp32) {
     CK(h, cudaStreamSynchronize(h->stream));
     const int r = set_state32(h, a, psi);
-    if (r == SPARC_OK) CK(h, cudaMemset(h->d_err, 0, 4));
-    return r;
+    if (r != SPARC_OK) return r;
+    CK(h, cudaMemsetAsync(h->d_err, 0, 4, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    return SPARC_OK;
   }
   if (a)
     CK(h, cudaMemcpyAsync(h->buf[h->ra], a, (size_t)h->V * h->N * 8,
@@ -800,8 +813,8 @@ int sparc_set_state(sparc_handle *h, const double *a, const double *psi) {
         off += F.cnt * F.P;
       }
   }
+  CK(h, cudaMemsetAsync(h->d_err, 0, 4, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
-  CK(h, cudaMemset(h->d_err, 0, 4));
   return SPARC_OK;
 }
 

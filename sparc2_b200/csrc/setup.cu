@@ -240,11 +240,13 @@ __global__ void k_max(long long N, const double *x, unsigned long long *out) {
     if (!cuda_ok(h, (x), #x)) return SPARC_ERR_CUDA;   \
   } while (0)
 
+// Device copy of n host doubles, ordered on the handle's stream (the set-up
+// kernels run there); a pageable source may be released on return.
 static double *up(Handle *h, const double *src, size_t n) {
   double *d = (double *)dev_alloc(h, n * sizeof(double));
   if (d && src)
-    if (!cuda_ok(h, cudaMemcpy(d, src, n * sizeof(double),
-                               cudaMemcpyHostToDevice), "upload"))
+    if (!cuda_ok(h, cudaMemcpyAsync(d, src, n * sizeof(double), cudaMemcpyHostToDevice,
+                                    h->stream), "upload"))
       return nullptr;
   return d;
 }

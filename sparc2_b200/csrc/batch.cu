@@ -158,18 +158,22 @@ int rebuild(Batch *b) {
   }
   const int counts[4] = {(int)items.size(), (int)fitems.size(), (int)pitems.size(), n_int};
   BCK(b, cudaStreamSynchronize(b->stream));
+  // ordered on the batch stream (its kernels read these), finished before
+  // the host arrays go
   if (!items.empty())
-    BCK(b, cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(int4),
-                      cudaMemcpyHostToDevice));
+    BCK(b, cudaMemcpyAsync(b->d_items, items.data(), items.size() * sizeof(int4),
+                           cudaMemcpyHostToDevice, b->stream));
   if (!fitems.empty())
-    BCK(b, cudaMemcpy(b->d_fitems, fitems.data(), fitems.size() * sizeof(int4),
-                      cudaMemcpyHostToDevice));
+    BCK(b, cudaMemcpyAsync(b->d_fitems, fitems.data(), fitems.size() * sizeof(int4),
+                           cudaMemcpyHostToDevice, b->stream));
   if (!pitems.empty())
-    BCK(b, cudaMemcpy(b->d_pitems, pitems.data(), pitems.size() * sizeof(int4),
-                      cudaMemcpyHostToDevice));
-  BCK(b, cudaMemcpy(b->d_counts, counts, sizeof(counts), cudaMemcpyHostToDevice));
-  BCK(b, cudaMemcpy(b->d_slots, b->slots.data(), b->cap * sizeof(Slot32),
-                    cudaMemcpyHostToDevice));
+    BCK(b, cudaMemcpyAsync(b->d_pitems, pitems.data(), pitems.size() * sizeof(int4),
+                           cudaMemcpyHostToDevice, b->stream));
+  BCK(b, cudaMemcpyAsync(b->d_counts, counts, sizeof(counts), cudaMemcpyHostToDevice,
+                         b->stream));
+  BCK(b, cudaMemcpyAsync(b->d_slots, b->slots.data(), b->cap * sizeof(Slot32),
+                         cudaMemcpyHostToDevice, b->stream));
+  BCK(b, cudaStreamSynchronize(b->stream));
   for (int q = 0; q < b->cap; ++q) b->on_device[q] = b->members[q] != nullptr;
   b->dirty = false;
   return SPARC_OK;
@@ -246,8 +250,9 @@ int sparc_batch_create(int device, int capacity, sparc_batch **out) {
             cudaMalloc(&b->d_slots, capacity * sizeof(Slot32)) == cudaSuccess &&
             cudaMalloc(&b->d_counts, 4 * sizeof(int)) == cudaSuccess &&
             cudaMalloc(&b->d_wctr, 14 * sizeof(unsigned)) == cudaSuccess &&
-            cudaMemset(b->d_slots, 0, capacity * sizeof(Slot32)) == cudaSuccess &&
-            cudaMemset(b->d_counts, 0, 4 * sizeof(int)) == cudaSuccess;
+            cudaMemsetAsync(b->d_slots, 0, capacity * sizeof(Slot32), b->stream) == cudaSuccess &&
+            cudaMemsetAsync(b->d_counts, 0, 4 * sizeof(int), b->stream) == cudaSuccess &&
+            cudaStreamSynchronize(b->stream) == cudaSuccess;
   if (!ok) {
     cudaGetLastError();
     sparc_batch_destroy(b);
@@ -291,7 +296,8 @@ int sparc_batch_add(sparc_batch *b, sparc_handle *hh, int64_t first, int64_t cou
   if (q == b->cap) return bfail(b, SPARC_ERR_NOMEM, "batch is full");
   cudaSetDevice(b->device);
   BCK(b, cudaStreamSynchronize(h->stream));
-  BCK(b, cudaMemcpy(h->d_iter, &first, 8, cudaMemcpyHostToDevice));
+  BCK(b, cudaMemcpyAsync(h->d_iter, &first, 8, cudaMemcpyHostToDevice, h->stream));
+  BCK(b, cudaStreamSynchronize(h->stream));
   Slot32 L{};
   L.S = make_sim32(h);
   L.has_psr = h->src.kind == SPARC_SRC_PSR && h->psr_khi > h->psr_klo;

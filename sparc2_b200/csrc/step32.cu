@@ -1137,8 +1137,8 @@ int setup32(Handle *h) {
   h->f_sc = (float *)dev_alloc(h, sc.size() * sizeof(float));
   if (!h->f_sc) return SPARC_ERR_NOMEM;
   h->f_isc = h->f_sc + (size_t)V * nz;
-  if (cudaMemcpy(h->f_sc, sc.data(), sc.size() * sizeof(float), cudaMemcpyHostToDevice) !=
-      cudaSuccess)
+  if (cudaMemcpyAsync(h->f_sc, sc.data(), sc.size() * sizeof(float), cudaMemcpyHostToDevice,
+                      s) != cudaSuccess)
     return SPARC_ERR_CUDA;
   // background
   struct Src {

@@ -96,6 +96,32 @@ class SparcDiag(C.Structure):
     ]
 
 
+class SparcTrol(C.Structure):
+    """include/sparc_trol.h: a .trol parameter file as read by
+    sparc_read_trol (READ_SPARC_PARAMETERS, initialize.f90:1385-1924)."""
+    _fields_ = [
+        ("params", SparcParams), ("source", SparcSource),
+        ("pulse", C.c_int32), ("psr_npulses", C.c_int32),
+        ("restart", C.c_int32), ("time0", C.c_int32),
+        ("twod", C.c_int32), ("twop5d", C.c_int32), ("displ", C.c_int32),
+        ("flows", C.c_int32), ("damping", C.c_int32),
+        ("timestamp_size", C.c_int32),
+        ("xcb", C.c_int32), ("xct", C.c_int32), ("ycb", C.c_int32),
+        ("yct", C.c_int32), ("zcb", C.c_int32), ("zct", C.c_int32),
+        ("fullout", C.c_int32), ("chunkout", C.c_int32),
+        ("solartime", C.c_double), ("wall_time", C.c_double),
+        ("fulloutputcad", C.c_double), ("chunkoutputcad", C.c_double),
+        ("minsavtime", C.c_double),
+        ("maxtime", C.c_int64), ("init", C.c_int64),
+        ("xyfreq", C.c_int64), ("zfreq", C.c_int64),
+        ("fulloutputsteps", C.c_int64), ("chunkoutputsteps", C.c_int64),
+        ("num_steps", C.c_int64),
+        ("lines_read", C.c_int32), ("stopped_line", C.c_int32),
+        ("dir_bkg", C.c_char * 200), ("dir_out", C.c_char * 200),
+        ("simname", C.c_char * 240), ("forcingfunc", C.c_char * 200),
+    ]
+
+
 class SparcError(RuntimeError):
     """A negative status returned across the C ABI."""
 
@@ -111,7 +137,7 @@ class SparcError(RuntimeError):
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG_DIR, "_lib", "libsparc_gpu.so")
 
-# Every entry point declared in include/sparc_gpu.h.
+# Every entry point declared in include/sparc_gpu.h and include/sparc_trol.h.
 EXPORTS = [
     "sparc_create", "sparc_destroy", "sparc_set_background",
     "sparc_set_source", "sparc_sizes", "sparc_set_state", "sparc_get_state",
@@ -129,6 +155,7 @@ EXPORTS = [
     "sparc_serve_submit", "sparc_serve_next", "sparc_serve_params",
     "sparc_serve_attach", "sparc_serve_result", "sparc_serve_release",
     "sparc_serve_state", "sparc_serve_stats", "sparc_server_last_error",
+    "sparc_read_trol", "sparc_parse_trol",
 ]
 
 _lib = None
@@ -140,6 +167,8 @@ def _declare(lib):
     h = C.c_void_p
     sig = {
         "sparc_create": (C.c_int, [P(SparcParams), C.c_int, P(C.c_void_p)]),
+        "sparc_read_trol": (C.c_int, [C.c_char_p, P(SparcTrol), C.c_char_p, C.c_int]),
+        "sparc_parse_trol": (C.c_int, [C.c_char_p, P(SparcTrol), C.c_char_p, C.c_int]),
         "sparc_destroy": (C.c_int, [h]),
         "sparc_set_background": (C.c_int, [h, d, d, d, d, d, d, d, d]),
         "sparc_set_source": (C.c_int, [h, P(SparcSource)]),

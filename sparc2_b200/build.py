@@ -27,6 +27,9 @@ UNITS = {
     "serve.cu": [],
 }
 HEADERS = ["internal.h", "mhd_body.cuh"]
+# host C units (gcc): the .trol reader
+HOST_UNITS = {"sparc_trol.c": ["-O2", "-std=c99", "-Wall", "-fPIC"]}
+HOST = os.path.join(HERE, "host")
 
 
 def nvcc():
@@ -49,6 +52,16 @@ def build(force=False, verbose=False, ptxas_v=False):
     hdrs = [os.path.join(CSRC, h) for h in HEADERS]
     hdrs.append(os.path.join(HERE, "..", "include", "sparc_gpu.h"))
     objs = []
+    for unit, flags in HOST_UNITS.items():
+        src = os.path.join(HOST, unit)
+        obj = os.path.join(BUILD, unit + ".o")
+        objs.append(obj)
+        deps = [src, os.path.join(HERE, "..", "include", "sparc_trol.h"), hdrs[-1], __file__]
+        if force or _stale(obj, deps):
+            cmd = ["gcc", *flags, "-I", os.path.join(HERE, "..", "include"), "-c", src, "-o", obj]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.check_call(cmd)
     for unit, extra in UNITS.items():
         src = os.path.join(CSRC, unit)
         obj = os.path.join(BUILD, unit + ".o")

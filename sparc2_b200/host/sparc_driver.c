@@ -13,6 +13,13 @@
  *   pulses.bin  npulses sparc_pulse         (source.bin kind PULSE = 2)
  *   series.bin  nx*ny*nseries doubles       (source.bin kind PULSE = 0)
  * source.bin is optional; its pointer fields are replaced by the tables.
+ * With --trol FILE the parameters and the source come from the reference's
+ * .trol control file instead of params.bin and source.bin (sparc_read_trol,
+ * READ_SPARC_PARAMETERS); the background files and the PULSE = 2 table /
+ * PULSE = 0 series still come from DIR (the .trol names an HDF5 background,
+ * a FITS forcing cube and a clock-seeded pulse draw, none of which this
+ * caller reads).  FIRST and COUNT may then be "-": the .trol's own run,
+ * iterations init .. maxtime (driver.f90:64-69, 123).
  *
  * Output: one line per iteration, "nn ke_norm min_rho min_p status".
  * Exit status: 0 done, 1 bad input, 2 library error, 3 no usable device,
@@ -20,7 +27,7 @@
  *
  * Build: cc -O2 -I include sparc2_b200/host/sparc_driver.c \
  *           -L sparc2_b200/_lib -lsparc_gpu -Wl,-rpath,sparc2_b200/_lib
- * Run:   sparc_driver DIR FIRST COUNT [DEVICE | --dry-run]
+ * Run:   sparc_driver DIR FIRST COUNT [DEVICE | --dry-run] [--trol FILE]
  * --dry-run reads and checks the inputs, prints one summary line and exits
  * without touching a device.
  */
@@ -29,6 +36,7 @@
 #include <string.h>
 
 #include "sparc_gpu.h"
+#include "sparc_trol.h"
 
 static void *slurp(const char *dir, const char *name, size_t *bytes) {
   char path[4096];
@@ -61,19 +69,49 @@ static double *field(const char *dir, const char *name, size_t count) {
 
 int main(int argc, char **argv) {
   if (argc < 4) {
-    fprintf(stderr, "usage: %s DIR FIRST COUNT [DEVICE | --dry-run]\n", argv[0]);
+    fprintf(stderr, "usage: %s DIR FIRST COUNT [DEVICE | --dry-run] [--trol FILE]\n", argv[0]);
     return 1;
   }
   const char *dir = argv[1];
-  const long long first = atoll(argv[2]), count = atoll(argv[3]);
-  const int dry = argc > 4 && strcmp(argv[4], "--dry-run") == 0;
-  const int device = argc > 4 && !dry ? atoi(argv[4]) : 0;
-  size_t n = 0;
-  sparc_params *p = (sparc_params *)slurp(dir, "params.bin", &n);
-  if (!p || n != sizeof *p) {
-    fprintf(stderr, "params.bin: want %zu bytes\n", sizeof *p);
-    return 1;
+  const char *trol_path = NULL;
+  int dry = 0, device = 0;
+  for (int q = 4; q < argc; ++q) {
+    if (strcmp(argv[q], "--dry-run") == 0) dry = 1;
+    else if (strcmp(argv[q], "--trol") == 0 && q + 1 < argc) trol_path = argv[++q];
+    else device = atoi(argv[q]);
   }
+  size_t n = 0;
+  sparc_params *p = NULL;
+  sparc_source *src = NULL;
+  sparc_trol trol;
+  if (trol_path) {
+    char err[256];
+    if (sparc_read_trol(trol_path, &trol, err, sizeof err) != SPARC_OK) {
+      fprintf(stderr, "%s: %s\n", trol_path, err);
+      return 1;
+    }
+    if (trol.stopped_line)
+      fprintf(stderr, "%s: reading stopped at line %d (a value failed to read), as the "
+              "reference's does\n", trol_path, trol.stopped_line);
+    if (trol.twod || trol.displ || trol.flows || trol.damping) {
+      fprintf(stderr, "%s: TWOD, MODE = 1, FLOWS and DAMPING are not supported\n", trol_path);
+      return 1;
+    }
+    p = (sparc_params *)malloc(sizeof *p);
+    src = (sparc_source *)malloc(sizeof *src);
+    if (!p || !src) return 1;
+    *p = trol.params;
+    *src = trol.source;
+  } else {
+    p = (sparc_params *)slurp(dir, "params.bin", &n);
+    if (!p || n != sizeof *p) {
+      fprintf(stderr, "params.bin: want %zu bytes\n", sizeof *p);
+      return 1;
+    }
+  }
+  const int whole = trol_path && (strcmp(argv[2], "-") == 0 || strcmp(argv[3], "-") == 0);
+  const long long first = whole ? trol.init : atoll(argv[2]);
+  const long long count = whole ? trol.maxtime - trol.init + 1 : atoll(argv[3]);
   const size_t N = (size_t)p->nx * p->ny * p->nz;
   double *rho0 = field(dir, "rho0.bin", N), *pre0 = field(dir, "pre0.bin", N),
          *cs0 = field(dir, "cs0.bin", N), *zaxis = field(dir, "zaxis.bin", p->nz),
@@ -89,10 +127,12 @@ int main(int argc, char **argv) {
     fprintf(stderr, "missing background files\n");
     return 1;
   }
-  sparc_source *src = (sparc_source *)slurp(dir, "source.bin", &n);
-  if (src && n != sizeof *src) {
-    fprintf(stderr, "source.bin: want %zu bytes\n", sizeof *src);
-    return 1;
+  if (!trol_path) {
+    src = (sparc_source *)slurp(dir, "source.bin", &n);
+    if (src && n != sizeof *src) {
+      fprintf(stderr, "source.bin: want %zu bytes\n", sizeof *src);
+      return 1;
+    }
   }
   sparc_pulse *pulses = NULL;
   double *series = NULL;
@@ -126,10 +166,12 @@ int main(int argc, char **argv) {
     double ssum = 0.0;
     if (series)
       for (size_t q = 0; q < (size_t)p->nx * p->ny * (size_t)src->nseries; ++q) ssum += series[q];
-    printf("inputs ok: %d x %d x %d, magnetic %d, source %d, pulses %d, series %d (sum %.17g)\n",
+    printf("inputs ok: %d x %d x %d, magnetic %d, source %d, pulses %d, series %d (sum %.17g)"
+           ", iterations %lld..%lld\n",
            p->nx, p->ny, p->nz, p->magnetic, src ? src->kind : -1,
            src && src->kind == SPARC_SRC_PSR ? src->npulses : 0,
-           src && src->kind == SPARC_SRC_RANDOM ? src->nseries : 0, ssum);
+           src && src->kind == SPARC_SRC_RANDOM ? src->nseries : 0, ssum, first,
+           first + count - 1);
     return 0;
   }
 

@@ -12,6 +12,7 @@ from sparc2_b200 import abi
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "sparc_gpu.h")
+HEADERS = [HEADER, os.path.join(ROOT, "include", "sparc_trol.h")]
 
 
 @pytest.fixture(scope="module")
@@ -22,7 +23,7 @@ def lib():
 
 
 def declared():
-    text = open(HEADER).read()
+    text = "".join(open(h).read() for h in HEADERS)
     return sorted(set(re.findall(r"\b(sparc_[a-z_0-9]+)\s*\(", text)))
 
 
@@ -40,9 +41,10 @@ def _c_layout(tmp_path):
         "sparc_pulse": [f for f, _ in abi.SparcPulse._fields_],
         "sparc_source": [f for f, _ in abi.SparcSource._fields_],
         "sparc_diag": [f for f, _ in abi.SparcDiag._fields_],
+        "sparc_trol": [f for f, _ in abi.SparcTrol._fields_],
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>',
-             f'#include "{HEADER}"', 'int main(void) {']
+             f'#include "{HEADERS[1]}"', 'int main(void) {']
     for s, fs in fields.items():
         lines.append(f'printf("{s} size %zu\\n", sizeof({s}));')
         for f in fs:
@@ -51,7 +53,8 @@ def _c_layout(tmp_path):
     src = tmp_path / "layout.c"
     exe = tmp_path / "layout"
     src.write_text("\n".join(lines))
-    subprocess.check_call(["gcc", "-std=c99", "-o", str(exe), str(src)])
+    subprocess.check_call(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"),
+                           "-o", str(exe), str(src)])
     out = subprocess.check_output([str(exe)]).decode().split("\n")
     res = {}
     for line in out:
@@ -66,7 +69,8 @@ def test_struct_layout_matches_header(tmp_path):
     for cname, cls in (("sparc_params", abi.SparcParams),
                        ("sparc_pulse", abi.SparcPulse),
                        ("sparc_source", abi.SparcSource),
-                       ("sparc_diag", abi.SparcDiag)):
+                       ("sparc_diag", abi.SparcDiag),
+                       ("sparc_trol", abi.SparcTrol)):
         assert lay[(cname, "size")] == C.sizeof(cls), cname
         for f, _ in cls._fields_:
             assert lay[(cname, f)] == getattr(cls, f).offset, (cname, f)
@@ -152,3 +156,24 @@ def test_c_driver_reads_every_source_kind(tmp_path, name):
     if src.kind == abi.SPARC_SRC_RANDOM:
         (tmp_path / "series.bin").write_bytes(b"\0" * 16)
         assert c_driver.run(exe, tmp_path, 0, 1, "--dry-run").returncode == 1
+
+
+@pytest.mark.parametrize("name", ["quiet_periodic", "mhd_hpml"])
+def test_c_driver_reads_a_trol_file(tmp_path, name):
+    """The C caller started from a .trol control file: the grid, physics,
+    source kind and the run's iteration range (init .. maxtime) come from
+    the file (its --dry-run needs no device)."""
+    from tests import c_driver, cases
+    exe = c_driver.build(tmp_path)
+    p, bg, src = cases.CASES[name]()
+    c_driver.write_inputs(tmp_path, p, bg, src)
+    (tmp_path / "params.bin").write_bytes(b"not read with --trol")
+    (tmp_path / "run.trol").write_text(c_driver.trol_text(p, src, solartime_h=0.01))
+    r = c_driver.run(exe, tmp_path, "-", "-", "--dry-run", "--trol", str(tmp_path / "run.trol"))
+    assert r.returncode == 0, r.stderr
+    words = r.stdout.replace(",", "").replace("(", "").replace(")", "").split()
+    assert words[2:5] == [str(p.nx), "x", str(p.ny)] and words[6] == str(p.nz)
+    assert int(words[words.index("magnetic") + 1]) == p.magnetic
+    assert int(words[words.index("source") + 1]) == src.kind
+    maxtime = 2 * (int(36.0 / p.timestep) // 2)
+    assert words[-1] == f"0..{maxtime}"

@@ -30,3 +30,37 @@ def test_c_driver_matches_the_python_loop(tmp_path, name):
         if nn:
             sim.filter_vars(nn)
     sim.close()
+
+
+@pytest.mark.parametrize("name", ["quiet_periodic", "mhd_hpml"])
+def test_c_driver_from_a_trol_file(tmp_path, name):
+    """The C caller started from a .trol file runs the same iterations as
+    the Python loop over the parameters sparc_parse_trol reads from it."""
+    import ctypes as C
+    from sparc2_b200 import abi
+    exe = c_driver.build(tmp_path)
+    p, bg, src = cases.CASES[name]()
+    c_driver.write_inputs(tmp_path, p, bg, src)
+    text = c_driver.trol_text(p, src)
+    (tmp_path / "run.trol").write_text(text)
+    r = c_driver.run(exe, tmp_path, 0, 25, "--trol", str(tmp_path / "run.trol"))
+    assert r.returncode == 0, r.stderr
+    rows = [line.split() for line in r.stdout.strip().splitlines()]
+    t = abi.SparcTrol()
+    lib = abi.load()
+    assert lib.sparc_parse_trol(text.encode(), C.byref(t), None, 0) == abi.SPARC_OK
+    tp = t.params
+    if src.kind == abi.SPARC_SRC_PSR:
+        s2 = src
+    else:
+        s2 = t.source
+    sim = Simulation(tp, bg, s2)
+    for nn in range(25):
+        sim.step(nn)
+        d, st = sim.diagnostics()
+        got = rows[nn]
+        assert int(got[0]) == nn and int(got[4]) == st
+        assert float(got[1]) == d.ke_norm and float(got[2]) == d.min_rho
+        if nn:
+            sim.filter_vars(nn)
+    sim.close()

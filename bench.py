@@ -66,6 +66,12 @@ def parse():
                     help="fp64: plain form; fp32: precision form (depth-scaled "
                     "FP32 state, compensated RK update)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serve", action="store_true",
+                    help="cfg1: skip the bounded serving leg of the default run")
+    ap.add_argument("--serve-rate", type=float, default=5.0,
+                    help="cfg1 serving leg: arrivals per second")
+    ap.add_argument("--serve-duration", type=float, default=30.0,
+                    help="cfg1 serving leg: seconds of arrivals")
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--kernel-steps", type=int, default=10)
     ap.add_argument("--timed-only", action="store_true",
@@ -219,14 +225,20 @@ def cpu_baseline(steps=None, threads=None):
 
 
 def run_reference(args, world, rank):
+    """The reference arm: the oracle (the FP64 C++/OpenMP restatement of the
+    reference; the Fortran/MPI reference cannot be built here) on the
+    headline configuration itself, 256x256x300, with every host thread; one
+    step is one driver iteration (about 6 s on 16 cores)."""
     if rank != 0:
         return
     import oracle
     oracle.build()
     threads = os.cpu_count()
     oracle.set_threads(threads)
-    p, bg, src, desc = workload("cfg1", grid=CPU_SAMPLE)
+    p, bg, src, desc = workload(args.workload if args.workload in ("cfg0", "cfg1")
+                                else "cfg1", grid=args.grid)
     o = oracle.Oracle(p, bg, src)
+    del bg
     o.run(0, args.warmup)
     t = time.perf_counter()
     o.run(args.warmup, args.steps)
@@ -235,15 +247,16 @@ def run_reference(args, world, rank):
     v = pts * args.steps / dt
     sample = (f"each step one driver iteration of the oracle (FP64 C++/OpenMP "
               f"restatement of the reference; the Fortran/MPI reference cannot "
-              f"be built here) on a {CPU_SAMPLE[0]}x{CPU_SAMPLE[1]}x"
-              f"{CPU_SAMPLE[2]} sub-grid of the same flux-tube physics")
+              f"be built here) on the full {p.nx}x{p.ny}x{p.nz} grid of the "
+              f"benchmark configuration, {threads} threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded analytic background and pulse table)",
-        "config": {"workload": desc, "sample_grid": list(CPU_SAMPLE)},
+        "config": {"workload": desc, "grid": [p.nx, p.ny, p.nz],
+                   "same_config": True},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads,
                          "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -372,9 +385,18 @@ def run_gpu(args, world, rank, local):
         sim.close()
         sim = None
         extras["fp32_precision_form"] = measure_fp32_cfg2(dev)
+        extras["fp32_precision_form"]["ratio_vs_fp64_plain"] = \
+            extras["fp32_precision_form"]["value"] / value
+        extras["fp32_precision_form"]["error_vs_oracle"] = fp32_errors(dev)
         extras["fp32_batched"] = measure_ensemble(dev, members=args.members)
         extras["fp32_batched"]["ratio_vs_fp64_plain"] = \
             extras["fp32_batched"]["value"] / value
+        extras["fp32_batched"]["error_vs_oracle"] = fp32_errors(dev, batched=True)
+        if not args.no_serve:
+            sv, _, rec, _, _ = measure_serve(dev, args.serve_rate, args.serve_duration,
+                                             args.steps_scale, args.budget_gb)
+            rec["ratio_vs_fp64_plain"] = sv / value
+            extras["fp32_served"] = rec
 
     if rank != 0:
         if sim is not None:
@@ -438,6 +460,59 @@ def fp64_plain_rate(dev, steps=20, warmup=3):
     ms = e0.elapsed_time(e1) / steps
     sim.close()
     return p.nx * p.ny * p.nz / (ms / 1e3), ms
+
+
+def fp32_errors(dev, batched=False):
+    """Errors of the precision form against the FP64 oracle: the flux-tube
+    physics on 96x96x300 columns (the committed oracle fixture
+    tests/golden/fluxtube_96x96x300.npz, 1000 iterations from rest), run
+    alone or as a member of the batched engine.  Per field, the relative L2
+    and the max-norm error (relative to max |oracle|) over the fixture's
+    strided sample of the state at iterations 100, 500 and 1000."""
+    from sparc2_b200 import Simulation
+    from sparc2_b200.batch import Batch
+    from tests.golden import make_fluxtube_1000 as F
+    path = os.path.join(ROOT, "tests", "golden", F.NAME + ".npz")
+    if not os.path.exists(path):
+        return None
+    ref = np.load(path)
+    p, bg, src = F.config()
+    p.precision = abi.SPARC_FP32
+    sim = Simulation(p, bg, src, device=dev)
+    del bg
+    out = {}
+    done = 0
+    batch = Batch(1, device=dev) if batched else None
+    for it in F.CHECKPOINTS:
+        if batched:
+            q = batch.add(sim, done, it - done)
+            batch.run(it - done)
+            batch.synchronize()
+            batch.remove(q)
+        else:
+            sim.run(done, it - done)
+        done = it
+        a, psi = sim.get_state()
+        samp = F.sample(a, psi)["samp"]
+        rl2, mx = [], []
+        for l in range(samp.shape[0]):
+            o = ref[f"it{it}_samp"][l]
+            g = samp[l]
+            den = np.sqrt(np.sum(o * o))
+            rl2.append(float(np.sqrt(np.sum((g - o) ** 2)) / den) if den > 0 else 0.0)
+            m = np.max(np.abs(o))
+            mx.append(float(np.max(np.abs(g - o)) / m) if m > 0 else 0.0)
+        out[str(it)] = {"rel_l2": rl2, "max_norm": mx,
+                        "max_rel_l2": max(rl2), "max_max_norm": max(mx)}
+    if batch is not None:
+        batch.close()
+    sim.close()
+    return {"against": "FP64 oracle fixture, flux tube 96x96x300 (37.5 Mm, "
+            "CPML 10 on 6 faces, 200 seeded PSR pulses), 1000 iterations from "
+            "rest%s" % (", run as a batch member" if batched else ""),
+            "fields": ["rho", "vx", "vy", "vz", "p", "bx", "by", "bz"],
+            "sample": "every %dth value of each field" % F.STRIDE,
+            "iterations": out}
 
 
 def measure_fp32_cfg2(dev, steps=40, warmup=3):
@@ -653,24 +728,19 @@ def run_ensemble(args, world, rank, local):
     rep.close()
 
 
-def run_serve(args, world, rank, local):
-    """Served solves, FP32: Poisson arrivals (seeded) of requests with
-    random grid, background, source and duration, admitted by a device
-    memory budget into the running batch; latency percentiles beside the
-    served grid-point update rate."""
-    import torch
+def measure_serve(dev, rate, duration, steps_scale, budget_gb=150.0):
+    """Served solves, FP32: seeded Poisson arrivals at `rate` per second for
+    `duration` seconds, request durations scaled by steps_scale, through
+    the serving loop (budget admission into the running batch).  Returns
+    (served rate, stats, the serve record)."""
     from sparc2_b200.serve import Server, drive
-    from sparc2_b200.replicas import Replicas
-    dev = local
-    torch.cuda.set_device(dev)
-    rep = Replicas("nccl")
-    draws = W.serve_draws(args.rate, args.duration,
-                          steps_scale=args.steps_scale)
+    draws = W.serve_draws(rate, duration, steps_scale=steps_scale)
     reqs = []
     for d in draws:
         p = W.member_params(d["nx"], d["nz"], d["B0"])
         reqs.append((d["arrival"], d["key"], p, 0, d["steps"]))
     res = {}
+    timings = {}
 
     def build(key):
         _, bg, src = W.serve_request(draws[key])
@@ -680,22 +750,57 @@ def run_serve(args, world, rank, local):
         d, _ = sim.diagnostics()
         res[key] = (state, times.copy(), d.ke_norm)
 
-    clocks = Clocks(dev)
-    srv = Server(capacity=64, budget_bytes=int(args.budget_gb * 1e9),
-                 quantum=10, device=dev)
-    wall = drive(srv, reqs, build, on_result, builders=4,
-                 deadline_s=20 * args.duration + 600)
+    srv = Server(capacity=64, budget_bytes=int(budget_gb * 1e9), quantum=10, device=dev)
+    wall = drive(srv, reqs, build, on_result, builders=4, prefetch=4, timings=timings,
+                 deadline_s=20 * duration + 600)
     st = srv.stats()
     srv.close()
-    clk = clocks.stop() if clocks else None
     lat = np.array([t[3] - t[0] for _, t, _ in res.values()])
     wait = np.array([t[1] - t[0] for _, t, _ in res.values()])
     setup = np.array([t[2] - t[1] for _, t, _ in res.values()])
     serv = np.array([t[3] - t[2] for _, t, _ in res.values()])
+    hb = np.array([v["host_build_s"] for v in timings.values() if "host_build_s" in v])
+    ds = np.array([v["device_setup_s"] for v in timings.values() if "device_setup_s" in v])
     pu = st["point_updates"]
     offered = sum(d["nx"] * d["nx"] * d["nz"] * d["steps"] for d in draws)
-    value = pu / wall
     pct = lambda a, q: float(np.percentile(a, q)) if a.size else None
+    rec = {"p50_latency_s": pct(lat, 50), "p99_latency_s": pct(lat, 99),
+           "p50_queue_wait_s": pct(wait, 50), "p99_queue_wait_s": pct(wait, 99),
+           "p50_setup_s": pct(setup, 50), "p99_setup_s": pct(setup, 99),
+           "p50_host_input_build_s": pct(hb, 50),
+           "p50_device_setup_s": pct(ds, 50),
+           "p50_service_s": pct(serv, 50), "p99_service_s": pct(serv, 99),
+           "offered_point_updates_per_s": offered / duration,
+           "served_point_updates": pu, "served_rate": pu / wall, "wall_s": wall,
+           "requests": len(draws), "completed": len(res),
+           "max_concurrent": st["max_concurrent"],
+           "max_running_together": st["max_running"],
+           "joined_running_batch": st["joined_running"],
+           "worker_gpu_wait_s": st["worker_gpu_wait_s"],
+           "workload": "served solves, FP32: Poisson arrivals at %g/s for %g s, "
+           "nx=ny in [64,256], nz in [128,300], quiet or flux tube (B0 0.5-3 kG), "
+           "one pulse or 50-500 PSR pulses, 500-4000 iterations x %g"
+           % (rate, duration, steps_scale),
+           "note": "latency = done - submit; set-up = start - admit (the admitted "
+           "request's device set-up and attach; host inputs are built ahead of "
+           "admission); the offered load is several times what one B200 serves"}
+    return pu / wall, st, rec, len(draws), len(res)
+
+
+def run_serve(args, world, rank, local):
+    """Served solves, FP32: Poisson arrivals (seeded) of requests with
+    random grid, background, source and duration, admitted by a device
+    memory budget into the running batch; latency percentiles beside the
+    served grid-point update rate."""
+    import torch
+    from sparc2_b200.replicas import Replicas
+    dev = local
+    torch.cuda.set_device(dev)
+    rep = Replicas("nccl")
+    clocks = Clocks(dev)
+    value, st, rec, nreq, ndone = measure_serve(dev, args.rate, args.duration,
+                                                args.steps_scale, args.budget_gb)
+    clk = clocks.stop() if clocks else None
     if rank != 0:
         rep.close()
         return
@@ -710,17 +815,9 @@ def run_serve(args, world, rank, local):
                    "flux tube (B0 0.5-3 kG), one pulse or 50-500 PSR pulses, "
                    "500-4000 iterations x %g" % (args.rate, args.duration,
                                                   args.steps_scale),
-                   "requests": len(draws), "completed": len(res),
+                   "requests": nreq, "completed": ndone,
                    "budget_gb": args.budget_gb, "slots": 64, "quantum": 10},
-        "serve": {"p50_latency_s": pct(lat, 50), "p99_latency_s": pct(lat, 99),
-                  "p50_queue_wait_s": pct(wait, 50),
-                  "p99_queue_wait_s": pct(wait, 99),
-                  "p50_setup_s": pct(setup, 50),
-                  "p50_service_s": pct(serv, 50), "p99_service_s": pct(serv, 99),
-                  "offered_point_updates_per_s": offered / args.duration,
-                  "served_point_updates": pu, "wall_s": wall,
-                  "max_concurrent": st["max_concurrent"],
-                  "worker_gpu_wait_s": st["worker_gpu_wait_s"]},
+        "serve": rec,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": None,
                 "d2h_bytes_per_step": None,
                 "note": "the served rate is end to end: host background "

@@ -214,16 +214,22 @@ const char *sparc_last_error(const sparc_handle *h);
 
 /* ------------------------------------------------ allocation-free path
  * No counterpart in the reference.  The kinetic-energy norm of the handle's
- * current state -- the quantity sparc_diagnostics reports as ke_norm
- * (driver.f90:161, norm() of all_modules.f90:684-706) -- computed without
- * allocating memory: the reduction's scratch is a static device array of
- * 33,024 bytes, so grids above 67,108,864 points are rejected
- * (SPARC_ERR_INVALID).  For callers that must not allocate, e.g. a monitor
- * polling a simulation whose device memory is fully committed to the
- * serving loop's budget.  The scratch is shared by every call on a device:
- * calls that overlap in time race and must be serialised by the caller.
- * The first call on a device looks up the scratch address; make it before
- * any stream capture.  Waits for the handle's stream. */
+ * current state (norm() of all_modules.f90:684-706 as driver.f90:161 uses
+ * it) computed without allocating memory: the reduction's scratch is a
+ * static device array of 33,024 bytes, so grids above 67,108,864 points are
+ * rejected (SPARC_ERR_INVALID).  For callers that must not allocate, e.g. a
+ * monitor polling a simulation whose device memory is fully committed to
+ * the serving loop's budget.  It equals sparc_diagnostics' ke_norm only
+ * when called right after an iteration's stages, before that iteration's
+ * filter (sparc_filter_vars, or a filter iteration inside sparc_run) or a
+ * sparc_set_state replaces the state; sparc_diagnostics keeps the norm of
+ * the stage-5 state as driver.f90:161 does before FILTER_VARS.  Works on a
+ * batch member too (it reads the member's live state buffer, ordered on the
+ * batch's stream).  The scratch is shared by every call on a device: calls
+ * that overlap in time race and must be serialised by the caller.  The
+ * first call on a device looks up the scratch address; make it before any
+ * stream capture, and not after cudaDeviceReset (the cached address does
+ * not survive a reset).  Waits for the handle's (or batch's) stream. */
 int sparc_ke_norm_noalloc(sparc_handle *h, double *ke_norm);
 
 /* ---------------------------------------------------- failure injection
@@ -346,10 +352,12 @@ int sparc_serve_release(sparc_server *s, int64_t ticket);
 
 int sparc_serve_state(sparc_server *s, int64_t ticket, int *state);
 
-/* stats[0..9]: queued, admitted, running, done, budget bytes in use, max
- * concurrent requests, batched steps run, service rounds, grid-point
- * updates, seconds the worker waited on batched steps. */
-int sparc_serve_stats(sparc_server *s, double *stats10);
+/* stats[0..11]: queued, admitted, running, done, budget bytes in use, max
+ * concurrent requests (admitted or running), batched steps run, service
+ * rounds, grid-point updates, seconds the worker waited on batched steps,
+ * max requests running in the batch at once, requests attached while
+ * others were running (their work joined a batch already on the device). */
+int sparc_serve_stats(sparc_server *s, double *stats12);
 
 const char *sparc_server_last_error(const sparc_server *s);
 

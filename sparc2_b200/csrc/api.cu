@@ -222,19 +222,19 @@ static int filter_kind(Handle *h, long long nn) {
   return fk;
 }
 
-// precision form: the filtered state starts a new compensated sum (its
-// carry is cleared after the passes)
+// precision form: the first pass of an event filters the compensated
+// value stored - carry; the filtered state starts a new compensated sum
+// (its carry is cleared after the passes)
 static int enqueue_filter32(Handle *h, int fk, cudaStream_t s, int *nk) {
   int r = SPARC_OK;
-  if (fk & 1) {
-    for (int dir = 1; dir >= 0; --dir) {  // y, then x
-      r |= launch_filter32(h, dir, h->fbuf[h->ra], h->fbuf[h->rf1], s);
-      rotate(h);
-      ++*nk;
-    }
+  if (fk & 1) {  // y then x, fused
+    r |= launch_filter_event32(h, true, h->fbuf[h->ra], h->f_carry, h->fbuf[h->rf1], s);
+    rotate(h);
+    ++*nk;
   }
   if (fk & 2) {
-    r |= launch_filter32(h, 2, h->fbuf[h->ra], h->fbuf[h->rf1], s);
+    r |= launch_filter_event32(h, false, h->fbuf[h->ra], (fk & 1) ? nullptr : h->f_carry,
+                               h->fbuf[h->rf1], s);
     rotate(h);
     ++*nk;
   }
@@ -246,15 +246,13 @@ static int enqueue_filter32(Handle *h, int fk, cudaStream_t s, int *nk) {
 static int enqueue_filter(Handle *h, int fk, cudaStream_t s, int *nk) {
   if (h->fp32) return enqueue_filter32(h, fk, s, nk);
   int r = SPARC_OK;
-  if (fk & 1) {
-    for (int dir = 1; dir >= 0; --dir) {  // y, then x
-      r |= launch_filter_pass(h, dir, h->buf[h->ra], h->buf[h->rf1], s);
-      rotate(h);
-      ++*nk;
-    }
+  if (fk & 1) {  // y then x, fused
+    r |= launch_filter_event(h, true, h->buf[h->ra], h->buf[h->rf1], s);
+    rotate(h);
+    ++*nk;
   }
   if (fk & 2) {
-    r |= launch_filter_pass(h, 2, h->buf[h->ra], h->buf[h->rf1], s);
+    r |= launch_filter_event(h, false, h->buf[h->ra], h->buf[h->rf1], s);
     rotate(h);
     ++*nk;
   }
@@ -422,8 +420,18 @@ int sparc_create(const sparc_params *p, int device, sparc_handle **out) {
   if (const char *kv = std::getenv("SPARC_TMA64"))  // A/B timing only
     h->allow_tma64 = std::atoi(kv) != 0;
   int r = SPARC_OK;
-  if (!cuda_ok(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream") ||
-      !cuda_ok(h, cudaStreamCreateWithFlags(&h->aux, cudaStreamNonBlocking), "stream") ||
+  // A handle's streams take the device's greatest priority: when a handle
+  // is set up beside a running batch (serving), its set-up kernels are
+  // scheduled ahead of the batch launches queued at the same time.
+  int prio_least = 0, prio_greatest = 0;
+  if (cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest) != cudaSuccess) {
+    cudaGetLastError();
+    prio_greatest = 0;
+  }
+  if (!cuda_ok(h, cudaStreamCreateWithPriority(&h->stream, cudaStreamNonBlocking, prio_greatest),
+               "stream") ||
+      !cuda_ok(h, cudaStreamCreateWithPriority(&h->aux, cudaStreamNonBlocking, prio_greatest),
+               "stream") ||
       !cuda_ok(h, cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming), "event") ||
       !cuda_ok(h, cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming), "event")) {
     r = SPARC_ERR_CUDA;

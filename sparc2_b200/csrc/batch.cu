@@ -225,6 +225,25 @@ int pull_all(Batch *b) {
 
 }  // namespace
 
+namespace sparc {
+
+// The slot of batch member h: its device slot when the slot table holding
+// it has been uploaded (the device then owns its buffer roles), else null
+// (the handle's own roles are still current).
+int batch_member_slot(const Handle *h, const Slot32 **dslot) {
+  *dslot = nullptr;
+  const Batch *b = static_cast<const Batch *>(h->batch);
+  if (!b) return SPARC_ERR_INVALID;
+  for (int q = 0; q < b->cap; ++q)
+    if (b->members[q] == h) {
+      if (b->on_device[q]) *dslot = b->d_slots + q;
+      return SPARC_OK;
+    }
+  return SPARC_ERR_INVALID;
+}
+
+}  // namespace sparc
+
 extern "C" {
 
 int sparc_batch_create(int device, int capacity, sparc_batch **out) {
@@ -286,8 +305,6 @@ int sparc_batch_add(sparc_batch *b, sparc_handle *hh, int64_t first, int64_t cou
   if (!b || !hh || count < 0) return SPARC_ERR_INVALID;
   Handle *h = reinterpret_cast<Handle *>(hh);
   if (!h->fp32) return bfail(b, SPARC_ERR_INVALID, "batched simulations use SPARC_FP32");
-  if (h->src.kind == SPARC_SRC_RANDOM)
-    return bfail(b, SPARC_ERR_INVALID, "a random-source (PULSE = 0) simulation runs alone");
   if (!h->bg_ready) return bfail(b, SPARC_ERR_ORDER, "set the background first");
   if (h->batch) return bfail(b, SPARC_ERR_ORDER, "handle is already in a batch");
   if (h->device != b->device) return bfail(b, SPARC_ERR_INVALID, "handle on another device");
@@ -302,6 +319,16 @@ int sparc_batch_add(sparc_batch *b, sparc_handle *hh, int64_t first, int64_t cou
   L.S = make_sim32(h);
   L.has_psr = h->src.kind == SPARC_SRC_PSR && h->psr_khi > h->psr_klo;
   if (L.has_psr) L.psr = make_psr32(h);
+  L.has_rnd = h->src.kind == SPARC_SRC_RANDOM;
+  if (L.has_rnd) {  // the member's own forcing plane, rebuilt every step
+    L.rnd.series = h->d_series;
+    L.rnd.damp = h->f_sd;
+    L.rnd.out = h->f_f2d;
+    L.rnd.nxy = h->nx * h->ny;
+    L.rnd.ns = h->src.nseries;
+    L.rnd.timestep = h->P.timestep;
+    L.rnd.cad = h->src.cadforcing;
+  }
   for (int i = 0; i < 3; ++i) L.buf[i] = h->fbuf[i];
   L.role[0] = h->ra;
   L.role[1] = h->rf1;

@@ -61,6 +61,7 @@ struct SimT {
   int nx, ny, nz;
   long long N;
   int periodic, magnetic, bg1d;
+  int sponge_slabs;            // the sponge vanishes outside the CPML slabs
   int V;
   double stretchx, stretchy;
   const R *stretch;            // nz
@@ -101,6 +102,16 @@ struct Psr32 {
   const long long *iter;
 };
 
+// PULSE = 0 forcing of a batch member: the series, source_damp(:,:,1) and
+// the member's forcing plane, rebuilt at the start of each batched step.
+struct Rnd32 {
+  const double *series;        // nxy * ns, times randomexciteampl / dimc
+  const float *damp;           // nxy
+  float *out;                  // nxy (the plane the stage kernels read)
+  int nxy, ns;
+  double timestep, cad;
+};
+
 // One simulation of a batch, as the batched kernels read it.  Buffer roles,
 // the steps left and the completion counter live here and are advanced on
 // the device, so a captured step stays valid while simulations come and go.
@@ -113,6 +124,8 @@ struct Slot32 {
   long long remaining;         // driver iterations left
   int active;                  // set at the start of each step
   int has_psr;
+  int has_rnd;
+  Rnd32 rnd;
   int first_item, n_items;     // stage items of the interior part (MHD only)
   int first_item2, n_items2;   // stage items of the general part
   int f_first, f_items;        // filter work-list range
@@ -184,6 +197,9 @@ struct Handle {
   FaceDev faces[6]{};  // z_bot, z_top, x_bot, x_top, y_bot, y_top
   std::vector<double> g_blk;  // host copy of the gravity table
   bool bg1d = false;
+  // the sponge is zero outside the CPML slabs (the base sponges of
+  // initialize.f90:899-947 all vanish): stage kernels skip its loads there
+  bool sponge_slabs = false;
 
   // forcing
   sparc_source src{};
@@ -273,6 +289,7 @@ int launch_stage(Handle *h, const SimDev &S, int stage, const double *a,
                  const double *tin, double *tout, cudaStream_t s);
 int launch_psr_forcing(Handle *h, const SimDev &S, cudaStream_t s);
 int launch_random_forcing(Handle *h, cudaStream_t s);
+int launch_filter_event(Handle *h, bool xy, const double *in, double *out, cudaStream_t s);
 int launch_filter_pass(Handle *h, int dir, const double *in, double *out,
                        cudaStream_t s);
 int stage_geometry(Handle *h);
@@ -288,9 +305,15 @@ Psr32 make_psr32(Handle *h);
 int launch_batch_step(const BatchLaunch &B, cudaStream_t s, int *nkernels);
 size_t batch_stage_smem();
 int launch_filter32(Handle *h, int dir, const float *in, float *out, cudaStream_t s);
+int launch_filter_event32(Handle *h, bool xy, const float *in, const float *carry, float *out,
+                          cudaStream_t s);
 int encode_tensor_maps32(Handle *h);
 int setup32(Handle *h);
 int source32(Handle *h);
+
+// batch.cu: the device slot of batch member h (null while the slot table
+// holding it has not been uploaded)
+int batch_member_slot(const Handle *h, const Slot32 **dslot);
 
 // api.cu
 void *dev_alloc(Handle *h, size_t bytes);

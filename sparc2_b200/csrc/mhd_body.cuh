@@ -466,9 +466,27 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
     pos(tid, hs0, ho0);
     if (role == 1) pos(tid + NC, hs1, ho1);
   }
-  const unsigned own_bytes =
-      (MODE == F_FIRST ? 15u : (MODE == F_MID ? 23u : 24u)) * NC * (unsigned)sizeof(R) +
-      (TH ? (unsigned)(NH * HXL * HY * sizeof(R)) : 0u);
+  // Own-point arrays not read: in the plain form rhoinv (the kernel forms
+  // 1/rho0, the same IEEE quotient initialize.f90:1012 stores; the
+  // precision form, closer to issue-bound, measured faster loading it) and,
+  // where the sponge vanishes outside the CPML slabs, the sponge of layers
+  // whose points lie in no slab (a CTA-uniform test per layer).
+  constexpr bool DERIVE_RI = sizeof(R) == 8;
+  const bool slab_xy = !INT && ((S.xb.on && (x0 < S.xb.np || x0 + TX > nx - S.xt.np)) ||
+                                (S.yb.on && (y0 < S.yb.np || y0 + TY > ny - S.yt.np)));
+  auto sponge_at = [&](int k) -> bool {
+    return !S.sponge_slabs || slab_xy || (S.zb.on && (k < S.zb.np || k >= nz - S.zt.np));
+  };
+  auto skip_own = [&](int c, int k) -> bool {
+    return (MODE == F_FIRST && c >= O_A && c < O_BG) || (MODE != F_LAST && c == O_P0) ||
+           (DERIVE_RI && c == O_BG + B_RHOINV) || (c == O_BG + B_SPONGE && !sponge_at(k));
+  };
+  auto own_bytes = [&](int k) -> unsigned {
+    return ((MODE == F_FIRST ? 15u : (MODE == F_MID ? 23u : 24u)) - (DERIVE_RI ? 1u : 0u) -
+            (sponge_at(k) ? 0u : 1u)) *
+               NC * (unsigned)sizeof(R) +
+           (TH ? (unsigned)(NH * HXL * HY * sizeof(R)) : 0u);
+  };
   auto issue = [&](int k, int b) {
     const int kb = k * NXY;
     if (!TH && hs0 >= 0) {
@@ -500,8 +518,11 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
       } else {
         const R *bg[14] = {S.red, S.sponge, S.rho0, S.grx, S.gry, S.grz,
                                S.c2rho0, S.gpx, S.gpy, S.gpz, S.rhoinv, S.cbx, S.cby, S.cbz};
+        const bool spg = sponge_at(k);
 #pragma unroll
-        for (int n = 0; n < 14; ++n) cp_r(ob + (O_BG + n) * NC, bg[n] + id);
+        for (int n = 0; n < 14; ++n)
+          if ((!DERIVE_RI || n != B_RHOINV) && (n != B_SPONGE || spg))
+            cp_r(ob + (O_BG + n) * NC, bg[n] + id);
         if (MODE == F_LAST) cp_r(ob + O_P0 * NC, S.p0 + id);
       }
     }
@@ -511,12 +532,12 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
     // background arrays, p0); with TH, copy 24 + s is halo plane s (state
     // fields 1..7, then B0 x, y, z)
     if (TMA && tid < 32) {
-      if (tid == 0) mbar_tx_t(&bar[b], own_bytes);
+      if (tid == 0) mbar_tx_t(&bar[b], own_bytes(k));
       __syncwarp();
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       R *ob = smem + b * BUF;
       for (int c = tid; c < (TH ? NO + NH : NO); c += 32) {
-        if ((MODE == F_FIRST && c >= O_A && c < O_BG) || (MODE != F_LAST && c == O_P0)) continue;
+        if (skip_own(c, k)) continue;
         int map = mt, xx = x0, yy = y0, z = k;
         R *dst = ob + c * NC;
         if (c >= O_A && c < O_BG) {
@@ -744,14 +765,15 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
       const R fac = MODE == F_LAST ? dt : bnext;
       const R rho = O(b, O_RHO) * IS(0, k), vx = Hv(0) * iv, vy = Hv(1) * iv,
                   vz = Hv(2) * iv;
-      const R red = O(b, O_BG + B_RED), sg = O(b, O_BG + B_SPONGE);
+      const R red = O(b, O_BG + B_RED);
+      const R sg = sponge_at(k) ? O(b, O_BG + B_SPONGE) : R(0);
       if (role == 0) {
         own_loads();
         const R ib = IS(5, k);
         const R dzby = X[NC + cid];
         const R cbx = d4 - dzby, cby = d5, cbz = d7;
         const R c1 = cby * oz - cbz * oy, c2 = ox * cbz - cbx * oz, c3 = cbx * oy - cby * ox;
-        const R ri = O(b, O_BG + B_RHOINV);
+        const R ri = DERIVE_RI ? R(1) / O(b, O_BG + B_RHO0) : O(b, O_BG + B_RHOINV);
         R vxr = -ri * (d0 - (c1 * red)) - sg * vx;
         R vyr = -ri * (d1 - (c2 * red)) - sg * vy;
         R vzr = -ri * (d2 - (c3 * red)) - sg * vz;

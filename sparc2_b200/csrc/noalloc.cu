@@ -1,7 +1,12 @@
 // noalloc.cu -- sparc_ke_norm_noalloc: the kinetic-energy norm of a handle's
-// current state (the quantity sparc_diagnostics reports as ke_norm,
-// driver.f90:161 with norm() of all_modules.f90:684-706), computed without
-// allocating any memory.
+// current state (norm() of all_modules.f90:684-706 as driver.f90:161 uses
+// it), computed without allocating any memory.  It equals the ke_norm of
+// sparc_diagnostics when called right after an iteration's stages, before
+// that iteration's filter or a sparc_set_state replaces the state.
+//
+// For a handle in a batch the batch owns the buffer roles and rotates them
+// on the device every step; the kernel then reads the live role from the
+// member's device slot instead of the handle's (stale) host copy.
 //
 // The reduction is a variant of the last-block-done diagnostics reduction
 // of the stage kernels.  Its scratch is the file-scope static device array
@@ -20,6 +25,9 @@
 // Setup: the first call on a device looks up the scratch's device address
 // with cudaGetSymbolAddress (that device current) and caches it; the first
 // call on each device should therefore happen before any stream capture.
+// The cached address belongs to the device's primary context as it was at
+// that first call: after cudaDeviceReset (which tears that context down)
+// the cache is stale, so do not use this entry point after a reset.
 
 #include <mutex>
 
@@ -46,9 +54,10 @@ struct KeSrc {
   const double *a;                       // FP64 form
   const float *fa, *carry, *isc, *frho0; // FP32 form
   const double *rho0;
+  const Slot32 *slot;                    // batch member: live roles (or null)
 };
 
-__device__ __forceinline__ double ke_density(const KeSrc &S, long long n) {
+__device__ __forceinline__ double ke_density(const KeSrc &S, const float *fa, long long n) {
   const int k = (int)(n / S.NXY);
   double r, v1, v2, v3, r0;
   if (S.a) {
@@ -60,7 +69,7 @@ __device__ __forceinline__ double ke_density(const KeSrc &S, long long n) {
   } else {
     auto ph = [&](int l) {
       const long long q = l * S.N + n;
-      return ((double)S.fa[q] - (double)S.carry[q]) * (double)S.isc[l * S.nz + k];
+      return ((double)fa[q] - (double)S.carry[q]) * (double)S.isc[l * S.nz + k];
     };
     r = ph(0);
     v1 = ph(1);
@@ -81,9 +90,11 @@ __global__ void __launch_bounds__(kNoallocThreads)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const long long p0 = (long long)blockIdx.x * kBlockPoints;
   const long long p1 = min(S.N, p0 + kBlockPoints);
+  // a batch member's state is the buffer of its slot's current role 0
+  const float *fa = S.slot ? S.slot->buf[S.slot->role[0]] : S.fa;
   double s = 0.0;
   for (long long n = p0 + tid; n < p1; n += kNoallocThreads) {
-    const double m = ke_density(S, n);
+    const double m = ke_density(S, fa, n);
     s += m * m;
   }
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
@@ -161,6 +172,15 @@ extern "C" int sparc_ke_norm_noalloc(sparc_handle *hh, double *ke_norm) {
   S.N = h->N;
   S.NXY = (long long)h->nx * h->ny;
   S.nz = h->nz;
+  if (h->batch) {
+    // the batch owns the roles: read the live one from the member's device
+    // slot (until the batch's first upload the handle's roles are current)
+    r = batch_member_slot(h, &S.slot);
+    if (r) {
+      h->err = "handle's batch does not list it";
+      return r;
+    }
+  }
   if (h->fp32) {
     S.fa = h->fbuf[h->ra];
     S.carry = h->f_carry;

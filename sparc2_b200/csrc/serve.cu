@@ -88,6 +88,11 @@ struct Server {
   std::vector<int64_t> to_attach;
   int active = 0;  // ADMITTED + RUNNING
   int max_active = 0;
+  int running = 0, max_running = 0;  // members of the batch
+  int64_t joined = 0;                // attached while others were running
+  // steps per round: as many as fit in about round_s seconds (at most
+  // quantum), so a built request waits about that long to be attached
+  double round_s = 0.25, step_s = 0.0;
   int64_t steps_run = 0, rounds = 0;
   double point_updates = 0, gpu_busy_s = 0;
   std::string err;
@@ -151,20 +156,27 @@ static void serve_loop(Server *s) {
       t->left = t->steps;
       t->state = SPARC_REQ_RUNNING;
       t->t_start = s->now();
+      if (s->running > 0) ++s->joined;
+      ++s->running;
+      s->max_running = std::max(s->max_running, s->running);
       s->used -= t->reserved - t->resident;  // set-up memory is released
       t->reserved = t->resident;
       pts[slot] = (double)t->p.nx * t->p.ny * t->p.nz;
       work = true;
     }
     if (!work) continue;
+    int steps = s->quantum;
+    if (s->step_s > 0.0)
+      steps = std::max(1, std::min(s->quantum, (int)(s->round_s / s->step_s)));
     const double g0 = s->now();
-    int r = sparc_batch_run(s->batch, s->quantum);
+    int r = sparc_batch_run(s->batch, steps);
     if (!r) r = sparc_batch_remaining(s->batch, rem.data());  // waits for the steps
     const double g1 = s->now();
     std::lock_guard<std::mutex> lock(s->mu);
     s->gpu_busy_s += g1 - g0;
+    s->step_s = (g1 - g0) / steps;
     ++s->rounds;
-    s->steps_run += s->quantum;
+    s->steps_run += steps;
     if (r) {
       s->err = sparc_batch_last_error(s->batch);
       for (auto &kv : s->tickets)
@@ -172,6 +184,7 @@ static void serve_loop(Server *s) {
           kv.second.state = SPARC_REQ_FAILED;
           kv.second.t_done = g1;
         }
+      s->running = 0;
       s->stop = true;
       s->cv.notify_all();
       return;
@@ -186,6 +199,7 @@ static void serve_loop(Server *s) {
         t.slot = -1;
         t.state = SPARC_REQ_DONE;
         t.t_done = g1;
+        --s->running;
       }
     }
     s->cv.notify_all();
@@ -380,11 +394,12 @@ int sparc_serve_state(sparc_server *s, int64_t ticket, int *state) {
   return SPARC_OK;
 }
 
-// stats[0..9]: queued, admitted, running, done (not yet released), budget
+// stats[0..11]: queued, admitted, running, done (not yet released), budget
 // used (bytes), max concurrent active, batched steps run, service rounds,
-// point updates, seconds the worker waited on batched steps
-int sparc_serve_stats(sparc_server *s, double *stats10) {
-  if (!s || !stats10) return SPARC_ERR_INVALID;
+// point updates, seconds the worker waited on batched steps, max members
+// running at once, requests attached while others were running
+int sparc_serve_stats(sparc_server *s, double *stats12) {
+  if (!s || !stats12) return SPARC_ERR_INVALID;
   std::lock_guard<std::mutex> lock(s->mu);
   double q = 0, a = 0, r = 0, d = 0;
   for (auto &kv : s->tickets) {
@@ -394,10 +409,10 @@ int sparc_serve_stats(sparc_server *s, double *stats10) {
     r += st == SPARC_REQ_RUNNING;
     d += st == SPARC_REQ_DONE || st == SPARC_REQ_COLLECTED;
   }
-  const double v[10] = {q, a, r, d, (double)s->used, (double)s->max_active,
+  const double v[12] = {q, a, r, d, (double)s->used, (double)s->max_active,
                         (double)s->steps_run, (double)s->rounds, s->point_updates,
-                        s->gpu_busy_s};
-  for (int i = 0; i < 10; ++i) stats10[i] = v[i];
+                        s->gpu_busy_s, (double)s->max_running, (double)s->joined};
+  for (int i = 0; i < 12; ++i) stats12[i] = v[i];
   return SPARC_OK;
 }
 

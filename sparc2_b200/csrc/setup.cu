@@ -226,6 +226,37 @@ __global__ void k_vamax(long long N, double T, double dimb2, double den0,
   if ((threadIdx.x & 31) == 0) atomic_max_pos(out, m);
 }
 
+// The Alfven-speed maximum of initialize.f90:974 for up to kVaCand limiter
+// candidates T[c] at once: out[c] = max over points of the square of
+// v(T[c]) (sqrt is monotone and correctly rounded, so sqrt(max v^2) equals
+// the maximum of the square roots the reference takes).
+constexpr int kVaCand = 12;
+struct VaCand {
+  double T[kVaCand];
+  int n;
+};
+__global__ void k_vamax_multi(long long N, VaCand C, double dimb2, double den0,
+                              const double *box, const double *boy, const double *boz,
+                              const double *red, const double *rho0, unsigned long long *out) {
+  double m[kVaCand];
+#pragma unroll
+  for (int c = 0; c < kVaCand; ++c) m[c] = 0.0;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < N;
+       n += (long long)gridDim.x * blockDim.x) {
+    const double b2 = box[n] * box[n] + boy[n] * boy[n] + boz[n] * boz[n];
+    const double r = red[n], q = den0 * rho0[n];
+#pragma unroll
+    for (int c = 0; c < kVaCand; ++c)
+      if (c < C.n) m[c] = fmax(m[c], dimb2 * C.T[c] / (C.T[c] + r) * b2 / q);
+  }
+#pragma unroll
+  for (int c = 0; c < kVaCand; ++c) {
+    double v = m[c];
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0 && c < C.n) atomic_max_pos(out + c, v);
+  }
+}
+
 __global__ void k_max(long long N, const double *x, unsigned long long *out) {
   double m = 0.0;
   for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < N;
@@ -406,6 +437,10 @@ int setup_background(Handle *h, const double *rho0_in, const double *pre0_in,
         sy[j] = P.sp_str * (1.0 - 1.0 / ((1.0 + std::exp((s0 - h->yaxis[j]) / P.sp_decay)) *
                                          (1.0 + std::exp((h->yaxis[j] - s1) / P.sp_decay))));
     }
+    h->sponge_slabs = true;
+    for (double v : sz) h->sponge_slabs = h->sponge_slabs && v == 0.0;
+    for (double v : sx) h->sponge_slabs = h->sponge_slabs && v == 0.0;
+    for (double v : sy) h->sponge_slabs = h->sponge_slabs && v == 0.0;
     std::vector<double> all(nz + nx + ny);
     std::copy(sz.begin(), sz.end(), all.begin());
     std::copy(sx.begin(), sx.end(), all.begin() + nz);
@@ -426,7 +461,7 @@ int setup_background(Handle *h, const double *rho0_in, const double *pre0_in,
     // Alfven limiter, initialize.f90:962-991
     double *red = h->red = up(h, nullptr, N);
     double *dcq = up(h, h->cq.data(), nz);
-    unsigned long long *dmax = (unsigned long long *)dev_alloc(h, 8);
+    unsigned long long *dmax = (unsigned long long *)dev_alloc(h, 8 * kVaCand);
     if (!red || !dcq || !dmax) return SPARC_ERR_NOMEM;
     const long long NXY = (long long)nx * ny;
     each(N, s, [=] __device__(long long n) {
@@ -448,14 +483,45 @@ int setup_background(Handle *h, const double *rho0_in, const double *pre0_in,
       std::memcpy(out, &bits, 8);
       return SPARC_OK;
     };
+    // The decade search of initialize.f90:966-975: the inner loop steps T
+    // by dtemp until the maximum Alfven speed reaches maxva.  The steps of
+    // one pass are formed on the host by the same repeated additions and
+    // their maxima evaluated together (one synchronisation per pass instead
+    // of one per step); the loop then stops at the same step.
+    auto vamax_steps = [&](double T0, double d, double *Tstop, double *vastop) -> int {
+      double Tc = T0;
+      for (;;) {
+        VaCand C{};
+        C.n = 0;
+        while (C.n < kVaCand) {
+          Tc = Tc + d;
+          C.T[C.n++] = Tc;
+          if (!(Tc < 1.0e10)) break;  // the loop tests T < 1e10 before a step
+        }
+        CK(cudaMemsetAsync(dmax, 0, 8 * kVaCand, s));
+        k_vamax_multi<<<grid_for(N), 256, 0, s>>>(N, C, dimb * dimb, 4.0 * PI * dimrho, box,
+                                                  boy, boz, red, rho0, dmax);
+        unsigned long long bits[kVaCand];
+        CK(cudaMemcpyAsync(bits, dmax, 8 * kVaCand, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        for (int c = 0; c < C.n; ++c) {
+          double v2;
+          std::memcpy(&v2, &bits[c], 8);
+          const double v = sqrt(v2);
+          if (!(v < P.maxva) || !(C.T[c] < 1.0e10)) {
+            *Tstop = C.T[c];
+            *vastop = v;
+            return SPARC_OK;
+          }
+        }
+      }
+    };
     double va = 0.0, dtemp = 1.0e9, T = -dtemp, mx = 0.0;
     if (devmax(false, 0.0, &mx)) return SPARC_ERR_CUDA;
     if (mx > 0.0) {
       while (dtemp > 1.0e-5 && T < 1.0e10 - 1.1) {
-        while (va < P.maxva && T < 1.0e10) {
-          T = T + dtemp;
-          if (devmax(true, T, &va)) return SPARC_ERR_CUDA;
-        }
+        if (va < P.maxva && T < 1.0e10)
+          if (vamax_steps(T, dtemp, &T, &va)) return SPARC_ERR_CUDA;
         T = T - dtemp;
         dtemp = dtemp / 10.0;
         va = 0.0;
@@ -612,14 +678,19 @@ int setup_background(Handle *h, const double *rho0_in, const double *pre0_in,
         sponge[gidx] = sponge[gidx] + q3 * tin * rn1;
       });
       if (axis == 2) {  // gravity of each ZBOT/ZTOP rank: its local (1,1)
+        // the inner-plane value of each block column's first point, read
+        // back in one synchronisation (a set-up that shares the device with
+        // a running batch pays for every synchronisation)
+        std::vector<double> tins(BXY);
         for (int b = 0; b < BXY; ++b) {
           int i0 = h->bxs[b % P.block_x], j0 = h->bys[b / P.block_x];
+          CK(cudaMemcpyAsync(&tins[b], tempin + I(i0, j0, inner), 8, cudaMemcpyDeviceToHost, s));
+        }
+        CK(cudaStreamSynchronize(s));
+        for (int b = 0; b < BXY; ++b) {
           for (int kk = 0; kk < np; ++kk) {
             int gk = top ? nz - np + kk : kk;
-            double tin;
-            CK(cudaMemcpyAsync(&tin, tempin + I(i0, j0, inner), 8,
-                               cudaMemcpyDeviceToHost, s));
-            CK(cudaStreamSynchronize(s));
+            const double tin = tins[b];
             double damp = q0 * tin * (q1 + 1.0) / (2.0 * L) * Ly.rn[kk];
             double kap = Ly.kap[kk], alpha = Ly.alpha[kk];
             double &gg = h->g_blk[(size_t)b * nz + gk];

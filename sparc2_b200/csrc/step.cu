@@ -17,7 +17,9 @@
 #include <cstdlib>
 #include <cstring>
 
+#include "filter_body.cuh"
 #include "mhd_body.cuh"
+#include "random_forcing.cuh"
 
 namespace sparc {
 
@@ -29,6 +31,10 @@ enum { FIRST = 0, MID = 1, LAST = 2 };
 template <>
 __device__ __forceinline__ double dcoef<double>(int r, int m) {
   return c_dp[r][m];
+}
+template <>
+__device__ __forceinline__ double fcoef<double>(int t, int m) {
+  return c_df[t][m];
 }
 
 int step_constants() {
@@ -700,6 +706,36 @@ int launch_filter_pass(Handle *h, int dir, const double *in, double *out,
   return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
 }
 
+// FILTER_VARS of a filter event (filter_body.cuh): the fused y-then-x pass
+// over (32 x 8) layer tiles, and the z pass over columns.
+__global__ void __launch_bounds__(fb::TX *fb::TY) k_filt_xy64(FiltArgs<double> F) {
+  const int l = blockIdx.z / F.nz, k = blockIdx.z - l * F.nz;
+  filt_xy_tile(F, l, k, blockIdx.x * fb::TX, blockIdx.y * fb::TY);
+}
+__global__ void __launch_bounds__(256) k_filt_z64(FiltArgs<double> F) {
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
+  if (i < F.nx && j < F.ny) filt_z_column(F, blockIdx.z, i, j);
+}
+
+// xy: the y and x passes fused; z: the z pass (in -> out, never in place)
+int launch_filter_event(Handle *h, bool xy, const double *in, double *out, cudaStream_t s) {
+  FiltArgs<double> F{};
+  F.nx = h->nx; F.ny = h->ny; F.nz = h->nz; F.V = h->V; F.N = h->N;
+  F.periodic = h->periodic ? 1 : 0;
+  F.g = xy ? h->gxy : h->gz;
+  F.mode2 = F.g == 3;
+  F.s = xy ? h->P.s_xy : h->P.s_z;
+  F.in = in;
+  F.out = out;
+  if (xy)
+    k_filt_xy64<<<dim3((h->nx + fb::TX - 1) / fb::TX, (h->ny + fb::TY - 1) / fb::TY,
+                       h->V * h->nz), dim3(fb::TX, fb::TY), 0, s>>>(F);
+  else
+    k_filt_z64<<<dim3((h->nx + 31) / 32, (h->ny + 7) / 8, h->V), dim3(32, 8), 0, s>>>(F);
+  ++h->launches;
+  return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
+}
+
 // Both stencils stay resident, so handles with different filter modes can
 // coexist; a pass picks its table by half-width.
 int filter_constants() {
@@ -710,52 +746,15 @@ int filter_constants() {
                                                                : SPARC_ERR_CUDA;
 }
 
-// PULSE = 0: LAGRANGE_INTERP (all_modules.f90:1892-1950) of the forcing
-// series at the device's iteration, times source_damp(:,:,1)
-// (driver.f90:131-132), one value per column; the stage kernels add
-// f2d(i,j) * source_dep(k) to RHSv_z (RHS.f90:147, 641).  FP64 in the
-// reference's operation order, without contraction; samples the reference
-// would read past the end of the series count as absent.
+// PULSE = 0: the forcing plane of the device's iteration
+// (random_forcing.cuh), one value per column.
 template <class D, class T>
 __global__ void k_random(const double *__restrict__ vr, const D *__restrict__ damp, int nxy,
                          int ns, double timestep, double cad, const long long *iter,
                          T *__restrict__ out) {
-  const long long nn = *iter;
-  double xt = __ddiv_rn(__dmul_rn((double)nn, timestep), cad);
-  const long long time1 = (long long)floor(xt) + 1;
-  xt = __dmul_rn((double)nn, timestep);
-  double x[7], den[7];
-  bool use[7];
-#pragma unroll
-  for (int j = 0; j < 7; ++j) x[j] = __dmul_rn((double)(time1 - 4 + j), cad);
-#pragma unroll
-  for (int j = 0; j < 7; ++j) {
-    const long long m = time1 - 4 + j;
-    use[j] = (j < 4 ? x[j] >= 0.0 : (j == 4 ? true : (j == 5 ? time1 < ns : time1 < ns - 1))) &&
-             m >= 0 && m < ns;
-    double d = 0.0;
-    bool first = true;
-#pragma unroll
-    for (int q = 0; q < 7; ++q) {
-      if (q == j) continue;
-      const double e = __dsub_rn(x[j], x[q]);
-      d = first ? e : __dmul_rn(d, e);
-      first = false;
-    }
-    den[j] = d;
-  }
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nxy; q += gridDim.x * blockDim.x) {
-    double f = 0.0;
-#pragma unroll
-    for (int j = 0; j < 7; ++j) {
-      double t = use[j] ? __ddiv_rn(vr[q + (long long)nxy * (time1 - 4 + j)], den[j]) : 0.0;
-#pragma unroll
-      for (int m = 0; m < 7; ++m)
-        if (m != j) t = __dmul_rn(t, __dsub_rn(xt, x[m]));
-      f = j == 0 ? t : __dadd_rn(f, t);
-    }
-    out[q] = (T)__dmul_rn(f, (double)damp[q]);
-  }
+  const RndStencil R = rnd_stencil(*iter, timestep, cad, ns);
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nxy; q += gridDim.x * blockDim.x)
+    out[q] = (T)rnd_column(R, vr, nxy, q, damp[q]);
 }
 
 int launch_random_forcing(Handle *h, cudaStream_t s) {
@@ -815,6 +814,7 @@ SimDev make_simdev(Handle *h) {
   S.periodic = h->periodic ? 1 : 0;
   S.magnetic = h->magnetic ? 1 : 0;
   S.bg1d = h->bg1d ? 1 : 0;
+  S.sponge_slabs = h->sponge_slabs ? 1 : 0;
   S.V = h->V;
   S.stretchx = h->stretchx;
   S.stretchy = h->stretchy;

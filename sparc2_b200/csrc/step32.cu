@@ -23,7 +23,9 @@
 #include <cstring>
 #include <vector>
 
+#include "filter_body.cuh"
 #include "mhd_body.cuh"
+#include "random_forcing.cuh"
 
 namespace sparc {
 
@@ -47,6 +49,10 @@ int step32_constants() {
 template <>
 __device__ __forceinline__ float dcoef<float>(int r, int m) {
   return f_dp[r][m];
+}
+template <>
+__device__ __forceinline__ float fcoef<float>(int t, int m) {
+  return f_df[t][m];
 }
 
 using Sim32 = SimT<float>;
@@ -460,7 +466,7 @@ struct Filt32 {
 // Filtered value of element t (field-major over V x N).
 template <int DIR>
 __device__ __forceinline__ float filter_point32(const Filt32 &F, const float *__restrict__ in,
-                                                long long t) {
+                                                const float *__restrict__ carry, long long t) {
   const int n = DIR == 0 ? F.nx : (DIR == 1 ? F.ny : F.nz);
   const long long st = DIR == 0 ? 1 : (DIR == 1 ? F.nx : (long long)F.nx * F.ny);
   const bool per = DIR != 2 && F.periodic;
@@ -475,8 +481,10 @@ __device__ __forceinline__ float filter_point32(const Filt32 &F, const float *__
   else q = (int)(pnt / ((long long)F.nx * F.ny));
   const long long base = t - (long long)q * st;
   // physical (z) or stored (x, y) value at index qq
+  // the compensated value stored - carry on the first pass of an event
   auto val = [&](int qq) -> float {
-    const float v = __ldg(in + base + (long long)qq * st);
+    const long long id = base + (long long)qq * st;
+    const float v = carry ? __ldg(in + id) - __ldg(carry + id) : __ldg(in + id);
     return DIR == 2 ? v * F.isc[l * F.nz + qq] : v;
   };
   auto pre = [&](int qq) -> float {
@@ -507,7 +515,43 @@ __global__ void k_filter32(Filt32 F, const float *__restrict__ in, float *__rest
   const long long total = F.N * F.V;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x)
-    out[t] = filter_point32<DIR>(F, in, t);
+    out[t] = filter_point32<DIR>(F, in, nullptr, t);
+}
+
+// FILTER_VARS of a filter event in the precision form (filter_body.cuh):
+// the fused y-then-x pass over stored values (one depth scale per layer)
+// and the z pass over physical values; `carry` (the first pass of an event)
+// is subtracted on load, so the filter acts on the compensated value.
+__global__ void __launch_bounds__(fb::TX *fb::TY) k_filt_xy32(FiltArgs<float> F) {
+  const int l = blockIdx.z / F.nz, k = blockIdx.z - l * F.nz;
+  filt_xy_tile(F, l, k, blockIdx.x * fb::TX, blockIdx.y * fb::TY);
+}
+__global__ void __launch_bounds__(256) k_filt_z32(FiltArgs<float> F) {
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
+  if (i < F.nx && j < F.ny) filt_z_column(F, blockIdx.z, i, j);
+}
+
+int launch_filter_event32(Handle *h, bool xy, const float *in, const float *carry, float *out,
+                          cudaStream_t s) {
+  FiltArgs<float> F{};
+  F.nx = h->nx; F.ny = h->ny; F.nz = h->nz; F.V = h->V; F.N = h->N;
+  F.periodic = h->periodic ? 1 : 0;
+  F.g = xy ? h->gxy : h->gz;
+  F.mode2 = F.g == 3;
+  F.s = (float)(xy ? h->P.s_xy : h->P.s_z);
+  F.in = in;
+  F.out = out;
+  F.carry = carry;
+  if (xy) {
+    k_filt_xy32<<<dim3((h->nx + fb::TX - 1) / fb::TX, (h->ny + fb::TY - 1) / fb::TY,
+                       h->V * h->nz), dim3(fb::TX, fb::TY), 0, s>>>(F);
+  } else {
+    F.sc = h->f_sc;
+    F.isc = h->f_isc;
+    k_filt_z32<<<dim3((h->nx + 31) / 32, (h->ny + 7) / 8, h->V), dim3(32, 8), 0, s>>>(F);
+  }
+  ++h->launches;
+  return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
 }
 
 int launch_filter32(Handle *h, int dir, const float *in, float *out, cudaStream_t s) {
@@ -640,6 +684,7 @@ Sim32 make_sim32(Handle *h) {
   S.periodic = h->periodic ? 1 : 0;
   S.magnetic = h->magnetic ? 1 : 0;
   S.bg1d = h->bg1d ? 1 : 0;
+  S.sponge_slabs = h->sponge_slabs ? 1 : 0;
   S.V = h->V;
   S.stretchx = h->stretchx;
   S.stretchy = h->stretchy;
@@ -898,8 +943,9 @@ __global__ void k_batch_begin(Slot32 *slots, int n) {
 }
 
 // PART 0: the interior MHD items (a prefix of the list, branch-free body);
-// PART 1: the rest (MHD tiles at edges/CPML, quiet tiles).  Two launches per
-// stage so that each kernel carries only its own bodies' registers.
+// PART 1: the rest (MHD tiles at edges/CPML, quiet tiles); PART 2: the whole
+// list in one launch (interior items first, then the rest, so no launch
+// boundary separates the two parts).
 template <int MODE, int PART>
 __global__ void __launch_bounds__(BT, 1)
     k_batch_stage(Slot32 *__restrict__ slots, const int4 *__restrict__ items,
@@ -911,7 +957,7 @@ __global__ void __launch_bounds__(BT, 1)
   float *qzt = smem + 2 * MhdBuf<float>::BUF + MhdBuf<float>::XCH;  // quiet items' scale table
   Sim32 &sS = *reinterpret_cast<Sim32 *>(sS_raw);
   const int tid = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
-  const int lo = PART == 0 ? 0 : counts[3], hi = PART == 0 ? counts[3] : counts[0];
+  const int lo = PART == 1 ? counts[3] : 0, hi = PART == 0 ? counts[3] : counts[0];
   int cur = -1;
   for (;;) {
     if (tid == 0) s_w = lo + (int)atomicAdd(wctr, 1u);
@@ -938,7 +984,7 @@ __global__ void __launch_bounds__(BT, 1)
     const float bnext = (float)(stage < 5 ? L.betas[stage] : sS.deltat);
     const int x0 = it.y, y0 = it.z, k0 = it.w & 0xffff, k1 = it.w >> 16;
     double ke = 0.0, mr = 1e300, mp = 1e300;
-    if (PART == 0)
+    if (PART == 0 || (PART == 2 && w < counts[3]))
       mhd_body<float, MODE, false, true>(sS, nullptr, smem, a, tin, so, beta, bnext, x0, y0, k0, k1,
                                   0, 0, ke, mr, mp);
     else if (sS.magnetic)
@@ -952,6 +998,21 @@ __global__ void __launch_bounds__(BT, 1)
                                       threadIdx.y + 8 * threadIdx.z, qzt, ke, mr, mp);
     if (MODE == F_LAST) batch_finish_step(L, sS, w, ke, mr, mp, tid);
     __syncthreads();
+  }
+}
+
+// PULSE = 0 forcing planes of the random-source members, at each member's
+// iteration (random_forcing.cuh); every block strides over every such
+// member's plane.
+__global__ void __launch_bounds__(BT)
+    k_batch_random(Slot32 *__restrict__ slots, int nslots) {
+  for (int q = 0; q < nslots; ++q) {
+    const Slot32 &L = slots[q];
+    if (!L.active || !L.has_rnd) continue;
+    const Rnd32 &D = L.rnd;
+    const RndStencil R = rnd_stencil(*L.S.iter, D.timestep, D.cad, D.ns);
+    for (int p = blockIdx.x * BT + threadIdx.x; p < D.nxy; p += gridDim.x * BT)
+      D.out[p] = (float)rnd_column(R, D.series, D.nxy, p, D.damp[p]);
   }
 }
 
@@ -1026,10 +1087,10 @@ __global__ void __launch_bounds__(BT)
     if (w >= total) break;
     const int4 it = items[w];
     Slot32 &L = slots[it.x];
-    bool need = false, need_z = false;
+    bool need = false, need_z = false, need_xy = false;
     if (L.active) {
       const long long nn = *L.S.iter - 1;
-      const bool need_xy = nn != 0 && nn % L.xyfreq == 0;
+      need_xy = nn != 0 && nn % L.xyfreq == 0;
       need_z = nn != 0 && nn % L.zfreq == 0;
       need = DIR == 2 ? need_z : need_xy;
     }
@@ -1049,13 +1110,12 @@ __global__ void __launch_bounds__(BT)
     F.isc = L.S.isc;
     const float *in = L.buf[L.role[0]];
     float *out = L.buf[L.role[1]];
-    float *carry = L.S.carry;
-    const bool zc = DIR == 2 || (DIR == 0 && !need_z);
+    // the first pass of the event (y, or z alone) filters stored - carry;
+    // k_batch_carry_clear zeroes the carry after the last pass
+    const bool first = DIR == 1 || (DIR == 2 && !need_xy);
+    const float *carry = first ? L.S.carry : nullptr;
     const long long t0 = it.y, t1 = t0 + it.z;
-    for (long long t = t0 + tid; t < t1; t += BT) {
-      out[t] = filter_point32<DIR>(F, in, t);
-      if (zc) carry[t] = 0.f;
-    }
+    for (long long t = t0 + tid; t < t1; t += BT) out[t] = filter_point32<DIR>(F, in, carry, t);
     __syncthreads();
     if (tid == 0) {
       const unsigned c = atomicAdd(&L.counter, 1u);
@@ -1067,38 +1127,55 @@ __global__ void __launch_bounds__(BT)
   }
 }
 
+// After a member's filter event its filtered state starts a new compensated
+// sum: zero its carry over the filter items' ranges.
+__global__ void __launch_bounds__(BT)
+    k_batch_carry_clear(Slot32 *__restrict__ slots, const int4 *__restrict__ items,
+                        const int *__restrict__ counts, unsigned *wctr) {
+  __shared__ int s_w;
+  const int total = counts[1];
+  for (;;) {
+    if (threadIdx.x == 0) s_w = (int)atomicAdd(wctr, 1u);
+    __syncthreads();
+    const int w = s_w;
+    __syncthreads();
+    if (w >= total) break;
+    const int4 it = items[w];
+    const Slot32 &L = slots[it.x];
+    if (!L.active) continue;
+    const long long nn = *L.S.iter - 1;
+    if (nn == 0 || (nn % L.xyfreq != 0 && nn % L.zfreq != 0)) continue;
+    for (long long t = it.y + threadIdx.x; t < (long long)it.y + it.z; t += BT) L.S.carry[t] = 0.f;
+  }
+}
+
 size_t batch_stage_smem() { return MhdBuf<float>::SMEM; }
 
 int launch_batch_step(const BatchLaunch &B, cudaStream_t s, int *nkernels) {
   const int sm = (int)MhdBuf<float>::smem_bytes(B.zmax);
-  cudaFuncSetAttribute(k_batch_stage<F_FIRST, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  cudaFuncSetAttribute(k_batch_stage<F_MID, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  cudaFuncSetAttribute(k_batch_stage<F_LAST, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  cudaFuncSetAttribute(k_batch_stage<F_FIRST, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  cudaFuncSetAttribute(k_batch_stage<F_MID, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  cudaFuncSetAttribute(k_batch_stage<F_LAST, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_batch_stage<F_FIRST, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_batch_stage<F_MID, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_batch_stage<F_LAST, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   if (cudaMemsetAsync(B.wctr, 0, 14 * sizeof(unsigned), s) != cudaSuccess) return SPARC_ERR_CUDA;
   k_batch_begin<<<(B.nslots + 255) / 256, 256, 0, s>>>(B.slots, B.nslots);
   k_batch_psr<<<B.grid, BT, B.psr_smem, s>>>(B.slots, B.pitems, B.counts, B.wctr + 0);
+  k_batch_random<<<B.grid, BT, 0, s>>>(B.slots, B.nslots);
   const dim3 blk(t32::TX, t32::TY, 2);
-  // per stage: interior part (counter 1..5), then general part (9..13)
+  // one persistent launch per stage over the whole work-list (counter st)
   for (int st = 1; st <= 5; ++st) {
-    unsigned *c0 = B.wctr + st, *c1 = B.wctr + 8 + st;
-    if (st == 1) {
-      k_batch_stage<F_FIRST, 0><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c0, st);
-      k_batch_stage<F_FIRST, 1><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c1, st);
-    } else if (st < 5) {
-      k_batch_stage<F_MID, 0><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c0, st);
-      k_batch_stage<F_MID, 1><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c1, st);
-    } else {
-      k_batch_stage<F_LAST, 0><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c0, st);
-      k_batch_stage<F_LAST, 1><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c1, st);
-    }
+    unsigned *c = B.wctr + st;
+    if (st == 1)
+      k_batch_stage<F_FIRST, 2><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c, st);
+    else if (st < 5)
+      k_batch_stage<F_MID, 2><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c, st);
+    else
+      k_batch_stage<F_LAST, 2><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c, st);
   }
   k_batch_filter<1><<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 6);
   k_batch_filter<0><<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 7);
   k_batch_filter<2><<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 8);
-  *nkernels = 15;
+  k_batch_carry_clear<<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 9);
+  *nkernels = 12;
   return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
 }
 

@@ -3,10 +3,12 @@
 The server (C++, a worker thread over one batch) queues requests, admits
 them by a device-memory budget and runs them as batch members.  This module
 drives it the way a service front end would: requests arrive on a seeded
-Poisson schedule and are submitted as they arrive; builder threads turn
-admitted requests into SPARC_FP32 handles (background, source) while the
-batch keeps stepping; a collector thread takes finished requests, reads
-their result and releases their memory.  The reference has no counterpart.
+Poisson schedule and are submitted as they arrive; prefetch threads build
+their host inputs (background arrays, source) in arrival order, a bounded
+window ahead of admission; builder threads turn admitted requests into
+SPARC_FP32 handles (the device set-up) while the batch keeps stepping; a
+collector thread takes finished requests, reads their result and releases
+their memory.  The reference has no counterpart.
 """
 import ctypes as C
 import threading
@@ -84,12 +86,12 @@ class Server:
                     "sparc_serve_release")
 
     def stats(self):
-        v = np.zeros(10)
+        v = np.zeros(12)
         self._check(self.lib.sparc_serve_stats(self.s, abi.dptr(v)),
                     "sparc_serve_stats")
         keys = ["queued", "admitted", "running", "done", "budget_used",
                 "max_concurrent", "batched_steps", "rounds", "point_updates",
-                "worker_gpu_wait_s"]
+                "worker_gpu_wait_s", "max_running", "joined_running"]
         return dict(zip(keys, v.tolist()))
 
 
@@ -101,16 +103,20 @@ def estimate_bytes(params):
 
 
 def drive(server, requests, build, on_result, builders=2, poll_s=0.05,
-          horizon_s=None, deadline_s=None):
+          horizon_s=None, deadline_s=None, prefetch=4, timings=None):
     """Runs a request stream through `server`.
 
     requests: list of (arrival_s, key, params, first, steps), sorted by
-    arrival; build(key) -> (background, source) makes a request's inputs;
-    on_result(key, sim, state, times) sees each finished request before its
-    handle is closed.  Requests arriving after horizon_s are not submitted.
-    Raises TimeoutError if the stream has not drained deadline_s seconds
-    after the start.  Returns the wall time from the start to the last
-    result."""
+    arrival; build(key) -> (background, source) makes a request's host
+    inputs; on_result(key, sim, state, times) sees each finished request
+    before its handle is closed.  Requests arriving after horizon_s are not
+    submitted.  prefetch: how many submitted requests may have their host
+    inputs built ahead of admission (0: build after admission).  timings:
+    an optional dict that receives, per key, the seconds spent building the
+    host inputs and on the device set-up (sparc_create, background and
+    source).  Raises TimeoutError if the stream has not drained deadline_s
+    seconds after the start.  Returns the wall time from the start to the
+    last result."""
     keys = {}
     lock = threading.Lock()
     done = threading.Event()
@@ -118,6 +124,40 @@ def drive(server, requests, build, on_result, builders=2, poll_s=0.05,
     collected = [0]
     errors = []
     sims = {}
+    # host inputs built ahead of admission: ticket -> [event, (bg, src)];
+    # admission is first-in first-out, so building in submission order
+    # always has the next admitted request's inputs first
+    order = []
+    inputs = {}
+    window = threading.Semaphore(max(1, prefetch))
+    cv = threading.Condition(lock)
+
+    def host_inputs(tk, key):
+        t = time.perf_counter()
+        bg, src = build(key)
+        if timings is not None:
+            timings.setdefault(key, {})["host_build_s"] = time.perf_counter() - t
+        return bg, src
+
+    def prefetcher():
+        while not done.is_set():
+            with cv:
+                while not order and not done.is_set():
+                    cv.wait(poll_s)
+                if done.is_set():
+                    return
+                tk = order.pop(0)
+                key, _ = keys[tk]
+            while not window.acquire(timeout=poll_s):
+                if done.is_set():
+                    return
+            try:
+                res = host_inputs(tk, key)
+            except Exception as e:
+                res = e
+            with lock:
+                inputs[tk][1] = res
+            inputs[tk][0].set()
 
     def submitter():
         t0 = time.perf_counter()
@@ -131,6 +171,10 @@ def drive(server, requests, build, on_result, builders=2, poll_s=0.05,
                 tk = server.submit(params, first, steps)
                 keys[tk] = (key, params)
                 submitted[0] += 1
+                if prefetch > 0:
+                    inputs[tk] = [threading.Event(), None]
+                    order.append(tk)
+                    cv.notify_all()
         with lock:
             submitted.append(True)    # marks the end of submissions
 
@@ -142,8 +186,23 @@ def drive(server, requests, build, on_result, builders=2, poll_s=0.05,
             with lock:
                 key, params = keys[tk]
             try:
-                bg, src = build(key)
+                if prefetch > 0:
+                    ev = inputs[tk][0]
+                    while not ev.wait(poll_s):
+                        if done.is_set():
+                            return
+                    with lock:
+                        res = inputs.pop(tk)[1]
+                    window.release()
+                    if isinstance(res, Exception):
+                        raise res
+                    bg, src = res
+                else:
+                    bg, src = host_inputs(tk, key)
+                t = time.perf_counter()
                 sim = Simulation(params, bg, src, device=server.device)
+                if timings is not None:
+                    timings.setdefault(key, {})["device_setup_s"] = time.perf_counter() - t
                 del bg
                 with lock:
                     sims[tk] = sim
@@ -179,6 +238,9 @@ def drive(server, requests, build, on_result, builders=2, poll_s=0.05,
     threads = [threading.Thread(target=submitter, daemon=True)]
     threads += [threading.Thread(target=builder, daemon=True)
                 for _ in range(builders)]
+    if prefetch > 0:
+        threads += [threading.Thread(target=prefetcher, daemon=True)
+                    for _ in range(min(prefetch, 2))]
     threads.append(threading.Thread(target=collector, daemon=True))
     for t in threads:
         t.start()

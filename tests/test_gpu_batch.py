@@ -27,6 +27,9 @@ MEMBERS = {
     "mhd_hpml_nx42": lambda: cases.mhd_hpml(nx=42, ny=40),
     "mhd_periodic": cases.mhd_periodic,
     "mhd_hpml_96": cases.CASES["mhd_hpml_96"],   # interior tiles: the batch's first part
+    # PULSE = 0 members: their forcing planes are rebuilt each batched step
+    "quiet_random": cases.quiet_random,
+    "mhd_random": lambda: cases.mhd_random(nx=40, ny=40),
 }
 
 
@@ -62,7 +65,7 @@ def check(name, sim, ref):
 def test_batch_members_match_their_single_runs():
     counts = {n: 60 - 7 * i for i, n in enumerate(sorted(MEMBERS))}
     refs = {n: alone(n, 0, c) for n, c in counts.items()}
-    with Batch(8) as b:
+    with Batch(len(MEMBERS)) as b:
         sims = {}
         for n, c in counts.items():
             sims[n] = Simulation(*fp32(n))

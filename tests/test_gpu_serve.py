@@ -62,6 +62,14 @@ def test_served_results_equal_their_alone_runs():
         st = srv.stats()
     assert len(got) == len(plan)
     assert st["max_concurrent"] <= 3
+    # continuous batching: requests ran on the device together, and some
+    # joined a batch that was already running others
+    assert st["max_running"] >= 2, st
+    assert st["joined_running"] >= 1, st
+    spans = [got[k][3][2:4] for k in got]        # (start, done) per request
+    overlap = [(a, b) for a in range(len(spans)) for b in range(a + 1, len(spans))
+               if spans[a][0] < spans[b][1] and spans[b][0] < spans[a][1]]
+    assert overlap, spans
     for key, (arr, kind, steps) in enumerate(plan):
         a, psi, d, times = got[key]
         ra, rpsi, rd = alone(kind, steps)

@@ -19,3 +19,22 @@ def test_oracle_matches_golden(name):
         assert r.shape == g.shape, key
         scale = np.max(np.abs(r)) if r.size else 0.0
         assert np.max(np.abs(g - r)) <= 1e-12 * max(scale, 1e-300), key
+
+
+def test_fluxtube_fixture_head_reproduces():
+    """The full-depth flux-tube fixture (1000 iterations, written by
+    make_fluxtube_1000.py in about an hour) is pinned here by its first
+    iterations: the oracle rerun for 4 iterations gives the same KE norm,
+    min rho and min p (a reordered OpenMP sum may change the last bits)."""
+    from tests.golden import make_fluxtube_1000 as F
+    import oracle
+    ref = np.load(os.path.join(HERE, F.NAME + ".npz"))
+    assert ref["stride"][0] == F.STRIDE
+    p, bg, src = F.config()
+    o = oracle.Oracle(p, bg, src)
+    for nn in range(4):
+        o.run(nn, 1)
+        d, r = o.diagnostics()
+        assert r == 0
+        got = np.array([d.ke_norm, d.min_rho, d.min_p])
+        assert np.all(np.abs(got - ref["diag"][nn]) <= 1e-12 * np.abs(ref["diag"][nn])), nn

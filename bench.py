@@ -72,7 +72,10 @@ def parse():
                     help="cfg1 serving leg: arrivals per second")
     ap.add_argument("--serve-duration", type=float, default=30.0,
                     help="cfg1 serving leg: seconds of arrivals")
-    ap.add_argument("--e2e-steps", type=int, default=30)
+    ap.add_argument("--e2e-steps", type=int, default=60,
+                    help="iterations between the state upload and read-back of "
+                    "the end-to-end leg (the reference driver reads the state "
+                    "back only at its output cadence, e.g. 1200 iterations)")
     ap.add_argument("--kernel-steps", type=int, default=10)
     ap.add_argument("--timed-only", action="store_true",
                     help="only the warm-up and the timed region (profiling)")
@@ -340,6 +343,30 @@ def run_gpu(args, world, rank, local):
         except Exception:
             traffic = None
 
+    # FILTER_VARS alone: an xy + z filter event (the fused y-then-x pass and
+    # the z pass) on the current state, timed over a few events; algorithmic
+    # bytes per event: a read and a write of the state per pass (2 passes),
+    # plus the carry read of the first pass in the precision form
+    F_EV = 5
+    ev_xy = int(np.floor(max(p.t_xy, p.timestep) / p.timestep + 1e-5))
+    ev_z = int(np.floor(max(p.t_z, p.timestep) / p.timestep + 1e-5))
+    nn_f = ev_xy * ev_z  # an iteration on both cadences
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    sim.filter_vars(nn_f)
+    f0.record(stream)
+    for _ in range(F_EV):
+        sim.filter_vars(nn_f)
+    f1.record(stream)
+    f1.synchronize()
+    fms = f0.elapsed_time(f1) / F_EV
+    fbytes = wsize * p_V(p) * pts * (4 + (1 if fp32 else 0))
+    filt_roof = {"bound": "hbm", "achieved": fbytes / (fms / 1e3) / 1e9, "peak": hbm,
+                 "unit": "GB/s", "frac": fbytes / (fms / 1e3) / 1e9 / hbm,
+                 "peak_kind": peak_kind, "kernel": "one FILTER_VARS event (xy and z): "
+                 "fused y-then-x pass + z pass", "algorithmic_bytes_per_launch": fbytes,
+                 "ms_per_launch": fms}
+
     # end to end through the per-iteration C-ABI calls of the reference's
     # driver loop (STEP, norm readback, FILTER_VARS): state uploaded from
     # pinned host memory at the start, read back at the end, diagnostics
@@ -422,8 +449,13 @@ def run_gpu(args, world, rank, local):
                      "one iteration",
                      "algorithmic_bytes_per_launch": stage_bytes,
                      "ms_per_launch": kms},
+        "filter_roofline": filt_roof,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "steps": E},
+                "d2h_bytes_per_step": d2h, "steps": E,
+                "pattern": "state uploaded from pinned host memory, then per "
+                "iteration sparc_step, sparc_diagnostics read back (the "
+                "reference's per-iteration norm) and sparc_filter_vars; state "
+                "and CPML fields read back after the %d iterations" % E},
         "gpu_launches": launches,
         "diag": {"ke_norm": d.ke_norm, "iteration": d.iteration,
                  "status": int(status)},
@@ -559,6 +591,7 @@ def measure_ensemble(dev, members=64, steps=10, warmup=2):
         batch.add(sm, 0, 1000)
     stream = torch.cuda.ExternalStream(batch.stream, device=dev)
     tiles = batch.tune(steps_per_trial=1)
+    batch_rows = batch.tile_rows
     batch.run(warmup)
     batch.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -574,7 +607,8 @@ def measure_ensemble(dev, members=64, steps=10, warmup=2):
     nq = sum(1 for d in draws if d[2] <= 0)
     return {"value": pts / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "steps": steps,
             "dtype": "f32", "members": len(draws), "quiet_members": nq,
-            "grid_points": pts, "tiles": {"zchunk_mhd": tiles[0], "zchunk_quiet": tiles[1]},
+            "grid_points": pts, "tiles": {"zchunk_mhd": tiles[0], "zchunk_quiet": tiles[1],
+                      "mhd_tile": [32, batch_rows]},
             "setup_s": setup,
             "workload": "batched ensemble: %d seeded members (nx=ny in {96..256}, nz in "
                         "[150, 300], quiet or flux tube, one pulse each), a step advances "
@@ -610,6 +644,7 @@ def run_ensemble(args, world, rank, local):
         batch.add(s, 0, total_steps)
     stream = torch.cuda.ExternalStream(batch.stream, device=dev)
     tiles = batch.tune(steps_per_trial=2)
+    tuned_rows = batch.tile_rows
     tuned_steps = 1000 - int(batch.remaining()[0])
     batch.run(W_)
     batch.synchronize()
@@ -700,6 +735,7 @@ def run_ensemble(args, world, rank, local):
                    % (len(draws), nq, len(draws) - nq),
                    "members": len(draws), "grid_points": pts,
                    "tiles": {"zchunk_mhd": tiles[0], "zchunk_quiet": tiles[1],
+                             "mhd_tile": [32, tuned_rows],
                              "autotuner_steps": tuned_steps},
                    "setup_s": t_setup,
                    "parallelism": "replicas" if world > 1 else "single GPU",

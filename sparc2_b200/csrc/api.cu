@@ -276,7 +276,7 @@ static Handle::GraphEntry *graph_for(Handle *h, int fk) {
   for (auto &g : h->graphs)
     if (g.ra == h->ra && g.rf1 == h->rf1 && g.rf2 == h->rf2 && g.fk == fk)
       return &g;
-  Handle::GraphEntry e{h->ra, h->rf1, h->rf2, fk, nullptr, 0};
+  Handle::GraphEntry e{h->ra, h->rf1, h->rf2, fk, nullptr, 0, 0, 0, 0};
   const int ra = h->ra, rf1 = h->rf1, rf2 = h->rf2;
   const long long launches = h->launches;
   cudaGraph_t graph;
@@ -287,6 +287,8 @@ static Handle::GraphEntry *graph_for(Handle *h, int fk) {
   int r = enqueue_step(h, h->stream, &nk);
   r |= enqueue_filter(h, fk, h->stream, &nk);
   cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
+  // the roles the iteration leaves (as many rotations as its launches made)
+  e.out_ra = h->ra; e.out_rf1 = h->rf1; e.out_rf2 = h->rf2;
   h->ra = ra; h->rf1 = rf1; h->rf2 = rf2;  // capture does not execute
   h->launches = launches;
   if (r || !cuda_ok(h, ce, "cudaStreamEndCapture")) return nullptr;
@@ -893,10 +895,10 @@ int sparc_run(sparc_handle *h, int64_t first, int64_t count) {
     if (!g) return SPARC_ERR_CUDA;
     CK(h, cudaGraphLaunch(g->exec, h->stream));
     h->launches += g->nkernels;
-    // roles after the step and the filter passes
-    rotate(h);
-    if (fk & 1) { rotate(h); rotate(h); }
-    if (fk & 2) rotate(h);
+    // roles after the step and the filter passes, as recorded at capture
+    h->ra = g->out_ra;
+    h->rf1 = g->out_rf1;
+    h->rf2 = g->out_rf2;
   }
   return SPARC_OK;
 }

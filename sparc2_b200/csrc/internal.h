@@ -145,6 +145,7 @@ struct BatchLaunch {
   unsigned *wctr;                       // [14] work counters, zeroed per step
   int grid;                             // persistent CTAs
   int zmax;                             // largest z extent of a stage item
+  int mhd_rows;                         // rows of an MHD work item (8 or 16)
   size_t psr_smem;
 };
 
@@ -263,6 +264,7 @@ struct Handle {
     int ra, rf1, rf2, fk;
     cudaGraphExec_t exec;
     int nkernels;
+    int out_ra, out_rf1, out_rf2;  // buffer roles after the captured iteration
   };
   std::vector<GraphEntry> graphs;
 };

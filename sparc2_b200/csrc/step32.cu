@@ -412,11 +412,18 @@ __global__ void __launch_bounds__(TX *TY)
 
 // -------------------------------------------- MP_MHD_3D, precision form
 // The two-role body of mhd_body.cuh in FP32 with depth scaling (field
-// scales: 0 rho, 1-3 v, 4 p, 5-7 b).  Own-point arrays of a layer arrive by
-// TMA (32x8 FP32 boxes), halos by cp.async; one CTA of 512 threads per SM.
+// scales: 0 rho, 1-3 v, 4 p, 5-7 b), one row of columns per thread: a CTA
+// of 512 threads owns a 32 x 8 column tile.  Own-point arrays of a layer
+// arrive by TMA (32x8 FP32 boxes), halos by cp.async; one CTA per SM.  (Two
+// rows per thread measured 30 % slower on the 256x256x300 flux tube: the
+// register spills of the doubled windows land in L2, the shared-memory
+// carve-out leaving little L1.)
 
 namespace t32 {
 using namespace mg;
+constexpr int NR = 1;          // rows of columns per thread
+constexpr int TYT = TY * NR;   // tile rows
+using MB = MhdBuf<float, false, NR>;
 }  // namespace t32
 
 // One RK stage of the MHD equations.  A stage is two launches over one
@@ -435,16 +442,16 @@ __global__ void __launch_bounds__(t32::NT, 1)
   float *smem = (float *)(((size_t)smem_raw32 + 127) & ~(size_t)127);
   const int tx_ = INT ? blockIdx.x + ix0 : blockIdx.x;
   const int ty_ = INT ? blockIdx.y + iy0 : blockIdx.y;
-  const int x0 = tx_ * t32::TX, y0 = ty_ * t32::TY;
-  if (!INT && mhd_interior(S, x0, y0)) return;
+  const int x0 = tx_ * t32::TX, y0 = ty_ * t32::TYT;
+  if (!INT && mhd_interior<float, t32::TYT>(S, x0, y0)) return;
   if (sm_addr_t(smem) & 127u) {
     if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) atomicExch(S.err, 2);
     return;
   }
   double ke = 0.0, mr = 1e300, mp = 1e300;
   const int k0 = blockIdx.z * zchunk;
-  if (!mhd_body<float, MODE, TMA, INT>(S, &T, smem, a, tin, so, beta, bnext, x0, y0, k0,
-                                min(S.nz, k0 + zchunk), mt, ma, ke, mr, mp))
+  if (!mhd_body<float, MODE, TMA, INT, t32::NR>(S, &T, smem, a, tin, so, beta, bnext, x0, y0,
+                                                k0, min(S.nz, k0 + zchunk), mt, ma, ke, mr, mp))
     return;
   if (MODE == F_LAST)
     diag_reduce_t(S, ke, mr, mp, tx_ + (long long)gx * (ty_ + (long long)gy * blockIdx.z),
@@ -772,17 +779,17 @@ int launch_stage32(Handle *h, const Sim32 &S, int stage, const float *a,
     if (h->tma32)
       for (int n = 0; n < 18; ++n) T.m[n] = h->tmaps32[n];
     dim3 blk(TX, TY, 2);
-    dim3 grd((h->nx + TX - 1) / TX, (h->ny + TY - 1) / TY, (h->nz + h->zchunk - 1) / h->zchunk);
+    dim3 grd((h->nx + TX - 1) / TX, (h->ny + TYT - 1) / TYT, (h->nz + h->zchunk - 1) / h->zchunk);
     // interior tile rectangle (see mhd_interior), in tile units
-    const int gx = (h->nx + TX - 1) / TX, gy = (h->ny + TY - 1) / TY;
+    const int gx = (h->nx + TX - 1) / TX, gy = (h->ny + TYT - 1) / TYT;
     const FaceT<float> *F = h->f_faces;
     const int xm = std::max(5, F[2].on ? F[2].np : 0), xM = std::max(5, F[3].on ? F[3].np : 0);
     const int ym = std::max(5, F[4].on ? F[4].np : 0), yM = std::max(5, F[5].on ? F[5].np : 0);
     const int ix0 = (xm + TX - 1) / TX, ix1 = (h->nx - xM - TX) / TX + 1;
-    const int iy0 = (ym + TY - 1) / TY, iy1 = (h->ny - yM - TY) / TY + 1;
-    const bool has_int = h->nx - xM - TX >= 0 && h->ny - yM - TY >= 0 && ix1 > ix0 && iy1 > iy0;
+    const int iy0 = (ym + TYT - 1) / TYT, iy1 = (h->ny - yM - TYT) / TYT + 1;
+    const bool has_int = h->nx - xM - TX >= 0 && h->ny - yM - TYT >= 0 && ix1 > ix0 && iy1 > iy0;
     dim3 gint(has_int ? ix1 - ix0 : 1, has_int ? iy1 - iy0 : 1, grd.z);
-    const int smz = (int)MhdBuf<float>::smem_bytes(h->zchunk);
+    const int smz = (int)MB::smem_bytes(h->zchunk);
 #define ML32(M, U)                                                                          \
   do {                                                                                      \
     cudaFuncSetAttribute(k_mhd32<M, U, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smz); \
@@ -820,7 +827,7 @@ int launch_stage32(Handle *h, const Sim32 &S, int stage, const float *a,
   return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
 }
 
-// FP32 tensor maps (32x8x1 boxes) of the own-point arrays of the MHD kernel
+// FP32 tensor maps (32 x TYT x 1 boxes) of the own-point arrays of the MHD kernel
 // (needs 16-byte row strides: nx a multiple of 4).
 int encode_tensor_maps32(Handle *h) {
   h->tma32 = false;
@@ -839,7 +846,7 @@ int encode_tensor_maps32(Handle *h) {
   auto one = [&](CUtensorMap *m, const float *base, unsigned long long depth) {
     cuuint64_t dims[3] = {(cuuint64_t)h->nx, (cuuint64_t)h->ny, (cuuint64_t)depth};
     cuuint64_t strides[2] = {(cuuint64_t)h->nx * 4, (cuuint64_t)h->nx * h->ny * 4};
-    cuuint32_t box[3] = {32, 8, 1};
+    cuuint32_t box[3] = {32, (cuuint32_t)t32::TYT, 1};
     cuuint32_t es[3] = {1, 1, 1};
     return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)base, dims, strides, box, es,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -946,15 +953,16 @@ __global__ void k_batch_begin(Slot32 *slots, int n) {
 // PART 1: the rest (MHD tiles at edges/CPML, quiet tiles); PART 2: the whole
 // list in one launch (interior items first, then the rest, so no launch
 // boundary separates the two parts).
-template <int MODE, int PART>
+template <int MODE, int PART, int NR>
 __global__ void __launch_bounds__(BT, 1)
     k_batch_stage(Slot32 *__restrict__ slots, const int4 *__restrict__ items,
                   const int *__restrict__ counts, unsigned *wctr, int stage) {
+  using MB = MhdBuf<float, false, NR>;
   extern __shared__ __align__(1024) float smem_raw32[];
   __shared__ __align__(16) unsigned long long sS_raw[(sizeof(Sim32) + 7) / 8];
   __shared__ int s_w;
   float *smem = (float *)(((size_t)smem_raw32 + 127) & ~(size_t)127);
-  float *qzt = smem + 2 * MhdBuf<float>::BUF + MhdBuf<float>::XCH;  // quiet items' scale table
+  float *qzt = smem + 2 * MB::BUF + MB::XCH;  // quiet items' scale table
   Sim32 &sS = *reinterpret_cast<Sim32 *>(sS_raw);
   const int tid = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
   const int lo = PART == 1 ? counts[3] : 0, hi = PART == 0 ? counts[3] : counts[0];
@@ -985,11 +993,11 @@ __global__ void __launch_bounds__(BT, 1)
     const int x0 = it.y, y0 = it.z, k0 = it.w & 0xffff, k1 = it.w >> 16;
     double ke = 0.0, mr = 1e300, mp = 1e300;
     if (PART == 0 || (PART == 2 && w < counts[3]))
-      mhd_body<float, MODE, false, true>(sS, nullptr, smem, a, tin, so, beta, bnext, x0, y0, k0, k1,
-                                  0, 0, ke, mr, mp);
+      mhd_body<float, MODE, false, true, NR>(sS, nullptr, smem, a, tin, so, beta, bnext, x0, y0,
+                                             k0, k1, 0, 0, ke, mr, mp);
     else if (sS.magnetic)
-      mhd_body<float, MODE, false, false>(sS, nullptr, smem, a, tin, so, beta, bnext, x0, y0, k0, k1,
-                                   0, 0, ke, mr, mp);
+      mhd_body<float, MODE, false, false, NR>(sS, nullptr, smem, a, tin, so, beta, bnext, x0, y0,
+                                              k0, k1, 0, 0, ke, mr, mp);
     else if (sS.bg1d)
       quiet_body<32, 16, MODE, true>(sS, a, tin, so, beta, bnext, x0, y0, k0, k1, threadIdx.x,
                                      threadIdx.y + 8 * threadIdx.z, qzt, ke, mr, mp);
@@ -1149,28 +1157,35 @@ __global__ void __launch_bounds__(BT)
   }
 }
 
-size_t batch_stage_smem() { return MhdBuf<float>::SMEM; }
+size_t batch_stage_smem() { return t32::MB::SMEM; }
+
+// One persistent launch per RK stage over the whole work-list, MHD items of
+// 32 x 8*NR columns.
+template <int NR>
+static void launch_batch_stages(const BatchLaunch &B, cudaStream_t s) {
+  const int sm = (int)MhdBuf<float, false, NR>::smem_bytes(B.zmax);
+  cudaFuncSetAttribute(k_batch_stage<F_FIRST, 2, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_batch_stage<F_MID, 2, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_batch_stage<F_LAST, 2, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  const dim3 blk(t32::TX, t32::TY, 2);
+  for (int st = 1; st <= 5; ++st) {
+    unsigned *c = B.wctr + st;  // work counter of stage st
+    if (st == 1)
+      k_batch_stage<F_FIRST, 2, NR><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c, st);
+    else if (st < 5)
+      k_batch_stage<F_MID, 2, NR><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c, st);
+    else
+      k_batch_stage<F_LAST, 2, NR><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c, st);
+  }
+}
 
 int launch_batch_step(const BatchLaunch &B, cudaStream_t s, int *nkernels) {
-  const int sm = (int)MhdBuf<float>::smem_bytes(B.zmax);
-  cudaFuncSetAttribute(k_batch_stage<F_FIRST, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  cudaFuncSetAttribute(k_batch_stage<F_MID, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  cudaFuncSetAttribute(k_batch_stage<F_LAST, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   if (cudaMemsetAsync(B.wctr, 0, 14 * sizeof(unsigned), s) != cudaSuccess) return SPARC_ERR_CUDA;
   k_batch_begin<<<(B.nslots + 255) / 256, 256, 0, s>>>(B.slots, B.nslots);
   k_batch_psr<<<B.grid, BT, B.psr_smem, s>>>(B.slots, B.pitems, B.counts, B.wctr + 0);
   k_batch_random<<<B.grid, BT, 0, s>>>(B.slots, B.nslots);
-  const dim3 blk(t32::TX, t32::TY, 2);
-  // one persistent launch per stage over the whole work-list (counter st)
-  for (int st = 1; st <= 5; ++st) {
-    unsigned *c = B.wctr + st;
-    if (st == 1)
-      k_batch_stage<F_FIRST, 2><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c, st);
-    else if (st < 5)
-      k_batch_stage<F_MID, 2><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c, st);
-    else
-      k_batch_stage<F_LAST, 2><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c, st);
-  }
+  if (B.mhd_rows == 8) launch_batch_stages<1>(B, s);
+  else launch_batch_stages<2>(B, s);
   k_batch_filter<1><<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 6);
   k_batch_filter<0><<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 7);
   k_batch_filter<2><<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 8);

@@ -122,16 +122,23 @@ def test_tile_extent_does_not_change_results():
     assert np.array_equal(res[0][1], res[1][1])
 
 
-def test_random_source_member_is_refused():
-    """PULSE = 0 simulations run alone (sparc_run); a batch refuses them."""
-    p, bg, src = cases.quiet_random()
-    p.precision = abi.SPARC_FP32
-    s = Simulation(p, bg, src)
-    with Batch(2) as b:
-        with pytest.raises(abi.SparcError) as e:
-            b.add(s, 0, 10)
-        assert e.value.code == abi.SPARC_ERR_INVALID
-    s.close()
+def test_tile_shape_does_not_change_results():
+    """MHD work items of 32 x 8 and 32 x 16 columns (one or two rows of
+    columns per thread) evaluate the same per-point arithmetic: the same
+    state, bit for bit, on a grid with interior and edge tiles."""
+    res = []
+    for rows in (8, 16):
+        with Batch(1) as b:
+            s = Simulation(*fp32("mhd_hpml_96"))
+            b.set_tile_rows(rows)
+            assert b.tile_rows == rows
+            b.add(s, 0, 12)
+            b.run(12)
+            for q in list(b.members):
+                b.remove(q)
+        res.append(s.get_state())
+    assert np.array_equal(res[0][0], res[1][0])
+    assert np.array_equal(res[0][1], res[1][1])
 
 
 def test_tuner_and_membership_rules():
@@ -143,6 +150,7 @@ def test_tuner_and_membership_rules():
         zm, zq = b.tune(steps_per_trial=1)
         assert zm >= 11 and zq >= 11
         assert b.tiles() == (zm, zq)
+        assert b.tile_rows in (8, 16)
         with pytest.raises(abi.SparcError) as e:
             s.step(0)
         assert e.value.code == abi.SPARC_ERR_ORDER

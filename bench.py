@@ -571,7 +571,7 @@ def measure_fp32_cfg2(dev, steps=40, warmup=3):
             "dtype": "f32", "workload": desc}
 
 
-def measure_ensemble(dev, members=64, steps=10, warmup=2):
+def measure_ensemble(dev, members=64, steps=100, warmup=2):
     """The batched precision form: `members` seeded FP32 simulations through
     the batched engine (autotuned tiles), one graph launch per step."""
     import torch
@@ -787,7 +787,9 @@ def measure_serve(dev, rate, duration, steps_scale, budget_gb=150.0):
         res[key] = (state, times.copy(), d.ke_norm)
 
     srv = Server(capacity=64, budget_bytes=int(budget_gb * 1e9), quantum=10, device=dev)
-    wall = drive(srv, reqs, build, on_result, builders=4, prefetch=4, timings=timings,
+    # a build (sparc_create, background and source set-up beside the running
+    # batch) mostly waits on synchronisations: twelve builders overlap them
+    wall = drive(srv, reqs, build, on_result, builders=12, prefetch=8, timings=timings,
                  deadline_s=20 * duration + 600)
     st = srv.stats()
     srv.close()

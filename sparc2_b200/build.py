@@ -76,8 +76,21 @@ def build(force=False, verbose=False, ptxas_v=False):
     if force or _stale(LIB, objs):
         tmp = LIB + ".tmp"
         subprocess.check_call([nvcc(), *ARCH, "-shared", "-o", tmp, *objs])
+        _check_resolved(tmp)
         os.replace(tmp, LIB)
     return LIB
+
+
+def _check_resolved(lib):
+    """A shared library links with unresolved symbols; refuse one that
+    leaves any of its own (namespace sparc) undefined."""
+    out = subprocess.run(["nm", "-u", "-C", lib], capture_output=True, text=True)
+    if out.returncode != 0:
+        return  # no nm: nothing to check with
+    missing = [l.strip() for l in out.stdout.splitlines() if "sparc::" in l]
+    if missing:
+        os.remove(lib)
+        raise RuntimeError("unresolved library symbols: " + "; ".join(missing))
 
 
 if __name__ == "__main__":

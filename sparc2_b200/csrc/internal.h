@@ -292,8 +292,6 @@ int launch_stage(Handle *h, const SimDev &S, int stage, const double *a,
 int launch_psr_forcing(Handle *h, const SimDev &S, cudaStream_t s);
 int launch_random_forcing(Handle *h, cudaStream_t s);
 int launch_filter_event(Handle *h, bool xy, const double *in, double *out, cudaStream_t s);
-int launch_filter_pass(Handle *h, int dir, const double *in, double *out,
-                       cudaStream_t s);
 int stage_geometry(Handle *h);
 int encode_tensor_maps(Handle *h);
 
@@ -306,7 +304,6 @@ int launch_psr32(Handle *h, cudaStream_t s);
 Psr32 make_psr32(Handle *h);
 int launch_batch_step(const BatchLaunch &B, cudaStream_t s, int *nkernels);
 size_t batch_stage_smem();
-int launch_filter32(Handle *h, int dir, const float *in, float *out, cudaStream_t s);
 int launch_filter_event32(Handle *h, bool xy, const float *in, const float *carry, float *out,
                           cudaStream_t s);
 int encode_tensor_maps32(Handle *h);

@@ -340,7 +340,7 @@ inline void mhd_interior_rect(int nx, int ny, const int np[4], int &ix0, int &ix
 
 // The body covers the tile (x0, y0) over layers [k0, k1) with a block of
 // 32 x 8 x 2 threads (threadIdx.z is the role); each thread serves NR rows
-// of columns (rows ty, ty + 8, ...), so the tile is 32 x 8*NR columns.
+// of columns (rows ty, ty + 8), so the tile is 32 x 8*NR columns.
 // smem is the 128-byte aligned dynamic buffer.  TMA = false: the own-point
 // arrays are fetched by cp.async too (any nx).  INT: the tile's stencil
 // footprint touches no non-periodic edge, no x/y CPML slab and needs no
@@ -355,7 +355,8 @@ inline void mhd_interior_rect(int nx, int ny, const int np[4], int &ix0, int &ix
 // 8 + ty) exchanges d(vz)/dz and d(by)/dz: nothing else crosses warps
 // until the next layer's barrier.  With NR = 2 the per-layer work that does
 // not depend on the column (barriers, copy issue, depth scales, layer
-// flags, loop control) is shared by two points.
+// flags, loop control) is shared by two points, at the price of register
+// spills (the batched engine's tuner weighs the two).
 template <class R, int MODE, bool TMA, bool INT, int NR = 1>
 __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *smem,
                                          const R *__restrict__ a,
@@ -365,17 +366,20 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
                                          double &ke, double &mr, double &mp) {
   using namespace mg;
   static_assert(NR == 1 || NR == 2, "one or two rows per thread");
+  constexpr int TW = TY;                       // thread rows per role
+  constexpr int TYT = TW * NR;                 // tile rows
+  constexpr int NTW = 2 * TX * TW, NCW = TX * TW;  // threads, threads per role
   // halo planes by TMA in the plain form's interior kernel (measured: 4 %
   // faster in FP64; in FP32 the 48-wide boxes cost more than the cp.async
   // copies they replace)
-  constexpr bool TH = TMA && INT && sizeof(R) == 8 && NR == 1;
-  using MB = MhdBuf<R, TH, NR>;
+  constexpr bool TH = TMA && INT && sizeof(R) == 8 && TYT == 8;
+  using MB = MhdBuf<R, TH, TYT / 8>;
   constexpr int BUF = MB::BUF, HXL = MB::HXL, XOFF = MB::XOFF, HSL = MB::HSL;
-  constexpr int TYT = MB::TYT, NCT = MB::NCT, HYT = MB::HYT, HST = MB::HST;
+  constexpr int NCT = MB::NCT, HYT = MB::HYT, HST = MB::HST;
   constexpr bool SCALED = sizeof(R) == 4;
   __shared__ unsigned long long bar[2];
   const int tx = threadIdx.x, ty = threadIdx.y, role = threadIdx.z;
-  const int tid = (role * TY + ty) * TX + tx;
+  const int tid = (role * TW + ty) * TX + tx;
   const int nx = S.nx, ny = S.ny, nz = S.nz;
   const int N = (int)S.N, NXY = nx * ny;
   const int i = x0 + tx;
@@ -389,11 +393,11 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
   bool act[NR];
 #pragma unroll
   for (int r = 0; r < NR; ++r) {
-    jr[r] = y0 + ty + r * TY;
-    cid[r] = (ty + r * TY) * TX + tx;
+    jr[r] = y0 + ty + r * TW;
+    cid[r] = (ty + r * TW) * TX + tx;
     act[r] = INT || (i < nx && jr[r] < ny);
     col[r] = jr[r] * nx + i;
-    ryr[r] = y0 - yo + ty + r * TY;
+    ryr[r] = y0 - yo + ty + r * TW;
     own[r] = ryr[r] * HXL + rx + XOFF;
   }
   const R *isc = S.isc, *sc = S.sc;
@@ -403,7 +407,7 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
   const int zb = max(0, min(k0 - 5, nz - 11));
   if constexpr (SCALED) {
     const int ze = min(nz, max(k1 + 5, zb + 11));
-    for (int t = tid; t < (ze - zb) * 16; t += NT) {
+    for (int t = tid; t < (ze - zb) * 16; t += NTW) {
       const int kk = zb + (t >> 4), l = t & 15;
       ZT[t] = l < 8 ? isc[l * nz + kk] : sc[(l - 8) * nz + kk];
     }
@@ -454,13 +458,15 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  auto O = [&](int b, int slot, int r) -> R { return smem[b * BUF + slot * NCT + cid[r]]; };
+  // per-row values are passed in (not the row index), so no per-row array is
+  // indexed inside a helper that the compiler might not inline
+  auto O = [&](int b, int slot, int c) -> R { return smem[b * BUF + slot * NCT + c]; };
   auto Hp = [&](int b, int slot) -> R * { return smem + b * BUF + NO * NCT + slot * HSL; };
   R *X = smem + 2 * BUF;
-  // halo positions this thread copies (and turns into fluxes): NR = 1
-  // positions 0..511 one per thread, 512..755 on role 1 (role 0 carries the
-  // TMA issue and the heavier momentum update); NR = 2 positions 0..1023
-  // two per thread, 1024..1091 on role 1
+  // halo positions this thread copies (and turns into fluxes): 32 x 8
+  // tile: positions 0..511 one per thread, 512..755 on role 1 (role 0
+  // carries the TMA issue and the heavier momentum update); 32 x 16 tile:
+  // 0..1023 two per thread, 1024..1091 on role 1
   constexpr int NP = NR + 1;
   int hs[NP], ho[NP];
   {
@@ -491,10 +497,10 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
     };
     pos(tid, hs[0], ho[0]);
     if (NR == 1) {
-      if (role == 1) pos(tid + NC, hs[1], ho[1]);
+      if (role == 1) pos(tid + NCW, hs[1], ho[1]);
     } else {
-      pos(tid + NT, hs[1], ho[1]);
-      if (role == 1) pos(tid + 2 * NT - NC, hs[2], ho[2]);
+      pos(tid + NTW, hs[1], ho[1]);
+      if (role == 1) pos(tid + 2 * NTW - NCW, hs[2], ho[2]);
     }
   }
   // Own-point arrays not read: in the plain form rhoinv (the kernel forms
@@ -600,8 +606,8 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
     H[9 * HSL] = -vy_ * bx0 + vx_ * by0;
   };
   R w0[NR][11], w1[NR][11], w2[NR][11];  // physical values
-  auto head = [&](int kk, int r, R &v0, R &v1, R &v2) {
-    const int id = kk * NXY + col[r];
+  auto head = [&](int kk, int colr, R &v0, R &v1, R &v2) {
+    const int id = kk * NXY + colr;
     if (role == 0) {
       v0 = __ldg(tin + 3 * N + id) * IS(3, kk);
       v1 = __ldg(tin + 4 * N + id) * IS(4, kk);
@@ -648,7 +654,7 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
 #pragma unroll
       for (int m = 0; m < 11; ++m) {
         const int kk = b0 + m;
-        if (act[r] && kk >= 0) head(kk, r, w0[r][m], w1[r][m], w2[r][m]);
+        if (act[r] && kk >= 0) head(kk, col[r], w0[r][m], w1[r][m], w2[r][m]);
         else w0[r][m] = w1[r][m] = w2[r][m] = R(0);
       }
   }
@@ -672,7 +678,7 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
 #pragma unroll
     for (int r = 0; r < NR; ++r) {
       h0[r] = h1[r] = h2[r] = R(0);
-      if (sh && act[r]) head(k + 5, r, h0[r], h1[r], h2[r]);
+      if (sh && act[r]) head(k + 5, col[r], h0[r], h1[r], h2[r]);
     }
     prefetch(k + 7);
     // precision form, last stage: the compensation carries of layer k + 2
@@ -729,8 +735,8 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
       }
     }
     const R szk = __ldg(S.stretch + k);
-    auto DX = [&](int slot, int r) {
-      const R *row = Hp(b, slot) + ryr[r] * HXL + XOFF;
+    auto DX = [&](int slot, int ryl) {  // ryl: the row's tile row in the halo plane
+      const R *row = Hp(b, slot) + ryl * HXL + XOFF;
       if (INT) return sx * csum_t(row + tx, 1);
       if (cen_x) return sx * csum_t(row + cxo + tx, 1);
       const R *rr = row + cxb[tx], *c = cxs + tx * 11;
@@ -739,8 +745,7 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
       for (int m = 0; m < 11; ++m) sum += rr[m] * c[m];
       return sx * sum;
     };
-    auto DY = [&](int slot, int r) {
-      const int ly = ty + r * TY;  // row of the tile
+    auto DY = [&](int slot, int ly) {  // ly: row of the tile
       const R *colp = Hp(b, slot) + rx + XOFF;
       if (INT) return sy * csum_t(colp + ly * HXL, HXL);
       if (cen_y) return sy * csum_t(colp + (cyo + ly) * HXL, HXL);
@@ -752,27 +757,27 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
     };
     const bool zpml = S.zb.on && (k < S.zb.np || k >= nz - S.zt.np);
     const bool xpml_i = !INT && S.xb.on && (i < S.xb.np || i >= nx - S.xt.np);
-    auto pz = [&](int r, int s0, int s1, int s2, R &da, R &db, R &dc) {
+    auto pz = [&](int colr, int s0, int s1, int s2, R &da, R &db, R &dc) {
       const bool bot = k < S.zb.np;
       const FaceT<R> &F = bot ? S.zb : S.zt;
       const int kl = bot ? k : k - (nz - S.zt.np);
-      cpml3_t<R, MODE>(F, (long long)kl * NXY + col[r], kl, s0, s1, s2, beta, dt, da, db, dc);
+      cpml3_t<R, MODE>(F, (long long)kl * NXY + colr, kl, s0, s1, s2, beta, dt, da, db, dc);
     };
-    auto px = [&](int r, int s0, int s1, int s2, R &da, R &db, R &dc) {
+    auto px = [&](int j, int s0, int s1, int s2, R &da, R &db, R &dc) {
       const bool bot = i < S.xb.np;
       const FaceT<R> &F = bot ? S.xb : S.xt;
       const int il = bot ? i : i - (nx - S.xt.np);
-      cpml3_t<R, MODE>(F, il + (long long)F.np * (jr[r] + (long long)ny * k), il, s0, s1, s2,
+      cpml3_t<R, MODE>(F, il + (long long)F.np * (j + (long long)ny * k), il, s0, s1, s2,
                        beta, dt, da, db, dc);
     };
-    auto py = [&](int r, int s0, int s1, int s2, R &da, R &db, R &dc) {
-      const bool bot = jr[r] < S.yb.np;
+    auto py = [&](int j, int s0, int s1, int s2, R &da, R &db, R &dc) {
+      const bool bot = j < S.yb.np;
       const FaceT<R> &F = bot ? S.yb : S.yt;
-      const int jl = bot ? jr[r] : jr[r] - (ny - S.yt.np);
+      const int jl = bot ? j : j - (ny - S.yt.np);
       cpml3_t<R, MODE>(F, i + (long long)nx * (jl + (long long)F.np * k), jl, s0, s1, s2, beta,
                        dt, da, db, dc);
     };
-    auto Hv = [&](int slot, int r) { return Hp(b, slot)[own[r]]; };
+    auto Hv = [&](int slot, int ownr) { return Hp(b, slot)[ownr]; };
     const R iv = IS(1, k);  // velocity (and flux) scale of this layer
     R d0[NR], d1[NR], d2[NR], d3[NR], d4[NR], d5[NR], d6[NR], d7[NR], d8[NR];
 #pragma unroll
@@ -782,27 +787,28 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
       const bool xpml = xpml_i;
       const bool ypml = !INT && S.yb.on && (jr[r] < S.yb.np || jr[r] >= ny - S.yt.np);
       const R ip = IS(4, k), ib = IS(5, k);
+      const int yr = ryr[r], lr = ty + r * TW, colr = col[r], jrr = jr[r];
       if (role == 0) {
-        d0[r] = ip * DX(3, r); d5[r] = ib * DX(6, r); d7[r] = ib * DX(5, r);
-        d1[r] = ip * DY(3, r); d4[r] = ib * DY(6, r); d8[r] = ib * DY(4, r);
+        d0[r] = ip * DX(3, yr); d5[r] = ib * DX(6, yr); d7[r] = ib * DX(5, yr);
+        d1[r] = ip * DY(3, lr); d4[r] = ib * DY(6, lr); d8[r] = ib * DY(4, lr);
         d3[r] = dz_t(w0[r], k, nz, szk); d2[r] = dz_t(w1[r], k, nz, szk);
         d6[r] = dz_t(w2[r], k, nz, szk);
-        if (zpml) pz(r, 1, 0, 2, d2[r], d3[r], d6[r]);
-        if (xpml) px(r, 1, 3, 2, d0[r], d5[r], d7[r]);
-        if (ypml) py(r, 1, 3, 2, d1[r], d4[r], d8[r]);
+        if (zpml) pz(colr, 1, 0, 2, d2[r], d3[r], d6[r]);
+        if (xpml) px(jrr, 1, 3, 2, d0[r], d5[r], d7[r]);
+        if (ypml) py(jrr, 1, 3, 2, d1[r], d4[r], d8[r]);
         X[cid[r]] = d3[r];
         // curl b: y and z components now, x after the exchange (fewer live
         // registers across the barrier; the same arithmetic)
         d5[r] = -d5[r] + d6[r];
         d7[r] = d7[r] - d8[r];
       } else {
-        d0[r] = iv * DX(0, r); d2[r] = iv * DX(9, r); d3[r] = iv * DX(8, r);
-        d1[r] = iv * DY(1, r); d4[r] = iv * DY(9, r); d5[r] = iv * DY(7, r);
+        d0[r] = iv * DX(0, yr); d2[r] = iv * DX(9, yr); d3[r] = iv * DX(8, yr);
+        d1[r] = iv * DY(1, lr); d4[r] = iv * DY(9, lr); d5[r] = iv * DY(7, lr);
         d6[r] = dz_t(w0[r], k, nz, szk); d7[r] = dz_t(w1[r], k, nz, szk);
         d8[r] = dz_t(w2[r], k, nz, szk);
-        if (zpml) pz(r, 4, 5, 3, d7[r], d6[r], d8[r]);
-        if (xpml) px(r, 0, 4, 5, d0[r], d2[r], d3[r]);
-        if (ypml) py(r, 0, 4, 5, d1[r], d4[r], d5[r]);
+        if (zpml) pz(colr, 4, 5, 3, d7[r], d6[r], d8[r]);
+        if (xpml) px(jrr, 0, 4, 5, d0[r], d2[r], d3[r]);
+        if (ypml) py(jrr, 0, 4, 5, d1[r], d4[r], d5[r]);
         X[NCT + cid[r]] = d8[r];
         // curl(v x B0) and d(vx)/dx + d(vy)/dy now (fewer live registers
         // across the barrier; the same arithmetic)
@@ -820,13 +826,14 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
       an_rho[r] = 0.0;
       if (!act[r]) continue;
       const int id = k * NXY + col[r];
+      const int cr = cid[r], ownr = own[r];
       const bool zero = k == 0 || k == nz - 1 ||
                         (!INT && !per && (i == 0 || i == nx - 1 || jr[r] == 0 || jr[r] == ny - 1));
       const R fac = MODE == F_LAST ? dt : bnext;
-      const R rho = O(b, O_RHO, r) * IS(0, k), vx = Hv(0, r) * iv, vy = Hv(1, r) * iv,
-              vz = Hv(2, r) * iv;
-      const R red = O(b, O_BG + B_RED, r);
-      const R sg = sponge_at(k) ? O(b, O_BG + B_SPONGE, r) : R(0);
+      const R rho = O(b, O_RHO, cr) * IS(0, k), vx = Hv(0, ownr) * iv, vy = Hv(1, ownr) * iv,
+              vz = Hv(2, ownr) * iv;
+      const R red = O(b, O_BG + B_RED, cr);
+      const R sg = sponge_at(k) ? O(b, O_BG + B_SPONGE, cr) : R(0);
       if (role == 0) {
         const R ox = __ldg(S.box + id), oy = __ldg(S.boy + id), oz = __ldg(S.boz + id);
         const R gk = __ldg(gcol[r] + k);
@@ -834,14 +841,14 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
         const R dzby = X[NCT + cid[r]];
         const R cbx = d4[r] - dzby, cby = d5[r], cbz = d7[r];
         const R c1 = cby * oz - cbz * oy, c2 = ox * cbz - cbx * oz, c3 = cbx * oy - cby * ox;
-        const R ri = DERIVE_RI ? R(1) / O(b, O_BG + B_RHO0, r) : O(b, O_BG + B_RHOINV, r);
+        const R ri = DERIVE_RI ? R(1) / O(b, O_BG + B_RHO0, cr) : O(b, O_BG + B_RHOINV, cr);
         R vxr = -ri * (d0[r] - (c1 * red)) - sg * vx;
         R vyr = -ri * (d1[r] - (c2 * red)) - sg * vy;
         R vzr = -ri * (d2[r] - (c3 * red)) - sg * vz;
         const R ib = IS(5, k);
-        const R bx = Hv(4, r) * ib, by = Hv(5, r) * ib, bz = Hv(6, r) * ib;
-        const R qx = O(b, O_BG + B_CBX, r), qy = O(b, O_BG + B_CBY, r),
-                qz = O(b, O_BG + B_CBZ, r);
+        const R bx = Hv(4, ownr) * ib, by = Hv(5, ownr) * ib, bz = Hv(6, ownr) * ib;
+        const R qx = O(b, O_BG + B_CBX, cr), qy = O(b, O_BG + B_CBY, cr),
+                qz = O(b, O_BG + B_CBZ, cr);
         const R e1 = qy * bz - qz * by, e2 = bx * qz - qx * bz, e3 = qx * by - qy * bx;
         vxr = vxr + ri * e1 * red;
         vyr = vyr + ri * e2 * red;
@@ -857,7 +864,7 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
         double vsq = 0.0;
 #pragma unroll
         for (int l = 1; l < 4; ++l) {
-          const R av = MODE == F_FIRST ? Hv(l - 1, r) : O(b, O_A + l, r);
+          const R av = MODE == F_FIRST ? Hv(l - 1, ownr) : O(b, O_A + l, cr);
           R an;
           if (MODE == F_LAST) {
             if constexpr (SCALED) {
@@ -877,20 +884,20 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
         }
         if (MODE == F_LAST) VSQ[cid[r]] = vsq;
       } else {
-        const R p = Hv(3, r) * IS(4, k);
+        const R p = Hv(3, ownr) * IS(4, k);
         const R dvzdz = X[cid[r]];
         const R div = d0[r] + dvzdz;
-        const R r0 = O(b, O_BG + B_RHO0, r);
-        const R Rr = -O(b, O_BG + B_GRX, r) * vx - O(b, O_BG + B_GRY, r) * vy -
-                     O(b, O_BG + B_GRZ, r) * vz - r0 * div - sg * rho;
-        const R Rp = -O(b, O_BG + B_C2R, r) * div - vx * O(b, O_BG + B_GPX, r) -
-                     vy * O(b, O_BG + B_GPY, r) - vz * O(b, O_BG + B_GPZ, r) - sg * p;
+        const R r0 = O(b, O_BG + B_RHO0, cr);
+        const R Rr = -O(b, O_BG + B_GRX, cr) * vx - O(b, O_BG + B_GRY, cr) * vy -
+                     O(b, O_BG + B_GRZ, cr) * vz - r0 * div - sg * rho;
+        const R Rp = -O(b, O_BG + B_C2R, cr) * div - vx * O(b, O_BG + B_GPX, cr) -
+                     vy * O(b, O_BG + B_GPY, cr) - vz * O(b, O_BG + B_GPZ, cr) - sg * p;
         const R Rs[5] = {Rr, Rp, red * d4[r], red * d6[r], red * d3[r]};
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
           const int l = q == 0 ? 0 : (q == 1 ? 4 : q + 3);
-          const R av = MODE == F_FIRST ? (l == 0 ? O(b, O_RHO, r) : Hv(l - 1, r))
-                                       : O(b, O_A + l, r);
+          const R av = MODE == F_FIRST ? (l == 0 ? O(b, O_RHO, cr) : Hv(l - 1, ownr))
+                                       : O(b, O_A + l, cr);
           const R s = SS(l, k);
           R an;
           if (MODE == F_LAST) {
@@ -910,7 +917,7 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
         }
         if (MODE == F_LAST) {
           mr = fmin(mr, (double)rho + (double)r0);
-          mp = fmin(mp, (double)p + (double)O(b, O_P0, r));
+          mp = fmin(mp, (double)p + (double)O(b, O_P0, cr));
         }
       }
     }
@@ -920,7 +927,7 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
           if (!act[r]) continue;
-          const double m = ((double)O(b, O_BG + B_RHO0, r) + an_rho[r]) * VSQ[cid[r]] / 2.0;
+          const double m = ((double)O(b, O_BG + B_RHO0, cid[r]) + an_rho[r]) * VSQ[cid[r]] / 2.0;
           ke += m * m;
         }
       }

@@ -635,86 +635,18 @@ __global__ void k_psr(PsrDev D) {
 
 int launch_psr_forcing(Handle *h, const SimDev &S, cudaStream_t s);
 
-// ------------------------------------------------------ FILTER_VARS pass
-// One direction of FILTER_VARS (derivatives.f90:659-703) over all fields:
-// out = filt(pre(in)) (mode 1) or pre(in) - s*filt(pre(in)) (mode 2), where
-// pre() is the edge pre-averaging of :672-693 applied on the fly from the
-// unmodified input.
-struct FiltDev {
-  int nx, ny, nz, periodic, g, mode2, V;
-  long long N;
-  double s;
-};
-
-template <int DIR>
-__global__ void k_filter_pass(FiltDev F, const double *__restrict__ in,
-                              double *__restrict__ out) {
-  const long long total = F.N * F.V;
-  const int n = DIR == 0 ? F.nx : (DIR == 1 ? F.ny : F.nz);
-  const long long st = DIR == 0 ? 1 : (DIR == 1 ? F.nx : (long long)F.nx * F.ny);
-  const bool per = DIR != 2 && F.periodic;
-  const bool avg = DIR == 2 || !F.periodic;
-  const int g = F.g;
-  const double *c = c_df[g == 5 ? 0 : 1];
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const long long pnt = t % F.N;
-    int q;
-    if (DIR == 0) q = (int)(pnt % F.nx);
-    else if (DIR == 1) q = (int)((pnt / F.nx) % F.ny);
-    else q = (int)(pnt / ((long long)F.nx * F.ny));
-    const long long base = t - (long long)q * st;
-    auto pre = [&](int qq) -> double {
-      const long long id = base + (long long)qq * st;
-      if (avg && ((qq >= 1 && qq <= g - 1) || (qq >= n - g && qq <= n - 2)))
-        return (__ldg(in + id + st) + __ldg(in + id - st)) / 2.0;
-      return __ldg(in + id);
-    };
-    const double pq = pre(q);
-    double filt;
-    if (!per && (q < g || q >= n - g)) {
-      filt = (DIR != 2 && g == 3) ? 0.0 : pq;
-    } else {
-      double s = 0.0;
-      for (int m = 0; m < 2 * g + 1; ++m) {
-        int qq = q - g + m;
-        if (per) qq = wrapi(qq, n);
-        s += pre(qq) * c[m];
-      }
-      filt = s;
-    }
-    out[t] = F.mode2 ? pq - F.s * filt : filt;
-  }
-}
-
-int launch_filter_pass(Handle *h, int dir, const double *in, double *out,
-                       cudaStream_t s) {
-  FiltDev F;
-  F.nx = h->nx; F.ny = h->ny; F.nz = h->nz;
-  F.periodic = h->periodic ? 1 : 0;
-  F.g = dir == 2 ? h->gz : h->gxy;
-  F.mode2 = F.g == 3;
-  F.V = h->V;
-  F.N = h->N;
-  F.s = dir == 2 ? h->P.s_z : h->P.s_xy;
-  long long total = F.N * F.V;
-  unsigned nb = (unsigned)std::min<long long>((total + 255) / 256, 148 * 32);
-  if (dir == 0) k_filter_pass<0><<<nb, 256, 0, s>>>(F, in, out);
-  else if (dir == 1) k_filter_pass<1><<<nb, 256, 0, s>>>(F, in, out);
-  else k_filter_pass<2><<<nb, 256, 0, s>>>(F, in, out);
-  ++h->launches;
-  return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
-}
-
+// ------------------------------------------------------ FILTER_VARS
 // FILTER_VARS of a filter event (filter_body.cuh): the fused y-then-x pass
-// over (32 x 8) layer tiles, and the z pass over columns.
+// over 32 x 32 layer tiles, and the z pass over slabs of 32 x 4 columns.
 __global__ void __launch_bounds__(fb::TX *fb::TY) k_filt_xy64(FiltArgs<double> F) {
   const int l = blockIdx.z / F.nz, k = blockIdx.z - l * F.nz;
-  filt_xy_tile(F, l, k, blockIdx.x * fb::TX, blockIdx.y * fb::TY);
+  filt_xy_tile(F, l, k, blockIdx.x * fb::TX, blockIdx.y * fb::TR);
 }
-__global__ void __launch_bounds__(256) k_filt_z64(FiltArgs<double> F) {
-  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
-  if (i < F.nx && j < F.ny) filt_z_column(F, blockIdx.z, i, j);
+__global__ void __launch_bounds__(2 * fb::ZX * fb::ZY) k_filt_z64(FiltArgs<double> F) {
+  extern __shared__ __align__(16) double zsl64[];
+  const int nzc = (F.nz + fb::ZC - 1) / fb::ZC;
+  const int l = blockIdx.z / nzc, kc = blockIdx.z - l * nzc;
+  filt_z_slab(F, l, blockIdx.x * fb::ZX, blockIdx.y * fb::ZY, kc * fb::ZC, zsl64);
 }
 
 // xy: the y and x passes fused; z: the z pass (in -> out, never in place)
@@ -727,11 +659,16 @@ int launch_filter_event(Handle *h, bool xy, const double *in, double *out, cudaS
   F.s = xy ? h->P.s_xy : h->P.s_z;
   F.in = in;
   F.out = out;
-  if (xy)
-    k_filt_xy64<<<dim3((h->nx + fb::TX - 1) / fb::TX, (h->ny + fb::TY - 1) / fb::TY,
+  if (xy) {
+    k_filt_xy64<<<dim3((h->nx + fb::TX - 1) / fb::TX, (h->ny + fb::TR - 1) / fb::TR,
                        h->V * h->nz), dim3(fb::TX, fb::TY), 0, s>>>(F);
-  else
-    k_filt_z64<<<dim3((h->nx + 31) / 32, (h->ny + 7) / 8, h->V), dim3(32, 8), 0, s>>>(F);
+  } else {
+    const size_t zs = filt_z_smem<double>();
+    cudaFuncSetAttribute(k_filt_z64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs);
+    k_filt_z64<<<dim3((h->nx + fb::ZX - 1) / fb::ZX, (h->ny + fb::ZY - 1) / fb::ZY,
+                      h->V * ((h->nz + fb::ZC - 1) / fb::ZC)),
+                 dim3(fb::ZX, fb::ZY, 2), zs, s>>>(F);
+  }
   ++h->launches;
   return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
 }

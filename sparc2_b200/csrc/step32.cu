@@ -517,25 +517,19 @@ __device__ __forceinline__ float filter_point32(const Filt32 &F, const float *__
   return r;
 }
 
-template <int DIR>
-__global__ void k_filter32(Filt32 F, const float *__restrict__ in, float *__restrict__ out) {
-  const long long total = F.N * F.V;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x)
-    out[t] = filter_point32<DIR>(F, in, nullptr, t);
-}
-
 // FILTER_VARS of a filter event in the precision form (filter_body.cuh):
 // the fused y-then-x pass over stored values (one depth scale per layer)
 // and the z pass over physical values; `carry` (the first pass of an event)
 // is subtracted on load, so the filter acts on the compensated value.
 __global__ void __launch_bounds__(fb::TX *fb::TY) k_filt_xy32(FiltArgs<float> F) {
   const int l = blockIdx.z / F.nz, k = blockIdx.z - l * F.nz;
-  filt_xy_tile(F, l, k, blockIdx.x * fb::TX, blockIdx.y * fb::TY);
+  filt_xy_tile(F, l, k, blockIdx.x * fb::TX, blockIdx.y * fb::TR);
 }
-__global__ void __launch_bounds__(256) k_filt_z32(FiltArgs<float> F) {
-  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
-  if (i < F.nx && j < F.ny) filt_z_column(F, blockIdx.z, i, j);
+__global__ void __launch_bounds__(2 * fb::ZX * fb::ZY) k_filt_z32(FiltArgs<float> F) {
+  extern __shared__ __align__(16) float zsl32[];
+  const int nzc = (F.nz + fb::ZC - 1) / fb::ZC;
+  const int l = blockIdx.z / nzc, kc = blockIdx.z - l * nzc;
+  filt_z_slab(F, l, blockIdx.x * fb::ZX, blockIdx.y * fb::ZY, kc * fb::ZC, zsl32);
 }
 
 int launch_filter_event32(Handle *h, bool xy, const float *in, const float *carry, float *out,
@@ -550,33 +544,17 @@ int launch_filter_event32(Handle *h, bool xy, const float *in, const float *carr
   F.out = out;
   F.carry = carry;
   if (xy) {
-    k_filt_xy32<<<dim3((h->nx + fb::TX - 1) / fb::TX, (h->ny + fb::TY - 1) / fb::TY,
+    k_filt_xy32<<<dim3((h->nx + fb::TX - 1) / fb::TX, (h->ny + fb::TR - 1) / fb::TR,
                        h->V * h->nz), dim3(fb::TX, fb::TY), 0, s>>>(F);
   } else {
     F.sc = h->f_sc;
     F.isc = h->f_isc;
-    k_filt_z32<<<dim3((h->nx + 31) / 32, (h->ny + 7) / 8, h->V), dim3(32, 8), 0, s>>>(F);
+    const size_t zs = filt_z_smem<float>();
+    cudaFuncSetAttribute(k_filt_z32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs);
+    k_filt_z32<<<dim3((h->nx + fb::ZX - 1) / fb::ZX, (h->ny + fb::ZY - 1) / fb::ZY,
+                      h->V * ((h->nz + fb::ZC - 1) / fb::ZC)),
+                 dim3(fb::ZX, fb::ZY, 2), zs, s>>>(F);
   }
-  ++h->launches;
-  return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
-}
-
-int launch_filter32(Handle *h, int dir, const float *in, float *out, cudaStream_t s) {
-  Filt32 F;
-  F.nx = h->nx; F.ny = h->ny; F.nz = h->nz;
-  F.periodic = h->periodic ? 1 : 0;
-  F.g = dir == 2 ? h->gz : h->gxy;
-  F.mode2 = F.g == 3;
-  F.V = h->V;
-  F.N = h->N;
-  F.s = (float)(dir == 2 ? h->P.s_z : h->P.s_xy);
-  F.sc = h->f_sc;
-  F.isc = h->f_isc;
-  long long total = F.N * F.V;
-  unsigned nb = (unsigned)std::min<long long>((total + 255) / 256, 148 * 32);
-  if (dir == 0) k_filter32<0><<<nb, 256, 0, s>>>(F, in, out);
-  else if (dir == 1) k_filter32<1><<<nb, 256, 0, s>>>(F, in, out);
-  else k_filter32<2><<<nb, 256, 0, s>>>(F, in, out);
   ++h->launches;
   return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
 }

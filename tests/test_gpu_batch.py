@@ -124,8 +124,10 @@ def test_tile_extent_does_not_change_results():
 
 def test_tile_shape_does_not_change_results():
     """MHD work items of 32 x 8 and 32 x 16 columns (one or two rows of
-    columns per thread) evaluate the same per-point arithmetic: the same
-    state, bit for bit, on a grid with interior and edge tiles."""
+    columns per thread) give the same state to FP32 rounding: the tile
+    height moves some rows between interior tiles (centred stencil as
+    antisymmetric pairs) and edge tiles (the coefficient-table sum), so the
+    order of the same terms differs there."""
     res = []
     for rows in (8, 16):
         with Batch(1) as b:
@@ -137,8 +139,9 @@ def test_tile_shape_does_not_change_results():
             for q in list(b.members):
                 b.remove(q)
         res.append(s.get_state())
-    assert np.array_equal(res[0][0], res[1][0])
-    assert np.array_equal(res[0][1], res[1][1])
+    for l in range(res[0][0].shape[0]):
+        assert rel_l2(res[1][0][l], res[0][0][l]) <= TOL, l
+    assert rel_l2(res[1][1], res[0][1]) <= TOL
 
 
 def test_tuner_and_membership_rules():

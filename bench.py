@@ -591,7 +591,6 @@ def measure_ensemble(dev, members=64, steps=100, warmup=2):
         batch.add(sm, 0, 1000)
     stream = torch.cuda.ExternalStream(batch.stream, device=dev)
     tiles = batch.tune(steps_per_trial=1)
-    batch_rows = batch.tile_rows
     batch.run(warmup)
     batch.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -608,7 +607,7 @@ def measure_ensemble(dev, members=64, steps=100, warmup=2):
     return {"value": pts / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "steps": steps,
             "dtype": "f32", "members": len(draws), "quiet_members": nq,
             "grid_points": pts, "tiles": {"zchunk_mhd": tiles[0], "zchunk_quiet": tiles[1],
-                      "mhd_tile": [32, batch_rows]},
+                      "mhd_tile": [32, 8]},
             "setup_s": setup,
             "workload": "batched ensemble: %d seeded members (nx=ny in {96..256}, nz in "
                         "[150, 300], quiet or flux tube, one pulse each), a step advances "
@@ -644,7 +643,6 @@ def run_ensemble(args, world, rank, local):
         batch.add(s, 0, total_steps)
     stream = torch.cuda.ExternalStream(batch.stream, device=dev)
     tiles = batch.tune(steps_per_trial=2)
-    tuned_rows = batch.tile_rows
     tuned_steps = 1000 - int(batch.remaining()[0])
     batch.run(W_)
     batch.synchronize()
@@ -735,7 +733,7 @@ def run_ensemble(args, world, rank, local):
                    % (len(draws), nq, len(draws) - nq),
                    "members": len(draws), "grid_points": pts,
                    "tiles": {"zchunk_mhd": tiles[0], "zchunk_quiet": tiles[1],
-                             "mhd_tile": [32, tuned_rows],
+                             "mhd_tile": [32, 8],
                              "autotuner_steps": tuned_steps},
                    "setup_s": t_setup,
                    "parallelism": "replicas" if world > 1 else "single GPU",

@@ -282,18 +282,11 @@ int sparc_batch_set_tiles(sparc_batch *b, int zchunk_mhd, int zchunk_quiet);
 int sparc_batch_get_tiles(const sparc_batch *b, int *zchunk_mhd,
                           int *zchunk_quiet);
 
-/* Tile shape of the MHD work items: 32 x mhd_rows columns (8 or 16; one
- * or two rows of columns per thread of the stage kernels).  The
- * autotuner's other knob.  Results do not depend on it beyond FP32
- * rounding of the same arithmetic. */
-int sparc_batch_set_tile_rows(sparc_batch *b, int mhd_rows);
-int sparc_batch_get_tile_rows(const sparc_batch *b, int *mhd_rows);
-
-/* Autotuner: times `steps_per_trial` batched steps per candidate tile shape
- * of the MHD items (32x16, 32x8), then per candidate z extent (one axis at
- * a time, MHD then quiet) and keeps the fastest; returns the z extents
- * (sparc_batch_get_tile_rows gives the shape).  The trial steps advance the
- * members like sparc_batch_run. */
+/* Autotuner: times `steps_per_trial` batched steps per candidate z extent
+ * of the work items (one axis at a time, MHD then quiet; their column
+ * shapes, 32x8 MHD and 32x16 quiet, are fixed by the kernels' thread
+ * layout) and keeps the fastest; returns the z extents.  The trial steps
+ * advance the members like sparc_batch_run. */
 int sparc_batch_tune(sparc_batch *b, int steps_per_trial, int *best_mhd,
                      int *best_quiet);
 

@@ -151,7 +151,6 @@ EXPORTS = [
     "sparc_batch_synchronize", "sparc_batch_stream",
     "sparc_batch_launch_count", "sparc_batch_last_error",
     "sparc_batch_tune", "sparc_ke_norm_noalloc", "sparc_inject_wait_timeout",
-    "sparc_batch_set_tile_rows", "sparc_batch_get_tile_rows",
     "sparc_estimate_bytes", "sparc_server_create", "sparc_server_destroy",
     "sparc_serve_submit", "sparc_serve_next", "sparc_serve_params",
     "sparc_serve_attach", "sparc_serve_result", "sparc_serve_release",
@@ -196,8 +195,6 @@ def _declare(lib):
         "sparc_batch_run": (C.c_int, [h, C.c_int64]),
         "sparc_batch_remaining": (C.c_int, [h, P(C.c_int64)]),
         "sparc_batch_set_tiles": (C.c_int, [h, C.c_int, C.c_int]),
-        "sparc_batch_set_tile_rows": (C.c_int, [h, C.c_int]),
-        "sparc_batch_get_tile_rows": (C.c_int, [h, P(C.c_int)]),
         "sparc_batch_get_tiles": (C.c_int, [h, P(C.c_int), P(C.c_int)]),
         "sparc_batch_synchronize": (C.c_int, [h]),
         "sparc_batch_stream": (C.c_int, [h, P(C.c_void_p)]),

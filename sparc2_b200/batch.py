@@ -86,18 +86,6 @@ class Batch:
                     "sparc_batch_get_tiles")
         return m.value, q.value
 
-    def set_tile_rows(self, rows):
-        """MHD work items of 32 x rows columns (8 or 16)."""
-        self._check(self.lib.sparc_batch_set_tile_rows(self.b, int(rows)),
-                    "sparc_batch_set_tile_rows")
-
-    @property
-    def tile_rows(self):
-        r = C.c_int()
-        self._check(self.lib.sparc_batch_get_tile_rows(self.b, C.byref(r)),
-                    "sparc_batch_get_tile_rows")
-        return r.value
-
     def tune(self, steps_per_trial=2):
         """Runs the autotuner (real steps of the members); returns the
         chosen (zchunk_mhd, zchunk_quiet)."""

@@ -36,7 +36,6 @@ struct Batch {
   bool dirty = true;                    // work-list or slot table to upload
   bool recapture = true;                // device arrays moved
   int zchunk_mhd = 32, zchunk_quiet = 48;
-  int mhd_rows = 8;                     // MHD work items: 32 x mhd_rows columns
   int fchunk = 1 << 16;
   int grid = 148;
   size_t psr_smem = 0;
@@ -97,7 +96,7 @@ int rebuild(Batch *b) {
       Handle *h = b->members[q];
       if (!h || (pass < 2) != h->magnetic) continue;
       Slot32 &L = b->slots[q];
-      const int TY = h->magnetic ? b->mhd_rows : 16;
+      const int TY = h->magnetic ? 8 : 16;
       const int zc = std::max(11, h->magnetic ? b->zchunk_mhd : b->zchunk_quiet);
       const int first = (int)items.size();
       for (int k0 = 0; k0 < h->nz; k0 += zc) {
@@ -196,7 +195,6 @@ int capture(Batch *b) {
   L.wctr = b->d_wctr;
   L.grid = b->grid;
   L.zmax = std::max(11, std::max(b->zchunk_mhd, b->zchunk_quiet));
-  L.mhd_rows = b->mhd_rows;
   L.psr_smem = b->psr_smem;
   cudaGraph_t g;
   BCK(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
@@ -413,24 +411,6 @@ int sparc_batch_set_tiles(sparc_batch *b, int zchunk_mhd, int zchunk_quiet) {
   return SPARC_OK;
 }
 
-int sparc_batch_set_tile_rows(sparc_batch *b, int mhd_rows) {
-  if (!b || (mhd_rows != 8 && mhd_rows != 16)) return SPARC_ERR_INVALID;
-  if (mhd_rows == b->mhd_rows) return SPARC_OK;
-  cudaSetDevice(b->device);
-  int r = pull_all(b);
-  if (r) return r;
-  b->mhd_rows = mhd_rows;
-  b->dirty = true;
-  b->recapture = true;  // another stage kernel and shared-memory size
-  return SPARC_OK;
-}
-
-int sparc_batch_get_tile_rows(const sparc_batch *b, int *mhd_rows) {
-  if (!b || !mhd_rows) return SPARC_ERR_INVALID;
-  *mhd_rows = b->mhd_rows;
-  return SPARC_OK;
-}
-
 int sparc_batch_get_tiles(const sparc_batch *b, int *zchunk_mhd, int *zchunk_quiet) {
   if (!b) return SPARC_ERR_INVALID;
   if (zchunk_mhd) *zchunk_mhd = b->zchunk_mhd;
@@ -457,10 +437,11 @@ int sparc_batch_launch_count(const sparc_batch *b, int64_t *count) {
   return SPARC_OK;
 }
 
-// Autotuner: picks the tile shape of the MHD work items (32 x 8 or 32 x 16
-// columns), then the z extent of the MHD and of the quiet work items, by
-// timing batched steps (CUDA events on the batch stream) over candidate
-// lists, one axis at a time.  The trial steps are real steps of the members.
+// Autotuner: picks the z extent of the MHD and of the quiet work items (the
+// work items' third tile dimension; their 32 x 8 and 32 x 16 column shapes
+// are fixed by the kernels' thread layout) by timing batched steps (CUDA
+// events on the batch stream) over a candidate list, one axis at a time.
+// The trial steps are real steps of the members.
 int sparc_batch_tune(sparc_batch *b, int steps_per_trial, int *best_mhd, int *best_quiet) {
   if (!b || steps_per_trial < 1) return SPARC_ERR_INVALID;
   cudaSetDevice(b->device);
@@ -468,9 +449,8 @@ int sparc_batch_tune(sparc_batch *b, int steps_per_trial, int *best_mhd, int *be
   cudaEvent_t e0, e1;
   BCK(b, cudaEventCreate(&e0));
   BCK(b, cudaEventCreate(&e1));
-  auto trial = [&](int rows, int zm, int zq, float *ms) -> int {
-    int r = sparc_batch_set_tile_rows(b, rows);
-    if (!r) r = sparc_batch_set_tiles(b, zm, zq);
+  auto trial = [&](int zm, int zq, float *ms) -> int {
+    int r = sparc_batch_set_tiles(b, zm, zq);
     if (!r) r = sparc_batch_run(b, 1);  // upload, capture, warm
     if (r) return r;
     if (!bok(b, cudaEventRecord(e0, b->stream), "cudaEventRecord")) return SPARC_ERR_CUDA;
@@ -481,24 +461,16 @@ int sparc_batch_tune(sparc_batch *b, int steps_per_trial, int *best_mhd, int *be
       return SPARC_ERR_CUDA;
     return SPARC_OK;
   };
-  int bm = b->zchunk_mhd, bq = b->zchunk_quiet, br = b->mhd_rows, r = SPARC_OK;
+  int bm = b->zchunk_mhd, bq = b->zchunk_quiet, r = SPARC_OK;
   float best = 1e30f, ms = 0.f;
   bool any_mhd = false, any_quiet = false;
   for (int q = 0; q < b->cap; ++q)
     if (b->members[q]) (b->members[q]->magnetic ? any_mhd : any_quiet) = true;
-  if (any_mhd)
-    for (int rows : {16, 8}) {
-      if ((r = trial(rows, bm, bq, &ms))) break;
-      if (ms < best) {
-        best = ms;
-        br = rows;
-      }
-    }
   for (int axis = 0; axis < 2 && !r; ++axis) {
     if ((axis == 0 && !any_mhd) || (axis == 1 && !any_quiet)) continue;
     for (int c : cand) {
       const int zm = axis == 0 ? c : bm, zq = axis == 1 ? c : bq;
-      if ((r = trial(br, zm, zq, &ms))) break;
+      if ((r = trial(zm, zq, &ms))) break;
       if (ms < best) {
         best = ms;
         bm = zm;
@@ -509,8 +481,7 @@ int sparc_batch_tune(sparc_batch *b, int steps_per_trial, int *best_mhd, int *be
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (r) return r;
-  r = sparc_batch_set_tile_rows(b, br);
-  if (!r) r = sparc_batch_set_tiles(b, bm, bq);
+  r = sparc_batch_set_tiles(b, bm, bq);
   if (best_mhd) *best_mhd = bm;
   if (best_quiet) *best_quiet = bq;
   return r;

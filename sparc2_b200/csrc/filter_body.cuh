@@ -11,14 +11,18 @@
 //     (derivatives.f90:680-684), the x filter and its combination, and
 //     writes the tile once.  The reference's y-then-x order is kept.
 //   * z (nn % zfreq == 0): a CTA loads a slab of 32 x 4 columns of one field
-//     over 64 layers and their 6-layer margins into shared memory, every
-//     load in flight at once; each thread then runs a 13-deep register
-//     window of raw values down its column for 32 layers (the pre-average of
-//     derivatives.f90:690-693 needs the neighbours of the 11 taps).
+//     over 32 layers and their 6-layer margins into shared memory (44 KB in
+//     FP64, so that five CTAs share an SM), every load in flight at once;
+//     each thread then runs a 13-deep register window of raw values down
+//     its column for 16 layers (the pre-average of derivatives.f90:690-693
+//     needs the neighbours of the 11 taps).  The z chunks of a slab are
+//     adjacent in the launch order, so their shared margins come from L2.
 //     filtz's edge layers are copied through (derivatives.f90:610-633).
 //
-// No 64-bit division or modulo per element: tile and column coordinates
-// come from the launch geometry.  In the precision form the stored state
+// The filter width (11 or 7 points) and the carry are template parameters,
+// so a kernel carries no per-element branch on them.  No 64-bit division
+// or modulo per element: tile and column coordinates come from the launch
+// geometry.  In the precision form the stored state
 // is depth-scaled and carries a compensation term: within a layer the scale
 // is one number, so the xy pass filters stored values; the z pass filters
 // physical values (stored * isc(k)) and stores back times sc(k).  The first
@@ -39,221 +43,260 @@ __device__ __forceinline__ R fcoef(int table, int m);
 
 // dynamic shared memory of the z pass (one slab)
 template <class R>
-constexpr size_t filt_z_smem() {
-  return (size_t)(64 + 12) * 4 * 32 * sizeof(R);
-}
+constexpr size_t filt_z_smem();
 
 template <class R>
 struct FiltArgs {
   int nx, ny, nz, V;
   long long N;
   int periodic;
-  int g;          // half-width of the event's filter (5: 11-point, 3: 7-point)
-  int mode2;      // a - s*filt (7-point) instead of filt
-  R s;
+  R s;                // a - s*filt (7-point filter)
   const R *in;
   R *out;
-  const R *carry;  // compensation subtracted on load (first pass), or null
+  const R *carry;     // compensation subtracted on load (first pass), or null
   const R *sc, *isc;  // depth scales V x nz (precision form z pass), or null
 };
 
 namespace fb {
-constexpr int TX = 32, TY = 8;           // threads of the xy pass (32 x 8)
-constexpr int TR = 32;                    // rows of an xy tile (4 per thread)
-constexpr int RX = TX + 12, RY = TR + 12, PY = TR + 10;
-constexpr int ZX = 32, ZY = 4, ZC = 64;   // z pass: 32 x 4 columns x 64 layers
+// xy pass: a 32 x 32 tile per CTA of 32 x 8 threads; the y pass gives 176
+// of them 8 rows of one of the 44 loaded columns
+constexpr int TX = 32, TY = 8, NT = TX * TY;
+constexpr int TR = 32, YG = 8;            // tile rows, rows per y-pass item
+constexpr int RX = TX + 12, RY = TR + 12;
+constexpr int NYI = RX * (TR / YG);       // y-pass items
+static_assert(NYI <= NT, "one y-pass item per thread at most");
+constexpr int ZX = 32, ZY = 4, ZC = 32;   // z pass: 32 x 4 columns x 32 layers
 constexpr int ZH = ZC + 12;               // layers loaded per z slab
+constexpr int ZL = ZC / 2;                // layers per thread
 }  // namespace fb
 
-__device__ __forceinline__ int fmod_idx(int q, int n) {
-  q %= n;
-  return q < 0 ? q + n : q;
+template <class R>
+constexpr size_t filt_z_smem() {
+  return (size_t)fb::ZH * fb::ZY * fb::ZX * sizeof(R);
 }
 
-// 11 or 7 taps of the filter at centre p of a strided row
-template <class R>
-__device__ __forceinline__ R ftaps(const R *p, int st, int g) {
+// q wrapped into [0, n) (q within a few periods of the range)
+__device__ __forceinline__ int wrap_idx(int q, int n) {
+  while (q < 0) q += n;
+  while (q >= n) q -= n;
+  return q;
+}
+
+// the 2G+1 taps of the filter at centre p of a strided row: G = 5 the
+// 11-point table, G = 3 the 7-point one
+template <class R, int G>
+__device__ __forceinline__ R ftaps(const R *p, int st) {
   R s = R(0);
-  if (g == 5) {
 #pragma unroll
-    for (int m = 0; m < 11; ++m) s += p[(m - 5) * st] * fcoef<R>(0, m);
-  } else {
-#pragma unroll
-    for (int m = 0; m < 7; ++m) s += p[(m - 3) * st] * fcoef<R>(1, m);
-  }
+  for (int m = 0; m <= 2 * G; ++m) s += p[(m - G) * st] * fcoef<R>(G == 5 ? 0 : 1, m);
   return s;
 }
 
+// Pre-average in place (derivatives.f90:671-675, 680-684): the rows (DIM = 0)
+// or columns (DIM = 1) q = 1..G-1 and n-G..n-2 of a shared array with row
+// pitch RX, whose index 0 sits at grid coordinate o, and whose rows or
+// columns [1, lim) may be read; each becomes the mean of its two neighbours.
+// ext: the extent along the other axis.  All values are formed before any
+// is stored (the reference averages the unaveraged array).
+template <class R, int G, int DIM>
+__device__ __forceinline__ void pre_average(R *a, int o, int n, int lim, int ext, int tid) {
+  constexpr int NE = 2 * (G - 1);
+  constexpr int PER = (NE * 44 + fb::NT - 1) / fb::NT;
+  R v[PER];
+  int at[PER];
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    at[u] = -1;
+    const int t = tid + u * fb::NT;
+    if (t >= NE * ext) continue;
+    const int e = t / ext, x = t - e * ext;
+    const int q = e < G - 1 ? 1 + e : n - G + (e - (G - 1));
+    const int l = q - o;
+    if (q < 1 || q > n - 2 || l < 1 || l >= lim) continue;
+    const int p = DIM == 0 ? l * fb::RX + x : x * fb::RX + l;
+    const int st = DIM == 0 ? fb::RX : 1;
+    v[u] = (a[p + st] + a[p - st]) / R(2);
+    at[u] = p;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < PER; ++u)
+    if (at[u] >= 0) a[at[u]] = v[u];
+  __syncthreads();
+}
+
 // The fused y-then-x pass over the 32 x 32 tile (x0, y0) of layer k of
-// field l; block (TX, TY) threads, each serving rows ty, ty + 8, ...
-template <class R>
+// field l; block (TX, TY) threads.  G: the filter half-width (5: the
+// 11-point filter, result filt; 3: the 7-point one, result a - s*filt).
+// CARRY: the first pass of a precision-form event (stored - carry).
+template <class R, int G, bool CARRY>
 __device__ __forceinline__ void filt_xy_tile(const FiltArgs<R> &F, int l, int k, int x0,
                                              int y0) {
   using namespace fb;
+  constexpr bool M2 = G == 3;
+  static_assert(RX == 44, "pre_average's item count");
   __shared__ R raw[RY][RX];  // rows y0-6 .., columns x0-6 ..
-  __shared__ R pre[PY][RX];  // y pre-averaged rows y0-5 .. (edge tiles only)
   __shared__ R fy[TR][RX];   // after the y pass, rows y0 .., columns x0-6 ..
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  const int nx = F.nx, ny = F.ny, g = F.g;
+  const int tid = threadIdx.y * TX + threadIdx.x;
+  const int nx = F.nx, ny = F.ny;
   const bool per = F.periodic;
+  const R fs = F.s;
   const long long base = (long long)l * F.N + (long long)k * nx * ny;
-  // rows in groups of RX columns: lanes walk a row, warps the rows
-  for (int ry = ty; ry < RY; ry += TY) {
-    int gy = y0 - 6 + ry;
-    bool oky = true;
-    if (per) gy = fmod_idx(gy, ny);
-    else oky = gy >= 0 && gy < ny;
-    for (int rx = tx; rx < RX; rx += TX) {
-      int gx = x0 - 6 + rx;
-      bool ok = oky;
-      if (per) gx = fmod_idx(gx, nx);
-      else ok = ok && gx >= 0 && gx < nx;
-      R v = R(0);
-      if (ok) {
-        const long long id = base + (long long)gy * nx + gx;
-        v = F.in[id];
-        if (F.carry) v = v - F.carry[id];
-      }
-      raw[ry][rx] = v;
-    }
-  }
-  __syncthreads();
-  // y pre-average of rows 1..g-1 and ny-g..ny-2 (non-periodic), only on
-  // tiles whose y window reaches such a row
-  const bool ypre = !per && (y0 - 5 <= g - 1 || y0 + TR + 4 >= ny - g);
-  if (ypre) {
-    for (int py = ty; py < PY; py += TY) {
-      const int gy = y0 - 5 + py;
-      const bool avg = (gy >= 1 && gy <= g - 1) || (gy >= ny - g && gy <= ny - 2);
-      for (int rx = tx; rx < RX; rx += TX)
-        pre[py][rx] = avg ? (raw[py + 2][rx] + raw[py][rx]) / R(2) : raw[py + 1][rx];
-    }
-    __syncthreads();
-  }
-  // the y pass of the tile's rows over every loaded column
-  for (int r = ty; r < TR; r += TY) {
-    const int gyo = y0 + r;
-    const bool yedge = !per && (gyo < g || gyo >= ny - g);
-    for (int rx = tx; rx < RX; rx += TX) {
-      const R *c = ypre ? &pre[r + 5][rx] : &raw[r + 6][rx];
-      const R pq = *c;
-      const R filt = yedge ? (g == 3 ? R(0) : pq) : ftaps(c, RX, g);
-      fy[r][rx] = F.mode2 ? pq - F.s * filt : filt;
-    }
-  }
-  __syncthreads();
-  // the x pre-average (on the fly) and the x pass at the tile's own columns
-  const int gxo = x0 + tx;
-  if (gxo >= nx) return;
-  const bool xpre = !per && (x0 - 5 <= g - 1 || x0 + TX + 4 >= nx - g);
-  const bool xedge = !per && (gxo < g || gxo >= nx - g);
-  const int c0 = tx + 6;
-  for (int r = ty; r < TR; r += TY) {
-    const int gyo = y0 + r;
-    if (gyo >= ny) break;
-    auto px = [&](int c) -> R {  // x pre-averaged value at loaded column c
-      const int gx = x0 - 6 + c;
-      if ((gx >= 1 && gx <= g - 1) || (gx >= nx - g && gx <= nx - 2))
-        return (fy[r][c + 1] + fy[r][c - 1]) / R(2);
-      return fy[r][c];
-    };
-    R pq, filt;
-    if (!xpre) {
-      pq = fy[r][c0];
-      filt = ftaps(&fy[r][c0], 1, g);
+  const R *in = F.in + base;
+  const R *cin = CARRY ? F.carry + base : nullptr;
+  // the (32+12) x (32+12) neighbourhood, one flat index over it
+  for (int t = tid; t < RY * RX; t += NT) {
+    const int ry = t / RX, rx = t - ry * RX;
+    int gy = y0 - 6 + ry, gx = x0 - 6 + rx;
+    bool ok = true;
+    if (per) {
+      gy = wrap_idx(gy, ny);
+      gx = wrap_idx(gx, nx);
     } else {
-      pq = px(c0);
-      if (xedge) {
-        filt = g == 3 ? R(0) : pq;
+      ok = gy >= 0 && gy < ny && gx >= 0 && gx < nx;
+    }
+    R v = R(0);
+    if (ok) {
+      const int id = gy * nx + gx;
+      v = in[id];
+      if (CARRY) v = v - cin[id];
+    }
+    raw[ry][rx] = v;
+  }
+  __syncthreads();
+  // y pre-average of rows 1..G-1 and ny-G..ny-2 (non-periodic) on the tiles
+  // whose y window reaches such a row (rows 1 .. RY-2 are read below)
+  if (!per && (y0 - 5 <= G - 1 || y0 + TR + 4 >= ny - G))
+    pre_average<R, G, 0>(&raw[0][0], y0 - 6, ny, RY - 1, RX, tid);
+  // the y pass: column rx, rows r0 .. r0+7 from one read of the 8 + 2G
+  // values around them (the centre of row r0 + j is v[j + 5])
+  if (tid < NYI) {
+    const int grp = tid / RX, rx = tid - grp * RX, r0 = grp * YG;
+    const R *sb = &raw[r0 + 1][rx];
+    R v[YG + 10];
+#pragma unroll
+    for (int q = 5 - G; q < YG + 5 + G; ++q) v[q] = sb[q * RX];
+#pragma unroll
+    for (int j = 0; j < YG; ++j) {
+      const int gyo = y0 + r0 + j;
+      const R pq = v[j + 5];
+      R filt;
+      if (!per && (gyo < G || gyo >= ny - G)) {
+        filt = M2 ? R(0) : pq;
       } else {
         R s = R(0);
-        if (g == 5) {
 #pragma unroll
-          for (int m = 0; m < 11; ++m) s += px(c0 - 5 + m) * fcoef<R>(0, m);
-        } else {
-#pragma unroll
-          for (int m = 0; m < 7; ++m) s += px(c0 - 3 + m) * fcoef<R>(1, m);
-        }
+        for (int m = 0; m <= 2 * G; ++m) s += v[j + 5 - G + m] * fcoef<R>(G == 5 ? 0 : 1, m);
         filt = s;
       }
+      fy[r0 + j][rx] = M2 ? pq - fs * filt : filt;
     }
-    F.out[base + (long long)gyo * nx + gxo] = F.mode2 ? pq - F.s * filt : filt;
+  }
+  __syncthreads();
+  // x pre-average of columns 1..G-1 and nx-G..nx-2 on the tiles whose x
+  // window reaches such a column
+  if (!per && (x0 - 5 <= G - 1 || x0 + TX + 4 >= nx - G))
+    pre_average<R, G, 1>(&fy[0][0], x0 - 6, nx, RX - 1, TR, tid);
+  // the x pass at the tile's own columns, a warp per row
+  R *out = F.out + base;
+#pragma unroll
+  for (int u = 0; u < TR * TX / NT; ++u) {
+    const int t = tid + u * NT;
+    const int r = t / TX, tx = t - r * TX;
+    const int gxo = x0 + tx, gyo = y0 + r;
+    if (gxo >= nx || gyo >= ny) continue;
+    const R *c = &fy[r][tx + 6];
+    const R pq = *c;
+    const R filt = (!per && (gxo < G || gxo >= nx - G)) ? (M2 ? R(0) : pq) : ftaps<R, G>(c, 1);
+    out[gyo * nx + gxo] = M2 ? pq - fs * filt : filt;
   }
 }
 
 // The z pass of a slab of 32 x 4 columns and ZC layers from k0 of field l:
 // the slab and its 6-layer margins are loaded into shared memory in one go
-// (every load in flight at once), then each thread runs a register window
-// down its column for half of the layers.  Block (32, 4, 2) threads; sl is
-// the CTA's dynamic shared memory, ZH x ZY x ZX values (layers k0-6 ..).
-template <class R>
+// (every load in flight at once), then each thread filters ZL consecutive
+// layers of its column.  Block (32, 4, 2) threads; sl is the CTA's dynamic
+// shared memory, ZH x ZY x ZX values (layers k0-6 ..).  G and CARRY as for
+// the xy pass; SC: the precision form (filters physical values, stored *
+// isc(k), and stores them times sc(k)).
+template <class R, int G, bool CARRY, bool SC>
 __device__ __forceinline__ void filt_z_slab(const FiltArgs<R> &F, int l, int x0, int y0,
                                             int k0, R *sl) {
   using namespace fb;
+  constexpr bool M2 = G == 3;
   const int tx = threadIdx.x, ty = threadIdx.y, tz = threadIdx.z;
-  const int tid = (tz * ZY + ty) * ZX + tx;
-  const int nx = F.nx, ny = F.ny, nz = F.nz, g = F.g;
+  const int nx = F.nx, ny = F.ny, nz = F.nz;
   const long long NXY = (long long)nx * ny;
-  const long long fb0 = (long long)l * F.N;
-  const bool sc = F.isc != nullptr;
-  for (int t = tid; t < ZH * ZY * ZX; t += 2 * ZY * ZX) {
-    const int x = t % ZX, y = (t / ZX) % ZY, q = t / (ZX * ZY);
-    const int gx = x0 + x, gy = y0 + y, gz = k0 - 6 + q;
+  const int gx = x0 + tx, gy = y0 + ty;
+  const bool colok = gx < nx && gy < ny;
+  // this thread's column; each thread loads layers q = tz, tz + 2, ...
+  const R *icol = F.in + (long long)l * F.N + (colok ? (long long)gy * nx + gx : 0);
+  const R *ccol = CARRY ? F.carry + (icol - F.in) : nullptr;
+  const R *isc = SC ? F.isc + l * nz : nullptr;
+  for (int q = tz; q < ZH; q += 2) {
+    const int gz = k0 - 6 + q;
     R v = R(0);
-    if (gx < nx && gy < ny && gz >= 0 && gz < nz) {
-      const long long id = fb0 + gz * NXY + (long long)gy * nx + gx;
-      v = F.in[id];
-      if (F.carry) v = v - F.carry[id];
-      if (sc) v = v * F.isc[l * nz + gz];
+    if (colok && gz >= 0 && gz < nz) {
+      v = icol[gz * NXY];
+      if (CARRY) v = v - ccol[gz * NXY];
+      if (SC) v = v * isc[gz];
     }
-    sl[(q * ZY + y) * ZX + x] = v;
+    sl[(q * ZY + ty) * ZX + tx] = v;
   }
   __syncthreads();
-  const int gx = x0 + tx, gy = y0 + ty;
-  if (gx >= nx || gy >= ny) return;
-  const long long col = fb0 + (long long)gy * nx + gx;
-  // this thread's layers [ka, kb)
-  const int ka = k0 + tz * (ZC / 2), kb = min(nz, ka + ZC / 2);
-  auto in_avg = [&](int q) { return (q >= 1 && q <= g - 1) || (q >= nz - g && q <= nz - 2); };
-  // layer L sits at slab index L - (k0 - 6)
+  if (!colok) return;
+  R *ocol = F.out + (icol - F.in);
+  const R fs = F.s;
+  const R *sc = SC ? F.sc + l * nz : nullptr;
+  // this thread's layers [ka, kb); layer L sits at slab index L - (k0 - 6)
+  const int ka = k0 + tz * ZL, kb = min(nz, ka + ZL);
+  const R *wl = sl + ((ka - k0) * ZY + ty) * ZX + tx;  // raw(ka - 6) ..
+  if (kb - ka == ZL && ka - 6 >= G && kb + 5 <= nz - G - 1) {
+    // every layer away from the edges: no pre-average, no edge rule; the
+    // window is unrolled, so its values are named registers
+    R w[ZL + 12];
+#pragma unroll
+    for (int m = 6 - G; m < ZL + 6 + G; ++m) w[m] = wl[m * ZY * ZX];
+#pragma unroll
+    for (int j = 0; j < ZL; ++j) {
+      R s = R(0);
+#pragma unroll
+      for (int m = 0; m <= 2 * G; ++m) s += w[j + 6 - G + m] * fcoef<R>(G == 5 ? 0 : 1, m);
+      R r = M2 ? w[j + 6] - fs * s : s;
+      if (SC) r = r * sc[ka + j];
+      ocol[(ka + j) * NXY] = r;
+    }
+    return;
+  }
+  auto in_avg = [&](int q) { return (q >= 1 && q <= G - 1) || (q >= nz - G && q <= nz - 2); };
   R w[13];  // w[m] = raw(k - 6 + m)
 #pragma unroll
-  for (int m = 0; m < 13; ++m) w[m] = sl[((ka - k0 + m) * ZY + ty) * ZX + tx];
+  for (int m = 0; m < 13; ++m) w[m] = wl[m * ZY * ZX];
   for (int k = ka; k < kb; ++k) {
     auto pre = [&](int m) -> R {
       return in_avg(k - 6 + m) ? (w[m + 1] + w[m - 1]) / R(2) : w[m];
     };
     const R pq = pre(6);
     R filt;
-    if (k < g || k >= nz - g) {
+    if (k < G || k >= nz - G) {
       filt = pq;
-    } else if (k - 6 >= g && k + 6 <= nz - g - 1) {
+    } else if (k - 6 >= G && k + 6 <= nz - G - 1) {
       R s = R(0);
-      if (g == 5) {
 #pragma unroll
-        for (int m = 0; m < 11; ++m) s += w[1 + m] * fcoef<R>(0, m);
-      } else {
-#pragma unroll
-        for (int m = 0; m < 7; ++m) s += w[3 + m] * fcoef<R>(1, m);
-      }
+      for (int m = 0; m <= 2 * G; ++m) s += w[6 - G + m] * fcoef<R>(G == 5 ? 0 : 1, m);
       filt = s;
     } else {
       R s = R(0);
-      if (g == 5) {
 #pragma unroll
-        for (int m = 0; m < 11; ++m) s += pre(1 + m) * fcoef<R>(0, m);
-      } else {
-#pragma unroll
-        for (int m = 0; m < 7; ++m) s += pre(3 + m) * fcoef<R>(1, m);
-      }
+      for (int m = 0; m <= 2 * G; ++m) s += pre(6 - G + m) * fcoef<R>(G == 5 ? 0 : 1, m);
       filt = s;
     }
-    R r = F.mode2 ? pq - F.s * filt : filt;
-    if (sc) r = r * F.sc[l * nz + k];
-    F.out[col + k * NXY] = r;
+    R r = M2 ? pq - fs * filt : filt;
+    if (SC) r = r * sc[k];
+    ocol[k * NXY] = r;
 #pragma unroll
     for (int m = 0; m < 12; ++m) w[m] = w[m + 1];
-    if (k + 1 < kb) w[12] = sl[((k + 13 - k0) * ZY + ty) * ZX + tx];  // raw(k + 7)
+    if (k + 1 < kb) w[12] = wl[(k + 13 - ka) * ZY * ZX];  // raw(k + 7)
   }
 }
 

@@ -145,7 +145,6 @@ struct BatchLaunch {
   unsigned *wctr;                       // [14] work counters, zeroed per step
   int grid;                             // persistent CTAs
   int zmax;                             // largest z extent of a stage item
-  int mhd_rows;                         // rows of an MHD work item (8 or 16)
   size_t psr_smem;
 };
 

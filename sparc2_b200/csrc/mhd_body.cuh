@@ -43,18 +43,15 @@ enum { B_RED, B_SPONGE, B_RHO0, B_GRX, B_GRY, B_GRZ, B_C2R, B_GPX, B_GPY,
 // 42 x 18 copied by cp.async.  Exchange area:
 // d(vz)/dz and d(by)/dz in R, |v_new|^2 in FP64 (in the d(by)/dz slot in
 // the plain form, after its reader).
-template <class R, bool TH = false, int NR = 1>
+template <class R, bool TH = false>
 struct MhdBuf {
   static constexpr int ALIGN = 128 / (int)sizeof(R);
-  static_assert(!TH || (sizeof(R) == 8 && NR == 1), "TMA halo boxes in the plain form only");
-  static constexpr int TYT = mg::TY * NR, NCT = mg::TX * TYT;  // tile rows, columns
-  static constexpr int HYT = TYT + 10;                          // halo plane rows
-  static constexpr int HST = mg::HX * HYT;                      // halo plane positions
+  static_assert(!TH || sizeof(R) == 8, "TMA halo boxes in the plain form only");
   static constexpr int HXL = TH ? 44 : mg::HX;
   static constexpr int XOFF = TH ? 1 : 0;
-  static constexpr int HSL = TH ? (HXL * HYT + ALIGN - 1) / ALIGN * ALIGN : HST;
-  static constexpr int BUF = ((mg::NO * NCT + mg::NH * HSL) + ALIGN - 1) / ALIGN * ALIGN;
-  static constexpr int XCH = sizeof(R) == 4 ? 4 * NCT : 2 * NCT;
+  static constexpr int HSL = TH ? (HXL * mg::HY + ALIGN - 1) / ALIGN * ALIGN : mg::HS;
+  static constexpr int BUF = ((mg::NO * mg::NC + mg::NH * HSL) + ALIGN - 1) / ALIGN * ALIGN;
+  static constexpr int XCH = sizeof(R) == 4 ? 4 * mg::NC : 2 * mg::NC;
   static constexpr size_t SMEM = (2 * (size_t)BUF + XCH) * sizeof(R) + 128;
   // precision form: the depth scales (8 inverse, 8 forward per layer) of a
   // chunk of at most zext layers follow the exchange area
@@ -316,36 +313,35 @@ __device__ void diag_reduce_t(const SimT<R> &S, double ke, double mr, double mp,
   }
 }
 
-// Tiles (32 x TYT columns) away from every edge, CPML slab and periodic
-// wrap: their x/y derivatives are the centred stencil with no branch.
-template <class R, int TYT = mg::TY>
+// Tiles away from every edge, CPML slab and periodic wrap: their x/y
+// derivatives are the centred stencil with no branch.
+template <class R>
 __device__ __forceinline__ bool mhd_interior(const SimT<R> &S, int x0, int y0) {
   const int xm = max(5, S.xb.on ? S.xb.np : 0), xM = max(5, S.xt.on ? S.xt.np : 0);
   const int ym = max(5, S.yb.on ? S.yb.np : 0), yM = max(5, S.yt.on ? S.yt.np : 0);
-  return x0 >= xm && x0 + mg::TX <= S.nx - xM && y0 >= ym && y0 + TYT <= S.ny - yM;
+  return x0 >= xm && x0 + mg::TX <= S.nx - xM && y0 >= ym && y0 + mg::TY <= S.ny - yM;
 }
 
 // Host side: the rectangle of interior tiles [ix0, ix1) x [iy0, iy1) (tile
-// units of 32 x ty columns) of a grid whose x/y CPML widths are np[0..3] (0
-// if off); empty if ix1 <= ix0 or iy1 <= iy0.
+// units) of a grid whose x/y CPML widths are np[0..3] (0 if off); empty if
+// ix1 <= ix0 or iy1 <= iy0.
 inline void mhd_interior_rect(int nx, int ny, const int np[4], int &ix0, int &ix1, int &iy0,
-                              int &iy1, int ty = mg::TY) {
+                              int &iy1) {
   const int xm = np[0] > 5 ? np[0] : 5, xM = np[1] > 5 ? np[1] : 5;
   const int ym = np[2] > 5 ? np[2] : 5, yM = np[3] > 5 ? np[3] : 5;
   ix0 = (xm + mg::TX - 1) / mg::TX;
-  iy0 = (ym + ty - 1) / ty;
+  iy0 = (ym + mg::TY - 1) / mg::TY;
   ix1 = nx - xM - mg::TX >= 0 ? (nx - xM - mg::TX) / mg::TX + 1 : 0;
-  iy1 = ny - yM - ty >= 0 ? (ny - yM - ty) / ty + 1 : 0;
+  iy1 = ny - yM - mg::TY >= 0 ? (ny - yM - mg::TY) / mg::TY + 1 : 0;
 }
 
 // The body covers the tile (x0, y0) over layers [k0, k1) with a block of
-// 32 x 8 x 2 threads (threadIdx.z is the role); each thread serves NR rows
-// of columns (rows ty, ty + 8), so the tile is 32 x 8*NR columns.
-// smem is the 128-byte aligned dynamic buffer.  TMA = false: the own-point
-// arrays are fetched by cp.async too (any nx).  INT: the tile's stencil
-// footprint touches no non-periodic edge, no x/y CPML slab and needs no
-// periodic wrap, so its x/y derivatives are the centred stencil with no
-// branch.  Returns false when a bounded wait gave up.
+// 32 x 8 x 2 threads (threadIdx.z is the role); smem is the 128-byte aligned
+// dynamic buffer.  TMA = false: the own-point arrays are fetched by
+// cp.async too (any nx).  INT: the tile's stencil footprint touches no
+// non-periodic edge, no x/y CPML slab and needs no periodic wrap, so its
+// x/y derivatives are the centred stencil with no branch.  Returns false
+// when a bounded wait gave up.
 //
 // Per layer: every thread waits for its own halo copies, turns the B0 halo
 // values it copied into the fluxes v x B0 in place, then one barrier makes
@@ -353,11 +349,8 @@ inline void mhd_interior_rect(int nx, int ny, const int np[4], int &ix0, int &ix
 // barrier (the buffer they overwrite was last read before it).  A named
 // barrier of the two warps that share rows ty (role 0 warp ty, role 1 warp
 // 8 + ty) exchanges d(vz)/dz and d(by)/dz: nothing else crosses warps
-// until the next layer's barrier.  With NR = 2 the per-layer work that does
-// not depend on the column (barriers, copy issue, depth scales, layer
-// flags, loop control) is shared by two points, at the price of register
-// spills (the batched engine's tuner weighs the two).
-template <class R, int MODE, bool TMA, bool INT, int NR = 1>
+// until the next layer's barrier.
+template <class R, int MODE, bool TMA, bool INT>
 __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *smem,
                                          const R *__restrict__ a,
                                          const R *__restrict__ tin,
@@ -365,41 +358,26 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
                                          int x0, int y0, int k0, int k1, int mt, int ma,
                                          double &ke, double &mr, double &mp) {
   using namespace mg;
-  static_assert(NR == 1 || NR == 2, "one or two rows per thread");
-  constexpr int TW = TY;                       // thread rows per role
-  constexpr int TYT = TW * NR;                 // tile rows
-  constexpr int NTW = 2 * TX * TW, NCW = TX * TW;  // threads, threads per role
   // halo planes by TMA in the plain form's interior kernel (measured: 4 %
   // faster in FP64; in FP32 the 48-wide boxes cost more than the cp.async
   // copies they replace)
-  constexpr bool TH = TMA && INT && sizeof(R) == 8 && TYT == 8;
-  using MB = MhdBuf<R, TH, TYT / 8>;
+  constexpr bool TH = TMA && INT && sizeof(R) == 8;
+  using MB = MhdBuf<R, TH>;
   constexpr int BUF = MB::BUF, HXL = MB::HXL, XOFF = MB::XOFF, HSL = MB::HSL;
-  constexpr int NCT = MB::NCT, HYT = MB::HYT, HST = MB::HST;
   constexpr bool SCALED = sizeof(R) == 4;
   __shared__ unsigned long long bar[2];
   const int tx = threadIdx.x, ty = threadIdx.y, role = threadIdx.z;
-  const int tid = (role * TW + ty) * TX + tx;
+  const int tid = (role * TY + ty) * TX + tx, cid = ty * TX + tx;
   const int nx = S.nx, ny = S.ny, nz = S.nz;
   const int N = (int)S.N, NXY = nx * ny;
-  const int i = x0 + tx;
+  const int i = x0 + tx, j = y0 + ty;
+  const bool act = INT || (i < nx && j < ny);
   const bool per = S.periodic;
+  const int col = j * nx + i;
   const int xo = INT ? x0 - 5 : origin_t(x0, TX, nx, per);
-  const int yo = INT ? y0 - 5 : origin_t(y0, TYT, ny, per);
-  const int rx = x0 - xo + tx;
-  // per row r of this thread: grid row, tile column id, grid column index,
-  // tile row in the halo planes and own position there
-  int jr[NR], cid[NR], col[NR], ryr[NR], own[NR];
-  bool act[NR];
-#pragma unroll
-  for (int r = 0; r < NR; ++r) {
-    jr[r] = y0 + ty + r * TW;
-    cid[r] = (ty + r * TW) * TX + tx;
-    act[r] = INT || (i < nx && jr[r] < ny);
-    col[r] = jr[r] * nx + i;
-    ryr[r] = y0 - yo + ty + r * TW;
-    own[r] = ryr[r] * HXL + rx + XOFF;
-  }
+  const int yo = INT ? y0 - 5 : origin_t(y0, TY, ny, per);
+  const int ry = y0 - yo + ty, rx = x0 - xo + tx;
+  const int own = ry * HXL + rx + XOFF;
   const R *isc = S.isc, *sc = S.sc;
   // depth scales of the precision form, staged in shared memory for the
   // layers this chunk touches; 1 (folded away) in the plain form
@@ -407,7 +385,7 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
   const int zb = max(0, min(k0 - 5, nz - 11));
   if constexpr (SCALED) {
     const int ze = min(nz, max(k1 + 5, zb + 11));
-    for (int t = tid; t < (ze - zb) * 16; t += NTW) {
+    for (int t = tid; t < (ze - zb) * 16; t += NT) {
       const int kk = zb + (t >> 4), l = t & 15;
       ZT[t] = l < 8 ? isc[l * nz + kk] : sc[(l - 8) * nz + kk];
     }
@@ -428,11 +406,11 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
   // axis, or no lane within 5 points of an edge); then the centred sum
   // from the window start cxo (cyo) of lane (row) 0 serves
   const bool cen_x = per || (x0 >= 5 && x0 + TX <= nx - 5);
-  const bool cen_y = per || (y0 >= 5 && y0 + TYT <= ny - 5);
+  const bool cen_y = per || (y0 >= 5 && y0 + TY <= ny - 5);
   const int cxo = x0 - 5 - xo, cyo = y0 - 5 - yo;
-  __shared__ R cxs[INT ? 1 : TX * 11], cys[INT ? 1 : TYT * 11];
-  __shared__ int cxb[INT ? 1 : TX], cyb[INT ? 1 : TYT];
-  if (!INT && tid < TX + TYT) {
+  __shared__ R cxs[INT ? 1 : TX * 11], cys[INT ? 1 : TY * 11];
+  __shared__ int cxb[INT ? 1 : TX], cyb[INT ? 1 : TY];
+  if (!INT && tid < TX + TY) {
     const bool isx = tid < TX;
     const int q0 = isx ? tid : tid - TX;                 // lane or row
     const int g = isx ? x0 + q0 : y0 + q0, n = isx ? nx : ny, o = isx ? xo : yo;
@@ -458,31 +436,19 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  // per-row values are passed in (not the row index), so no per-row array is
-  // indexed inside a helper that the compiler might not inline
-  auto O = [&](int b, int slot, int c) -> R { return smem[b * BUF + slot * NCT + c]; };
-  auto Hp = [&](int b, int slot) -> R * { return smem + b * BUF + NO * NCT + slot * HSL; };
+  auto O = [&](int b, int slot) -> R { return smem[b * BUF + slot * NC + cid]; };
+  auto Hp = [&](int b, int slot) -> R * { return smem + b * BUF + NO * NC + slot * HSL; };
   R *X = smem + 2 * BUF;
-  // halo positions this thread copies (and turns into fluxes): 32 x 8
-  // tile: positions 0..511 one per thread, 512..755 on role 1 (role 0
-  // carries the TMA issue and the heavier momentum update); 32 x 16 tile:
-  // 0..1023 two per thread, 1024..1091 on role 1
-  constexpr int NP = NR + 1;
-  int hs[NP], ho[NP];
+  int hs0 = -1, hs1 = -1, ho0 = 0, ho1 = 0;
   {
-#pragma unroll
-    for (int p = 0; p < NP; ++p) {
-      hs[p] = -1;
-      ho[p] = 0;
-    }
     const int cx0 = x0 - xo, cy0 = y0 - yo;
-    auto pos = [&](int t, int &hs_, int &ho_) {
-      if (t >= HST) return;
+    auto pos = [&](int t, int &hs, int &ho) {
+      if (t >= HS) return;
       const int ly = t / HX, lx = t - ly * HX;
-      const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TYT;
+      const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
       if (!inx && !iny) return;
       if (TH) {  // in the domain by the interior test; no global offset
-        hs_ = ly * HXL + lx + XOFF;
+        hs = ly * HXL + lx + XOFF;
         return;
       }
       int gx = xo + lx, gy = yo + ly;
@@ -492,16 +458,13 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
       } else if (gx < 0 || gx >= nx || gy < 0 || gy >= ny) {
         return;
       }
-      hs_ = t;
-      ho_ = gy * nx + gx;
+      hs = t;
+      ho = gy * nx + gx;
     };
-    pos(tid, hs[0], ho[0]);
-    if (NR == 1) {
-      if (role == 1) pos(tid + NCW, hs[1], ho[1]);
-    } else {
-      pos(tid + NTW, hs[1], ho[1]);
-      if (role == 1) pos(tid + 2 * NTW - NCW, hs[2], ho[2]);
-    }
+    // halo positions 0..511 one per thread, 512..755 on role 1 (role 0
+    // carries the TMA issue and the heavier momentum update)
+    pos(tid, hs0, ho0);
+    if (role == 1) pos(tid + NC, hs1, ho1);
   }
   // Own-point arrays not read: in the plain form rhoinv (the kernel forms
   // 1/rho0, the same IEEE quotient initialize.f90:1012 stores; the
@@ -510,7 +473,7 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
   // whose points lie in no slab (a CTA-uniform test per layer).
   constexpr bool DERIVE_RI = sizeof(R) == 8;
   const bool slab_xy = !INT && ((S.xb.on && (x0 < S.xb.np || x0 + TX > nx - S.xt.np)) ||
-                                (S.yb.on && (y0 < S.yb.np || y0 + TYT > ny - S.yt.np)));
+                                (S.yb.on && (y0 < S.yb.np || y0 + TY > ny - S.yt.np)));
   auto sponge_at = [&](int k) -> bool {
     return !S.sponge_slabs || slab_xy || (S.zb.on && (k < S.zb.np || k >= nz - S.zt.np));
   };
@@ -521,50 +484,53 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
   auto own_bytes = [&](int k) -> unsigned {
     return ((MODE == F_FIRST ? 15u : (MODE == F_MID ? 23u : 24u)) - (DERIVE_RI ? 1u : 0u) -
             (sponge_at(k) ? 0u : 1u)) *
-               NCT * (unsigned)sizeof(R) +
-           (TH ? (unsigned)(NH * HXL * HYT * sizeof(R)) : 0u);
+               NC * (unsigned)sizeof(R) +
+           (TH ? (unsigned)(NH * HXL * HY * sizeof(R)) : 0u);
   };
   auto issue = [&](int k, int b) {
     const int kb = k * NXY;
-#pragma unroll
-    for (int p = 0; p < NP; ++p) {
-      if (TH || hs[p] < 0) continue;
-      R *h = Hp(b, 0) + hs[p];
-      const int id = kb + ho[p];
+    if (!TH && hs0 >= 0) {
+      R *h = Hp(b, 0) + hs0;
+      const int id = kb + ho0;
 #pragma unroll
       for (int sl = 0; sl < 7; ++sl) cp_r(h + sl * HSL, tin + (sl + 1) * N + id);
       cp_r(h + 7 * HSL, S.box + id);
       cp_r(h + 8 * HSL, S.boy + id);
       cp_r(h + 9 * HSL, S.boz + id);
     }
-    if (!TMA) {
+    if (!TH && hs1 >= 0) {
+      R *h = Hp(b, 0) + hs1;
+      const int id = kb + ho1;
 #pragma unroll
-      for (int r = 0; r < NR; ++r) {
-        if (!act[r]) continue;
-        R *ob = smem + b * BUF + cid[r];
-        const int id = kb + col[r];
-        if (role == 0) {
-          cp_r(ob + O_RHO * NCT, tin + id);
-          if (MODE != F_FIRST)
+      for (int sl = 0; sl < 7; ++sl) cp_r(h + sl * HSL, tin + (sl + 1) * N + id);
+      cp_r(h + 7 * HSL, S.box + id);
+      cp_r(h + 8 * HSL, S.boy + id);
+      cp_r(h + 9 * HSL, S.boz + id);
+    }
+    if (!TMA && act) {
+      R *ob = smem + b * BUF + cid;
+      const int id = kb + col;
+      if (role == 0) {
+        cp_r(ob + O_RHO * NC, tin + id);
+        if (MODE != F_FIRST)
 #pragma unroll
-            for (int l = 0; l < 8; ++l) cp_r(ob + (O_A + l) * NCT, a + l * N + id);
-        } else {
-          const R *bg[14] = {S.red, S.sponge, S.rho0, S.grx, S.gry, S.grz,
-                             S.c2rho0, S.gpx, S.gpy, S.gpz, S.rhoinv, S.cbx, S.cby, S.cbz};
-          const bool spg = sponge_at(k);
+          for (int l = 0; l < 8; ++l) cp_r(ob + (O_A + l) * NC, a + l * N + id);
+      } else {
+        const R *bg[14] = {S.red, S.sponge, S.rho0, S.grx, S.gry, S.grz,
+                               S.c2rho0, S.gpx, S.gpy, S.gpz, S.rhoinv, S.cbx, S.cby, S.cbz};
+        const bool spg = sponge_at(k);
 #pragma unroll
-          for (int n = 0; n < 14; ++n)
-            if ((!DERIVE_RI || n != B_RHOINV) && (n != B_SPONGE || spg))
-              cp_r(ob + (O_BG + n) * NCT, bg[n] + id);
-          if (MODE == F_LAST) cp_r(ob + O_P0 * NCT, S.p0 + id);
-        }
+        for (int n = 0; n < 14; ++n)
+          if ((!DERIVE_RI || n != B_RHOINV) && (n != B_SPONGE || spg))
+            cp_r(ob + (O_BG + n) * NC, bg[n] + id);
+        if (MODE == F_LAST) cp_r(ob + O_P0 * NC, S.p0 + id);
       }
     }
     cp_commit_t();
     // TMA copies of the layer, spread over warp 0 (lane l issues copies l
     // and l + 32): copy c < 24 is own slot c (stage rho, a[0..7], 14
-    // background arrays, p0) as one 32 x TYT box; with TH, copy 24 + s is
-    // halo plane s (state fields 1..7, then B0 x, y, z)
+    // background arrays, p0); with TH, copy 24 + s is halo plane s (state
+    // fields 1..7, then B0 x, y, z)
     if (TMA && tid < 32) {
       if (tid == 0) mbar_tx_t(&bar[b], own_bytes(k));
       __syncwarp();
@@ -573,7 +539,7 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
       for (int c = tid; c < (TH ? NO + NH : NO); c += 32) {
         if (skip_own(c, k)) continue;
         int map = mt, xx = x0, yy = y0, z = k;
-        R *dst = ob + c * NCT;
+        R *dst = ob + c * NC;
         if (c >= O_A && c < O_BG) {
           map = ma;
           z = (c - O_A) * nz + k;
@@ -605,9 +571,9 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
     H[8 * HSL] = -vx_ * bz0 + vz_ * bx0;
     H[9 * HSL] = -vy_ * bx0 + vx_ * by0;
   };
-  R w0[NR][11], w1[NR][11], w2[NR][11];  // physical values
-  auto head = [&](int kk, int colr, R &v0, R &v1, R &v2) {
-    const int id = kk * NXY + colr;
+  R w0[11], w1[11], w2[11];  // physical values
+  auto head = [&](int kk, R &v0, R &v1, R &v2) {
+    const int id = kk * NXY + col;
     if (role == 0) {
       v0 = __ldg(tin + 3 * N + id) * IS(3, kk);
       v1 = __ldg(tin + 4 * N + id) * IS(4, kk);
@@ -626,23 +592,19 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
   // needed; an L2 prefetch two layers earlier takes that latency off the
   // layer loop
   auto prefetch = [&](int kk) {
-    if (kk >= nz) return;
-#pragma unroll
-    for (int r = 0; r < NR; ++r) {
-      if (!act[r]) continue;
-      const int id = kk * NXY + col[r];
-      if (role == 0) {
-        pf_l2(tin + 3 * N + id);
-        pf_l2(tin + 4 * N + id);
-        pf_l2(tin + 5 * N + id);
-      } else {
-        pf_l2(tin + N + id);
-        pf_l2(tin + 2 * N + id);
-        pf_l2(tin + 6 * N + id);
-        pf_l2(S.box + id);
-        pf_l2(S.boy + id);
-        pf_l2(S.boz + id);
-      }
+    if (!act || kk >= nz) return;
+    const int id = kk * NXY + col;
+    if (role == 0) {
+      pf_l2(tin + 3 * N + id);
+      pf_l2(tin + 4 * N + id);
+      pf_l2(tin + 5 * N + id);
+    } else {
+      pf_l2(tin + N + id);
+      pf_l2(tin + 2 * N + id);
+      pf_l2(tin + 6 * N + id);
+      pf_l2(S.box + id);
+      pf_l2(S.boy + id);
+      pf_l2(S.boz + id);
     }
   };
   issue(k0, 0);
@@ -650,205 +612,173 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
   {
     const int b0 = min(k0 - 5, nz - 11);
 #pragma unroll
-    for (int r = 0; r < NR; ++r)
-#pragma unroll
-      for (int m = 0; m < 11; ++m) {
-        const int kk = b0 + m;
-        if (act[r] && kk >= 0) head(kk, col[r], w0[r][m], w1[r][m], w2[r][m]);
-        else w0[r][m] = w1[r][m] = w2[r][m] = R(0);
-      }
+    for (int m = 0; m < 11; ++m) {
+      const int kk = b0 + m;
+      if (act && kk >= 0) head(kk, w0[m], w1[m], w2[m]);
+      else w0[m] = w1[m] = w2[m] = R(0);
+    }
   }
   unsigned phase = 0;
   bool ok = true;
   const R dt = (R)S.deltat;
   const R sx = (R)S.stretchx, sy = (R)S.stretchy;
-  const R *gcol[NR];
-#pragma unroll
-  for (int r = 0; r < NR; ++r)
-    gcol[r] = S.gblk + (act[r] ? S.colx[i] + S.bxdim * S.coly[jr[r]] : 0) * nz;
+  const R *gcol = S.gblk + (act ? S.colx[i] + S.bxdim * S.coly[j] : 0) * nz;
   // PULSE = 1 time factor: the iteration is fixed during a stage
   const R Tp = S.frc.kind == SPARC_SRC_PULSE ? pulse_time_t(S, *S.iter) : R(0);
   // |v_new|^2 of the last stage (role 0 writes, role 1 reads after a barrier)
-  double *VSQ = (double *)(SCALED ? X + 2 * NCT : X + NCT);
+  double *VSQ = (double *)(SCALED ? X + 2 * NC : X + NC);
 
   for (int k = k0; k < k1; ++k) {
     const int b = (k - k0) & 1;
-    R h0[NR], h1[NR], h2[NR];
+    const int id = k * NXY + col;
+    R h0 = 0, h1 = 0, h2 = 0;
     const bool sh = k > k0 && k <= nz - 6;
-#pragma unroll
-    for (int r = 0; r < NR; ++r) {
-      h0[r] = h1[r] = h2[r] = R(0);
-      if (sh && act[r]) head(k + 5, col[r], h0[r], h1[r], h2[r]);
-    }
+    if (sh && act) head(k + 5, h0, h1, h2);
     prefetch(k + 7);
     // precision form, last stage: the compensation carries of layer k + 2
     // into L2 (they are read just before their use)
-    if (SCALED && MODE == F_LAST && k + 2 < k1) {
-#pragma unroll
-      for (int r = 0; r < NR; ++r) {
-        if (!act[r]) continue;
-        const int id2 = (k + 2) * NXY + col[r];
-        if (role == 0) {
-          pf_l2(S.carry + N + id2);
-          pf_l2(S.carry + 2 * N + id2);
-          pf_l2(S.carry + 3 * N + id2);
-        } else {
-          pf_l2(S.carry + id2);
-          pf_l2(S.carry + 4 * N + id2);
-          pf_l2(S.carry + 5 * N + id2);
-          pf_l2(S.carry + 6 * N + id2);
-          pf_l2(S.carry + 7 * N + id2);
-        }
+    if (SCALED && MODE == F_LAST && act && k + 2 < k1) {
+      const int id2 = (k + 2) * NXY + col;
+      if (role == 0) {
+        pf_l2(S.carry + N + id2);
+        pf_l2(S.carry + 2 * N + id2);
+        pf_l2(S.carry + 3 * N + id2);
+      } else {
+        pf_l2(S.carry + id2);
+        pf_l2(S.carry + 4 * N + id2);
+        pf_l2(S.carry + 5 * N + id2);
+        pf_l2(S.carry + 6 * N + id2);
+        pf_l2(S.carry + 7 * N + id2);
       }
     }
     // momentum role: own-point B0 (its halo slots will hold the fluxes),
     // gravity and forcing, prefetched into L1 here and loaded after the
     // exchange barrier (not live across the derivatives: fewer registers)
-    if (role == 0) {
-#pragma unroll
-      for (int r = 0; r < NR; ++r) {
-        if (!act[r]) continue;
-        const int id = k * NXY + col[r];
-        pf_l1(S.box + id);
-        pf_l1(S.boy + id);
-        pf_l1(S.boz + id);
-      }
+    R ox = 0, oy = 0, oz = 0, gk = 0, frc = 0;
+    auto own_loads = [&] {
+      ox = __ldg(S.box + id);
+      oy = __ldg(S.boy + id);
+      oz = __ldg(S.boz + id);
+      gk = __ldg(gcol + k);
+      if (S.frc.kind != SPARC_SRC_NONE) frc = forcing_t(S, Tp, i, j, k);
+    };
+    if (role == 0 && act) {
+      pf_l1(S.box + id);
+      pf_l1(S.boy + id);
+      pf_l1(S.boz + id);
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     bool mine = true;
     // TH: every thread waits for the layer's TMA copies (its flux positions
     // arrive that way); otherwise thread 0 alone, before the barrier
     if (TH) mine = mbar_wait_t(&bar[b], (phase >> b) & 1u, S.err);
-#pragma unroll
-    for (int p = 0; p < NP; ++p)
-      if (mine && hs[p] >= 0) flux(b, hs[p]);
+    if (mine && hs0 >= 0) flux(b, hs0);
+    if (mine && hs1 >= 0) flux(b, hs1);
     if (TMA && !TH && tid == 0) mine = mbar_wait_t(&bar[b], (phase >> b) & 1u, S.err);
     phase ^= 1u << b;
     if (!__syncthreads_and(mine)) { ok = false; break; }
     if (k + 1 < k1) issue(k + 1, b ^ 1);
-    if (sh) {
-#pragma unroll
-      for (int r = 0; r < NR; ++r) {
-        shift_t(w0[r], h0[r]);
-        shift_t(w1[r], h1[r]);
-        shift_t(w2[r], h2[r]);
-      }
-    }
+    if (sh) { shift_t(w0, h0); shift_t(w1, h1); shift_t(w2, h2); }
     const R szk = __ldg(S.stretch + k);
-    auto DX = [&](int slot, int ryl) {  // ryl: the row's tile row in the halo plane
-      const R *row = Hp(b, slot) + ryl * HXL + XOFF;
+    auto DX = [&](int slot) {
+      const R *row = Hp(b, slot) + ry * HXL + XOFF;
       if (INT) return sx * csum_t(row + tx, 1);
       if (cen_x) return sx * csum_t(row + cxo + tx, 1);
-      const R *rr = row + cxb[tx], *c = cxs + tx * 11;
+      const R *r = row + cxb[tx], *c = cxs + tx * 11;
       R sum = R(0);
 #pragma unroll
-      for (int m = 0; m < 11; ++m) sum += rr[m] * c[m];
+      for (int m = 0; m < 11; ++m) sum += r[m] * c[m];
       return sx * sum;
     };
-    auto DY = [&](int slot, int ly) {  // ly: row of the tile
+    auto DY = [&](int slot) {
       const R *colp = Hp(b, slot) + rx + XOFF;
-      if (INT) return sy * csum_t(colp + ly * HXL, HXL);
-      if (cen_y) return sy * csum_t(colp + (cyo + ly) * HXL, HXL);
-      const R *rr = colp + cyb[ly] * HXL, *c = cys + ly * 11;
+      if (INT) return sy * csum_t(colp + ty * HXL, HXL);
+      if (cen_y) return sy * csum_t(colp + (cyo + ty) * HXL, HXL);
+      const R *r = colp + cyb[ty] * HXL, *c = cys + ty * 11;
       R sum = R(0);
 #pragma unroll
-      for (int m = 0; m < 11; ++m) sum += rr[m * HXL] * c[m];
+      for (int m = 0; m < 11; ++m) sum += r[m * HXL] * c[m];
       return sy * sum;
     };
     const bool zpml = S.zb.on && (k < S.zb.np || k >= nz - S.zt.np);
-    const bool xpml_i = !INT && S.xb.on && (i < S.xb.np || i >= nx - S.xt.np);
-    auto pz = [&](int colr, int s0, int s1, int s2, R &da, R &db, R &dc) {
+    const bool xpml = !INT && S.xb.on && act && (i < S.xb.np || i >= nx - S.xt.np);
+    const bool ypml = !INT && S.yb.on && act && (j < S.yb.np || j >= ny - S.yt.np);
+    auto pz = [&](int s0, int s1, int s2, R &da, R &db, R &dc) {
       const bool bot = k < S.zb.np;
       const FaceT<R> &F = bot ? S.zb : S.zt;
       const int kl = bot ? k : k - (nz - S.zt.np);
-      cpml3_t<R, MODE>(F, (long long)kl * NXY + colr, kl, s0, s1, s2, beta, dt, da, db, dc);
+      cpml3_t<R, MODE>(F, (long long)kl * NXY + col, kl, s0, s1, s2, beta, dt, da, db, dc);
     };
-    auto px = [&](int j, int s0, int s1, int s2, R &da, R &db, R &dc) {
+    auto px = [&](int s0, int s1, int s2, R &da, R &db, R &dc) {
       const bool bot = i < S.xb.np;
       const FaceT<R> &F = bot ? S.xb : S.xt;
       const int il = bot ? i : i - (nx - S.xt.np);
-      cpml3_t<R, MODE>(F, il + (long long)F.np * (j + (long long)ny * k), il, s0, s1, s2,
-                       beta, dt, da, db, dc);
+      cpml3_t<R, MODE>(F, il + (long long)F.np * (j + (long long)ny * k), il, s0, s1, s2, beta,
+                     dt, da, db, dc);
     };
-    auto py = [&](int j, int s0, int s1, int s2, R &da, R &db, R &dc) {
+    auto py = [&](int s0, int s1, int s2, R &da, R &db, R &dc) {
       const bool bot = j < S.yb.np;
       const FaceT<R> &F = bot ? S.yb : S.yt;
       const int jl = bot ? j : j - (ny - S.yt.np);
       cpml3_t<R, MODE>(F, i + (long long)nx * (jl + (long long)F.np * k), jl, s0, s1, s2, beta,
-                       dt, da, db, dc);
+                     dt, da, db, dc);
     };
-    auto Hv = [&](int slot, int ownr) { return Hp(b, slot)[ownr]; };
+    auto Hv = [&](int slot) { return Hp(b, slot)[own]; };
     const R iv = IS(1, k);  // velocity (and flux) scale of this layer
-    R d0[NR], d1[NR], d2[NR], d3[NR], d4[NR], d5[NR], d6[NR], d7[NR], d8[NR];
-#pragma unroll
-    for (int r = 0; r < NR; ++r) {
-      d0[r] = d1[r] = d2[r] = d3[r] = d4[r] = d5[r] = d6[r] = d7[r] = d8[r] = R(0);
-      if (!act[r]) continue;
-      const bool xpml = xpml_i;
-      const bool ypml = !INT && S.yb.on && (jr[r] < S.yb.np || jr[r] >= ny - S.yt.np);
+    R d0 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0, d6 = 0, d7 = 0, d8 = 0;
+    if (act) {
       const R ip = IS(4, k), ib = IS(5, k);
-      const int yr = ryr[r], lr = ty + r * TW, colr = col[r], jrr = jr[r];
       if (role == 0) {
-        d0[r] = ip * DX(3, yr); d5[r] = ib * DX(6, yr); d7[r] = ib * DX(5, yr);
-        d1[r] = ip * DY(3, lr); d4[r] = ib * DY(6, lr); d8[r] = ib * DY(4, lr);
-        d3[r] = dz_t(w0[r], k, nz, szk); d2[r] = dz_t(w1[r], k, nz, szk);
-        d6[r] = dz_t(w2[r], k, nz, szk);
-        if (zpml) pz(colr, 1, 0, 2, d2[r], d3[r], d6[r]);
-        if (xpml) px(jrr, 1, 3, 2, d0[r], d5[r], d7[r]);
-        if (ypml) py(jrr, 1, 3, 2, d1[r], d4[r], d8[r]);
-        X[cid[r]] = d3[r];
+        d0 = ip * DX(3); d5 = ib * DX(6); d7 = ib * DX(5);
+        d1 = ip * DY(3); d4 = ib * DY(6); d8 = ib * DY(4);
+        d3 = dz_t(w0, k, nz, szk); d2 = dz_t(w1, k, nz, szk); d6 = dz_t(w2, k, nz, szk);
+        if (zpml) pz(1, 0, 2, d2, d3, d6);
+        if (xpml) px(1, 3, 2, d0, d5, d7);
+        if (ypml) py(1, 3, 2, d1, d4, d8);
+        X[cid] = d3;
         // curl b: y and z components now, x after the exchange (fewer live
         // registers across the barrier; the same arithmetic)
-        d5[r] = -d5[r] + d6[r];
-        d7[r] = d7[r] - d8[r];
+        d5 = -d5 + d6;
+        d7 = d7 - d8;
       } else {
-        d0[r] = iv * DX(0, yr); d2[r] = iv * DX(9, yr); d3[r] = iv * DX(8, yr);
-        d1[r] = iv * DY(1, lr); d4[r] = iv * DY(9, lr); d5[r] = iv * DY(7, lr);
-        d6[r] = dz_t(w0[r], k, nz, szk); d7[r] = dz_t(w1[r], k, nz, szk);
-        d8[r] = dz_t(w2[r], k, nz, szk);
-        if (zpml) pz(colr, 4, 5, 3, d7[r], d6[r], d8[r]);
-        if (xpml) px(jrr, 0, 4, 5, d0[r], d2[r], d3[r]);
-        if (ypml) py(jrr, 0, 4, 5, d1[r], d4[r], d5[r]);
-        X[NCT + cid[r]] = d8[r];
+        d0 = iv * DX(0); d2 = iv * DX(9); d3 = iv * DX(8);
+        d1 = iv * DY(1); d4 = iv * DY(9); d5 = iv * DY(7);
+        d6 = dz_t(w0, k, nz, szk); d7 = dz_t(w1, k, nz, szk); d8 = dz_t(w2, k, nz, szk);
+        if (zpml) pz(4, 5, 3, d7, d6, d8);
+        if (xpml) px(0, 4, 5, d0, d2, d3);
+        if (ypml) py(0, 4, 5, d1, d4, d5);
+        X[NC + cid] = d8;
         // curl(v x B0) and d(vx)/dx + d(vy)/dy now (fewer live registers
         // across the barrier; the same arithmetic)
-        d4[r] = d4[r] - d7[r];
-        d6[r] = d6[r] - d2[r];
-        d3[r] = d3[r] - d5[r];
-        d0[r] = d0[r] + d1[r];
+        d4 = d4 - d7;
+        d6 = d6 - d2;
+        d3 = d3 - d5;
+        d0 = d0 + d1;
       }
     }
     // the exchange involves only the role-0 and role-1 warps of rows ty
     bar_pair_t(1 + ty);
-    double an_rho[NR];
-#pragma unroll
-    for (int r = 0; r < NR; ++r) {
-      an_rho[r] = 0.0;
-      if (!act[r]) continue;
-      const int id = k * NXY + col[r];
-      const int cr = cid[r], ownr = own[r];
+    double an_rho = 0.0;
+    if (act) {
       const bool zero = k == 0 || k == nz - 1 ||
-                        (!INT && !per && (i == 0 || i == nx - 1 || jr[r] == 0 || jr[r] == ny - 1));
+                        (!INT && !per && (i == 0 || i == nx - 1 || j == 0 || j == ny - 1));
       const R fac = MODE == F_LAST ? dt : bnext;
-      const R rho = O(b, O_RHO, cr) * IS(0, k), vx = Hv(0, ownr) * iv, vy = Hv(1, ownr) * iv,
-              vz = Hv(2, ownr) * iv;
-      const R red = O(b, O_BG + B_RED, cr);
-      const R sg = sponge_at(k) ? O(b, O_BG + B_SPONGE, cr) : R(0);
+      const R rho = O(b, O_RHO) * IS(0, k), vx = Hv(0) * iv, vy = Hv(1) * iv,
+                  vz = Hv(2) * iv;
+      const R red = O(b, O_BG + B_RED);
+      const R sg = sponge_at(k) ? O(b, O_BG + B_SPONGE) : R(0);
       if (role == 0) {
-        const R ox = __ldg(S.box + id), oy = __ldg(S.boy + id), oz = __ldg(S.boz + id);
-        const R gk = __ldg(gcol[r] + k);
-        const R frc = S.frc.kind != SPARC_SRC_NONE ? forcing_t(S, Tp, i, jr[r], k) : R(0);
-        const R dzby = X[NCT + cid[r]];
-        const R cbx = d4[r] - dzby, cby = d5[r], cbz = d7[r];
-        const R c1 = cby * oz - cbz * oy, c2 = ox * cbz - cbx * oz, c3 = cbx * oy - cby * ox;
-        const R ri = DERIVE_RI ? R(1) / O(b, O_BG + B_RHO0, cr) : O(b, O_BG + B_RHOINV, cr);
-        R vxr = -ri * (d0[r] - (c1 * red)) - sg * vx;
-        R vyr = -ri * (d1[r] - (c2 * red)) - sg * vy;
-        R vzr = -ri * (d2[r] - (c3 * red)) - sg * vz;
+        own_loads();
         const R ib = IS(5, k);
-        const R bx = Hv(4, ownr) * ib, by = Hv(5, ownr) * ib, bz = Hv(6, ownr) * ib;
-        const R qx = O(b, O_BG + B_CBX, cr), qy = O(b, O_BG + B_CBY, cr),
-                qz = O(b, O_BG + B_CBZ, cr);
+        const R dzby = X[NC + cid];
+        const R cbx = d4 - dzby, cby = d5, cbz = d7;
+        const R c1 = cby * oz - cbz * oy, c2 = ox * cbz - cbx * oz, c3 = cbx * oy - cby * ox;
+        const R ri = DERIVE_RI ? R(1) / O(b, O_BG + B_RHO0) : O(b, O_BG + B_RHOINV);
+        R vxr = -ri * (d0 - (c1 * red)) - sg * vx;
+        R vyr = -ri * (d1 - (c2 * red)) - sg * vy;
+        R vzr = -ri * (d2 - (c3 * red)) - sg * vz;
+        const R bx = Hv(4) * ib, by = Hv(5) * ib, bz = Hv(6) * ib;
+        const R qx = O(b, O_BG + B_CBX), qy = O(b, O_BG + B_CBY), qz = O(b, O_BG + B_CBZ);
         const R e1 = qy * bz - qz * by, e2 = bx * qz - qx * bz, e3 = qx * by - qy * bx;
         vxr = vxr + ri * e1 * red;
         vyr = vyr + ri * e2 * red;
@@ -864,7 +794,7 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
         double vsq = 0.0;
 #pragma unroll
         for (int l = 1; l < 4; ++l) {
-          const R av = MODE == F_FIRST ? Hv(l - 1, ownr) : O(b, O_A + l, cr);
+          const R av = MODE == F_FIRST ? Hv(l - 1) : O(b, O_A + l);
           R an;
           if (MODE == F_LAST) {
             if constexpr (SCALED) {
@@ -882,22 +812,22 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
           }
           so[l * N + id] = an;
         }
-        if (MODE == F_LAST) VSQ[cid[r]] = vsq;
+        if (MODE == F_LAST) VSQ[cid] = vsq;
       } else {
-        const R p = Hv(3, ownr) * IS(4, k);
-        const R dvzdz = X[cid[r]];
-        const R div = d0[r] + dvzdz;
-        const R r0 = O(b, O_BG + B_RHO0, cr);
-        const R Rr = -O(b, O_BG + B_GRX, cr) * vx - O(b, O_BG + B_GRY, cr) * vy -
-                     O(b, O_BG + B_GRZ, cr) * vz - r0 * div - sg * rho;
-        const R Rp = -O(b, O_BG + B_C2R, cr) * div - vx * O(b, O_BG + B_GPX, cr) -
-                     vy * O(b, O_BG + B_GPY, cr) - vz * O(b, O_BG + B_GPZ, cr) - sg * p;
-        const R Rs[5] = {Rr, Rp, red * d4[r], red * d6[r], red * d3[r]};
+        const R p = Hv(3) * IS(4, k);
+        const R dvzdz = X[cid];
+        const R div = d0 + dvzdz;
+        const R r0 = O(b, O_BG + B_RHO0);
+        const R Rr = -O(b, O_BG + B_GRX) * vx - O(b, O_BG + B_GRY) * vy -
+                         O(b, O_BG + B_GRZ) * vz - r0 * div - sg * rho;
+        const R Rp = -O(b, O_BG + B_C2R) * div - vx * O(b, O_BG + B_GPX) -
+                         vy * O(b, O_BG + B_GPY) - vz * O(b, O_BG + B_GPZ) - sg * p;
+        const R Rb[3] = {red * d4, red * d6, red * d3};
+        const R Rs[5] = {Rr, Rp, Rb[0], Rb[1], Rb[2]};
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
           const int l = q == 0 ? 0 : (q == 1 ? 4 : q + 3);
-          const R av = MODE == F_FIRST ? (l == 0 ? O(b, O_RHO, cr) : Hv(l - 1, ownr))
-                                       : O(b, O_A + l, cr);
+          const R av = MODE == F_FIRST ? (l == 0 ? O(b, O_RHO) : Hv(l - 1)) : O(b, O_A + l);
           const R s = SS(l, k);
           R an;
           if (MODE == F_LAST) {
@@ -905,10 +835,10 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
               R c = S.carry[l * N + id];
               an = zero ? av : kahan(av, fac * (s * Rs[q]), c);
               S.carry[l * N + id] = c;
-              if (q == 0) an_rho[r] = ((double)an - (double)c) * (double)IS(0, k);
+              if (q == 0) an_rho = ((double)an - (double)c) * (double)IS(0, k);
             } else {
               an = zero ? av : av + fac * Rs[q];
-              if (q == 0) an_rho[r] = an;
+              if (q == 0) an_rho = an;
             }
           } else {
             an = zero ? av : av + fac * (s * Rs[q]);
@@ -917,19 +847,15 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
         }
         if (MODE == F_LAST) {
           mr = fmin(mr, (double)rho + (double)r0);
-          mp = fmin(mp, (double)p + (double)O(b, O_P0, cr));
+          mp = fmin(mp, (double)p + (double)O(b, O_P0));
         }
       }
     }
     if (MODE == F_LAST) {
       bar_pair_t(1 + ty);
-      if (role == 1) {
-#pragma unroll
-        for (int r = 0; r < NR; ++r) {
-          if (!act[r]) continue;
-          const double m = ((double)O(b, O_BG + B_RHO0, cid[r]) + an_rho[r]) * VSQ[cid[r]] / 2.0;
-          ke += m * m;
-        }
+      if (act && role == 1) {
+        const double m = ((double)O(b, O_BG + B_RHO0) + an_rho) * VSQ[cid] / 2.0;
+        ke += m * m;
       }
     }
   }

@@ -637,16 +637,20 @@ int launch_psr_forcing(Handle *h, const SimDev &S, cudaStream_t s);
 
 // ------------------------------------------------------ FILTER_VARS
 // FILTER_VARS of a filter event (filter_body.cuh): the fused y-then-x pass
-// over 32 x 32 layer tiles, and the z pass over slabs of 32 x 4 columns.
-__global__ void __launch_bounds__(fb::TX *fb::TY) k_filt_xy64(FiltArgs<double> F) {
+template <int G>
+__global__ void __launch_bounds__(fb::NT, 5) k_filt_xy64(FiltArgs<double> F) {
   const int l = blockIdx.z / F.nz, k = blockIdx.z - l * F.nz;
-  filt_xy_tile(F, l, k, blockIdx.x * fb::TX, blockIdx.y * fb::TR);
+  filt_xy_tile<double, G, false>(F, l, k, blockIdx.x * fb::TX, blockIdx.y * fb::TR);
 }
+// the z pass: blockIdx.x is the z chunk (the chunks of a slab run
+// together), blockIdx.y the slab of the layer, blockIdx.z the field
+template <int G>
 __global__ void __launch_bounds__(2 * fb::ZX * fb::ZY) k_filt_z64(FiltArgs<double> F) {
   extern __shared__ __align__(16) double zsl64[];
-  const int nzc = (F.nz + fb::ZC - 1) / fb::ZC;
-  const int l = blockIdx.z / nzc, kc = blockIdx.z - l * nzc;
-  filt_z_slab(F, l, blockIdx.x * fb::ZX, blockIdx.y * fb::ZY, kc * fb::ZC, zsl64);
+  const int nxb = (F.nx + fb::ZX - 1) / fb::ZX;
+  const int yb = blockIdx.y / nxb, xb = blockIdx.y - yb * nxb;
+  filt_z_slab<double, G, false, false>(F, blockIdx.z, xb * fb::ZX, yb * fb::ZY, blockIdx.x * fb::ZC,
+                                zsl64);
 }
 
 // xy: the y and x passes fused; z: the z pass (in -> out, never in place)
@@ -654,20 +658,27 @@ int launch_filter_event(Handle *h, bool xy, const double *in, double *out, cudaS
   FiltArgs<double> F{};
   F.nx = h->nx; F.ny = h->ny; F.nz = h->nz; F.V = h->V; F.N = h->N;
   F.periodic = h->periodic ? 1 : 0;
-  F.g = xy ? h->gxy : h->gz;
-  F.mode2 = F.g == 3;
   F.s = xy ? h->P.s_xy : h->P.s_z;
   F.in = in;
   F.out = out;
+  const int g = xy ? h->gxy : h->gz;
   if (xy) {
-    k_filt_xy64<<<dim3((h->nx + fb::TX - 1) / fb::TX, (h->ny + fb::TR - 1) / fb::TR,
-                       h->V * h->nz), dim3(fb::TX, fb::TY), 0, s>>>(F);
+    const dim3 grid((h->nx + fb::TX - 1) / fb::TX, (h->ny + fb::TR - 1) / fb::TR, h->V * h->nz);
+    if (g == 5) k_filt_xy64<5><<<grid, dim3(fb::TX, fb::TY), 0, s>>>(F);
+    else k_filt_xy64<3><<<grid, dim3(fb::TX, fb::TY), 0, s>>>(F);
   } else {
     const size_t zs = filt_z_smem<double>();
-    cudaFuncSetAttribute(k_filt_z64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs);
-    k_filt_z64<<<dim3((h->nx + fb::ZX - 1) / fb::ZX, (h->ny + fb::ZY - 1) / fb::ZY,
-                      h->V * ((h->nz + fb::ZC - 1) / fb::ZC)),
-                 dim3(fb::ZX, fb::ZY, 2), zs, s>>>(F);
+    const long long slabs = (long long)((h->nx + fb::ZX - 1) / fb::ZX) *
+                            ((h->ny + fb::ZY - 1) / fb::ZY);
+    if (slabs > 65535) return SPARC_ERR_INVALID;
+    const dim3 grid((h->nz + fb::ZC - 1) / fb::ZC, (unsigned)slabs, h->V);
+    if (g == 5) {
+      cudaFuncSetAttribute(k_filt_z64<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs);
+      k_filt_z64<5><<<grid, dim3(fb::ZX, fb::ZY, 2), zs, s>>>(F);
+    } else {
+      cudaFuncSetAttribute(k_filt_z64<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs);
+      k_filt_z64<3><<<grid, dim3(fb::ZX, fb::ZY, 2), zs, s>>>(F);
+    }
   }
   ++h->launches;
   return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;

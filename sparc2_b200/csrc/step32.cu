@@ -421,9 +421,8 @@ __global__ void __launch_bounds__(TX *TY)
 
 namespace t32 {
 using namespace mg;
-constexpr int NR = 1;          // rows of columns per thread
-constexpr int TYT = TY * NR;   // tile rows
-using MB = MhdBuf<float, false, NR>;
+constexpr int TYT = TY;  // tile rows
+using MB = MhdBuf<float, false>;
 }  // namespace t32
 
 // One RK stage of the MHD equations.  A stage is two launches over one
@@ -443,15 +442,15 @@ __global__ void __launch_bounds__(t32::NT, 1)
   const int tx_ = INT ? blockIdx.x + ix0 : blockIdx.x;
   const int ty_ = INT ? blockIdx.y + iy0 : blockIdx.y;
   const int x0 = tx_ * t32::TX, y0 = ty_ * t32::TYT;
-  if (!INT && mhd_interior<float, t32::TYT>(S, x0, y0)) return;
+  if (!INT && mhd_interior(S, x0, y0)) return;
   if (sm_addr_t(smem) & 127u) {
     if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) atomicExch(S.err, 2);
     return;
   }
   double ke = 0.0, mr = 1e300, mp = 1e300;
   const int k0 = blockIdx.z * zchunk;
-  if (!mhd_body<float, MODE, TMA, INT, t32::NR>(S, &T, smem, a, tin, so, beta, bnext, x0, y0,
-                                                k0, min(S.nz, k0 + zchunk), mt, ma, ke, mr, mp))
+  if (!mhd_body<float, MODE, TMA, INT>(S, &T, smem, a, tin, so, beta, bnext, x0, y0, k0,
+                                       min(S.nz, k0 + zchunk), mt, ma, ke, mr, mp))
     return;
   if (MODE == F_LAST)
     diag_reduce_t(S, ke, mr, mp, tx_ + (long long)gx * (ty_ + (long long)gy * blockIdx.z),
@@ -521,15 +520,32 @@ __device__ __forceinline__ float filter_point32(const Filt32 &F, const float *__
 // the fused y-then-x pass over stored values (one depth scale per layer)
 // and the z pass over physical values; `carry` (the first pass of an event)
 // is subtracted on load, so the filter acts on the compensated value.
+template <int G, bool CARRY>
 __global__ void __launch_bounds__(fb::TX *fb::TY) k_filt_xy32(FiltArgs<float> F) {
   const int l = blockIdx.z / F.nz, k = blockIdx.z - l * F.nz;
-  filt_xy_tile(F, l, k, blockIdx.x * fb::TX, blockIdx.y * fb::TR);
+  filt_xy_tile<float, G, CARRY>(F, l, k, blockIdx.x * fb::TX, blockIdx.y * fb::TR);
 }
+// the z pass: blockIdx.x is the z chunk, blockIdx.y the slab, blockIdx.z
+// the field
+template <int G, bool CARRY>
 __global__ void __launch_bounds__(2 * fb::ZX * fb::ZY) k_filt_z32(FiltArgs<float> F) {
   extern __shared__ __align__(16) float zsl32[];
-  const int nzc = (F.nz + fb::ZC - 1) / fb::ZC;
-  const int l = blockIdx.z / nzc, kc = blockIdx.z - l * nzc;
-  filt_z_slab(F, l, blockIdx.x * fb::ZX, blockIdx.y * fb::ZY, kc * fb::ZC, zsl32);
+  const int nxb = (F.nx + fb::ZX - 1) / fb::ZX;
+  const int yb = blockIdx.y / nxb, xb = blockIdx.y - yb * nxb;
+  filt_z_slab<float, G, CARRY, true>(F, blockIdx.z, xb * fb::ZX, yb * fb::ZY, blockIdx.x * fb::ZC,
+                               zsl32);
+}
+
+template <int G, bool CARRY>
+static void filt_launch32(bool xy, const FiltArgs<float> &F, const dim3 &grid, size_t zs,
+                          cudaStream_t s) {
+  if (xy) {
+    k_filt_xy32<G, CARRY><<<grid, dim3(fb::TX, fb::TY), 0, s>>>(F);
+  } else {
+    cudaFuncSetAttribute(k_filt_z32<G, CARRY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)zs);
+    k_filt_z32<G, CARRY><<<grid, dim3(fb::ZX, fb::ZY, 2), zs, s>>>(F);
+  }
 }
 
 int launch_filter_event32(Handle *h, bool xy, const float *in, const float *carry, float *out,
@@ -537,23 +553,30 @@ int launch_filter_event32(Handle *h, bool xy, const float *in, const float *carr
   FiltArgs<float> F{};
   F.nx = h->nx; F.ny = h->ny; F.nz = h->nz; F.V = h->V; F.N = h->N;
   F.periodic = h->periodic ? 1 : 0;
-  F.g = xy ? h->gxy : h->gz;
-  F.mode2 = F.g == 3;
   F.s = (float)(xy ? h->P.s_xy : h->P.s_z);
   F.in = in;
   F.out = out;
   F.carry = carry;
+  const int g = xy ? h->gxy : h->gz;
+  dim3 grid;
+  size_t zs = 0;
   if (xy) {
-    k_filt_xy32<<<dim3((h->nx + fb::TX - 1) / fb::TX, (h->ny + fb::TR - 1) / fb::TR,
-                       h->V * h->nz), dim3(fb::TX, fb::TY), 0, s>>>(F);
+    grid = dim3((h->nx + fb::TX - 1) / fb::TX, (h->ny + fb::TR - 1) / fb::TR, h->V * h->nz);
   } else {
     F.sc = h->f_sc;
     F.isc = h->f_isc;
-    const size_t zs = filt_z_smem<float>();
-    cudaFuncSetAttribute(k_filt_z32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs);
-    k_filt_z32<<<dim3((h->nx + fb::ZX - 1) / fb::ZX, (h->ny + fb::ZY - 1) / fb::ZY,
-                      h->V * ((h->nz + fb::ZC - 1) / fb::ZC)),
-                 dim3(fb::ZX, fb::ZY, 2), zs, s>>>(F);
+    zs = filt_z_smem<float>();
+    const long long slabs = (long long)((h->nx + fb::ZX - 1) / fb::ZX) *
+                            ((h->ny + fb::ZY - 1) / fb::ZY);
+    if (slabs > 65535) return SPARC_ERR_INVALID;
+    grid = dim3((h->nz + fb::ZC - 1) / fb::ZC, (unsigned)slabs, h->V);
+  }
+  if (g == 5) {
+    if (carry) filt_launch32<5, true>(xy, F, grid, zs, s);
+    else filt_launch32<5, false>(xy, F, grid, zs, s);
+  } else {
+    if (carry) filt_launch32<3, true>(xy, F, grid, zs, s);
+    else filt_launch32<3, false>(xy, F, grid, zs, s);
   }
   ++h->launches;
   return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
@@ -931,11 +954,11 @@ __global__ void k_batch_begin(Slot32 *slots, int n) {
 // PART 1: the rest (MHD tiles at edges/CPML, quiet tiles); PART 2: the whole
 // list in one launch (interior items first, then the rest, so no launch
 // boundary separates the two parts).
-template <int MODE, int PART, int NR>
+template <int MODE, int PART>
 __global__ void __launch_bounds__(BT, 1)
     k_batch_stage(Slot32 *__restrict__ slots, const int4 *__restrict__ items,
                   const int *__restrict__ counts, unsigned *wctr, int stage) {
-  using MB = MhdBuf<float, false, NR>;
+  using MB = t32::MB;
   extern __shared__ __align__(1024) float smem_raw32[];
   __shared__ __align__(16) unsigned long long sS_raw[(sizeof(Sim32) + 7) / 8];
   __shared__ int s_w;
@@ -971,11 +994,11 @@ __global__ void __launch_bounds__(BT, 1)
     const int x0 = it.y, y0 = it.z, k0 = it.w & 0xffff, k1 = it.w >> 16;
     double ke = 0.0, mr = 1e300, mp = 1e300;
     if (PART == 0 || (PART == 2 && w < counts[3]))
-      mhd_body<float, MODE, false, true, NR>(sS, nullptr, smem, a, tin, so, beta, bnext, x0, y0,
-                                             k0, k1, 0, 0, ke, mr, mp);
+      mhd_body<float, MODE, false, true>(sS, nullptr, smem, a, tin, so, beta, bnext, x0, y0,
+                                         k0, k1, 0, 0, ke, mr, mp);
     else if (sS.magnetic)
-      mhd_body<float, MODE, false, false, NR>(sS, nullptr, smem, a, tin, so, beta, bnext, x0, y0,
-                                              k0, k1, 0, 0, ke, mr, mp);
+      mhd_body<float, MODE, false, false>(sS, nullptr, smem, a, tin, so, beta, bnext, x0, y0,
+                                          k0, k1, 0, 0, ke, mr, mp);
     else if (sS.bg1d)
       quiet_body<32, 16, MODE, true>(sS, a, tin, so, beta, bnext, x0, y0, k0, k1, threadIdx.x,
                                      threadIdx.y + 8 * threadIdx.z, qzt, ke, mr, mp);
@@ -1137,23 +1160,22 @@ __global__ void __launch_bounds__(BT)
 
 size_t batch_stage_smem() { return t32::MB::SMEM; }
 
-// One persistent launch per RK stage over the whole work-list, MHD items of
-// 32 x 8*NR columns.
-template <int NR>
+// One persistent launch per RK stage over the whole work-list (MHD items of
+// 32 x 8 columns).
 static void launch_batch_stages(const BatchLaunch &B, cudaStream_t s) {
-  const int sm = (int)MhdBuf<float, false, NR>::smem_bytes(B.zmax);
-  cudaFuncSetAttribute(k_batch_stage<F_FIRST, 2, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  cudaFuncSetAttribute(k_batch_stage<F_MID, 2, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  cudaFuncSetAttribute(k_batch_stage<F_LAST, 2, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  const int sm = (int)t32::MB::smem_bytes(B.zmax);
+  cudaFuncSetAttribute(k_batch_stage<F_FIRST, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_batch_stage<F_MID, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(k_batch_stage<F_LAST, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   const dim3 blk(t32::TX, t32::TY, 2);
   for (int st = 1; st <= 5; ++st) {
     unsigned *c = B.wctr + st;  // work counter of stage st
     if (st == 1)
-      k_batch_stage<F_FIRST, 2, NR><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c, st);
+      k_batch_stage<F_FIRST, 2><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c, st);
     else if (st < 5)
-      k_batch_stage<F_MID, 2, NR><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c, st);
+      k_batch_stage<F_MID, 2><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c, st);
     else
-      k_batch_stage<F_LAST, 2, NR><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c, st);
+      k_batch_stage<F_LAST, 2><<<B.grid, blk, (size_t)sm, s>>>(B.slots, B.items, B.counts, c, st);
   }
 }
 
@@ -1162,8 +1184,7 @@ int launch_batch_step(const BatchLaunch &B, cudaStream_t s, int *nkernels) {
   k_batch_begin<<<(B.nslots + 255) / 256, 256, 0, s>>>(B.slots, B.nslots);
   k_batch_psr<<<B.grid, BT, B.psr_smem, s>>>(B.slots, B.pitems, B.counts, B.wctr + 0);
   k_batch_random<<<B.grid, BT, 0, s>>>(B.slots, B.nslots);
-  if (B.mhd_rows == 8) launch_batch_stages<1>(B, s);
-  else launch_batch_stages<2>(B, s);
+  launch_batch_stages(B, s);
   k_batch_filter<1><<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 6);
   k_batch_filter<0><<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 7);
   k_batch_filter<2><<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 8);

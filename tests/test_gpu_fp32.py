@@ -85,6 +85,27 @@ def test_filter_vars_fp32(name):
         assert rel_l2(ga[l], oa[l]) <= 1e-6, l
 
 
+def test_filter_vars_7point_fp32():
+    """filter_mode 2 on both axes in the precision form (the z pass's scale
+    and the first pass's carry with the 7-point filter)."""
+    ps = []
+    for prec in (abi.SPARC_FP64, abi.SPARC_FP32):
+        p, bg, src = cases.mhd_hpml(nz=80)
+        p.filter_mode_xy = p.filter_mode_z = 2
+        p.precision = prec
+        ps.append(Simulation(p, bg, src))
+    s64, s32 = ps
+    a0, psi0 = cases.random_state(s64, seed=7)
+    for s in (s64, s32):
+        s.set_state(a0, psi0)
+        s.step(3)
+        s.filter_vars(30)
+    ga, _ = s32.get_state()
+    oa, _ = s64.get_state()
+    for l in range(s64.V):
+        assert rel_l2(ga[l], oa[l]) <= STEP_TOL32, l
+
+
 @pytest.mark.parametrize("name", ["quiet_periodic", "mhd_hpml"])
 def test_graph_run_equals_call_sequence_fp32(name):
     p, bg, src = CASES32[name]()

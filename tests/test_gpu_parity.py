@@ -106,6 +106,27 @@ def test_filter_vars(name):
         assert rel_l2(ga[l], oa[l]) <= 1e-14, l
 
 
+@pytest.mark.parametrize("name,kw", [("quiet_periodic", {}), ("mhd_hpml", {"nz": 80}),
+                                     ("quiet_hpml", {"nx": 70, "ny": 66})])
+def test_filter_vars_7point(name, kw):
+    """filter_mode 2 on both axes (derivatives.f90: the 7-point filter,
+    combined as a - s*filt, zero at the x/y edge points): nz = 80 gives the
+    z pass slabs away from both ends and slabs at them; 70 x 66 gives xy
+    tiles with and without the edge pre-average."""
+    p, bg, src = cases.CASES[name](**kw)
+    p.filter_mode_xy = p.filter_mode_z = 2
+    sim, orc = Simulation(p, bg, src), oracle.Oracle(p, bg, src)
+    a0, psi0 = cases.random_state(sim, seed=8)
+    for s in (sim, orc):
+        s.set_state(a0, psi0)
+    sim.filter_vars(30)
+    orc.filter_vars(30)
+    ga, _ = sim.get_state()
+    oa, _ = orc.get_state()
+    for l in range(sim.V):
+        assert rel_l2(ga[l], oa[l]) <= 1e-14, l
+
+
 @pytest.mark.parametrize("name", ["quiet_periodic", "mhd_hpml"])
 def test_graph_run_equals_call_sequence(name):
     """sparc_run (CUDA graphs) == sparc_step + sparc_filter_vars, bitwise."""

@@ -26,7 +26,8 @@ UNITS = {
     "noalloc.cu": [],
     "serve.cu": [],
 }
-HEADERS = ["internal.h", "mhd_body.cuh", "random_forcing.cuh", "filter_body.cuh"]
+HEADERS = ["internal.h", "mhd_body.cuh", "random_forcing.cuh", "filter_body.cuh",
+           "tmem_window.cuh"]
 # host C units (gcc): the .trol reader
 HOST_UNITS = {"sparc_trol.c": ["-O2", "-std=c99", "-Wall", "-fPIC"]}
 HOST = os.path.join(HERE, "host")

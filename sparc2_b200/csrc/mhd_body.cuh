@@ -16,6 +16,7 @@
 #pragma once
 
 #include "internal.h"
+#include "tmem_window.cuh"
 
 namespace sparc {
 
@@ -350,13 +351,19 @@ inline void mhd_interior_rect(int nx, int ny, const int np[4], int &ix0, int &ix
 // barrier of the two warps that share rows ty (role 0 warp ty, role 1 warp
 // 8 + ty) exchanges d(vz)/dz and d(by)/dz: nothing else crosses warps
 // until the next layer's barrier.
-template <class R, int MODE, bool TMA, bool INT>
+//
+// TW (FP64): the z windows live in tensor memory between layers
+// (tmem_window.cuh; tw is this warp's window address, the caller allocates
+// and frees): each layer loads them, shifts in the new head, stores them
+// back and forms the z derivatives, so they hold registers only then.
+template <class R, int MODE, bool TMA, bool INT, bool TW = false>
 __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *smem,
                                          const R *__restrict__ a,
                                          const R *__restrict__ tin,
                                          R *__restrict__ so, R beta, R bnext,
                                          int x0, int y0, int k0, int k1, int mt, int ma,
-                                         double &ke, double &mr, double &mp) {
+                                         double &ke, double &mr, double &mp, uint32_t tw = 0) {
+  static_assert(!TW || sizeof(R) == 8, "TMEM windows of FP64 values");
   using namespace mg;
   // halo planes by TMA in the plain form's interior kernel (measured: 4 %
   // faster in FP64; in FP32 the 48-wide boxes cost more than the cp.async
@@ -617,6 +624,13 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
       if (act && kk >= 0) head(kk, w0[m], w1[m], w2[m]);
       else w0[m] = w1[m] = w2[m] = R(0);
     }
+    if constexpr (TW) {
+      __syncwarp();
+      tm_wait_st();  // a previous work item's stores to these columns
+      tm_st_window(tm_window(tw, 0), w0);
+      tm_st_window(tm_window(tw, 1), w1);
+      tm_st_window(tm_window(tw, 2), w2);
+    }
   }
   unsigned phase = 0;
   bool ok = true;
@@ -678,8 +692,38 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
     phase ^= 1u << b;
     if (!__syncthreads_and(mine)) { ok = false; break; }
     if (k + 1 < k1) issue(k + 1, b ^ 1);
-    if (sh) { shift_t(w0, h0); shift_t(w1, h1); shift_t(w2, h2); }
+    if constexpr (!TW) {
+      if (sh) { shift_t(w0, h0); shift_t(w1, h1); shift_t(w2, h2); }
+    }
     const R szk = __ldg(S.stretch + k);
+    // TW: the z derivatives of the three windows, formed by the whole warp
+    // (the TMEM accesses are warp-collective)
+    R wz0 = R(0), wz1 = R(0), wz2 = R(0);
+    if constexpr (TW) {
+      __syncwarp();
+      tm_wait_st();  // the previous layer's store of these columns
+      auto zwin = [&](int f, R h) -> R {
+        R v[11];
+        tm_ld_window(tm_window(tw, f), v);
+        if (sh) {
+          shift_t(v, h);
+          tm_st_window(tm_window(tw, f), v);
+        }
+        return dz_t(v, k, nz, szk);
+      };
+      wz0 = zwin(0, h0);
+      wz1 = zwin(1, h1);
+      wz2 = zwin(2, h2);
+    }
+    auto DZ = [&](int f) -> R {
+      if constexpr (TW) {
+        return f == 0 ? wz0 : (f == 1 ? wz1 : wz2);
+      } else {
+        if (f == 0) return dz_t(w0, k, nz, szk);
+        if (f == 1) return dz_t(w1, k, nz, szk);
+        return dz_t(w2, k, nz, szk);
+      }
+    };
     auto DX = [&](int slot) {
       const R *row = Hp(b, slot) + ry * HXL + XOFF;
       if (INT) return sx * csum_t(row + tx, 1);
@@ -731,7 +775,7 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
       if (role == 0) {
         d0 = ip * DX(3); d5 = ib * DX(6); d7 = ib * DX(5);
         d1 = ip * DY(3); d4 = ib * DY(6); d8 = ib * DY(4);
-        d3 = dz_t(w0, k, nz, szk); d2 = dz_t(w1, k, nz, szk); d6 = dz_t(w2, k, nz, szk);
+        d3 = DZ(0); d2 = DZ(1); d6 = DZ(2);
         if (zpml) pz(1, 0, 2, d2, d3, d6);
         if (xpml) px(1, 3, 2, d0, d5, d7);
         if (ypml) py(1, 3, 2, d1, d4, d8);
@@ -743,7 +787,7 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
       } else {
         d0 = iv * DX(0); d2 = iv * DX(9); d3 = iv * DX(8);
         d1 = iv * DY(1); d4 = iv * DY(9); d5 = iv * DY(7);
-        d6 = dz_t(w0, k, nz, szk); d7 = dz_t(w1, k, nz, szk); d8 = dz_t(w2, k, nz, szk);
+        d6 = DZ(0); d7 = DZ(1); d8 = DZ(2);
         if (zpml) pz(4, 5, 3, d7, d6, d8);
         if (xpml) px(0, 4, 5, d0, d2, d3);
         if (ypml) py(0, 4, 5, d1, d4, d5);

@@ -488,9 +488,25 @@ __global__ void __launch_bounds__(mg::NT, 1)
   if (!INT && mhd_interior(S, x0, y0)) return;
   double ke = 0.0, mr = 1e300, mp = 1e300;
   const int k0 = blockIdx.z * zchunk;
-  if (!mhd_body<double, MODE, TMA, INT>(S, &T, smem, a, tin, so, beta, bnext, x0, y0, k0,
-                                         min(S.nz, k0 + zchunk), mt, ma, ke, mr, mp))
-    return;
+  // the z windows in tensor memory: all 512 columns for the CTA's 16 warps
+  __shared__ uint32_t s_tmem;
+  const int warp = (threadIdx.z * blockDim.y + threadIdx.y) * (blockDim.x / 32) + threadIdx.x / 32;
+  if (warp == 0) tm_alloc_all(&s_tmem);
+  tm_fence_before();
+  __syncthreads();
+  tm_fence_after();
+  const uint32_t tbase = s_tmem;
+  const bool ok = mhd_body<double, MODE, TMA, INT, true>(
+      S, &T, smem, a, tin, so, beta, bnext, x0, y0, k0, min(S.nz, k0 + zchunk), mt, ma, ke, mr,
+      mp, tm_warp_addr(tbase, warp));
+  // every exit frees the columns once all warps' accesses have completed
+  __syncwarp();
+  tm_wait_st();
+  tm_fence_before();
+  __syncthreads();
+  tm_fence_after();
+  if (warp == 0) tm_free_all(tbase);
+  if (!ok) return;
   if (MODE == F_LAST)
     diag_reduce_t(S, ke, mr, mp, tx_ + (long long)gx * (ty_ + (long long)gy * blockIdx.z),
                   (long long)gx * gy * gridDim.z);

@@ -235,9 +235,10 @@ int sparc_ke_norm_noalloc(sparc_handle *h, double *ke_norm);
 /* ---------------------------------------------------- failure injection
  * No counterpart in the reference.  For failure-detection tests: launches on
  * the handle's stream a kernel whose bounded wait on an mbarrier that nothing
- * completes gives up after `polls` polls (1 <= polls <= 2^26) and raises the
- * handle's device error flag, as a stage kernel's gave-up wait does.  The
- * GPU neither hangs nor faults.  The next sparc_diagnostics returns
+ * completes gives up after `polls` polls (1 <= polls <= 2^20) or 10 ms of
+ * the GPU's global timer, whichever comes first, and raises the handle's
+ * device error flag, as a stage kernel's gave-up wait does.  The GPU
+ * neither hangs nor faults.  The next sparc_diagnostics returns
  * SPARC_ERR_TIMEOUT; sparc_set_state (a restart from saved state) clears
  * the flag. */
 int sparc_inject_wait_timeout(sparc_handle *h, int64_t polls);

@@ -101,7 +101,12 @@ struct orc_handle {
   // ddx, derivatives.f90:10-116.  bc 1 on a non-periodic axis: one-sided rows
   // dpxy(1..5,:) at the low edge (:72) and -dpxy on the reversed field at the
   // high edge (:98); periodic: halo from the wrapped neighbour; bc 5 on a
-  // non-periodic axis: centred with zero ghosts.
+  // non-periodic axis: centred with zero ghosts.  A periodic axis wraps
+  // whatever bc is.  The reference would take the one-sided rows on its
+  // XBOT/XTOP ranks for bc 1 even in a periodic communicator
+  // (derivatives.f90:62-76, initialize.f90:66-67); its step passes bc 5
+  // whenever the axis is periodic, so that branch is never reached on the
+  // step's path, and the restatement leaves it out.
   void ddx(const double *in, double *out, int bc) const {
     const double *c = dp[5];
 #pragma omp parallel for collapse(2) schedule(static)

@@ -318,14 +318,19 @@ static void parallel_for(long long n, F f) {
 
 // Failure injection: one thread waits on an mbarrier that expects one
 // arrival which never comes; the bounded wait gives up after `polls` polls
-// and raises the error flag, as a stage kernel's gave-up wait does.
+// or 10 ms of the global timer, whichever comes first, and raises the error
+// flag, as a stage kernel's gave-up wait does.
 __global__ void k_wait_probe(int *err, long long polls) {
   __shared__ unsigned long long bar;
   if (threadIdx.x != 0) return;
   const unsigned a = (unsigned)__cvta_generic_to_shared(&bar);
   asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a) : "memory");
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  unsigned long long t0, t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
   for (long long n = 0; n < polls; ++n) {
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (t - t0 > 10000000ull) break;
     unsigned ok;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
@@ -831,8 +836,8 @@ int sparc_set_state(sparc_handle *h, const double *a, const double *psi) {
 int sparc_inject_wait_timeout(sparc_handle *h, int64_t polls) {
   if (!h) return SPARC_ERR_INVALID;
   NOT_IN_BATCH(h);
-  if (polls < 1 || polls > (1LL << 26))
-    return fail(h, SPARC_ERR_INVALID, "polls must be in [1, 2^26]");
+  if (polls < 1 || polls > (1LL << 20))
+    return fail(h, SPARC_ERR_INVALID, "polls must be in [1, 2^20]");
   cudaSetDevice(h->device);
   k_wait_probe<<<1, 32, 0, h->stream>>>(h->d_err, (long long)polls);
   ++h->launches;

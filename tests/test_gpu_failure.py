@@ -25,6 +25,7 @@ def test_gave_up_wait_is_reported_and_cleared_by_a_restart(precision):
         sim.diagnostics()
     assert e.value.code == abi.SPARC_ERR_TIMEOUT
     assert sim.lib.sparc_inject_wait_timeout(sim.h, 0) == abi.SPARC_ERR_INVALID
+    assert sim.lib.sparc_inject_wait_timeout(sim.h, (1 << 20) + 1) == abi.SPARC_ERR_INVALID
     sim.set_state(a, psi)          # restart from the saved state
     d, r = sim.diagnostics()
     assert r == abi.SPARC_OK

@@ -77,6 +77,8 @@ def parse():
                     "the end-to-end leg (the reference driver reads the state "
                     "back only at its output cadence, e.g. 1200 iterations)")
     ap.add_argument("--kernel-steps", type=int, default=10)
+    ap.add_argument("--zchunk", type=int, default=0,
+                    help="z extent of the stage work items (0: autotune)")
     ap.add_argument("--timed-only", action="store_true",
                     help="only the warm-up and the timed region (profiling)")
     ap.add_argument("--grid", type=int, nargs=3, default=None,
@@ -286,10 +288,17 @@ def run_gpu(args, world, rank, local):
     barrier = rep.barrier
     max_over_ranks = rep.max
 
-    # warm-up iterations (graph capture happens here)
+    # the z extent of the stage work items is autotuned on real iterations
+    # of the loop (untimed), then the warm-up iterations (graph capture
+    # happens here) run
     W_ = args.warmup
     K = args.steps
-    sim.run(0, W_)
+    if args.zchunk > 0:
+        sim.set_zchunk(args.zchunk)
+        start, zchunk = 0, sim.zchunk
+    else:
+        start, zchunk = sim.tune(0, steps_per_trial=2)
+    sim.run(start, W_)
     sim.synchronize()
     torch.cuda.synchronize(dev)
     clocks = Clocks(dev)
@@ -299,7 +308,7 @@ def run_gpu(args, world, rank, local):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    sim.run(W_, K)
+    sim.run(start + W_, K)
     e1.record(stream)
     e1.synchronize()
     torch.cuda.synchronize(dev)
@@ -324,7 +333,7 @@ def run_gpu(args, world, rank, local):
     k0 = torch.cuda.Event(enable_timing=True)
     k1 = torch.cuda.Event(enable_timing=True)
     k0.record(stream)
-    for nn in range(W_ + K, W_ + K + M):
+    for nn in range(start + W_ + K, start + W_ + K + M):
         sim.step(nn)
     k1.record(stream)
     k1.synchronize()
@@ -378,7 +387,7 @@ def run_gpu(args, world, rank, local):
                         pin_memory=True).numpy()
     pin_a[:] = a_host.ravel()
     pin_p[:psi_host.size] = psi_host
-    first = W_ + K + M
+    first = start + W_ + K + M
     barrier()
     torch.cuda.synchronize(dev)
     x0 = torch.cuda.Event(enable_timing=True)
@@ -439,6 +448,10 @@ def run_gpu(args, world, rank, local):
         "pulse table; no public dataset)",
         "config": {"workload": desc, "grid": [p.nx, p.ny, p.nz],
                    "precision": "fp32 precision form" if fp32 else "fp64 plain",
+                   "zchunk": zchunk,
+                   "zchunk_note": ("z extent of the stage work items, autotuned on "
+                                   "%d untimed iterations before the warm-up" % start)
+                   if args.zchunk <= 0 else "z extent of the stage work items, set",
                    "parallelism": "replicas" if world > 1 else "single GPU",
                    "l2": "working set %.1f GB > 126 MB L2 (no flush needed)"
                    % (3 * p_V(p) * wsize * pts / 1e9)},
@@ -481,12 +494,13 @@ def fp64_plain_rate(dev, steps=20, warmup=3):
     sim = Simulation(p, bg, src, device=dev)
     del bg
     stream = torch.cuda.ExternalStream(sim.stream, device=dev)
-    sim.run(0, warmup)
+    start, _ = sim.tune(0, steps_per_trial=2)
+    sim.run(start, warmup)
     sim.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    sim.run(warmup, steps)
+    sim.run(start + warmup, steps)
     e1.record(stream)
     e1.synchronize()
     ms = e0.elapsed_time(e1) / steps
@@ -556,19 +570,20 @@ def measure_fp32_cfg2(dev, steps=40, warmup=3):
     sim = Simulation(p, bg, src, device=dev)
     del bg
     stream = torch.cuda.ExternalStream(sim.stream, device=dev)
-    sim.run(0, warmup)
+    start, zchunk = sim.tune(0, steps_per_trial=2)
+    sim.run(start, warmup)
     sim.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    sim.run(warmup, steps)
+    sim.run(start + warmup, steps)
     e1.record(stream)
     e1.synchronize()
     ms = e0.elapsed_time(e1) / steps
     sim.close()
     pts = p.nx * p.ny * p.nz
     return {"value": pts / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "steps": steps,
-            "dtype": "f32", "workload": desc}
+            "dtype": "f32", "zchunk": zchunk, "workload": desc}
 
 
 def measure_ensemble(dev, members=64, steps=100, warmup=2):

@@ -169,6 +169,23 @@ int sparc_filter_vars(sparc_handle *h, int64_t nn);
  * Asynchronous; errors of the fail criterion surface in sparc_diagnostics. */
 int sparc_run(sparc_handle *h, int64_t first, int64_t count);
 
+/* z extent of the stage kernels' work items (a work item is a 32 x 8
+ * column tile over zchunk layers; each item pays 10 layers of z-window
+ * warm-up).  No counterpart in the reference.  11 <= zchunk (clamped to
+ * nz); set up from the grid size, changed by sparc_set_zchunk or
+ * sparc_tune.  Results do not depend on it. */
+int sparc_set_zchunk(sparc_handle *h, int zchunk);
+int sparc_get_zchunk(const sparc_handle *h, int *zchunk);
+
+/* Autotuner of the z extent: runs iterations first, first+1, ... of the
+ * driver loop exactly as sparc_run would (they are real iterations of the
+ * simulation), giving each candidate extent (16 .. 150 layers) one untimed
+ * iteration and then `steps_per_trial` iterations off the filter cadence
+ * timed with CUDA events; keeps the fastest.  *next receives the first
+ * iteration not yet run, *best the extent chosen.  Synchronous. */
+int sparc_tune(sparc_handle *h, int64_t first, int steps_per_trial, int64_t *next,
+               int *best);
+
 /* Waits for the handle's stream and returns the diagnostics of the last
  * iteration.  Returns SPARC_ERR_UNSTABLE when an iteration met the fail
  * criterion of driver.f90:175-183 (the diagnostics are still filled). */

@@ -141,7 +141,8 @@ LIB_PATH = os.path.join(PKG_DIR, "_lib", "libsparc_gpu.so")
 EXPORTS = [
     "sparc_create", "sparc_destroy", "sparc_set_background",
     "sparc_set_source", "sparc_sizes", "sparc_set_state", "sparc_get_state",
-    "sparc_step", "sparc_filter_vars", "sparc_run", "sparc_diagnostics",
+    "sparc_step", "sparc_filter_vars", "sparc_run", "sparc_set_zchunk",
+    "sparc_get_zchunk", "sparc_tune", "sparc_diagnostics",
     "sparc_synchronize", "sparc_stream", "sparc_launch_count",
     "sparc_derivative", "sparc_filter_field", "sparc_get_coeff",
     "sparc_get_scalars", "sparc_last_error",
@@ -178,6 +179,9 @@ def _declare(lib):
         "sparc_step": (C.c_int, [h, C.c_int64]),
         "sparc_filter_vars": (C.c_int, [h, C.c_int64]),
         "sparc_run": (C.c_int, [h, C.c_int64, C.c_int64]),
+        "sparc_set_zchunk": (C.c_int, [h, C.c_int]),
+        "sparc_get_zchunk": (C.c_int, [h, P(C.c_int)]),
+        "sparc_tune": (C.c_int, [h, C.c_int64, C.c_int, P(C.c_int64), P(C.c_int)]),
         "sparc_diagnostics": (C.c_int, [h, P(SparcDiag)]),
         "sparc_synchronize": (C.c_int, [h]),
         "sparc_stream": (C.c_int, [h, P(C.c_void_p)]),

@@ -488,7 +488,7 @@ int sparc_create(const sparc_params *p, int device, sparc_handle **out) {
   if (!r) {
     h->d_iter = (long long *)dev_alloc(h, 8);
     h->d_fail = (long long *)dev_alloc(h, 8);
-    h->d_partials = (double *)dev_alloc(h, (size_t)h->max_stage_blocks * 3 * 8);
+    h->d_partials = (double *)dev_alloc(h, (size_t)h->partials_blocks * 3 * 8);
     h->d_diag = (double *)dev_alloc(h, 4 * 8);
     h->d_counter = (unsigned int *)dev_alloc(h, 4);
     if (!h->d_iter || !h->d_fail || !h->d_partials || !h->d_diag || !h->d_counter)
@@ -905,6 +905,112 @@ int sparc_run(sparc_handle *h, int64_t first, int64_t count) {
     h->rf1 = g->out_rf1;
     h->rf2 = g->out_rf2;
   }
+  return SPARC_OK;
+}
+
+// z extent of the stage kernels' work items; the captured graphs hold the
+// old launch shapes and are dropped
+static int set_zchunk(Handle *h, int zc) {
+  zc = std::min(zc, h->nz);
+  const long long per = (long long)h->max_stage_blocks / ((h->nz + h->zchunk - 1) / h->zchunk);
+  const long long blocks = per * ((h->nz + zc - 1) / zc);
+  if (blocks > h->partials_blocks) return SPARC_ERR_INVALID;
+  if (zc != h->zchunk) drop_graphs(h);
+  h->zchunk = zc;
+  h->max_stage_blocks = (int)blocks;
+  return SPARC_OK;
+}
+
+int sparc_set_zchunk(sparc_handle *h, int zchunk) {
+  if (!h || zchunk < 11) return SPARC_ERR_INVALID;
+  NOT_IN_BATCH(h);
+  cudaSetDevice(h->device);
+  CK(h, cudaStreamSynchronize(h->stream));  // graphs in flight finish first
+  return set_zchunk(h, zchunk) ? fail(h, SPARC_ERR_INVALID, "z chunk out of range") : SPARC_OK;
+}
+
+int sparc_get_zchunk(const sparc_handle *h, int *zchunk) {
+  if (!h || !zchunk) return SPARC_ERR_INVALID;
+  *zchunk = h->zchunk;
+  return SPARC_OK;
+}
+
+// Autotuner of the z extent: iterations first, first+1, ... of the driver
+// loop run as in sparc_run; each candidate extent gets one untimed
+// iteration (new launch shapes), then `steps_per_trial` iterations off the
+// filter cadence are timed with CUDA events on the handle's stream (the
+// filter iterations between them run untimed, so every candidate is timed
+// on the same kind of iteration).  The fastest extent is kept.  Results do
+// not depend on the extent.
+int sparc_tune(sparc_handle *h, int64_t first, int steps_per_trial, int64_t *next,
+               int *best) {
+  if (!h || first < 0 || steps_per_trial < 1 || steps_per_trial > 1000)
+    return SPARC_ERR_INVALID;
+  NOT_IN_BATCH(h);
+  if (!h->bg_ready) return fail(h, SPARC_ERR_ORDER, "set the background first");
+  cudaSetDevice(h->device);
+  static const int cand[] = {16, 24, 32, 40, 48, 64, 80, 100, 150};
+  std::vector<int> cs;
+  for (int c : cand) {
+    const int z = std::min(c, h->nz);
+    if (std::find(cs.begin(), cs.end(), z) == cs.end()) cs.push_back(z);
+  }
+  int r = set_iter(h, first);
+  if (r) return r;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(h, cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return fail(h, SPARC_ERR_CUDA, "cudaEventCreate");
+  }
+  int64_t nn = first;
+  auto one = [&](int64_t it) -> int {
+    Handle::GraphEntry *g = graph_for(h, filter_kind(h, it));
+    if (!g) return SPARC_ERR_CUDA;
+    if (!cuda_ok(h, cudaGraphLaunch(g->exec, h->stream), "cudaGraphLaunch"))
+      return SPARC_ERR_CUDA;
+    h->launches += g->nkernels;
+    h->ra = g->out_ra;
+    h->rf1 = g->out_rf1;
+    h->rf2 = g->out_rf2;
+    return SPARC_OK;
+  };
+  float best_ms = 3.4e38f;
+  int bz = h->zchunk;
+  for (int c : cs) {
+    if (set_zchunk(h, c)) continue;  // more blocks than the partials hold
+    // the off-cadence graph is captured before anything is timed
+    if (!graph_for(h, 0)) { r = SPARC_ERR_CUDA; break; }
+    if ((r = one(nn++))) break;
+    float tot = 0.f;
+    for (int timed = 0; timed < steps_per_trial && !r; ++nn) {
+      if (filter_kind(h, nn) != 0) {
+        r = one(nn);
+        continue;
+      }
+      float ms = 0.f;
+      if (!cuda_ok(h, cudaEventRecord(e0, h->stream), "cudaEventRecord") || (r = one(nn)) ||
+          !cuda_ok(h, cudaEventRecord(e1, h->stream), "cudaEventRecord") ||
+          !cuda_ok(h, cudaEventSynchronize(e1), "cudaEventSynchronize") ||
+          !cuda_ok(h, cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime")) {
+        if (!r) r = SPARC_ERR_CUDA;
+        break;
+      }
+      tot += ms;
+      ++timed;
+    }
+    if (r) break;
+    if (tot < best_ms) {
+      best_ms = tot;
+      bz = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (r) return r;
+  if (set_zchunk(h, bz)) return fail(h, SPARC_ERR_INVALID, "z chunk out of range");
+  if (next) *next = nn;
+  if (best) *best = bz;
   return SPARC_OK;
 }
 

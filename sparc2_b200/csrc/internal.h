@@ -229,6 +229,7 @@ struct Handle {
   double *d_partials = nullptr, *d_diag = nullptr;
   unsigned int *d_counter = nullptr;
   int max_stage_blocks = 0;
+  int partials_blocks = 0;  // blocks the partials hold: any z chunk >= 11
 
   // stage launch geometry (quiet tiles tx x ty; MHD tiles 32 x 8)
   int tx = 32, ty = 8, zchunk = 32;

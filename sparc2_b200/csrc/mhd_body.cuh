@@ -473,12 +473,11 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
     pos(tid, hs0, ho0);
     if (role == 1) pos(tid + NC, hs1, ho1);
   }
-  // Own-point arrays not read: in the plain form rhoinv (the kernel forms
-  // 1/rho0, the same IEEE quotient initialize.f90:1012 stores; the
-  // precision form, closer to issue-bound, measured faster loading it) and,
-  // where the sponge vanishes outside the CPML slabs, the sponge of layers
-  // whose points lie in no slab (a CTA-uniform test per layer).
-  constexpr bool DERIVE_RI = sizeof(R) == 8;
+  // Own-point arrays not read: where the sponge vanishes outside the CPML
+  // slabs, the sponge of layers whose points lie in no slab (a CTA-uniform
+  // test per layer).  rhoinv is read, not formed as 1/rho0 in the kernel:
+  // the FP64 division measured 0.7 % slower than the load (FP64 kernels
+  // with TMEM windows), and more in the precision form.
   const bool slab_xy = !INT && ((S.xb.on && (x0 < S.xb.np || x0 + TX > nx - S.xt.np)) ||
                                 (S.yb.on && (y0 < S.yb.np || y0 + TY > ny - S.yt.np)));
   auto sponge_at = [&](int k) -> bool {
@@ -486,10 +485,10 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
   };
   auto skip_own = [&](int c, int k) -> bool {
     return (MODE == F_FIRST && c >= O_A && c < O_BG) || (MODE != F_LAST && c == O_P0) ||
-           (DERIVE_RI && c == O_BG + B_RHOINV) || (c == O_BG + B_SPONGE && !sponge_at(k));
+           (c == O_BG + B_SPONGE && !sponge_at(k));
   };
   auto own_bytes = [&](int k) -> unsigned {
-    return ((MODE == F_FIRST ? 15u : (MODE == F_MID ? 23u : 24u)) - (DERIVE_RI ? 1u : 0u) -
+    return ((MODE == F_FIRST ? 15u : (MODE == F_MID ? 23u : 24u)) -
             (sponge_at(k) ? 0u : 1u)) *
                NC * (unsigned)sizeof(R) +
            (TH ? (unsigned)(NH * HXL * HY * sizeof(R)) : 0u);
@@ -528,7 +527,7 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
         const bool spg = sponge_at(k);
 #pragma unroll
         for (int n = 0; n < 14; ++n)
-          if ((!DERIVE_RI || n != B_RHOINV) && (n != B_SPONGE || spg))
+          if (n != B_SPONGE || spg)
             cp_r(ob + (O_BG + n) * NC, bg[n] + id);
         if (MODE == F_LAST) cp_r(ob + O_P0 * NC, S.p0 + id);
       }
@@ -817,7 +816,7 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
         const R dzby = X[NC + cid];
         const R cbx = d4 - dzby, cby = d5, cbz = d7;
         const R c1 = cby * oz - cbz * oy, c2 = ox * cbz - cbx * oz, c3 = cbx * oy - cby * ox;
-        const R ri = DERIVE_RI ? R(1) / O(b, O_BG + B_RHO0) : O(b, O_BG + B_RHOINV);
+        const R ri = O(b, O_BG + B_RHOINV);
         R vxr = -ri * (d0 - (c1 * red)) - sg * vx;
         R vyr = -ri * (d1 - (c2 * red)) - sg * vy;
         R vzr = -ri * (d2 - (c3 * red)) - sg * vz;

@@ -404,6 +404,7 @@ int stage_geometry(Handle *h) {
   }
   h->zchunk = zc;
   h->max_stage_blocks = (int)(tiles * ((h->nz + zc - 1) / zc));
+  h->partials_blocks = (int)(tiles * ((h->nz + 10) / 11));
   return SPARC_OK;
 }
 

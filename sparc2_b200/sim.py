@@ -111,6 +111,24 @@ class Simulation:
         self._check(self.lib.sparc_run(self.h, int(first), int(count)),
                     "sparc_run")
 
+    @property
+    def zchunk(self):
+        """z extent of the stage kernels' work items (layers)."""
+        z = C.c_int()
+        self._check(self.lib.sparc_get_zchunk(self.h, C.byref(z)), "sparc_get_zchunk")
+        return z.value
+
+    def set_zchunk(self, zchunk):
+        self._check(self.lib.sparc_set_zchunk(self.h, int(zchunk)), "sparc_set_zchunk")
+
+    def tune(self, first, steps_per_trial=2):
+        """Runs the z-extent autotuner from iteration `first` (real driver
+        iterations, as sparc_run); returns (next iteration, extent)."""
+        nxt, best = C.c_int64(), C.c_int()
+        self._check(self.lib.sparc_tune(self.h, int(first), int(steps_per_trial),
+                                        C.byref(nxt), C.byref(best)), "sparc_tune")
+        return nxt.value, best.value
+
     def diagnostics(self):
         """(sparc_diag, status): status is SPARC_ERR_UNSTABLE after a
         failed iteration, SPARC_OK otherwise."""

@@ -71,7 +71,11 @@ typedef struct sparc_params {
     double  maxva;                 /* Alfven limiter, cm/s                    */
     double  sp_str, sp_length, sp_decay; /* horizontal sponge (no HPML)      */
     int32_t precision;             /* SPARC_FP64 or SPARC_FP32                */
-    int32_t reserved[7];
+    int32_t damping;               /* DAMPING: FFT horizontal damping of the
+                                      velocities in every RHS evaluation
+                                      (all_modules.f90:1803-1888; FP64
+                                      plain form only)                      */
+    int32_t reserved[6];
 } sparc_params;
 
 /* One entry of a PULSE = 2 table: the reference's psr_* arrays

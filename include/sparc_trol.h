@@ -51,7 +51,8 @@ typedef struct sparc_trol {
     int32_t psr_npulses;  /* pulses the reference draws for PULSE = 2
                              (driver.f90:50-54: 100 in 2-D, else 500)       */
     int32_t restart, time0;
-    int32_t twod, twop5d, displ, flows, damping;  /* unsupported when set    */
+    int32_t twod, twop5d, displ, flows;  /* unsupported when set             */
+    int32_t damping;      /* DAMPING as written (also params.damping)        */
     int32_t timestamp_size;
     int32_t xcb, xct, ycb, yct, zcb, zct;         /* chunk output box        */
     int32_t fullout, chunkout;                    /* output enabled          */

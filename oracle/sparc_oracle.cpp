@@ -480,6 +480,101 @@ struct orc_handle {
     for (size_t n = 0; n < N; ++n) R[n] = R[n] + forcing[n];
   }
 
+  // INIT_DAMPING, initialize.f90:1276-1340 (3-D): the rates of the half
+  // spectrum, kx = 0..nx/2 fastest, then ky (the negative frequencies of y
+  // from ny/2+1 on), kay2d in units of 1/Rsun, in the reference's order.
+  std::vector<double> damp_rates;
+  void init_damping() {
+    const int nh = nx / 2 + 1;
+    const double constx = 2.0 * PI * RSUN / P.xlength;
+    const double consty = 2.0 * PI * RSUN / P.ylength;
+    const double kayref = 902.0;
+    damp_rates.assign((size_t)nh * ny, 0.0);
+    for (int j = 0; j < ny; ++j) {
+      const double ky = j <= ny / 2 ? (double)j : (double)(ny - j);
+      for (int i = 0; i < nh; ++i) {
+        const double kay = std::pow(
+            constx * constx * ((double)i * (double)i) + consty * consty * (ky * ky), 0.5);
+        damp_rates[(size_t)j * nh + i] = diml / dimc / nx / ny * 1.0e-6 *
+                                         (500.0 * std::pow(kay / kayref, 2.2)) * 20.0;
+      }
+    }
+  }
+
+  // damp_velocity, all_modules.f90:1803-1888, applied as RHS.f90:166-172:
+  // RHSv -= term, term(:,:,k) = c2r(r2c(v(:,:,k)) * rates) with FFTW's
+  // unnormalised transforms (the 1/(nx*ny) is in the rates).  Restated as
+  // direct sums: r2c along x (kx = 0..nx/2), a complex transform along y,
+  // the product, its inverse along y, and c2r along x, which takes the
+  // real parts of the kx = 0 and (even nx) kx = nx/2 bins and twice the
+  // real part of the others, as a half-spectrum inverse does.
+  void damp_velocity(const double *T, double *S) {
+    const int nh = nx / 2 + 1;
+    std::vector<double> cx((size_t)nx), sx((size_t)nx), cy((size_t)ny), sy((size_t)ny);
+    for (int q = 0; q < nx; ++q) {
+      cx[q] = std::cos(2.0 * M_PI * q / nx);
+      sx[q] = std::sin(2.0 * M_PI * q / nx);
+    }
+    for (int q = 0; q < ny; ++q) {
+      cy[q] = std::cos(2.0 * M_PI * q / ny);
+      sy[q] = std::sin(2.0 * M_PI * q / ny);
+    }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int l = 1; l < 4; ++l)
+      for (int k = 0; k < nz; ++k) {
+        const double *v = T + (size_t)l * N + (size_t)k * nx * ny;
+        double *R = S + (size_t)l * N + (size_t)k * nx * ny;
+        std::vector<double> ar((size_t)ny * nh), ai((size_t)ny * nh), br((size_t)ny * nh),
+            bi((size_t)ny * nh);
+        for (int j = 0; j < ny; ++j)  // r2c along x
+          for (int m = 0; m < nh; ++m) {
+            double re = 0.0, im = 0.0;
+            for (int i = 0; i < nx; ++i) {
+              const int q = (int)(((long long)m * i) % nx);
+              re += v[(size_t)j * nx + i] * cx[q];
+              im -= v[(size_t)j * nx + i] * sx[q];
+            }
+            ar[(size_t)j * nh + m] = re;
+            ai[(size_t)j * nh + m] = im;
+          }
+        for (int p = 0; p < ny; ++p)  // along y, times the rates
+          for (int m = 0; m < nh; ++m) {
+            double re = 0.0, im = 0.0;
+            for (int j = 0; j < ny; ++j) {
+              const int q = (int)(((long long)p * j) % ny);
+              const double xr = ar[(size_t)j * nh + m], xi = ai[(size_t)j * nh + m];
+              re += xr * cy[q] + xi * sy[q];
+              im += xi * cy[q] - xr * sy[q];
+            }
+            const double d = damp_rates[(size_t)p * nh + m];
+            br[(size_t)p * nh + m] = re * d;
+            bi[(size_t)p * nh + m] = im * d;
+          }
+        for (int j = 0; j < ny; ++j)  // inverse along y
+          for (int m = 0; m < nh; ++m) {
+            double re = 0.0, im = 0.0;
+            for (int p = 0; p < ny; ++p) {
+              const int q = (int)(((long long)p * j) % ny);
+              const double xr = br[(size_t)p * nh + m], xi = bi[(size_t)p * nh + m];
+              re += xr * cy[q] - xi * sy[q];
+              im += xi * cy[q] + xr * sy[q];
+            }
+            ar[(size_t)j * nh + m] = re;
+            ai[(size_t)j * nh + m] = im;
+          }
+        for (int j = 0; j < ny; ++j)  // c2r along x, subtracted from RHSv
+          for (int i = 0; i < nx; ++i) {
+            double t = ar[(size_t)j * nh];
+            for (int m = 1; m < nh; ++m) {
+              const int q = (int)(((long long)m * i) % nx);
+              const double c = ar[(size_t)j * nh + m] * cx[q] - ai[(size_t)j * nh + m] * sx[q];
+              t += (2 * m == nx) ? c : 2.0 * c;
+            }
+            R[(size_t)j * nx + i] -= t;
+          }
+      }
+  }
+
   // scr zeroed on the global boundary planes (RHS.f90:154-164, 647-657).
   void zero_boundaries(double *S) const {
 #pragma omp parallel for collapse(2) schedule(static)
@@ -540,6 +635,7 @@ struct orc_handle {
     // the forcing joins RHSv between the v_z line and RHSp (RHS.f90:134-152)
     add_forcing(Rx, Ry, Rz);
     zero_boundaries(S);
+    if (P.damping) damp_velocity(T, S);  // RHS.f90:166-172
   }
 
   // MP_MHD_3D, RHS.f90:363-668 (FLOWS and DAMPING off).
@@ -652,6 +748,7 @@ struct orc_handle {
         }
     add_forcing(Rx, Ry, Rz);
     zero_boundaries(S);
+    if (P.damping) damp_velocity(T, S);  // RHS.f90:659-665
   }
   std::vector<double> extra[5];
 
@@ -992,6 +1089,7 @@ std::string orc_handle::setup(const sparc_params *pin, const double *rho0_in,
     return "non-periodic runs need >= 2 blocks along x and y";
   if (P.filter_mode_xy != 1 && P.filter_mode_xy != 2) return "filter_mode_xy";
   if (P.filter_mode_z != 1 && P.filter_mode_z != 2) return "filter_mode_z";
+  if (P.damping != 0 && P.damping != 1) return "damping must be 0 or 1";
   magnetic = P.magnetic == 2;
   quiet = P.magnetic == 0;
   V = magnetic ? 8 : 5;
@@ -1044,6 +1142,7 @@ std::string orc_handle::setup(const sparc_params *pin, const double *rho0_in,
   dimrho = rho0[0];
   diml = RSUN;
   dimb = std::sqrt(4.0 * PI * (dimc * dimc) * dimrho);
+  if (P.damping) init_damping();
   cq.resize(nz);
   invrho0q.resize(nz);
   for (int k = 0; k < nz; ++k) {

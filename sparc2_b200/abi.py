@@ -63,7 +63,8 @@ class SparcParams(C.Structure):
         ("sp_str", C.c_double), ("sp_length", C.c_double),
         ("sp_decay", C.c_double),
         ("precision", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("damping", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 

@@ -25,6 +25,7 @@ UNITS = {
     "batch.cu": [],
     "noalloc.cu": [],
     "serve.cu": [],
+    "damping.cu": [],
 }
 HEADERS = ["internal.h", "mhd_body.cuh", "random_forcing.cuh", "filter_body.cuh",
            "tmem_window.cuh"]
@@ -76,7 +77,7 @@ def build(force=False, verbose=False, ptxas_v=False):
             subprocess.check_call(cmd)
     if force or _stale(LIB, objs):
         tmp = LIB + ".tmp"
-        subprocess.check_call([nvcc(), *ARCH, "-shared", "-o", tmp, *objs])
+        subprocess.check_call([nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcufft"])
         _check_resolved(tmp)
         os.replace(tmp, LIB)
     return LIB

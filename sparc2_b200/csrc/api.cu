@@ -80,6 +80,9 @@ static std::string validate(const sparc_params &P) {
   if (!(P.timestep > 0)) return "timestep must be positive";
   if (P.precision != SPARC_FP64 && P.precision != SPARC_FP32)
     return "precision must be SPARC_FP64 or SPARC_FP32";
+  if (P.damping != 0 && P.damping != 1) return "damping must be 0 or 1";
+  if (P.damping && P.precision == SPARC_FP32)
+    return "DAMPING runs in the FP64 plain form only";
   if (P.precision == SPARC_FP32 && (long long)P.nx * P.ny * P.nz * 8 >= (1LL << 31))
     return "the precision form takes grids below 2^28 points";
   if (P.magnetic == 2 && (long long)P.nx * P.ny * P.nz * 8 >= (1LL << 31))
@@ -201,12 +204,14 @@ static int enqueue_step(Handle *h, cudaStream_t s, int *nk) {
   const long long l0 = h->launches;
   if (h->src.kind == SPARC_SRC_PSR && h->psr_khi > h->psr_klo) r |= launch_psr_forcing(h, S, s);
   if (h->src.kind == SPARC_SRC_RANDOM) r |= launch_random_forcing(h, s);
-  // stage k reads temp_k and writes temp_{k+1}; stage 5 writes a_new
-  r |= launch_stage(h, S, 1, a, a, f1, s);
-  r |= launch_stage(h, S, 2, a, f1, f2, s);
-  r |= launch_stage(h, S, 3, a, f2, f1, s);
-  r |= launch_stage(h, S, 4, a, f1, f2, s);
-  r |= launch_stage(h, S, 5, a, f2, f1, s);
+  // stage k reads temp_k and writes temp_{k+1}; stage 5 writes a_new.
+  // DAMPING: the velocity damping terms of each stage's input first
+  const double *tins[5] = {a, f1, f2, f1, f2};
+  double *sos[5] = {f1, f2, f1, f2, f1};
+  for (int st = 0; st < 5; ++st) {
+    if (h->damping) r |= damping_enqueue(h, tins[st], s);
+    r |= launch_stage(h, S, st + 1, a, tins[st], sos[st], s);
+  }
   *nk += (int)(h->launches - l0);
   rotate(h);
   return r ? SPARC_ERR_CUDA : SPARC_OK;
@@ -387,6 +392,7 @@ int sparc_create(const sparc_params *p, int device, sparc_handle **out) {
   h->use_pml = p->use_pml != 0 || h->use_hpml;
   h->V = h->magnetic ? 8 : 5;
   h->fp32 = p->precision == SPARC_FP32;
+  h->damping = p->damping != 0;
   h->Pp = h->magnetic ? 6 : 2;
   h->gxy = p->filter_mode_xy == 1 ? 5 : 3;
   h->gz = p->filter_mode_z == 1 ? 5 : 3;
@@ -522,6 +528,7 @@ int sparc_destroy(sparc_handle *h) {
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   drop_graphs(h);
+  damping_destroy(h);
   for (void *p : h->allocs) cudaFree(p);
   if (h->aux) cudaStreamSynchronize(h->aux);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
@@ -545,6 +552,7 @@ int sparc_set_background(sparc_handle *h, const double *rho0,
   cudaSetDevice(h->device);
   int r = setup_background(h, rho0, pre0, cs0, bx0, by0, bz0, zaxis_mm, grav);
   if (r) return r;
+  if (h->damping && (r = damping_setup(h))) return r == SPARC_ERR_CUDA ? fail(h, r, h->err) : r;
   if (h->fp32) {
     r = setup32(h);
     if (r) return r;

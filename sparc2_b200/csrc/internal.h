@@ -78,6 +78,7 @@ struct SimT {
   ForcingT<R> frc;
   const R *sc, *isc;           // V x nz depth scales (precision form)
   R *carry;                    // V x N compensated-sum carry (precision form)
+  const R *term;               // 3 x N velocity damping terms (DAMPING), or null
   // iteration bookkeeping and diagnostics (device)
   long long *iter;             // current driver iteration
   int *err;                    // device error flag (bounded waits)
@@ -201,6 +202,13 @@ struct Handle {
   // initialize.f90:899-947 all vanish): stage kernels skip its loads there
   bool sponge_slabs = false;
 
+  // DAMPING (damping.cu): cuFFT plans over the nz layers, the rates of the
+  // half spectrum, the spectrum and the three velocity terms
+  bool damping = false, fft_plans = false;
+  int fft_fwd = 0, fft_inv = 0;  // cufftHandle
+  double *d_damp = nullptr, *d_term = nullptr;
+  double2 *d_spec = nullptr;
+
   // forcing
   sparc_source src{};
   std::vector<sparc_pulse> pulses;
@@ -308,6 +316,9 @@ int launch_filter_event32(Handle *h, bool xy, const float *in, const float *carr
                           cudaStream_t s);
 int encode_tensor_maps32(Handle *h);
 int setup32(Handle *h);
+int damping_setup(Handle *h);
+int damping_enqueue(Handle *h, const double *tin, cudaStream_t s);
+void damping_destroy(Handle *h);
 int source32(Handle *h);
 
 // batch.cu: the device slot of batch member h (null while the slot table

@@ -833,7 +833,19 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
           else vzr = vzr + frc;
         }
         const R sv = SS(1, k);
-        const R Rv[3] = {vxr, vyr, vzr};
+        R Rv[3] = {vxr, vyr, vzr};
+        // DAMPING (plain form): the velocity RHS minus the damping term,
+        // after the boundary zeroing, so the boundary planes move by -term
+        // (RHS.f90:166-172, 659-665)
+        bool zv = zero;
+        if constexpr (!SCALED) {
+          if (S.term) {
+#pragma unroll
+            for (int l = 0; l < 3; ++l)
+              Rv[l] = (zero ? R(0) : Rv[l]) - __ldg(S.term + (long long)l * N + id);
+            zv = false;
+          }
+        }
         double vsq = 0.0;
 #pragma unroll
         for (int l = 1; l < 4; ++l) {
@@ -847,11 +859,11 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
               const double ph = ((double)an - (double)c) * (double)iv;
               vsq += ph * ph;
             } else {
-              an = zero ? av : av + fac * Rv[l - 1];
+              an = zv ? av : av + fac * Rv[l - 1];
               vsq += (double)an * (double)an;
             }
           } else {
-            an = zero ? av : av + fac * (sv * Rv[l - 1]);
+            an = zv ? av : av + fac * (sv * Rv[l - 1]);
           }
           so[l * N + id] = an;
         }

@@ -359,11 +359,21 @@ __global__ void __launch_bounds__(TX *TY)
     // boundary planes (RHS.f90:154-164)
     const bool zero = k == 0 || k == nz - 1 ||
                       (!per && (i == 0 || i == nx - 1 || j == 0 || j == ny - 1));
+    // DAMPING: the velocity RHS minus the damping term after the boundary
+    // zeroing (RHS.f90:166-172), so the boundary planes move by -term
+    bool zl[5] = {zero, zero, zero, zero, zero};
+    if (S.term) {
+#pragma unroll
+      for (int l = 1; l < 4; ++l) {
+        R[l] = (zero ? 0.0 : R[l]) - __ldg(S.term + (long long)(l - 1) * N + id);
+        zl[l] = false;
+      }
+    }
     if (MODE == LAST) {
       double an[5];
 #pragma unroll
       for (int l = 0; l < 5; ++l) {
-        an[l] = zero ? av[l] : av[l] + dt * R[l];
+        an[l] = zl[l] ? av[l] : av[l] + dt * R[l];
         so[l * N + id] = an[l];
       }
       const double p0v = __ldg(S.p0 + bi);
@@ -373,7 +383,7 @@ __global__ void __launch_bounds__(TX *TY)
       mp = fmin(mp, p + p0v);
     } else {
 #pragma unroll
-      for (int l = 0; l < 5; ++l) so[l * N + id] = zero ? av[l] : av[l] + bnext * R[l];
+      for (int l = 0; l < 5; ++l) so[l * N + id] = zl[l] ? av[l] : av[l] + bnext * R[l];
     }
   }
   if (MODE == LAST) diag_reduce(S, ke, mr, mp);
@@ -786,6 +796,7 @@ SimDev make_simdev(Handle *h) {
   S.stretch = h->d_stretch;
   S.deltat = h->deltat;
   S.dimc2rho = (h->dimc * h->dimc) * h->dimrho;
+  S.term = h->damping ? h->d_term : nullptr;
   if (h->bg1d) {
     S.rho0 = h->rho0_1; S.p0 = h->p0_1; S.rhoinv = h->rhoinv_1;
     S.c2rho0 = h->c2rho0_1; S.grz = h->grz_1; S.gpz = h->gpz_1;

@@ -93,8 +93,8 @@ int main(int argc, char **argv) {
     if (trol.stopped_line)
       fprintf(stderr, "%s: reading stopped at line %d (a value failed to read), as the "
               "reference's does\n", trol_path, trol.stopped_line);
-    if (trol.twod || trol.displ || trol.flows || trol.damping) {
-      fprintf(stderr, "%s: TWOD, MODE = 1, FLOWS and DAMPING are not supported\n", trol_path);
+    if (trol.twod || trol.displ || trol.flows) {
+      fprintf(stderr, "%s: TWOD, MODE = 1 and FLOWS are not supported\n", trol_path);
       return 1;
     }
     p = (sparc_params *)malloc(sizeof *p);

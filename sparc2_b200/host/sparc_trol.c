@@ -364,6 +364,7 @@ static void finish(const vars *v, sparc_trol *o) {
   o->displ = v->displ;
   o->flows = v->flows;
   o->damping = v->damping;
+  o->params.damping = v->damping ? 1 : 0;
   o->timestamp_size = (int32_t)v->timestamp_size;
   o->xcb = (int32_t)v->xcb; o->xct = (int32_t)v->xct;
   o->ycb = (int32_t)v->ycb; o->yct = (int32_t)v->yct;

@@ -242,3 +242,51 @@ def test_set_source_again_replaces_the_source(precision):
     assert a.diagnostics()[0].ke_norm == b.diagnostics()[0].ke_norm
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("name,kw", [("quiet_periodic", {}), ("quiet_hpml", {}),
+                                     ("mhd_hpml", {"nx": 42, "nz": 64})])
+def test_damping_against_the_oracle(name, kw):
+    """DAMPING = 1: the FFT horizontal damping of the velocities in every
+    RHS evaluation (cuFFT on the device, direct sums in the oracle), 12
+    driver iterations through the CUDA-graph loop."""
+    p, bg, src = cases.CASES[name](**kw)
+    p.damping = 1
+    sim, orc = Simulation(p, bg, src), oracle.Oracle(p, bg, src)
+    a0, psi0 = cases.random_state(sim, seed=31)
+    for s in (sim, orc):
+        s.set_state(a0, psi0)
+    sim.run(0, 12)
+    orc.run(0, 12)
+    ga, gpsi = sim.get_state()
+    oa, opsi = orc.get_state()
+    for l in range(sim.V):
+        assert rel_l2(ga[l], oa[l]) <= 1e-11, (l, rel_l2(ga[l], oa[l]))
+    if sim.n_psi:
+        assert rel_l2(gpsi, opsi) <= 1e-11
+    gd, _ = sim.diagnostics()
+    od, _ = orc.diagnostics()
+    assert gd.ke_norm == pytest.approx(od.ke_norm, rel=1e-11)
+
+
+def test_damping_changes_the_velocities_only_through_the_term():
+    """With and without DAMPING from the same state, one iteration: density
+    and pressure of stage 1 see the damped velocities only from stage 2 on,
+    and the damped run differs."""
+    p, bg, src = cases.quiet_hpml()
+    p2, _, _ = cases.quiet_hpml()
+    p2.damping = 1
+    s0, s1 = Simulation(p, bg, src), Simulation(p2, bg, src)
+    a0, psi0 = cases.random_state(s0, seed=5)
+    for s in (s0, s1):
+        s.set_state(a0, psi0)
+        s.step(3)
+    a, _ = s0.get_state()
+    b, _ = s1.get_state()
+    assert not np.array_equal(a[1], b[1])
+    # FP32 precision form: refused
+    p3, _, _ = cases.quiet_hpml()
+    p3.damping = 1
+    p3.precision = abi.SPARC_FP32
+    with pytest.raises(abi.SparcError):
+        Simulation(p3, bg, src)

@@ -173,3 +173,12 @@ def test_crlf_and_filter_modes(lib):
     assert r == abi.SPARC_OK
     assert t.params.filter_mode_xy == 2 and t.params.filter_mode_z == 0
     assert t.params.magnetic == 0 and t.simname == b"_3D_vq_"
+
+
+def test_damping_key_reaches_the_parameters(lib):
+    """DAMPING (initialize.f90:1512-1517, an integer switch: 0 off, any other
+    value on): the FFT damping the library runs in the FP64 plain form."""
+    r, t, _ = parse(lib, BASE + "DAMPING = 2\n")
+    assert r == abi.SPARC_OK and t.damping == 1 and t.params.damping == 1
+    r, t, _ = parse(lib, BASE + "DAMPING = 0\n")
+    assert r == abi.SPARC_OK and t.damping == 0 and t.params.damping == 0

@@ -64,6 +64,7 @@ constexpr int TX = 32, TY = 8, NT = TX * TY;
 constexpr int TR = 32, YG = 8;            // tile rows, rows per y-pass item
 constexpr int RX = TX + 12, RY = TR + 12;
 constexpr int NYI = RX * (TR / YG);       // y-pass items
+constexpr int LPB = 8;                    // layers per xy CTA (pipelined)
 static_assert(NYI <= NT, "one y-pass item per thread at most");
 constexpr int ZX = 32, ZY = 4, ZC = 32;   // z pass: 32 x 4 columns x 32 layers
 constexpr int ZH = ZC + 12;               // layers loaded per z slab
@@ -209,6 +210,113 @@ __device__ __forceinline__ void filt_xy_tile(const FiltArgs<R> &F, int l, int k,
     const R pq = *c;
     const R filt = (!per && (gxo < G || gxo >= nx - G)) ? (M2 ? R(0) : pq) : ftaps<R, G>(c, 1);
     out[gyo * nx + gxo] = M2 ? pq - fs * filt : filt;
+  }
+}
+
+// 4- or 8-byte cp.async of one value; ok = false fills the slot with zero
+// (no byte is read)
+template <class R>
+__device__ __forceinline__ void filt_cp(R *dst, const R *src, bool ok) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  const unsigned n = ok ? (unsigned)sizeof(R) : 0u;
+  if constexpr (sizeof(R) == 4)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(n)
+                 : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(n)
+                 : "memory");
+}
+
+// The fused y-then-x pass over layers k0 .. k0+nk-1 of the 32 x 32 tile
+// (x0, y0) of field l (no carry): the neighbourhood of the next layer is
+// copied into the second buffer by cp.async while a layer is filtered, so
+// the loads of one layer overlap the arithmetic of the previous one.  The
+// arithmetic is filt_xy_tile's.
+template <class R, int G>
+__device__ __forceinline__ void filt_xy_layers(const FiltArgs<R> &F, int l, int k0, int nk,
+                                               int x0, int y0) {
+  using namespace fb;
+  constexpr bool M2 = G == 3;
+  static_assert(RX == 44, "pre_average's item count");
+  __shared__ R raw2[2][RY][RX];  // two layers' rows y0-6 .., columns x0-6 ..
+  __shared__ R fy[TR][RX];       // after the y pass, rows y0 .., columns x0-6 ..
+  const int tid = threadIdx.y * TX + threadIdx.x;
+  const int nx = F.nx, ny = F.ny;
+  const bool per = F.periodic;
+  const R fs = F.s;
+  const long long NXY = (long long)nx * ny;
+  const R *inl = F.in + (long long)l * F.N;
+  R *outl = F.out + (long long)l * F.N;
+  auto issue = [&](int k, int b) {
+    const R *in = inl + (long long)k * NXY;
+#pragma unroll 1
+    for (int t = tid; t < RY * RX; t += NT) {
+      const int ry = t / RX, rx = t - ry * RX;
+      int gy = y0 - 6 + ry, gx = x0 - 6 + rx;
+      bool ok = true;
+      if (per) {
+        gy = wrap_idx(gy, ny);
+        gx = wrap_idx(gx, nx);
+      } else {
+        ok = gy >= 0 && gy < ny && gx >= 0 && gx < nx;
+      }
+      filt_cp(&raw2[b][ry][rx], ok ? in + gy * nx + gx : in, ok);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  const bool ypre = !per && (y0 - 5 <= G - 1 || y0 + TR + 4 >= ny - G);
+  const bool xpre = !per && (x0 - 5 <= G - 1 || x0 + TX + 4 >= nx - G);
+  issue(k0, 0);
+  for (int kk = 0; kk < nk; ++kk) {
+    const int b = kk & 1;
+    // the buffer being refilled was last read before the previous layer's
+    // post-y-pass barrier
+    if (kk + 1 < nk) {
+      issue(k0 + kk + 1, b ^ 1);
+      asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    }
+    __syncthreads();  // this layer's values visible; the previous x pass done
+    R(*raw)[RX] = raw2[b];
+    if (ypre) pre_average<R, G, 0>(&raw[0][0], y0 - 6, ny, RY - 1, RX, tid);
+    if (tid < NYI) {
+      const int grp = tid / RX, rx = tid - grp * RX, r0 = grp * YG;
+      const R *sb = &raw[r0 + 1][rx];
+      R v[YG + 10];
+#pragma unroll
+      for (int q = 5 - G; q < YG + 5 + G; ++q) v[q] = sb[q * RX];
+#pragma unroll
+      for (int j = 0; j < YG; ++j) {
+        const int gyo = y0 + r0 + j;
+        const R pq = v[j + 5];
+        R filt;
+        if (!per && (gyo < G || gyo >= ny - G)) {
+          filt = M2 ? R(0) : pq;
+        } else {
+          R sm = R(0);
+#pragma unroll
+          for (int m = 0; m <= 2 * G; ++m) sm += v[j + 5 - G + m] * fcoef<R>(G == 5 ? 0 : 1, m);
+          filt = sm;
+        }
+        fy[r0 + j][rx] = M2 ? pq - fs * filt : filt;
+      }
+    }
+    __syncthreads();
+    if (xpre) pre_average<R, G, 1>(&fy[0][0], x0 - 6, nx, RX - 1, TR, tid);
+    R *out = outl + (long long)(k0 + kk) * NXY;
+#pragma unroll
+    for (int u = 0; u < TR * TX / NT; ++u) {
+      const int t = tid + u * NT;
+      const int r = t / TX, tx = t - r * TX;
+      const int gxo = x0 + tx, gyo = y0 + r;
+      if (gxo >= nx || gyo >= ny) continue;
+      const R *c = &fy[r][tx + 6];
+      const R pq = *c;
+      const R filt =
+          (!per && (gxo < G || gxo >= nx - G)) ? (M2 ? R(0) : pq) : ftaps<R, G>(c, 1);
+      out[gyo * nx + gxo] = M2 ? pq - fs * filt : filt;
+    }
   }
 }
 

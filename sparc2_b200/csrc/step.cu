@@ -664,10 +664,13 @@ int launch_psr_forcing(Handle *h, const SimDev &S, cudaStream_t s);
 
 // ------------------------------------------------------ FILTER_VARS
 // FILTER_VARS of a filter event (filter_body.cuh): the fused y-then-x pass
+// (blockIdx.z: field and a group of LPB layers, pipelined)
 template <int G>
-__global__ void __launch_bounds__(fb::NT, 5) k_filt_xy64(FiltArgs<double> F) {
-  const int l = blockIdx.z / F.nz, k = blockIdx.z - l * F.nz;
-  filt_xy_tile<double, G, false>(F, l, k, blockIdx.x * fb::TX, blockIdx.y * fb::TR);
+__global__ void __launch_bounds__(fb::NT, 4) k_filt_xy64(FiltArgs<double> F) {
+  const int nzc = (F.nz + fb::LPB - 1) / fb::LPB;
+  const int l = blockIdx.z / nzc, k0 = (blockIdx.z - l * nzc) * fb::LPB;
+  filt_xy_layers<double, G>(F, l, k0, min(fb::LPB, F.nz - k0), blockIdx.x * fb::TX,
+                            blockIdx.y * fb::TR);
 }
 // the z pass: blockIdx.x is the z chunk (the chunks of a slab run
 // together), blockIdx.y the slab of the layer, blockIdx.z the field
@@ -690,7 +693,8 @@ int launch_filter_event(Handle *h, bool xy, const double *in, double *out, cudaS
   F.out = out;
   const int g = xy ? h->gxy : h->gz;
   if (xy) {
-    const dim3 grid((h->nx + fb::TX - 1) / fb::TX, (h->ny + fb::TR - 1) / fb::TR, h->V * h->nz);
+    const dim3 grid((h->nx + fb::TX - 1) / fb::TX, (h->ny + fb::TR - 1) / fb::TR,
+                    h->V * ((h->nz + fb::LPB - 1) / fb::LPB));
     if (g == 5) k_filt_xy64<5><<<grid, dim3(fb::TX, fb::TY), 0, s>>>(F);
     else k_filt_xy64<3><<<grid, dim3(fb::TX, fb::TY), 0, s>>>(F);
   } else {

@@ -204,6 +204,9 @@ static int enqueue_step(Handle *h, cudaStream_t s, int *nk) {
   const long long l0 = h->launches;
   if (h->src.kind == SPARC_SRC_PSR && h->psr_khi > h->psr_klo) r |= launch_psr_forcing(h, S, s);
   if (h->src.kind == SPARC_SRC_RANDOM) r |= launch_random_forcing(h, s);
+  // the persistent MHD stages' work counters
+  if (h->d_wctr64 && cudaMemsetAsync(h->d_wctr64, 0, 5 * sizeof(unsigned), s) != cudaSuccess)
+    r |= SPARC_ERR_CUDA;
   // stage k reads temp_k and writes temp_{k+1}; stage 5 writes a_new.
   // DAMPING: the velocity damping terms of each stage's input first
   const double *tins[5] = {a, f1, f2, f1, f2};
@@ -553,6 +556,7 @@ int sparc_set_background(sparc_handle *h, const double *rho0,
   int r = setup_background(h, rho0, pre0, cs0, bx0, by0, bz0, zaxis_mm, grav);
   if (r) return r;
   if (h->damping && (r = damping_setup(h))) return r == SPARC_ERR_CUDA ? fail(h, r, h->err) : r;
+  if ((r = mhd64_plan(h))) return fail(h, r, "MHD stage plan");
   if (h->fp32) {
     r = setup32(h);
     if (r) return r;

@@ -89,6 +89,14 @@ struct SimT {
 };
 using SimDev = SimT<double>;
 
+// z chunk boundaries of a persistent stage launch: chunk c covers layers
+// [b[c], b[c+1])
+struct ZSched {
+  static constexpr int MAX = 32;
+  int n;
+  int b[MAX + 1];
+};
+
 // PULSE = 2 forcing of the precision form: the per-layer pulse lists and
 // separable factors the forcing kernels read (all_modules.f90:521-663).
 struct Psr32 {
@@ -237,6 +245,12 @@ struct Handle {
   double *d_partials = nullptr, *d_diag = nullptr;
   unsigned int *d_counter = nullptr;
   int max_stage_blocks = 0;
+  // FP64 MHD stages as one persistent launch (step.cu:mhd64_plan): the
+  // edge/CPML tiles (tile coordinates), the interior rectangle, a work
+  // counter per stage, CTAs per launch
+  int2 *d_gen = nullptr;
+  int ngen = 0, gix0 = 0, giy0 = 0, gnix = 0, gniy = 0, pgrid = 0;
+  unsigned *d_wctr64 = nullptr;
   int partials_blocks = 0;  // blocks the partials hold: any z chunk >= 11
 
   // stage launch geometry (quiet tiles tx x ty; MHD tiles 32 x 8)
@@ -317,6 +331,7 @@ int launch_filter_event32(Handle *h, bool xy, const float *in, const float *carr
 int encode_tensor_maps32(Handle *h);
 int setup32(Handle *h);
 int damping_setup(Handle *h);
+int mhd64_plan(Handle *h);
 int damping_enqueue(Handle *h, const double *tin, cudaStream_t s);
 void damping_destroy(Handle *h);
 int source32(Handle *h);

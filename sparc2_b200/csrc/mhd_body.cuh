@@ -54,6 +54,11 @@ struct MhdBuf {
   static constexpr int BUF = ((mg::NO * mg::NC + mg::NH * HSL) + ALIGN - 1) / ALIGN * ALIGN;
   static constexpr int XCH = sizeof(R) == 4 ? 4 * mg::NC : 2 * mg::NC;
   static constexpr size_t SMEM = (2 * (size_t)BUF + XCH) * sizeof(R) + 128;
+  // plain form, general tiles: the per-lane and per-row coefficient tables
+  // follow the exchange area (dynamic, so one kernel can hold both bodies)
+  static constexpr size_t TABLES =
+      (size_t)(mg::TX + mg::TY) * 11 * sizeof(R) + (mg::TX + mg::TY) * sizeof(int);
+  static constexpr size_t SMEM_GEN = SMEM + (sizeof(R) == 8 ? TABLES : 0);
   // precision form: the depth scales (8 inverse, 8 forward per layer) of a
   // chunk of at most zext layers follow the exchange area
   static constexpr size_t smem_bytes(int zext) {
@@ -415,8 +420,20 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
   const bool cen_x = per || (x0 >= 5 && x0 + TX <= nx - 5);
   const bool cen_y = per || (y0 >= 5 && y0 + TY <= ny - 5);
   const int cxo = x0 - 5 - xo, cyo = y0 - 5 - yo;
-  __shared__ R cxs[INT ? 1 : TX * 11], cys[INT ? 1 : TY * 11];
-  __shared__ int cxb[INT ? 1 : TX], cyb[INT ? 1 : TY];
+  // the tables: FP64 in the dynamic buffer after the exchange area
+  // (MhdBuf::SMEM_GEN), FP32 static (its depth scales follow the exchange
+  // area)
+  constexpr bool DYN_T = !INT && !SCALED;
+  __shared__ R cxs_s[INT || DYN_T ? 1 : TX * 11], cys_s[INT || DYN_T ? 1 : TY * 11];
+  __shared__ int cxb_s[INT || DYN_T ? 1 : TX], cyb_s[INT || DYN_T ? 1 : TY];
+  R *cxs = cxs_s, *cys = cys_s;
+  int *cxb = cxb_s, *cyb = cyb_s;
+  if constexpr (DYN_T) {
+    cxs = smem + 2 * BUF + MB::XCH;
+    cys = cxs + TX * 11;
+    cxb = reinterpret_cast<int *>(cys + TY * 11);
+    cyb = cxb + TX;
+  }
   if (!INT && tid < TX + TY) {
     const bool isx = tid < TX;
     const int q0 = isx ? tid : tid - TX;                 // lane or row

@@ -480,107 +480,170 @@ int encode_tensor_maps(Handle *h) {
   return SPARC_OK;
 }
 
-// ------------------------- MP_MHD_3D, shared-body stage kernels (default)
-// One RK stage as two launches over one logical grid of (x tile, y tile, z
-// chunk) blocks: INT = true over the interior tile rectangle with the
-// branch-free body of mhd_body.cuh, INT = false over the whole grid,
-// returning at once on interior tiles (edge and CPML tiles).
-// TMA: the 24 own-point arrays of a layer arrive as 32x8x1 TMA boxes.
-template <int MODE, bool TMA, bool INT>
+// ------------------------- MP_MHD_3D, shared-body stage kernel
+
+// z chunk boundaries of the persistent launch: chunks of zchunk layers
+// (decreasing chunk sizes, so that the last items to start are short,
+// measured 1-3 % slower on the flux tube than equal chunks)
+static ZSched zsched(const Handle *h) {
+  ZSched Z{};
+  int n = 0;
+  for (int k = 0; k < h->nz && n < ZSched::MAX; k += h->zchunk) Z.b[n++] = k;
+  Z.b[n] = h->nz;
+  Z.n = n;
+  return Z;
+}
+
+// One FP64 MHD RK stage as a single persistent launch: each CTA (one per
+// SM) allocates its tensor memory once and pulls work items (32x8 tile, z
+// chunk) from a device counter until the list is done.  The edge/CPML
+// tiles' items come first (they are the slower ones, so the last items to
+// start are short), each list chunk-major so that neighbouring tiles of a
+// chunk run together; interior tiles take the branch-free body with TMA
+// halo planes, the others the general body.  The diagnostics partials are
+// per work item (the last stage reduces each item in the CTA and the item
+// that finishes last sums them in item order), so the norm does not depend
+// on which CTA took which item.
+template <int MODE, bool TMA>
 __global__ void __launch_bounds__(mg::NT, 1)
-    k_mhd64(const SimDev S, const __grid_constant__ TmaSet T, const double *__restrict__ a,
-            const double *__restrict__ tin, double *__restrict__ so, double beta, double bnext,
-            int zchunk, int mt, int ma, int ix0, int iy0, int gx, int gy) {
+    k_mhd64p(const SimDev S, const __grid_constant__ TmaSet T, const double *__restrict__ a,
+             const double *__restrict__ tin, double *__restrict__ so, double beta,
+             double bnext, const ZSched Z, int mt, int ma, int ix0, int iy0, int nix, int nint,
+             int ngen, const int2 *__restrict__ gen, unsigned *ctr) {
+  const int nch = Z.n;
   extern __shared__ __align__(1024) double smem_raw64[];
   double *smem = (double *)(((size_t)smem_raw64 + 127) & ~(size_t)127);
-  const int tx_ = INT ? blockIdx.x + ix0 : blockIdx.x;
-  const int ty_ = INT ? blockIdx.y + iy0 : blockIdx.y;
-  const int x0 = tx_ * mg::TX, y0 = ty_ * mg::TY;
-  if (!INT && mhd_interior(S, x0, y0)) return;
-  double ke = 0.0, mr = 1e300, mp = 1e300;
-  const int k0 = blockIdx.z * zchunk;
-  // the z windows in tensor memory: all 512 columns for the CTA's 16 warps
   __shared__ uint32_t s_tmem;
-  const int warp = (threadIdx.z * blockDim.y + threadIdx.y) * (blockDim.x / 32) + threadIdx.x / 32;
+  __shared__ int s_w;
+  const int tid = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
+  const int warp = tid / 32;
   if (warp == 0) tm_alloc_all(&s_tmem);
   tm_fence_before();
   __syncthreads();
   tm_fence_after();
-  const uint32_t tbase = s_tmem;
-  const bool ok = mhd_body<double, MODE, TMA, INT, true>(
-      S, &T, smem, a, tin, so, beta, bnext, x0, y0, k0, min(S.nz, k0 + zchunk), mt, ma, ke, mr,
-      mp, tm_warp_addr(tbase, warp));
-  // every exit frees the columns once all warps' accesses have completed
+  const uint32_t tbase = s_tmem, tw = tm_warp_addr(tbase, warp);
+  const int ngi = ngen * nch, total = (ngen + nint) * nch;
+  bool ok = true;
+  for (;;) {
+    if (tid == 0) s_w = (int)atomicAdd(ctr, 1u);
+    __syncthreads();
+    const int w = s_w;
+    if (w >= total) break;
+    int x0, y0, c;
+    const bool in = w >= ngi;
+    if (!in) {
+      c = w / ngen;
+      const int2 g = gen[w - c * ngen];
+      x0 = g.x * mg::TX;
+      y0 = g.y * mg::TY;
+    } else {
+      const int w2 = w - ngi;
+      c = w2 / nint;
+      const int t = w2 - c * nint;
+      const int ty = t / nix;
+      x0 = (ix0 + t - ty * nix) * mg::TX;
+      y0 = (iy0 + ty) * mg::TY;
+    }
+    const int k0 = Z.b[c], k1 = Z.b[c + 1];
+    // the body's first barrier orders every thread's read of s_w before
+    // thread 0 takes the next item
+    double ke = 0.0, mr = 1e300, mp = 1e300;
+    if (in)
+      ok = mhd_body<double, MODE, TMA, true, true>(S, &T, smem, a, tin, so, beta, bnext, x0, y0,
+                                                   k0, k1, mt, ma, ke, mr, mp, tw);
+    else
+      ok = mhd_body<double, MODE, TMA, false, true>(S, &T, smem, a, tin, so, beta, bnext, x0,
+                                                    y0, k0, k1, mt, ma, ke, mr, mp, tw);
+    if (!ok) break;
+    if (MODE == F_LAST) diag_reduce_t(S, ke, mr, mp, w, total);
+  }
   __syncwarp();
   tm_wait_st();
   tm_fence_before();
   __syncthreads();
   tm_fence_after();
   if (warp == 0) tm_free_all(tbase);
-  if (!ok) return;
-  if (MODE == F_LAST)
-    diag_reduce_t(S, ke, mr, mp, tx_ + (long long)gx * (ty_ + (long long)gy * blockIdx.z),
-                  (long long)gx * gy * gridDim.z);
 }
 
-static int launch_mhd64(Handle *h, const SimDev &S, int stage, const double *a,
-                        const double *tin, double *so, cudaStream_t s) {
-  const double beta = h->betas[stage - 1];
-  const double bnext = stage < 5 ? h->betas[stage] : h->deltat;
-  const int mode = stage == 1 ? FIRST : (stage == 5 ? LAST : MID);
-  dim3 blk(mg::TX, mg::TY, 2);
-  dim3 grd((h->nx + mg::TX - 1) / mg::TX, (h->ny + mg::TY - 1) / mg::TY,
-           (h->nz + h->zchunk - 1) / h->zchunk);
+// The persistent launch's plan: the edge/CPML tiles (all tiles outside the
+// interior rectangle), a work counter per stage (cleared at the start of
+// each step), one CTA per SM.
+int mhd64_plan(Handle *h) {
+  if (!h->magnetic || h->fp32) return SPARC_OK;
   const int np[4] = {h->faces[2].on ? h->faces[2].np : 0, h->faces[3].on ? h->faces[3].np : 0,
                      h->faces[4].on ? h->faces[4].np : 0, h->faces[5].on ? h->faces[5].np : 0};
   int ix0, ix1, iy0, iy1;
   mhd_interior_rect(h->nx, h->ny, np, ix0, ix1, iy0, iy1);
+  const int gx = (h->nx + mg::TX - 1) / mg::TX, gy = (h->ny + mg::TY - 1) / mg::TY;
   const bool has_int = ix1 > ix0 && iy1 > iy0;
-  dim3 gint(has_int ? ix1 - ix0 : 1, has_int ? iy1 - iy0 : 1, grd.z);
+  std::vector<int2> gen;
+  for (int ty = 0; ty < gy; ++ty)
+    for (int tx = 0; tx < gx; ++tx)
+      if (!(has_int && tx >= ix0 && tx < ix1 && ty >= iy0 && ty < iy1))
+        gen.push_back(make_int2(tx, ty));
+  h->gix0 = has_int ? ix0 : 0;
+  h->giy0 = has_int ? iy0 : 0;
+  h->gnix = has_int ? ix1 - ix0 : 0;
+  h->gniy = has_int ? iy1 - iy0 : 0;
+  h->ngen = (int)gen.size();
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+  h->pgrid = sms;
+  h->d_wctr64 = (unsigned *)dev_alloc(h, 8 * sizeof(unsigned));
+  if (!h->d_wctr64) return SPARC_ERR_NOMEM;
+  if (!gen.empty()) {
+    h->d_gen = (int2 *)dev_alloc(h, gen.size() * sizeof(int2));
+    if (!h->d_gen) return SPARC_ERR_NOMEM;
+    if (cudaMemcpy(h->d_gen, gen.data(), gen.size() * sizeof(int2), cudaMemcpyHostToDevice) !=
+        cudaSuccess)
+      return SPARC_ERR_CUDA;
+  }
+  return cudaMemset(h->d_wctr64, 0, 8 * sizeof(unsigned)) == cudaSuccess ? SPARC_OK
+                                                                        : SPARC_ERR_CUDA;
+}
+
+static int launch_mhd64p(Handle *h, const SimDev &S, int stage, const double *a,
+                         const double *tin, double *so, cudaStream_t s) {
+  const double beta = h->betas[stage - 1];
+  const double bnext = stage < 5 ? h->betas[stage] : h->deltat;
+  const int mode = stage == 1 ? FIRST : (stage == 5 ? LAST : MID);
   const bool tma = h->tma && h->allow_tma64;
-  // the interior kernel's layout holds TMA halo boxes when TMA is on
-  const size_t smg = MhdBuf<double>::SMEM;
-  const size_t smi = tma ? MhdBuf<double, true>::SMEM : smg;
+  const size_t sm = std::max(MhdBuf<double>::SMEM_GEN,
+                             tma ? MhdBuf<double, true>::SMEM : MhdBuf<double>::SMEM_GEN);
   int mt = -1, ma = -1;
   for (int b = 0; b < 3; ++b) {
     if (h->buf[b] == tin) mt = b;
     if (h->buf[b] == a) ma = b;
   }
-  if (mt < 0 || ma < 0) return SPARC_ERR_INVALID;
+  if (mt < 0 || ma < 0 || !h->d_wctr64) return SPARC_ERR_INVALID;
   TmaSet T;
   if (tma)
     for (int n = 0; n < 24; ++n) T.m[n] = h->tmaps_ty[n];
   else
     std::memset(&T, 0, sizeof(T));
-#define ML64(M, U)                                                                            \
-  do {                                                                                        \
-    cudaFuncSetAttribute(k_mhd64<M, U, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smi); \
-    cudaFuncSetAttribute(k_mhd64<M, U, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smg); \
-    if (has_int) {                                                                            \
-      cudaEventRecord(h->ev_fork, s);                                                         \
-      cudaStreamWaitEvent(h->aux, h->ev_fork, 0);                                             \
-      k_mhd64<M, U, false><<<grd, blk, smg, h->aux>>>(S, T, a, tin, so, beta, bnext, h->zchunk, \
-                                                     mt, ma, 0, 0, grd.x, grd.y);             \
-      cudaEventRecord(h->ev_join, h->aux);                                                    \
-      k_mhd64<M, U, true><<<gint, blk, smi, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt, \
-                                                ma, ix0, iy0, grd.x, grd.y);                  \
-      cudaStreamWaitEvent(s, h->ev_join, 0);                                                  \
-    } else {                                                                                  \
-      k_mhd64<M, U, false><<<grd, blk, smg, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, mt, \
-                                                ma, 0, 0, grd.x, grd.y);                      \
-    }                                                                                         \
+  const ZSched Z = zsched(h);
+  const int nch = Z.n;
+  const int nint = h->gnix * h->gniy;
+  const long long total = (long long)(h->ngen + nint) * nch;
+  const int grid = (int)std::min<long long>(h->pgrid, total);
+  unsigned *ctr = h->d_wctr64 + (stage - 1);
+  const dim3 blk(mg::TX, mg::TY, 2);
+#define MP64(M, U)                                                                           \
+  do {                                                                                       \
+    cudaFuncSetAttribute(k_mhd64p<M, U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
+    k_mhd64p<M, U><<<grid, blk, sm, s>>>(S, T, a, tin, so, beta, bnext, Z, mt, ma, h->gix0,   \
+                                        h->giy0, h->gnix, nint, h->ngen, h->d_gen, ctr);     \
   } while (0)
-  if (has_int) ++h->launches;  // the interior launch (launch_stage counts the other)
   if (tma) {
-    if (mode == FIRST) ML64(F_FIRST, true);
-    else if (mode == MID) ML64(F_MID, true);
-    else ML64(F_LAST, true);
+    if (mode == FIRST) MP64(F_FIRST, true);
+    else if (mode == MID) MP64(F_MID, true);
+    else MP64(F_LAST, true);
   } else {
-    if (mode == FIRST) ML64(F_FIRST, false);
-    else if (mode == MID) ML64(F_MID, false);
-    else ML64(F_LAST, false);
+    if (mode == FIRST) MP64(F_FIRST, false);
+    else if (mode == MID) MP64(F_MID, false);
+    else MP64(F_LAST, false);
   }
-#undef ML64
+#undef MP64
   return SPARC_OK;
 }
 
@@ -589,7 +652,7 @@ int launch_stage(Handle *h, const SimDev &S, int stage, const double *a,
   int r = SPARC_ERR_INVALID;
   if (h->magnetic) {
     if (h->tx != 32 || h->ty != 8) return SPARC_ERR_INVALID;
-    r = launch_mhd64(h, S, stage, a, tin, so, s);
+    r = launch_mhd64p(h, S, stage, a, tin, so, s);
     ++h->launches;
     if (r == SPARC_OK && cudaGetLastError() != cudaSuccess) r = SPARC_ERR_CUDA;
     return r;

@@ -44,13 +44,17 @@ enum { B_RED, B_SPONGE, B_RHO0, B_GRX, B_GRY, B_GRZ, B_C2R, B_GPX, B_GPY,
 // 42 x 18 copied by cp.async.  Exchange area:
 // d(vz)/dz and d(by)/dz in R, |v_new|^2 in FP64 (in the d(by)/dz slot in
 // the plain form, after its reader).
-template <class R, bool TH = false>
+template <class R, bool TH = false, bool HV = false>
 struct MhdBuf {
   static constexpr int ALIGN = 128 / (int)sizeof(R);
   static_assert(!TH || sizeof(R) == 8, "TMA halo boxes in the plain form only");
-  static constexpr int HXL = TH ? 44 : mg::HX;
-  static constexpr int XOFF = TH ? 1 : 0;
-  static constexpr int HSL = TH ? (HXL * mg::HY + ALIGN - 1) / ALIGN * ALIGN : mg::HS;
+  static_assert(!HV || sizeof(R) == 4, "16-byte halo vectors in the precision form only");
+  // HV: halo rows of 48 values from x0 - 8 (a 16-byte aligned start), copied
+  // as 4-value vectors
+  static constexpr int HXL = TH ? 44 : (HV ? 48 : mg::HX);
+  static constexpr int XOFF = TH ? 1 : (HV ? 3 : 0);
+  static constexpr int HSL =
+      (TH || HV) ? (HXL * mg::HY + ALIGN - 1) / ALIGN * ALIGN : mg::HS;
   static constexpr int BUF = ((mg::NO * mg::NC + mg::NH * HSL) + ALIGN - 1) / ALIGN * ALIGN;
   static constexpr int XCH = sizeof(R) == 4 ? 4 * mg::NC : 2 * mg::NC;
   static constexpr size_t SMEM = (2 * (size_t)BUF + XCH) * sizeof(R) + 128;
@@ -84,6 +88,12 @@ __device__ __forceinline__ void cp_r(R *dst, const R *src) {
   else
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sm_addr_t(dst)), "l"(src)
                  : "memory");
+}
+// one 16-byte cp.async (both addresses 16-byte aligned)
+template <class R>
+__device__ __forceinline__ void cp16_t(R *dst, const R *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sm_addr_t(dst)), "l"(src)
+               : "memory");
 }
 __device__ __forceinline__ void cp_commit_t() {
   asm volatile("cp.async.commit_group;\n" ::: "memory");
@@ -374,7 +384,12 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
   // faster in FP64; in FP32 the 48-wide boxes cost more than the cp.async
   // copies they replace)
   constexpr bool TH = TMA && INT && sizeof(R) == 8;
-  using MB = MhdBuf<R, TH>;
+  // precision form, interior tiles of a grid whose rows are 16-byte
+  // multiples (the TMA own-point condition): halo rows of 48 values from
+  // x0 - 8 copied as 16-byte vectors, 216 of them per plane, one per role-1
+  // thread, in place of one 4-byte copy per halo position
+  constexpr bool HV = TMA && INT && sizeof(R) == 4;
+  using MB = MhdBuf<R, TH, HV>;
   constexpr int BUF = MB::BUF, HXL = MB::HXL, XOFF = MB::XOFF, HSL = MB::HSL;
   constexpr bool SCALED = sizeof(R) == 4;
   __shared__ unsigned long long bar[2];
@@ -467,6 +482,17 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
   {
     const int cx0 = x0 - xo, cy0 = y0 - yo;
     auto pos = [&](int t, int &hs, int &ho) {
+      if constexpr (HV) {  // vector t of 216: row t / 12, values 4 (t % 12) ..
+        if (t >= HY * (HXL / 4)) return;
+        const int ly = t / (HXL / 4), lx = (t - ly * (HXL / 4)) * 4;
+        const int gx = x0 - 8 + lx, gy = yo + ly;
+        // inside the grid by the interior test (x0 >= 32, x0 + 40 <= nx
+        // with nx a multiple of 4); checked so that no copy can leave it
+        if (gx < 0 || gx + 3 >= nx || gy < 0 || gy >= ny) return;
+        hs = ly * HXL + lx;
+        ho = gy * nx + gx;
+        return;
+      }
       if (t >= HS) return;
       const int ly = t / HX, lx = t - ly * HX;
       const bool inx = lx >= cx0 && lx < cx0 + TX, iny = ly >= cy0 && ly < cy0 + TY;
@@ -486,9 +512,14 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
       ho = gy * nx + gx;
     };
     // halo positions 0..511 one per thread, 512..755 on role 1 (role 0
-    // carries the TMA issue and the heavier momentum update)
-    pos(tid, hs0, ho0);
-    if (role == 1) pos(tid + NC, hs1, ho1);
+    // carries the TMA issue and the heavier momentum update); HV: the
+    // vectors on role 1
+    if constexpr (HV) {
+      if (role == 1) pos(tid - NC, hs0, ho0);
+    } else {
+      pos(tid, hs0, ho0);
+      if (role == 1) pos(tid + NC, hs1, ho1);
+    }
   }
   // Own-point arrays not read: where the sponge vanishes outside the CPML
   // slabs, the sponge of layers whose points lie in no slab (a CTA-uniform
@@ -512,7 +543,16 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
   };
   auto issue = [&](int k, int b) {
     const int kb = k * NXY;
-    if (!TH && hs0 >= 0) {
+    if (HV && hs0 >= 0) {
+      R *h = Hp(b, 0) + hs0;
+      const int id = kb + ho0;
+#pragma unroll
+      for (int sl = 0; sl < 7; ++sl) cp16_t(h + sl * HSL, tin + (sl + 1) * N + id);
+      cp16_t(h + 7 * HSL, S.box + id);
+      cp16_t(h + 8 * HSL, S.boy + id);
+      cp16_t(h + 9 * HSL, S.boz + id);
+    }
+    if (!TH && !HV && hs0 >= 0) {
       R *h = Hp(b, 0) + hs0;
       const int id = kb + ho0;
 #pragma unroll
@@ -702,8 +742,14 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
     // TH: every thread waits for the layer's TMA copies (its flux positions
     // arrive that way); otherwise thread 0 alone, before the barrier
     if (TH) mine = mbar_wait_t(&bar[b], (phase >> b) & 1u, S.err);
-    if (mine && hs0 >= 0) flux(b, hs0);
-    if (mine && hs1 >= 0) flux(b, hs1);
+    if constexpr (HV) {
+      if (mine && hs0 >= 0)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) flux(b, hs0 + q);
+    } else {
+      if (mine && hs0 >= 0) flux(b, hs0);
+      if (mine && hs1 >= 0) flux(b, hs1);
+    }
     if (TMA && !TH && tid == 0) mine = mbar_wait_t(&bar[b], (phase >> b) & 1u, S.err);
     phase ^= 1u << b;
     if (!__syncthreads_and(mine)) { ok = false; break; }

@@ -791,9 +791,11 @@ int launch_stage32(Handle *h, const Sim32 &S, int stage, const float *a,
     const bool has_int = h->nx - xM - TX >= 0 && h->ny - yM - TYT >= 0 && ix1 > ix0 && iy1 > iy0;
     dim3 gint(has_int ? ix1 - ix0 : 1, has_int ? iy1 - iy0 : 1, grd.z);
     const int smz = (int)MB::smem_bytes(h->zchunk);
+    // the interior kernel's layout holds 48-wide halo rows with TMA own points
+    const int smi = h->tma32 ? (int)MhdBuf<float, false, true>::smem_bytes(h->zchunk) : smz;
 #define ML32(M, U)                                                                          \
   do {                                                                                      \
-    cudaFuncSetAttribute(k_mhd32<M, U, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smz); \
+    cudaFuncSetAttribute(k_mhd32<M, U, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smi); \
     cudaFuncSetAttribute(k_mhd32<M, U, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smz); \
     if (has_int) {                                                                          \
       cudaEventRecord(h->ev_fork, s);                                                       \
@@ -801,7 +803,7 @@ int launch_stage32(Handle *h, const Sim32 &S, int stage, const float *a,
       k_mhd32<M, U, false><<<grd, blk, smz, h->aux>>>(S, T, a, tin, so, beta, bnext,       \
                                                        h->zchunk, mt, ma, 0, 0, gx, gy);    \
       cudaEventRecord(h->ev_join, h->aux);                                                  \
-      k_mhd32<M, U, true><<<gint, blk, smz, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, \
+      k_mhd32<M, U, true><<<gint, blk, smi, s>>>(S, T, a, tin, so, beta, bnext, h->zchunk, \
                                                   mt, ma, ix0, iy0, gx, gy);                \
       cudaStreamWaitEvent(s, h->ev_join, 0);                                                \
     } else {                                                                                \

@@ -596,7 +596,7 @@ def measure_fp32_cfg2(dev, steps=40, warmup=3):
 
 def measure_ensemble(dev, members=64, steps=100, warmup=2):
     """The batched precision form: `members` seeded FP32 simulations through
-    the batched engine (autotuned tiles), one graph launch per step."""
+    the batched engine (autotuned z extents), one graph launch per step."""
     import torch
     from sparc2_b200 import Simulation
     from sparc2_b200.batch import Batch

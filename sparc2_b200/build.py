@@ -28,7 +28,7 @@ UNITS = {
     "damping.cu": [],
 }
 HEADERS = ["internal.h", "mhd_body.cuh", "random_forcing.cuh", "filter_body.cuh",
-           "tmem_window.cuh"]
+           "tmem_window.cuh", "tma_util.cuh"]
 # host C units (gcc): the .trol reader
 HOST_UNITS = {"sparc_trol.c": ["-O2", "-std=c99", "-Wall", "-fPIC"]}
 HOST = os.path.join(HERE, "host")

@@ -35,6 +35,7 @@
 #pragma once
 
 #include "internal.h"
+#include "tma_util.cuh"
 
 namespace sparc {
 
@@ -55,6 +56,7 @@ struct FiltArgs {
   R *out;
   const R *carry;     // compensation subtracted on load (first pass), or null
   const R *sc, *isc;  // depth scales V x nz (precision form z pass), or null
+  int *err;           // device error flag (bounded waits of the TMA xy pass)
 };
 
 namespace fb {
@@ -229,17 +231,26 @@ __device__ __forceinline__ void filt_cp(R *dst, const R *src, bool ok) {
 
 // The fused y-then-x pass over layers k0 .. k0+nk-1 of the 32 x 32 tile
 // (x0, y0) of field l (no carry): the neighbourhood of the next layer is
-// copied into the second buffer by cp.async while a layer is filtered, so
-// the loads of one layer overlap the arithmetic of the previous one.  The
-// arithmetic is filt_xy_tile's.
-template <class R, int G>
+// copied into the second buffer while a layer is filtered, so the loads of
+// one layer overlap the arithmetic of the previous one.  The arithmetic is
+// filt_xy_tile's.  TMA (non-periodic grids, rows a multiple of 16 bytes):
+// the neighbourhood is one 44 x 44 x 1 tile of `map` (the input buffer as
+// nx x ny x (V nz)) from (x0 - 6, y0 - 6), issued by one thread; the tensor
+// copy reads zero outside the grid, as the edge rule wants, and x0 - 6 is
+// even, so the start is 16-byte aligned.  Otherwise every thread copies
+// its share by cp.async (zero fill outside the grid, wrap on periodic
+// axes).
+template <class R, int G, bool TMA = false>
 __device__ __forceinline__ void filt_xy_layers(const FiltArgs<R> &F, int l, int k0, int nk,
-                                               int x0, int y0) {
+                                               int x0, int y0,
+                                               const CUtensorMap *map = nullptr) {
   using namespace fb;
   constexpr bool M2 = G == 3;
   static_assert(RX == 44, "pre_average's item count");
-  __shared__ R raw2[2][RY][RX];  // two layers' rows y0-6 .., columns x0-6 ..
+  static_assert(RY * RX * sizeof(R) % 128 == 0, "each layer buffer 128-byte aligned");
+  __shared__ __align__(128) R raw2[2][RY][RX];  // two layers' rows y0-6 .., columns x0-6 ..
   __shared__ R fy[TR][RX];       // after the y pass, rows y0 .., columns x0-6 ..
+  __shared__ unsigned long long fbar[2];
   const int tid = threadIdx.y * TX + threadIdx.x;
   const int nx = F.nx, ny = F.ny;
   const bool per = F.periodic;
@@ -247,22 +258,40 @@ __device__ __forceinline__ void filt_xy_layers(const FiltArgs<R> &F, int l, int 
   const long long NXY = (long long)nx * ny;
   const R *inl = F.in + (long long)l * F.N;
   R *outl = F.out + (long long)l * F.N;
-  auto issue = [&](int k, int b) {
-    const R *in = inl + (long long)k * NXY;
-#pragma unroll 1
-    for (int t = tid; t < RY * RX; t += NT) {
-      const int ry = t / RX, rx = t - ry * RX;
-      int gy = y0 - 6 + ry, gx = x0 - 6 + rx;
-      bool ok = true;
-      if (per) {
-        gy = wrap_idx(gy, ny);
-        gx = wrap_idx(gx, nx);
-      } else {
-        ok = gy >= 0 && gy < ny && gx >= 0 && gx < nx;
-      }
-      filt_cp(&raw2[b][ry][rx], ok ? in + gy * nx + gx : in, ok);
+  if constexpr (TMA) {
+    if (tid == 0) {
+      mbar_init_t(&fbar[0]);
+      mbar_init_t(&fbar[1]);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    __syncthreads();
+  }
+  auto issue = [&](int k, int b) {
+    if constexpr (TMA) {
+      if (tid == 0) {
+        // orders the generic reads and writes of this buffer (two layers
+        // back, before a barrier) before the tensor copy's writes
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_tx_t(&fbar[b], (unsigned)(RY * RX * sizeof(R)));
+        tma3d_t(&raw2[b][0][0], map, x0 - 6, y0 - 6, l * F.nz + k, &fbar[b]);
+      }
+    } else {
+      const R *in = inl + (long long)k * NXY;
+#pragma unroll 1
+      for (int t = tid; t < RY * RX; t += NT) {
+        const int ry = t / RX, rx = t - ry * RX;
+        int gy = y0 - 6 + ry, gx = x0 - 6 + rx;
+        bool ok = true;
+        if (per) {
+          gy = wrap_idx(gy, ny);
+          gx = wrap_idx(gx, nx);
+        } else {
+          ok = gy >= 0 && gy < ny && gx >= 0 && gx < nx;
+        }
+        filt_cp(&raw2[b][ry][rx], ok ? in + gy * nx + gx : in, ok);
+      }
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
   };
   const bool ypre = !per && (y0 - 5 <= G - 1 || y0 + TR + 4 >= ny - G);
   const bool xpre = !per && (x0 - 5 <= G - 1 || x0 + TX + 4 >= nx - G);
@@ -271,13 +300,24 @@ __device__ __forceinline__ void filt_xy_layers(const FiltArgs<R> &F, int l, int 
     const int b = kk & 1;
     // the buffer being refilled was last read before the previous layer's
     // post-y-pass barrier
-    if (kk + 1 < nk) {
-      issue(k0 + kk + 1, b ^ 1);
-      asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    if (kk + 1 < nk) issue(k0 + kk + 1, b ^ 1);
+    if constexpr (TMA) {
+      // every thread sees the tensor copy complete (buffer b's (kk/2)-th fill)
+      const bool ok = mbar_wait_t(&fbar[b], (unsigned)(kk >> 1) & 1u, F.err);
+      if (!__syncthreads_and(ok)) {
+        // gave up (error flag raised): wait, again bounded, for the copies
+        // still in flight into this CTA's buffers, then leave
+        if (tid == 0) {
+          mbar_wait_t(&fbar[b], (unsigned)(kk >> 1) & 1u, F.err);
+          if (kk + 1 < nk) mbar_wait_t(&fbar[b ^ 1], (unsigned)((kk + 1) >> 1) & 1u, F.err);
+        }
+        return;
+      }
     } else {
-      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+      if (kk + 1 < nk) asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+      else asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+      __syncthreads();  // this layer's values visible; the previous x pass done
     }
-    __syncthreads();  // this layer's values visible; the previous x pass done
     R(*raw)[RX] = raw2[b];
     if (ypre) pre_average<R, G, 0>(&raw[0][0], y0 - 6, ny, RY - 1, RX, tid);
     if (tid < NYI) {

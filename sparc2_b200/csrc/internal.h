@@ -239,6 +239,10 @@ struct Handle {
   // state buffers (nx, ny, nz*V), [3..17] the background arrays per layer
   bool tma = false;
   CUtensorMap tmaps_ty[24];
+  // FILTER_VARS xy pass (non-periodic FP64 grids, nx even): the state
+  // buffers in 44x44x1 boxes
+  bool ftma = false;
+  CUtensorMap fmaps[3];
   // device bookkeeping
   int *d_err = nullptr;
   long long *d_iter = nullptr, *d_fail = nullptr;

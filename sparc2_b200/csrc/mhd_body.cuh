@@ -16,6 +16,7 @@
 #pragma once
 
 #include "internal.h"
+#include "tma_util.cuh"
 #include "tmem_window.cuh"
 
 namespace sparc {
@@ -30,7 +31,7 @@ namespace mg {
 constexpr int TX = 32, TY = 8, NC = TX * TY, NT = 2 * NC;
 constexpr int HX = TX + 10, HY = TY + 10, HS = HX * HY;
 constexpr int NH = 10, NO = 24;
-constexpr long long WAIT_LIMIT = 1LL << 26;
+constexpr long long WAIT_LIMIT = kMbarWaitLimit;
 // own-point slots: stage rho, a[0..7], 14 background arrays, p0
 constexpr int O_RHO = 0, O_A = 1, O_BG = 9, O_P0 = 23;
 enum { B_RED, B_SPONGE, B_RHO0, B_GRX, B_GRY, B_GRZ, B_C2R, B_GPX, B_GPY,
@@ -77,9 +78,6 @@ struct TmaSet {
   CUtensorMap m[24];
 };
 
-__device__ __forceinline__ unsigned sm_addr_t(const void *p) {
-  return (unsigned)__cvta_generic_to_shared(p);
-}
 template <class R>
 __device__ __forceinline__ void cp_r(R *dst, const R *src) {
   if constexpr (sizeof(R) == 4)
@@ -97,37 +95,6 @@ __device__ __forceinline__ void cp16_t(R *dst, const R *src) {
 }
 __device__ __forceinline__ void cp_commit_t() {
   asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-__device__ __forceinline__ void mbar_init_t(unsigned long long *bar) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sm_addr_t(bar)) : "memory");
-}
-__device__ __forceinline__ void mbar_tx_t(unsigned long long *bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sm_addr_t(bar)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void tma3d_t(void *dst, const CUtensorMap *map, int x, int y, int z,
-                                        unsigned long long *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(sm_addr_t(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(z), "r"(sm_addr_t(bar))
-      : "memory");
-}
-// bounded wait: gives up after WAIT_LIMIT polls and raises the error flag
-__device__ __forceinline__ bool mbar_wait_t(unsigned long long *bar, unsigned parity, int *err) {
-  for (long long n = 0; n < mg::WAIT_LIMIT; ++n) {
-    unsigned ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(sm_addr_t(bar)), "r"(parity)
-        : "memory");
-    if (ok) return true;
-  }
-  atomicExch(err, 1);
-  return false;
 }
 
 // brings the line holding p into L2 (no register, no wait)

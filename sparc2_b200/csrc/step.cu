@@ -444,7 +444,12 @@ static int launch_quiet(Handle *h, const SimDev &S, int stage,
 
 int encode_tensor_maps(Handle *h) {
   h->tma = false;
-  if (!h->magnetic || (h->nx & 1)) return SPARC_OK;
+  h->ftma = false;
+  // rows of a multiple of 16 bytes; the filter's tiles read zero outside
+  // the grid, so its maps serve non-periodic grids only
+  const bool want_f = !h->periodic && !(h->nx & 1);
+  const bool want_m = h->magnetic && !(h->nx & 1);
+  if (!want_f && !want_m) return SPARC_OK;
   void *fn = nullptr;
   cudaDriverEntryPointQueryResult q;
   if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
@@ -456,17 +461,30 @@ int encode_tensor_maps(Handle *h) {
                           const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
                           const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
                           CUtensorMapL2promotion, CUtensorMapFloatOOBfill))fn;
-  auto one = [&](CUtensorMap *m, const double *base, unsigned long long depth, bool halo = false) {
+  auto boxed = [&](CUtensorMap *m, const double *base, unsigned long long depth, int bx,
+                   int by) {
     cuuint64_t dims[3] = {(cuuint64_t)h->nx, (cuuint64_t)h->ny, (cuuint64_t)depth};
     cuuint64_t strides[2] = {(cuuint64_t)h->nx * 8, (cuuint64_t)h->nx * h->ny * 8};
-    cuuint32_t box[3] = {(cuuint32_t)(halo ? MhdBuf<double, true>::HXL : mg::TX),
-                         (cuuint32_t)(halo ? mg::HY : mg::TY), 1};
+    cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
     cuuint32_t es[3] = {1, 1, 1};
     return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void *)base, dims, strides, box, es,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
   };
+  auto one = [&](CUtensorMap *m, const double *base, unsigned long long depth, bool halo = false) {
+    return boxed(m, base, depth, halo ? MhdBuf<double, true>::HXL : mg::TX,
+                 halo ? mg::HY : mg::TY);
+  };
+  if (want_f) {
+    // FILTER_VARS xy pass: the 44 x 44 neighbourhood of a 32 x 32 tile
+    bool fok = true;
+    for (int b = 0; b < 3; ++b)
+      fok = fok && boxed(&h->fmaps[b], h->buf[b], (unsigned long long)h->nz * h->V, fb::RX,
+                         fb::RY);
+    h->ftma = fok;
+  }
+  if (!want_m) return SPARC_OK;
   bool ok = true;
   for (int b = 0; b < 3; ++b) ok = ok && one(&h->tmaps_ty[b], h->buf[b], (unsigned long long)h->nz * h->V);
   const double *bg[15] = {h->red, h->sponge, h->rho0, h->grx, h->gry, h->grz, h->c2rho0,
@@ -728,12 +746,13 @@ int launch_psr_forcing(Handle *h, const SimDev &S, cudaStream_t s);
 // ------------------------------------------------------ FILTER_VARS
 // FILTER_VARS of a filter event (filter_body.cuh): the fused y-then-x pass
 // (blockIdx.z: field and a group of LPB layers, pipelined)
-template <int G>
-__global__ void __launch_bounds__(fb::NT, 4) k_filt_xy64(FiltArgs<double> F) {
+template <int G, bool TMA>
+__global__ void __launch_bounds__(fb::NT, 4)
+    k_filt_xy64(FiltArgs<double> F, const __grid_constant__ CUtensorMap map) {
   const int nzc = (F.nz + fb::LPB - 1) / fb::LPB;
   const int l = blockIdx.z / nzc, k0 = (blockIdx.z - l * nzc) * fb::LPB;
-  filt_xy_layers<double, G>(F, l, k0, min(fb::LPB, F.nz - k0), blockIdx.x * fb::TX,
-                            blockIdx.y * fb::TR);
+  filt_xy_layers<double, G, TMA>(F, l, k0, min(fb::LPB, F.nz - k0), blockIdx.x * fb::TX,
+                                 blockIdx.y * fb::TR, &map);
 }
 // the z pass: blockIdx.x is the z chunk (the chunks of a slab run
 // together), blockIdx.y the slab of the layer, blockIdx.z the field
@@ -754,12 +773,27 @@ int launch_filter_event(Handle *h, bool xy, const double *in, double *out, cudaS
   F.s = xy ? h->P.s_xy : h->P.s_z;
   F.in = in;
   F.out = out;
+  F.err = h->d_err;
   const int g = xy ? h->gxy : h->gz;
   if (xy) {
     const dim3 grid((h->nx + fb::TX - 1) / fb::TX, (h->ny + fb::TR - 1) / fb::TR,
                     h->V * ((h->nz + fb::LPB - 1) / fb::LPB));
-    if (g == 5) k_filt_xy64<5><<<grid, dim3(fb::TX, fb::TY), 0, s>>>(F);
-    else k_filt_xy64<3><<<grid, dim3(fb::TX, fb::TY), 0, s>>>(F);
+    // the tensor map of the input buffer (neighbourhoods by TMA), if any
+    int mb = -1;
+    if (h->ftma)
+      for (int b = 0; b < 3; ++b)
+        if (h->buf[b] == in) mb = b;
+    CUtensorMap map;
+    if (mb >= 0) map = h->fmaps[mb];
+    else std::memset(&map, 0, sizeof(map));
+    const dim3 blk(fb::TX, fb::TY);
+    if (mb >= 0) {
+      if (g == 5) k_filt_xy64<5, true><<<grid, blk, 0, s>>>(F, map);
+      else k_filt_xy64<3, true><<<grid, blk, 0, s>>>(F, map);
+    } else {
+      if (g == 5) k_filt_xy64<5, false><<<grid, blk, 0, s>>>(F, map);
+      else k_filt_xy64<3, false><<<grid, blk, 0, s>>>(F, map);
+    }
   } else {
     const size_t zs = filt_z_smem<double>();
     const long long slabs = (long long)((h->nx + fb::ZX - 1) / fb::ZX) *

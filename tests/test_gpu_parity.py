@@ -91,13 +91,18 @@ def test_one_iteration_from_random_state(name):
     assert gd.min_p == pytest.approx(od.min_p, rel=1e-13)
 
 
-@pytest.mark.parametrize("name", ["quiet_periodic", "mhd_hpml", "quiet_hpml"])
-def test_filter_vars(name):
-    sim, orc = pair(name)
+@pytest.mark.parametrize("name,kw", [("quiet_periodic", {}), ("mhd_hpml", {}), ("quiet_hpml", {}),
+                                     ("quiet_hpml", {"nx": 41, "ny": 38})])
+def test_filter_vars(name, kw):
+    """The 11-point filter on both axes.  Non-periodic grids with an even nx
+    take the xy pass whose neighbourhoods arrive as tensor copies; nx = 41
+    (rows not a multiple of 16 bytes) and the periodic grid take the
+    per-thread copies."""
+    sim, orc = pair(name, **kw)
     a0, psi0 = cases.random_state(sim, seed=7)
     for s in (sim, orc):
         s.set_state(a0, psi0)
-    nn = 30 if sim.params.timestep == 1.0 else 30  # xy and z cadence
+    nn = 30  # a multiple of both cadences: xy and z pass
     sim.filter_vars(nn)
     orc.filter_vars(nn)
     ga, _ = sim.get_state()
@@ -107,12 +112,14 @@ def test_filter_vars(name):
 
 
 @pytest.mark.parametrize("name,kw", [("quiet_periodic", {}), ("mhd_hpml", {"nz": 80}),
-                                     ("quiet_hpml", {"nx": 70, "ny": 66})])
+                                     ("quiet_hpml", {"nx": 70, "ny": 66}),
+                                     ("quiet_hpml", {"nx": 41, "ny": 38})])
 def test_filter_vars_7point(name, kw):
     """filter_mode 2 on both axes (derivatives.f90: the 7-point filter,
     combined as a - s*filt, zero at the x/y edge points): nz = 80 gives the
     z pass slabs away from both ends and slabs at them; 70 x 66 gives xy
-    tiles with and without the edge pre-average."""
+    tiles with and without the edge pre-average; nx = 41 the per-thread
+    copies on a non-periodic grid."""
     p, bg, src = cases.CASES[name](**kw)
     p.filter_mode_xy = p.filter_mode_z = 2
     sim, orc = Simulation(p, bg, src), oracle.Oracle(p, bg, src)

@@ -3,7 +3,8 @@
 // precision form (R = float, step32.cu).
 //
 //   * xy (nn % xyfreq == 0): one fused pass per layer tile.  A CTA loads a
-//     (32+12) x (32+12) tile of one field's layer into shared memory, forms
+//     (32+12) x (32+12) tile of one field's layer into shared memory (in
+//     FP64 on non-periodic grids as one TMA tensor copy per layer), forms
 //     the y pre-average of the non-periodic edge rows (derivatives.f90:671-
 //     675), the y filter of filty (derivatives.f90:345-447) with its edge
 //     rows (copy-through for the 11-point filter, zero for the 7-point one)
@@ -12,7 +13,8 @@
 //     writes the tile once.  The reference's y-then-x order is kept.
 //   * z (nn % zfreq == 0): a CTA loads a slab of 32 x 4 columns of one field
 //     over 32 layers and their 6-layer margins into shared memory (44 KB in
-//     FP64, so that five CTAs share an SM), every load in flight at once;
+//     FP64, so that five CTAs share an SM), every load in flight at once
+//     (in FP64 one 4-D TMA tensor copy);
 //     each thread then runs a 13-deep register window of raw values down
 //     its column for 16 layers (the pre-average of derivatives.f90:690-693
 //     needs the neighbours of the 11 taps).  The z chunks of a slab are
@@ -56,7 +58,7 @@ struct FiltArgs {
   R *out;
   const R *carry;     // compensation subtracted on load (first pass), or null
   const R *sc, *isc;  // depth scales V x nz (precision form z pass), or null
-  int *err;           // device error flag (bounded waits of the TMA xy pass)
+  int *err;           // device error flag (bounded waits of the TMA copies)
 };
 
 namespace fb {
@@ -366,12 +368,18 @@ __device__ __forceinline__ void filt_xy_layers(const FiltArgs<R> &F, int l, int 
 // layers of its column.  Block (32, 4, 2) threads; sl is the CTA's dynamic
 // shared memory, ZH x ZY x ZX values (layers k0-6 ..).  G and CARRY as for
 // the xy pass; SC: the precision form (filters physical values, stored *
-// isc(k), and stores them times sc(k)).
-template <class R, int G, bool CARRY, bool SC>
+// isc(k), and stores them times sc(k)).  TMA (no carry, no scaling; rows a
+// multiple of 16 bytes): the slab is one 32 x 4 x 44 x 1 tile of `map`
+// (the input buffer as nx x ny x nz x V) from (x0, y0, k0 - 6, l), whose
+// layout in shared memory is the slab's; it reads zero outside the grid,
+// as the per-thread loads do, and x0 is a multiple of 32; sl must be
+// 128-byte aligned and have 8 more bytes (the mbarrier).
+template <class R, int G, bool CARRY, bool SC, bool TMA = false>
 __device__ __forceinline__ void filt_z_slab(const FiltArgs<R> &F, int l, int x0, int y0,
-                                            int k0, R *sl) {
+                                            int k0, R *sl, const CUtensorMap *map = nullptr) {
   using namespace fb;
   constexpr bool M2 = G == 3;
+  static_assert(!TMA || (!CARRY && !SC), "the tensor copy moves stored values only");
   const int tx = threadIdx.x, ty = threadIdx.y, tz = threadIdx.z;
   const int nx = F.nx, ny = F.ny, nz = F.nz;
   const long long NXY = (long long)nx * ny;
@@ -379,19 +387,42 @@ __device__ __forceinline__ void filt_z_slab(const FiltArgs<R> &F, int l, int x0,
   const bool colok = gx < nx && gy < ny;
   // this thread's column; each thread loads layers q = tz, tz + 2, ...
   const R *icol = F.in + (long long)l * F.N + (colok ? (long long)gy * nx + gx : 0);
-  const R *ccol = CARRY ? F.carry + (icol - F.in) : nullptr;
-  const R *isc = SC ? F.isc + l * nz : nullptr;
-  for (int q = tz; q < ZH; q += 2) {
-    const int gz = k0 - 6 + q;
-    R v = R(0);
-    if (colok && gz >= 0 && gz < nz) {
-      v = icol[gz * NXY];
-      if (CARRY) v = v - ccol[gz * NXY];
-      if (SC) v = v * isc[gz];
+  if constexpr (TMA) {
+    // the mbarrier follows the slab in the dynamic buffer (a static one
+    // would cost a kilobyte of the CTA's shared allocation)
+    unsigned long long &zbar = *(unsigned long long *)(sl + ZH * ZY * ZX);
+    const bool lead = tx == 0 && ty == 0 && tz == 0;
+    if (lead) {
+      mbar_init_t(&zbar);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    sl[(q * ZY + ty) * ZX + tx] = v;
+    __syncthreads();
+    if (lead) {
+      mbar_tx_t(&zbar, (unsigned)(ZH * ZY * ZX * sizeof(R)));
+      tma4d_t(sl, map, x0, y0, k0 - 6, l, &zbar);
+    }
+    const bool ok = mbar_wait_t(&zbar, 0u, F.err);
+    if (!__syncthreads_and(ok)) {
+      // gave up (error flag raised): wait, again bounded, for the copy
+      // still in flight into this CTA's buffer, then leave
+      if (lead) mbar_wait_t(&zbar, 0u, F.err);
+      return;
+    }
+  } else {
+    const R *ccol = CARRY ? F.carry + (icol - F.in) : nullptr;
+    const R *isc = SC ? F.isc + l * nz : nullptr;
+    for (int q = tz; q < ZH; q += 2) {
+      const int gz = k0 - 6 + q;
+      R v = R(0);
+      if (colok && gz >= 0 && gz < nz) {
+        v = icol[gz * NXY];
+        if (CARRY) v = v - ccol[gz * NXY];
+        if (SC) v = v * isc[gz];
+      }
+      sl[(q * ZY + ty) * ZX + tx] = v;
+    }
+    __syncthreads();
   }
-  __syncthreads();
   if (!colok) return;
   R *ocol = F.out + (icol - F.in);
   const R fs = F.s;

@@ -243,6 +243,10 @@ struct Handle {
   // buffers in 44x44x1 boxes
   bool ftma = false;
   CUtensorMap fmaps[3];
+  // FILTER_VARS z pass (FP64, nx even): the state buffers as (nx, ny, nz, V)
+  // in 32x4x44x1 boxes
+  bool ztma = false;
+  CUtensorMap zmaps[3];
   // device bookkeeping
   int *d_err = nullptr;
   long long *d_iter = nullptr, *d_fail = nullptr;

@@ -449,7 +449,9 @@ int encode_tensor_maps(Handle *h) {
   // the grid, so its maps serve non-periodic grids only
   const bool want_f = !h->periodic && !(h->nx & 1);
   const bool want_m = h->magnetic && !(h->nx & 1);
-  if (!want_f && !want_m) return SPARC_OK;
+  h->ztma = false;
+  const bool want_z = !(h->nx & 1);
+  if (!want_f && !want_m && !want_z) return SPARC_OK;
   void *fn = nullptr;
   cudaDriverEntryPointQueryResult q;
   if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
@@ -483,6 +485,25 @@ int encode_tensor_maps(Handle *h) {
       fok = fok && boxed(&h->fmaps[b], h->buf[b], (unsigned long long)h->nz * h->V, fb::RX,
                          fb::RY);
     h->ftma = fok;
+  }
+  if (want_z) {
+    // FILTER_VARS z pass: a slab of 32 x 4 columns over 44 layers of one
+    // field, in a 4-D view (nx, ny, nz, V), so layers outside [0, nz) read
+    // zero instead of the neighbouring field
+    bool zok = true;
+    for (int b = 0; b < 3 && zok; ++b) {
+      cuuint64_t dims[4] = {(cuuint64_t)h->nx, (cuuint64_t)h->ny, (cuuint64_t)h->nz,
+                            (cuuint64_t)h->V};
+      cuuint64_t strides[3] = {(cuuint64_t)h->nx * 8, (cuuint64_t)h->nx * h->ny * 8,
+                               (cuuint64_t)h->nx * h->ny * h->nz * 8};
+      cuuint32_t box[4] = {(cuuint32_t)fb::ZX, (cuuint32_t)fb::ZY, (cuuint32_t)fb::ZH, 1};
+      cuuint32_t es[4] = {1, 1, 1, 1};
+      zok = enc(&h->zmaps[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void *)h->buf[b], dims,
+                strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    }
+    h->ztma = zok;
   }
   if (!want_m) return SPARC_OK;
   bool ok = true;
@@ -756,13 +777,17 @@ __global__ void __launch_bounds__(fb::NT, 4)
 }
 // the z pass: blockIdx.x is the z chunk (the chunks of a slab run
 // together), blockIdx.y the slab of the layer, blockIdx.z the field
-template <int G>
-__global__ void __launch_bounds__(2 * fb::ZX * fb::ZY) k_filt_z64(FiltArgs<double> F) {
-  extern __shared__ __align__(16) double zsl64[];
+// (the launch gives 128 bytes of slack for a 128-byte aligned slab and 16
+// for the mbarrier after it)
+template <int G, bool TMA>
+__global__ void __launch_bounds__(2 * fb::ZX * fb::ZY)
+    k_filt_z64(FiltArgs<double> F, const __grid_constant__ CUtensorMap map) {
+  extern __shared__ __align__(128) unsigned char zraw64[];
+  double *zsl = (double *)(zraw64 + ((128u - (sm_addr_t(zraw64) & 127u)) & 127u));
   const int nxb = (F.nx + fb::ZX - 1) / fb::ZX;
   const int yb = blockIdx.y / nxb, xb = blockIdx.y - yb * nxb;
-  filt_z_slab<double, G, false, false>(F, blockIdx.z, xb * fb::ZX, yb * fb::ZY, blockIdx.x * fb::ZC,
-                                zsl64);
+  filt_z_slab<double, G, false, false, TMA>(F, blockIdx.z, xb * fb::ZX, yb * fb::ZY,
+                                            blockIdx.x * fb::ZC, zsl, &map);
 }
 
 // xy: the y and x passes fused; z: the z pass (in -> out, never in place)
@@ -795,18 +820,34 @@ int launch_filter_event(Handle *h, bool xy, const double *in, double *out, cudaS
       else k_filt_xy64<3, false><<<grid, blk, 0, s>>>(F, map);
     }
   } else {
-    const size_t zs = filt_z_smem<double>();
+    const size_t zs = filt_z_smem<double>() + 128 + 16;
     const long long slabs = (long long)((h->nx + fb::ZX - 1) / fb::ZX) *
                             ((h->ny + fb::ZY - 1) / fb::ZY);
     if (slabs > 65535) return SPARC_ERR_INVALID;
     const dim3 grid((h->nz + fb::ZC - 1) / fb::ZC, (unsigned)slabs, h->V);
-    if (g == 5) {
-      cudaFuncSetAttribute(k_filt_z64<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs);
-      k_filt_z64<5><<<grid, dim3(fb::ZX, fb::ZY, 2), zs, s>>>(F);
+    // the tensor map of the input buffer (slabs by TMA), if any
+    int mb = -1;
+    if (h->ztma)
+      for (int b = 0; b < 3; ++b)
+        if (h->buf[b] == in) mb = b;
+    CUtensorMap map;
+    if (mb >= 0) map = h->zmaps[mb];
+    else std::memset(&map, 0, sizeof(map));
+    const dim3 blk(fb::ZX, fb::ZY, 2);
+#define ZP(GG, TT)                                                                          \
+  do {                                                                                      \
+    cudaFuncSetAttribute(k_filt_z64<GG, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
+                         (int)zs);                                                          \
+    k_filt_z64<GG, TT><<<grid, blk, zs, s>>>(F, map);                                       \
+  } while (0)
+    if (mb >= 0) {
+      if (g == 5) ZP(5, true);
+      else ZP(3, true);
     } else {
-      cudaFuncSetAttribute(k_filt_z64<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs);
-      k_filt_z64<3><<<grid, dim3(fb::ZX, fb::ZY, 2), zs, s>>>(F);
+      if (g == 5) ZP(5, false);
+      else ZP(3, false);
     }
+#undef ZP
   }
   ++h->launches;
   return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;

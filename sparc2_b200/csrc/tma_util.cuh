@@ -1,4 +1,4 @@
-// tma_util.cuh -- shared-memory addresses, mbarriers and 3-D TMA tile loads
+// tma_util.cuh -- shared-memory addresses, mbarriers and 3-D / 4-D TMA tile loads
 // (cp.async.bulk.tensor, no multicast), used by the stage and filter
 // kernels.  Every wait on an mbarrier is bounded.
 #pragma once
@@ -30,6 +30,15 @@ __device__ __forceinline__ void tma3d_t(void *dst, const CUtensorMap *map, int x
       "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
       " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(sm_addr_t(dst)),
       "l"(map), "r"(x), "r"(y), "r"(z), "r"(sm_addr_t(bar))
+      : "memory");
+}
+// the same for a 4-D tile at (x, y, z, w)
+__device__ __forceinline__ void tma4d_t(void *dst, const CUtensorMap *map, int x, int y, int z,
+                                        int w, unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(sm_addr_t(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(w), "r"(sm_addr_t(bar))
       : "memory");
 }
 // bounded wait: gives up after kMbarWaitLimit polls and raises the error flag

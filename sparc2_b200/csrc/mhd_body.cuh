@@ -161,6 +161,36 @@ __device__ __forceinline__ R dz_t(const R (&w)[11], int k, int nz, R sc) {
   return -sc * s;
 }
 
+// The z derivative of a window held as a ring: slot (RR + m) % 11 holds
+// logical value m (layer L + m); with sh the new head h replaces logical
+// value 10 (its slot still holds the layer it overwrites).  RR is a
+// template parameter, so the rotation is a renaming of registers.
+template <int RR, class R>
+__device__ __forceinline__ R dz_rot(const R (&v)[11], R h, bool sh, int k, int nz, R sc) {
+  R w[11];
+#pragma unroll
+  for (int m = 0; m < 11; ++m) w[m] = v[(RR + m) % 11];
+  if (sh) w[10] = h;
+  return dz_t(w, k, nz, sc);
+}
+template <class R>
+__device__ __forceinline__ R dz_ring(const R (&v)[11], R h, bool sh, int rr, int k, int nz,
+                                     R sc) {
+  switch (rr) {
+    case 0: return dz_rot<0>(v, h, sh, k, nz, sc);
+    case 1: return dz_rot<1>(v, h, sh, k, nz, sc);
+    case 2: return dz_rot<2>(v, h, sh, k, nz, sc);
+    case 3: return dz_rot<3>(v, h, sh, k, nz, sc);
+    case 4: return dz_rot<4>(v, h, sh, k, nz, sc);
+    case 5: return dz_rot<5>(v, h, sh, k, nz, sc);
+    case 6: return dz_rot<6>(v, h, sh, k, nz, sc);
+    case 7: return dz_rot<7>(v, h, sh, k, nz, sc);
+    case 8: return dz_rot<8>(v, h, sh, k, nz, sc);
+    case 9: return dz_rot<9>(v, h, sh, k, nz, sc);
+    default: return dz_rot<10>(v, h, sh, k, nz, sc);
+  }
+}
+
 // Compensated (Kahan) update a + inc with the running carry c.
 __device__ __forceinline__ float kahan(float a, float inc, float &c) {
   const float y = inc - c;
@@ -656,6 +686,7 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
     }
   }
   unsigned phase = 0;
+  int rr = 0;  // TW: ring position of the windows (logical value 0 in slot rr)
   bool ok = true;
   const R dt = (R)S.deltat;
   const R sx = (R)S.stretchx, sy = (R)S.stretchy;
@@ -731,14 +762,15 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
     if constexpr (TW) {
       __syncwarp();
       tm_wait_st();  // the previous layer's store of these columns
+      // the windows are rings: each layer with a new head stores only the
+      // head, into the slot of the layer it replaces, (rr + 10) % 11
+      if (sh) rr = rr == 10 ? 0 : rr + 1;
+      const uint32_t hslot = 2u * (uint32_t)(rr == 0 ? 10 : rr - 1);
       auto zwin = [&](int f, R h) -> R {
         R v[11];
         tm_ld_window(tm_window(tw, f), v);
-        if (sh) {
-          shift_t(v, h);
-          tm_st_window(tm_window(tw, f), v);
-        }
-        return dz_t(v, k, nz, szk);
+        if (sh) tm_st_one(tm_window(tw, f) + hslot, h);
+        return dz_ring(v, h, sh, rr, k, nz, szk);
       };
       wz0 = zwin(0, h0);
       wz1 = zwin(1, h1);

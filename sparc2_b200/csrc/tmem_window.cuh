@@ -5,12 +5,15 @@
 // three windows per thread.  In FP64 these 33 values take 66 of the 128
 // registers a thread of a 512-thread CTA may hold, for the whole layer
 // loop.  Kept in TMEM instead, they occupy registers only while the z
-// derivatives are formed: each layer loads the windows (tcgen05.ld), forms
-// the derivatives and stores the windows back shifted by one layer
-// (tcgen05.st of the same registers in shifted order).  Measured on the
+// derivatives are formed: each layer loads a window (tcgen05.ld, one wait
+// for its three pieces), forms the derivative and stores only the new
+// head value (tcgen05.st) into the slot of the layer it replaces, the
+// window being a ring whose rotation the caller tracks.  Measured on the
 // 256x256x300 flux tube: the FP64 stage kernels lose their register
-// spills and run 4.6 % faster; the FP32 kernels, which do not spill, ran
-// 4 % slower with their windows in TMEM and keep them in registers.
+// spills and run 4.6 % faster (with the whole window stored back shifted
+// each layer); storing the head alone into a ring is another 1.1 %; the
+// FP32 kernels, which do not spill, ran 4 % slower with their windows in
+// TMEM and keep them in registers.
 //
 // Layout: the CTA (16 warps) allocates all 512 columns.  Warp w may access
 // only the lane quarter w % 4 (lanes 32(w%4) .. +31; lane = the thread's
@@ -71,15 +74,19 @@ __device__ __forceinline__ uint32_t tm_warp_addr(uint32_t base, int warp) {
 }
 
 // One FP64 window (11 values, 22 columns) of this thread at address ta, in
-// pieces of 16, 4 and 2 columns: each load, its wait and the pairing of the
-// 32-bit columns into FP64 registers in one asm block (the registers are
-// valid only after the wait).  One window at a time keeps 22 registers
-// live, not the 66 of all three.
+// pieces of 16, 4 and 2 columns: the three loads, one wait and the pairing
+// of the 32-bit columns into FP64 registers in one asm block (the
+// registers are valid only after the wait), so a window costs one round
+// trip to TMEM.  One window at a time keeps 22 registers live, not the 66
+// of all three.
 __device__ __forceinline__ void tm_ld_window(uint32_t ta, double (&o)[11]) {
   asm volatile(
       "{\n"
       ".reg .b32 t0, t1, t2, t3, t4, t5, t6, t7, t8, t9, t10, t11, t12, t13, t14, t15;\n"
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {t0, t1, t2, t3, t4, t5, t6, t7, t8, t9, t10, t11, t12, t13, t14, t15}, [%8];\n"
+      ".reg .b32 u0, u1, u2, u3, u4, u5;\n"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {t0, t1, t2, t3, t4, t5, t6, t7, t8, t9, t10, t11, t12, t13, t14, t15}, [%11];\n"
+      "tcgen05.ld.sync.aligned.32x32b.x4.b32 {u0, u1, u2, u3}, [%12];\n"
+      "tcgen05.ld.sync.aligned.32x32b.x2.b32 {u4, u5}, [%13];\n"
       "tcgen05.wait::ld.sync.aligned;\n"
       "mov.b64 %0, {t0, t1};\n"
       "mov.b64 %1, {t2, t3};\n"
@@ -89,28 +96,13 @@ __device__ __forceinline__ void tm_ld_window(uint32_t ta, double (&o)[11]) {
       "mov.b64 %5, {t10, t11};\n"
       "mov.b64 %6, {t12, t13};\n"
       "mov.b64 %7, {t14, t15};\n"
+      "mov.b64 %8, {u0, u1};\n"
+      "mov.b64 %9, {u2, u3};\n"
+      "mov.b64 %10, {u4, u5};\n"
       "}"
-      : "=d"(o[0]), "=d"(o[1]), "=d"(o[2]), "=d"(o[3]), "=d"(o[4]), "=d"(o[5]), "=d"(o[6]), "=d"(o[7])
-      : "r"(ta + 0u));
-  asm volatile(
-      "{\n"
-      ".reg .b32 t0, t1, t2, t3;\n"
-      "tcgen05.ld.sync.aligned.32x32b.x4.b32 {t0, t1, t2, t3}, [%2];\n"
-      "tcgen05.wait::ld.sync.aligned;\n"
-      "mov.b64 %0, {t0, t1};\n"
-      "mov.b64 %1, {t2, t3};\n"
-      "}"
-      : "=d"(o[8]), "=d"(o[9])
-      : "r"(ta + 16u));
-  asm volatile(
-      "{\n"
-      ".reg .b32 t0, t1;\n"
-      "tcgen05.ld.sync.aligned.32x32b.x2.b32 {t0, t1}, [%1];\n"
-      "tcgen05.wait::ld.sync.aligned;\n"
-      "mov.b64 %0, {t0, t1};\n"
-      "}"
-      : "=d"(o[10])
-      : "r"(ta + 20u));
+      : "=d"(o[0]), "=d"(o[1]), "=d"(o[2]), "=d"(o[3]), "=d"(o[4]), "=d"(o[5]), "=d"(o[6]),
+        "=d"(o[7]), "=d"(o[8]), "=d"(o[9]), "=d"(o[10])
+      : "r"(ta + 0u), "r"(ta + 16u), "r"(ta + 20u));
 }
 
 // One FP64 window to address ta (completion: tm_wait_st)
@@ -144,6 +136,17 @@ __device__ __forceinline__ void tm_st_window(uint32_t ta, const double (&v)[11])
       "tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {t0, t1};\n"
       "}" ::"r"(ta + 20u),
       "d"(v[10]));
+}
+
+// One FP64 value to address ta (completion: tm_wait_st)
+__device__ __forceinline__ void tm_st_one(uint32_t ta, double v) {
+  asm volatile(
+      "{\n"
+      ".reg .b32 t0, t1;\n"
+      "mov.b64 {t0, t1}, %1;\n"
+      "tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {t0, t1};\n"
+      "}" ::"r"(ta),
+      "d"(v));
 }
 
 // column offset of window f (0, 1, 2) in a thread's slice

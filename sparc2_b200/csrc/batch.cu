@@ -15,6 +15,7 @@
 #include <string>
 #include <vector>
 
+#include "filter_body.cuh"
 #include "internal.h"
 
 namespace sparc {
@@ -27,8 +28,8 @@ struct Batch {
   std::vector<Handle *> members;        // nullptr: free slot
   std::vector<char> on_device;          // slot image uploaded (device owns roles)
   Slot32 *d_slots = nullptr;
-  int4 *d_items = nullptr, *d_fitems = nullptr, *d_pitems = nullptr;
-  size_t items_cap = 0, fitems_cap = 0, pitems_cap = 0, partials_cap = 0;
+  int4 *d_items = nullptr, *d_fitems = nullptr, *d_pitems = nullptr, *d_zitems = nullptr;
+  size_t items_cap = 0, fitems_cap = 0, pitems_cap = 0, zitems_cap = 0, partials_cap = 0;
   int *d_counts = nullptr;
   unsigned *d_wctr = nullptr;
   double *d_partials = nullptr;
@@ -84,7 +85,7 @@ int grow(Batch *b, T *&p, size_t &cap, size_t need) {
 // Rebuild the work-lists from the occupied slots and upload them with the
 // slot table (the batch stream is idle when this runs).
 int rebuild(Batch *b) {
-  std::vector<int4> items, fitems, pitems;
+  std::vector<int4> items, fitems, pitems, zitems;
   size_t npart = 0;
   size_t maxp = 0;
   // pass 0: interior MHD tiles (the list's prefix, run by the branch-free
@@ -138,6 +139,15 @@ int rebuild(Batch *b) {
     for (long long t = 0; t < tot; t += b->fchunk)
       fitems.push_back(make_int4(q, (int)t, (int)std::min<long long>(b->fchunk, tot - t), 0));
     L.f_items = (int)fitems.size() - L.f_first;
+    // z pass: (slot, field, slab of 32 x 4 columns, chunk of 32 layers), the
+    // chunks of a slab adjacent (their shared margins come from L2)
+    const int nxb = (h->nx + fb::ZX - 1) / fb::ZX, nyb = (h->ny + fb::ZY - 1) / fb::ZY;
+    const int nzc = (h->nz + fb::ZC - 1) / fb::ZC;
+    const size_t z0 = zitems.size();
+    for (int l = 0; l < h->V; ++l)
+      for (int sl = 0; sl < nxb * nyb; ++sl)
+        for (int c = 0; c < nzc; ++c) zitems.push_back(make_int4(q, l, sl, c));
+    L.z_items = (int)(zitems.size() - z0);
     if (L.has_psr) {
       for (int k = h->psr_klo; k < h->psr_khi; ++k) pitems.push_back(make_int4(q, k, 0, 0));
       maxp = std::max(maxp, h->pulses.size());
@@ -147,6 +157,7 @@ int rebuild(Batch *b) {
   r |= grow(b, b->d_items, b->items_cap, items.size());
   r |= grow(b, b->d_fitems, b->fitems_cap, fitems.size());
   r |= grow(b, b->d_pitems, b->pitems_cap, pitems.size());
+  r |= grow(b, b->d_zitems, b->zitems_cap, zitems.size());
   r |= grow(b, b->d_partials, b->partials_cap, 3 * npart);
   if (r) return r;
   for (int q = 0; q < b->cap; ++q)
@@ -156,7 +167,8 @@ int rebuild(Batch *b) {
     b->psr_smem = smem;
     b->recapture = true;
   }
-  const int counts[4] = {(int)items.size(), (int)fitems.size(), (int)pitems.size(), n_int};
+  const int counts[5] = {(int)items.size(), (int)fitems.size(), (int)pitems.size(), n_int,
+                         (int)zitems.size()};
   BCK(b, cudaStreamSynchronize(b->stream));
   // ordered on the batch stream (its kernels read these), finished before
   // the host arrays go
@@ -168,6 +180,9 @@ int rebuild(Batch *b) {
                            cudaMemcpyHostToDevice, b->stream));
   if (!pitems.empty())
     BCK(b, cudaMemcpyAsync(b->d_pitems, pitems.data(), pitems.size() * sizeof(int4),
+                           cudaMemcpyHostToDevice, b->stream));
+  if (!zitems.empty())
+    BCK(b, cudaMemcpyAsync(b->d_zitems, zitems.data(), zitems.size() * sizeof(int4),
                            cudaMemcpyHostToDevice, b->stream));
   BCK(b, cudaMemcpyAsync(b->d_counts, counts, sizeof(counts), cudaMemcpyHostToDevice,
                          b->stream));
@@ -191,6 +206,7 @@ int capture(Batch *b) {
   L.items = b->d_items;
   L.fitems = b->d_fitems;
   L.pitems = b->d_pitems;
+  L.zitems = b->d_zitems;
   L.counts = b->d_counts;
   L.wctr = b->d_wctr;
   L.grid = b->grid;
@@ -267,10 +283,10 @@ int sparc_batch_create(int device, int capacity, sparc_batch **out) {
   b->grid = sms;
   bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
             cudaMalloc(&b->d_slots, capacity * sizeof(Slot32)) == cudaSuccess &&
-            cudaMalloc(&b->d_counts, 4 * sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&b->d_counts, 5 * sizeof(int)) == cudaSuccess &&
             cudaMalloc(&b->d_wctr, 14 * sizeof(unsigned)) == cudaSuccess &&
             cudaMemsetAsync(b->d_slots, 0, capacity * sizeof(Slot32), b->stream) == cudaSuccess &&
-            cudaMemsetAsync(b->d_counts, 0, 4 * sizeof(int), b->stream) == cudaSuccess &&
+            cudaMemsetAsync(b->d_counts, 0, 5 * sizeof(int), b->stream) == cudaSuccess &&
             cudaStreamSynchronize(b->stream) == cudaSuccess;
   if (!ok) {
     cudaGetLastError();
@@ -292,6 +308,7 @@ int sparc_batch_destroy(sparc_batch *b) {
   cudaFree(b->d_items);
   cudaFree(b->d_fitems);
   cudaFree(b->d_pitems);
+  cudaFree(b->d_zitems);
   cudaFree(b->d_counts);
   cudaFree(b->d_wctr);
   cudaFree(b->d_partials);

@@ -1081,13 +1081,15 @@ __global__ void __launch_bounds__(BT)
   }
 }
 
-// One filter direction (y, x or z order as FILTER_VARS) over the simulations
-// whose cadence asks for it after the iteration just stepped.  The last
-// pass applied to a simulation starts a new compensated sum (carry 0).
+// One xy filter direction (y, then x, as FILTER_VARS) over the simulations
+// whose cadence asks for it after the iteration just stepped (the z
+// direction: k_batch_filter_z).  The last pass applied to a simulation
+// starts a new compensated sum (carry 0).
 template <int DIR>
 __global__ void __launch_bounds__(BT)
     k_batch_filter(Slot32 *__restrict__ slots, const int4 *__restrict__ items,
                    const int *__restrict__ counts, unsigned *wctr) {
+  static_assert(DIR == 0 || DIR == 1, "the z direction has its own kernel");
   __shared__ int s_w;
   const int tid = threadIdx.x;
   const int total = counts[1];
@@ -1131,6 +1133,66 @@ __global__ void __launch_bounds__(BT)
     if (tid == 0) {
       const unsigned c = atomicAdd(&L.counter, 1u);
       if (c == (unsigned)(L.f_items - 1)) {
+        rotate_roles(L);
+        L.counter = 0u;
+      }
+    }
+  }
+}
+
+// The z direction of FILTER_VARS for the members whose z cadence asks for
+// it: each work item is one (member, field, 32 x 4 column slab, 32-layer
+// chunk), filtered by the single path's slab kernel (filter_body.cuh,
+// filt_z_slab: physical values, stored back scaled; stored - carry when the
+// event has no xy part, as the first pass of the event).  Block (32, 4, 2).
+__global__ void __launch_bounds__(2 * fb::ZX * fb::ZY)
+    k_batch_filter_z(Slot32 *__restrict__ slots, const int4 *__restrict__ zitems,
+                     const int *__restrict__ counts, unsigned *wctr) {
+  extern __shared__ __align__(16) float zsl_b[];
+  __shared__ int s_w;
+  const int tid = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
+  const int total = counts[4];
+  for (;;) {
+    if (tid == 0) s_w = (int)atomicAdd(wctr, 1u);
+    __syncthreads();
+    const int w = s_w;
+    if (w >= total) break;
+    const int4 it = zitems[w];
+    Slot32 &L = slots[it.x];
+    bool need_z = false, need_xy = false;
+    if (L.active) {
+      const long long nn = *L.S.iter - 1;
+      need_xy = nn != 0 && nn % L.xyfreq == 0;
+      need_z = nn != 0 && nn % L.zfreq == 0;
+    }
+    if (!need_z) {
+      __syncthreads();
+      continue;
+    }
+    FiltArgs<float> F{};
+    F.nx = L.S.nx; F.ny = L.S.ny; F.nz = L.S.nz; F.V = L.S.V; F.N = L.S.N;
+    F.periodic = L.S.periodic;
+    F.s = L.s_z;
+    F.in = L.buf[L.role[0]];
+    F.out = L.buf[L.role[1]];
+    F.sc = L.S.sc;
+    F.isc = L.S.isc;
+    const bool first = !need_xy;
+    F.carry = first ? L.S.carry : nullptr;
+    const int nxb = (F.nx + fb::ZX - 1) / fb::ZX;
+    const int yb = it.z / nxb, xb = it.z - yb * nxb;
+    const int x0 = xb * fb::ZX, y0 = yb * fb::ZY, k0 = it.w * fb::ZC;
+    if (L.gz == 5) {
+      if (first) filt_z_slab<float, 5, true, true>(F, it.y, x0, y0, k0, zsl_b);
+      else filt_z_slab<float, 5, false, true>(F, it.y, x0, y0, k0, zsl_b);
+    } else {
+      if (first) filt_z_slab<float, 3, true, true>(F, it.y, x0, y0, k0, zsl_b);
+      else filt_z_slab<float, 3, false, true>(F, it.y, x0, y0, k0, zsl_b);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      const unsigned c = atomicAdd(&L.counter, 1u);
+      if (c == (unsigned)(L.z_items - 1)) {
         rotate_roles(L);
         L.counter = 0u;
       }
@@ -1189,7 +1251,8 @@ int launch_batch_step(const BatchLaunch &B, cudaStream_t s, int *nkernels) {
   launch_batch_stages(B, s);
   k_batch_filter<1><<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 6);
   k_batch_filter<0><<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 7);
-  k_batch_filter<2><<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 8);
+  k_batch_filter_z<<<B.grid * 6, dim3(fb::ZX, fb::ZY, 2), filt_z_smem<float>(), s>>>(
+      B.slots, B.zitems, B.counts, B.wctr + 8);
   k_batch_carry_clear<<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 9);
   *nkernels = 12;
   return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;

@@ -28,8 +28,10 @@ struct Batch {
   std::vector<Handle *> members;        // nullptr: free slot
   std::vector<char> on_device;          // slot image uploaded (device owns roles)
   Slot32 *d_slots = nullptr;
-  int4 *d_items = nullptr, *d_fitems = nullptr, *d_pitems = nullptr, *d_zitems = nullptr;
-  size_t items_cap = 0, fitems_cap = 0, pitems_cap = 0, zitems_cap = 0, partials_cap = 0;
+  int4 *d_items = nullptr, *d_fitems = nullptr, *d_pitems = nullptr, *d_zitems = nullptr,
+       *d_xyitems = nullptr;
+  size_t items_cap = 0, fitems_cap = 0, pitems_cap = 0, zitems_cap = 0, xyitems_cap = 0;
+  size_t partials_cap = 0;
   int *d_counts = nullptr;
   unsigned *d_wctr = nullptr;
   double *d_partials = nullptr;
@@ -85,7 +87,7 @@ int grow(Batch *b, T *&p, size_t &cap, size_t need) {
 // Rebuild the work-lists from the occupied slots and upload them with the
 // slot table (the batch stream is idle when this runs).
 int rebuild(Batch *b) {
-  std::vector<int4> items, fitems, pitems, zitems;
+  std::vector<int4> items, fitems, pitems, zitems, xyitems;
   size_t npart = 0;
   size_t maxp = 0;
   // pass 0: interior MHD tiles (the list's prefix, run by the branch-free
@@ -148,6 +150,14 @@ int rebuild(Batch *b) {
       for (int sl = 0; sl < nxb * nyb; ++sl)
         for (int c = 0; c < nzc; ++c) zitems.push_back(make_int4(q, l, sl, c));
     L.z_items = (int)(zitems.size() - z0);
+    // xy pass: (slot, field, group of LPB layers, 32 x 32 tile)
+    const int ntx = (h->nx + fb::TX - 1) / fb::TX, nty = (h->ny + fb::TR - 1) / fb::TR;
+    const int nlg = (h->nz + fb::LPB - 1) / fb::LPB;
+    const size_t xy0 = xyitems.size();
+    for (int l = 0; l < h->V; ++l)
+      for (int g = 0; g < nlg; ++g)
+        for (int t = 0; t < ntx * nty; ++t) xyitems.push_back(make_int4(q, l, g, t));
+    L.xy_items = (int)(xyitems.size() - xy0);
     if (L.has_psr) {
       for (int k = h->psr_klo; k < h->psr_khi; ++k) pitems.push_back(make_int4(q, k, 0, 0));
       maxp = std::max(maxp, h->pulses.size());
@@ -158,6 +168,7 @@ int rebuild(Batch *b) {
   r |= grow(b, b->d_fitems, b->fitems_cap, fitems.size());
   r |= grow(b, b->d_pitems, b->pitems_cap, pitems.size());
   r |= grow(b, b->d_zitems, b->zitems_cap, zitems.size());
+  r |= grow(b, b->d_xyitems, b->xyitems_cap, xyitems.size());
   r |= grow(b, b->d_partials, b->partials_cap, 3 * npart);
   if (r) return r;
   for (int q = 0; q < b->cap; ++q)
@@ -167,8 +178,8 @@ int rebuild(Batch *b) {
     b->psr_smem = smem;
     b->recapture = true;
   }
-  const int counts[5] = {(int)items.size(), (int)fitems.size(), (int)pitems.size(), n_int,
-                         (int)zitems.size()};
+  const int counts[6] = {(int)items.size(), (int)fitems.size(), (int)pitems.size(), n_int,
+                         (int)zitems.size(), (int)xyitems.size()};
   BCK(b, cudaStreamSynchronize(b->stream));
   // ordered on the batch stream (its kernels read these), finished before
   // the host arrays go
@@ -183,6 +194,9 @@ int rebuild(Batch *b) {
                            cudaMemcpyHostToDevice, b->stream));
   if (!zitems.empty())
     BCK(b, cudaMemcpyAsync(b->d_zitems, zitems.data(), zitems.size() * sizeof(int4),
+                           cudaMemcpyHostToDevice, b->stream));
+  if (!xyitems.empty())
+    BCK(b, cudaMemcpyAsync(b->d_xyitems, xyitems.data(), xyitems.size() * sizeof(int4),
                            cudaMemcpyHostToDevice, b->stream));
   BCK(b, cudaMemcpyAsync(b->d_counts, counts, sizeof(counts), cudaMemcpyHostToDevice,
                          b->stream));
@@ -207,6 +221,7 @@ int capture(Batch *b) {
   L.fitems = b->d_fitems;
   L.pitems = b->d_pitems;
   L.zitems = b->d_zitems;
+  L.xyitems = b->d_xyitems;
   L.counts = b->d_counts;
   L.wctr = b->d_wctr;
   L.grid = b->grid;
@@ -283,10 +298,10 @@ int sparc_batch_create(int device, int capacity, sparc_batch **out) {
   b->grid = sms;
   bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
             cudaMalloc(&b->d_slots, capacity * sizeof(Slot32)) == cudaSuccess &&
-            cudaMalloc(&b->d_counts, 5 * sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&b->d_counts, 6 * sizeof(int)) == cudaSuccess &&
             cudaMalloc(&b->d_wctr, 14 * sizeof(unsigned)) == cudaSuccess &&
             cudaMemsetAsync(b->d_slots, 0, capacity * sizeof(Slot32), b->stream) == cudaSuccess &&
-            cudaMemsetAsync(b->d_counts, 0, 5 * sizeof(int), b->stream) == cudaSuccess &&
+            cudaMemsetAsync(b->d_counts, 0, 6 * sizeof(int), b->stream) == cudaSuccess &&
             cudaStreamSynchronize(b->stream) == cudaSuccess;
   if (!ok) {
     cudaGetLastError();
@@ -309,6 +324,7 @@ int sparc_batch_destroy(sparc_batch *b) {
   cudaFree(b->d_fitems);
   cudaFree(b->d_pitems);
   cudaFree(b->d_zitems);
+  cudaFree(b->d_xyitems);
   cudaFree(b->d_counts);
   cudaFree(b->d_wctr);
   cudaFree(b->d_partials);

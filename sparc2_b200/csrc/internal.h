@@ -137,7 +137,8 @@ struct Slot32 {
   Rnd32 rnd;
   int first_item, n_items;     // stage items of the interior part (MHD only)
   int first_item2, n_items2;   // stage items of the general part
-  int f_first, f_items;        // filter work-list range (y and x passes, carry clear)
+  int f_first, f_items;        // carry-clear work-list range
+  int xy_items;                // xy-pass items (field, 8-layer group, 32x32 tile)
   int z_items;                 // z-pass items (field, 32x4 column slab, 32-layer chunk)
   int gxy, gz, xyfreq, zfreq;
   float s_xy, s_z;
@@ -150,10 +151,10 @@ struct BatchLaunch {
   Slot32 *slots;
   int nslots;
   const int4 *items, *fitems, *pitems;  // stage, filter, forcing items
-  const int4 *zitems;                   // z-pass filter items
-  const int *counts;                    // [5] stage, filter, forcing items,
-                                        // interior stage items (a prefix),
-                                        // z-pass items
+  const int4 *xyitems, *zitems;         // xy- and z-pass filter items
+  const int *counts;                    // [6] stage, carry-clear, forcing
+                                        // items, interior stage items (a
+                                        // prefix), z-pass, xy-pass items
   unsigned *wctr;                       // [14] work counters, zeroed per step
   int grid;                             // persistent CTAs
   int zmax;                             // largest z extent of a stage item

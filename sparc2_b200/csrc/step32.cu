@@ -458,64 +458,6 @@ __global__ void __launch_bounds__(t32::NT, 1)
 }
 
 // ---------------------------------------------- FILTER_VARS, precision form
-// One direction of FILTER_VARS over all fields in FP32 (derivatives.f90:
-// 659-703).  x and y filters act on the stored values (their scale is
-// constant in a layer); the z filter and its edge pre-averaging act on
-// physical values and scale back.
-struct Filt32 {
-  int nx, ny, nz, periodic, g, mode2, V;
-  long long N;
-  float s;
-  const float *sc, *isc;
-};
-
-// Filtered value of element t (field-major over V x N).
-template <int DIR>
-__device__ __forceinline__ float filter_point32(const Filt32 &F, const float *__restrict__ in,
-                                                const float *__restrict__ carry, long long t) {
-  const int n = DIR == 0 ? F.nx : (DIR == 1 ? F.ny : F.nz);
-  const long long st = DIR == 0 ? 1 : (DIR == 1 ? F.nx : (long long)F.nx * F.ny);
-  const bool per = DIR != 2 && F.periodic;
-  const bool avg = DIR == 2 || !F.periodic;
-  const int g = F.g;
-  const float *c = f_df[g == 5 ? 0 : 1];
-  const int l = (int)(t / F.N);
-  const long long pnt = t - (long long)l * F.N;
-  int q;
-  if (DIR == 0) q = (int)(pnt % F.nx);
-  else if (DIR == 1) q = (int)((pnt / F.nx) % F.ny);
-  else q = (int)(pnt / ((long long)F.nx * F.ny));
-  const long long base = t - (long long)q * st;
-  // physical (z) or stored (x, y) value at index qq
-  // the compensated value stored - carry on the first pass of an event
-  auto val = [&](int qq) -> float {
-    const long long id = base + (long long)qq * st;
-    const float v = carry ? __ldg(in + id) - __ldg(carry + id) : __ldg(in + id);
-    return DIR == 2 ? v * F.isc[l * F.nz + qq] : v;
-  };
-  auto pre = [&](int qq) -> float {
-    if (avg && ((qq >= 1 && qq <= g - 1) || (qq >= n - g && qq <= n - 2)))
-      return (val(qq + 1) + val(qq - 1)) / 2.0f;
-    return val(qq);
-  };
-  const float pq = pre(q);
-  float filt;
-  if (!per && (q < g || q >= n - g)) {
-    filt = (DIR != 2 && g == 3) ? 0.f : pq;
-  } else {
-    float sum = 0.f;
-    for (int m = 0; m < 2 * g + 1; ++m) {
-      int qq = q - g + m;
-      if (per) qq = wrap32(qq, n);
-      sum += pre(qq) * c[m];
-    }
-    filt = sum;
-  }
-  float r = F.mode2 ? pq - F.s * filt : filt;
-  if (DIR == 2) r = r * F.sc[l * F.nz + q];
-  return r;
-}
-
 // FILTER_VARS of a filter event in the precision form (filter_body.cuh):
 // the fused y-then-x pass over stored values (one depth scale per layer)
 // and the z pass over physical values; `carry` (the first pass of an event)
@@ -1081,58 +1023,54 @@ __global__ void __launch_bounds__(BT)
   }
 }
 
-// One xy filter direction (y, then x, as FILTER_VARS) over the simulations
-// whose cadence asks for it after the iteration just stepped (the z
-// direction: k_batch_filter_z).  The last pass applied to a simulation
-// starts a new compensated sum (carry 0).
-template <int DIR>
-__global__ void __launch_bounds__(BT)
-    k_batch_filter(Slot32 *__restrict__ slots, const int4 *__restrict__ items,
-                   const int *__restrict__ counts, unsigned *wctr) {
-  static_assert(DIR == 0 || DIR == 1, "the z direction has its own kernel");
+// The fused y-then-x pass of FILTER_VARS for the members whose xy cadence
+// asks for it after the iteration just stepped (always the first pass of
+// the event: stored - carry): work items (member, field, group of LPB
+// layers, 32 x 32 tile) of the single path's tile kernel (filter_body.cuh,
+// filt_xy_tile, stored values: one depth scale per layer).  Block (32, 8).
+// The last item of a member rotates its buffer roles.
+__global__ void __launch_bounds__(fb::NT)
+    k_batch_filter_xy(Slot32 *__restrict__ slots, const int4 *__restrict__ xyitems,
+                      const int *__restrict__ counts, unsigned *wctr) {
   __shared__ int s_w;
-  const int tid = threadIdx.x;
-  const int total = counts[1];
+  const int tid = threadIdx.y * fb::TX + threadIdx.x;
+  const int total = counts[5];
   for (;;) {
     if (tid == 0) s_w = (int)atomicAdd(wctr, 1u);
     __syncthreads();
     const int w = s_w;
     if (w >= total) break;
-    const int4 it = items[w];
+    const int4 it = xyitems[w];
     Slot32 &L = slots[it.x];
-    bool need = false, need_z = false, need_xy = false;
+    bool need_xy = false;
     if (L.active) {
       const long long nn = *L.S.iter - 1;
       need_xy = nn != 0 && nn % L.xyfreq == 0;
-      need_z = nn != 0 && nn % L.zfreq == 0;
-      need = DIR == 2 ? need_z : need_xy;
     }
-    if (!need) {
+    if (!need_xy) {
       __syncthreads();
       continue;
     }
-    Filt32 F;
-    F.nx = L.S.nx; F.ny = L.S.ny; F.nz = L.S.nz;
+    FiltArgs<float> F{};
+    F.nx = L.S.nx; F.ny = L.S.ny; F.nz = L.S.nz; F.V = L.S.V; F.N = L.S.N;
     F.periodic = L.S.periodic;
-    F.g = DIR == 2 ? L.gz : L.gxy;
-    F.mode2 = F.g == 3;
-    F.V = L.S.V;
-    F.N = L.S.N;
-    F.s = DIR == 2 ? L.s_z : L.s_xy;
-    F.sc = L.S.sc;
-    F.isc = L.S.isc;
-    const float *in = L.buf[L.role[0]];
-    float *out = L.buf[L.role[1]];
-    // the first pass of the event (y, or z alone) filters stored - carry;
-    // k_batch_carry_clear zeroes the carry after the last pass
-    const bool first = DIR == 1 || (DIR == 2 && !need_xy);
-    const float *carry = first ? L.S.carry : nullptr;
-    const long long t0 = it.y, t1 = t0 + it.z;
-    for (long long t = t0 + tid; t < t1; t += BT) out[t] = filter_point32<DIR>(F, in, carry, t);
+    F.s = L.s_xy;
+    F.in = L.buf[L.role[0]];
+    F.out = L.buf[L.role[1]];
+    F.carry = L.S.carry;
+    const int ntx = (F.nx + fb::TX - 1) / fb::TX;
+    const int ty = it.w / ntx, tx = it.w - ty * ntx;
+    const int k0 = it.z * fb::LPB, k1 = min(F.nz, k0 + fb::LPB);
+    // consecutive calls: each one's first barrier follows the previous
+    // one's last shared reads
+    for (int k = k0; k < k1; ++k) {
+      if (L.gxy == 5) filt_xy_tile<float, 5, true>(F, it.y, k, tx * fb::TX, ty * fb::TR);
+      else filt_xy_tile<float, 3, true>(F, it.y, k, tx * fb::TX, ty * fb::TR);
+    }
     __syncthreads();
     if (tid == 0) {
       const unsigned c = atomicAdd(&L.counter, 1u);
-      if (c == (unsigned)(L.f_items - 1)) {
+      if (c == (unsigned)(L.xy_items - 1)) {
         rotate_roles(L);
         L.counter = 0u;
       }
@@ -1249,12 +1187,12 @@ int launch_batch_step(const BatchLaunch &B, cudaStream_t s, int *nkernels) {
   k_batch_psr<<<B.grid, BT, B.psr_smem, s>>>(B.slots, B.pitems, B.counts, B.wctr + 0);
   k_batch_random<<<B.grid, BT, 0, s>>>(B.slots, B.nslots);
   launch_batch_stages(B, s);
-  k_batch_filter<1><<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 6);
-  k_batch_filter<0><<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 7);
+  k_batch_filter_xy<<<B.grid * 6, dim3(fb::TX, fb::TY), 0, s>>>(B.slots, B.xyitems, B.counts,
+                                                                 B.wctr + 6);
   k_batch_filter_z<<<B.grid * 6, dim3(fb::ZX, fb::ZY, 2), filt_z_smem<float>(), s>>>(
       B.slots, B.zitems, B.counts, B.wctr + 8);
   k_batch_carry_clear<<<B.grid * 2, BT, 0, s>>>(B.slots, B.fitems, B.counts, B.wctr + 9);
-  *nkernels = 12;
+  *nkernels = 11;
   return cudaGetLastError() == cudaSuccess ? SPARC_OK : SPARC_ERR_CUDA;
 }
 

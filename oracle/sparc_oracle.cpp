@@ -1,5 +1,10 @@
 // sparc_oracle.cpp -- TEST INFRASTRUCTURE (the oracle), not the product.
 //
+// Parity unpinned by the reference itself: the reference has no tests or
+// golden vectors and cannot be built here (Fortran, MPI, parallel HDF5
+// absent); this restatement is pinned by analytic known-answer tests and
+// by committed golden fixtures of its own output (sparc_oracle.h).
+//
 // CPU FP64 restatement of the reference SPARC linear wave time step over the
 // global domain (see sparc_oracle.h).  Array layout is the reference's:
 // Fortran order, x fastest; indices here are 0-based.  Expressions keep the

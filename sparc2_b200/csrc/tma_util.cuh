@@ -1,6 +1,7 @@
-// tma_util.cuh -- shared-memory addresses, mbarriers and 3-D / 4-D TMA tile loads
-// (cp.async.bulk.tensor, no multicast), used by the stage and filter
-// kernels.  Every wait on an mbarrier is bounded.
+// tma_util.cuh -- shared-memory addresses, mbarriers and 3-D / 4-D TMA
+// tile loads (cp.async.bulk.tensor, each into the issuing CTA's own shared
+// memory), used by the stage and filter kernels.  Every wait on an
+// mbarrier is bounded.
 #pragma once
 
 #include "internal.h"

@@ -736,6 +736,29 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
       pf_l1(S.boz + id);
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");
+    const R szk = __ldg(S.stretch + k);
+    // TW: the z derivatives of the three windows, formed by the whole warp
+    // (the TMEM accesses are warp-collective); they read no shared memory,
+    // so they are formed before the wait for the layer's copies and the
+    // layer barrier, overlapping both (0.6 % per iteration, A/B on one box)
+    R wz0 = R(0), wz1 = R(0), wz2 = R(0);
+    if constexpr (TW) {
+      __syncwarp();
+      tm_wait_st();  // the previous layer's store of these columns
+      // the windows are rings: each layer with a new head stores only the
+      // head, into the slot of the layer it replaces, (rr + 10) % 11
+      if (sh) rr = rr == 10 ? 0 : rr + 1;
+      const uint32_t hslot = 2u * (uint32_t)(rr == 0 ? 10 : rr - 1);
+      auto zwin = [&](int f, R h) -> R {
+        R v[11];
+        tm_ld_window(tm_window(tw, f), v);
+        if (sh) tm_st_one(tm_window(tw, f) + hslot, h);
+        return dz_ring(v, h, sh, rr, k, nz, szk);
+      };
+      wz0 = zwin(0, h0);
+      wz1 = zwin(1, h1);
+      wz2 = zwin(2, h2);
+    }
     bool mine = true;
     // TH: every thread waits for the layer's TMA copies (its flux positions
     // arrive that way); otherwise thread 0 alone, before the barrier
@@ -754,27 +777,6 @@ __device__ __forceinline__ bool mhd_body(const SimT<R> &S, const TmaSet *T, R *s
     if (k + 1 < k1) issue(k + 1, b ^ 1);
     if constexpr (!TW) {
       if (sh) { shift_t(w0, h0); shift_t(w1, h1); shift_t(w2, h2); }
-    }
-    const R szk = __ldg(S.stretch + k);
-    // TW: the z derivatives of the three windows, formed by the whole warp
-    // (the TMEM accesses are warp-collective)
-    R wz0 = R(0), wz1 = R(0), wz2 = R(0);
-    if constexpr (TW) {
-      __syncwarp();
-      tm_wait_st();  // the previous layer's store of these columns
-      // the windows are rings: each layer with a new head stores only the
-      // head, into the slot of the layer it replaces, (rr + 10) % 11
-      if (sh) rr = rr == 10 ? 0 : rr + 1;
-      const uint32_t hslot = 2u * (uint32_t)(rr == 0 ? 10 : rr - 1);
-      auto zwin = [&](int f, R h) -> R {
-        R v[11];
-        tm_ld_window(tm_window(tw, f), v);
-        if (sh) tm_st_one(tm_window(tw, f) + hslot, h);
-        return dz_ring(v, h, sh, rr, k, nz, szk);
-      };
-      wz0 = zwin(0, h0);
-      wz1 = zwin(1, h1);
-      wz2 = zwin(2, h2);
     }
     auto DZ = [&](int f) -> R {
       if constexpr (TW) {

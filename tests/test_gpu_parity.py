@@ -94,10 +94,11 @@ def test_one_iteration_from_random_state(name):
 @pytest.mark.parametrize("name,kw", [("quiet_periodic", {}), ("mhd_hpml", {}), ("quiet_hpml", {}),
                                      ("quiet_hpml", {"nx": 41, "ny": 38})])
 def test_filter_vars(name, kw):
-    """The 11-point filter on both axes.  Non-periodic grids with an even nx
-    take the xy pass whose neighbourhoods arrive as tensor copies; nx = 41
-    (rows not a multiple of 16 bytes) and the periodic grid take the
-    per-thread copies."""
+    """The 11-point filter on both axes.  Grids with an even nx take the z
+    pass whose slabs arrive as tensor copies, non-periodic ones also the xy
+    pass with tensor-copied neighbourhoods; nx = 41 (rows not a multiple of
+    16 bytes) takes the per-thread copies in both passes, the periodic grid
+    in the xy pass."""
     sim, orc = pair(name, **kw)
     a0, psi0 = cases.random_state(sim, seed=7)
     for s in (sim, orc):
